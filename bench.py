@@ -1,0 +1,449 @@
+"""Benchmark: capacitance solves/s on the 256x256x128 8-terminal extraction.
+
+One step = one full Maxwell capacitance extraction of the layered-dielectric,
+8-conductor-box workload (256x256x128 nodes, 10 nm pitch, grounded bottom
+plane, 8 right-hand sides solved to FP64 relres 1e-10): edge masses built on
+the device, Dirichlet elimination, block CG, FP64 charge integration.
+
+* ``value``  -- solves/s with inputs (permittivity, terminal node lists)
+  already in HBM when the timed region starts.
+* ``e2e``    -- solves/s through the public API
+  ``fieldspice_b200.extraction.capacitance_matrix`` with host inputs in
+  pinned memory; host->device copies and the C-matrix readback are inside
+  the timed region.
+* ``roofline`` -- the dominant CG kernel's algorithmic bytes per launch over
+  its CUDA-event duration sampled inside the timed region, against the
+  measured HBM copy bandwidth.
+* ``cpu_baseline`` -- the CPU oracle (SciPy Jacobi-CG, the reference's
+  algorithm) timed on a bounded sample of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); every rank extracts its own
+geometry (seed = rank), no data-path collective ("scaling": "weak");
+timing is the max over ranks.  ``--impl reference`` times the CPU oracle
+(the reference's algorithm) on the host cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SHAPE = (256, 256, 128)
+NBOX = 8
+TOL = 1e-10
+FULLSIZE_JSON = ROOT / "tests" / "golden" / "layered_256x256x128_s0.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--shape", default=",".join(map(str, SHAPE)))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-node DRAM bytes of the CG kernels from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def kernel_bytes(N: int, k: int, s: int) -> dict:
+    """Algorithmic bytes per launch of the CG kernels (each array once)."""
+    return {"pupdate": 3 * N * k * s,                 # read r, p; write p
+            "stencil": N * (2 * k * s + 3 * s),       # read p, 3 masses; write q
+            "update": 6 * N * k * s}                  # read p, q, x, r; write x, r
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from fieldspice_b200 import device as D
+    from fieldspice_b200 import extraction as EX
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
+    from fieldspice_b200.solvers.poisson import capacitance_report, extract_capacitance
+
+    shape = tuple(int(v) for v in args.shape.split(","))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = W.layered_boxes(shape, nbox=NBOX, seed=rank)
+    grid = w.grid()
+    bc = w.boundary_spec()
+    terms = w.terminal_objects()
+    # device-resident inputs for `value`
+    eps_dev = torch.as_tensor(w.eps_cell, device=dev)
+    term_dev = [torch.as_tensor(np.asarray(t, np.int64), device=dev) for t in w.terminals]
+    from fieldspice_b200.boundaries import dirichlet_nodes
+    wall = dirichlet_nodes(bc, grid)[0].astype(np.int64)
+    shield = np.setdiff1d(wall, np.concatenate(w.terminals)).astype(np.int64)
+    wall_dev = torch.as_tensor(wall, device=dev)
+    shield_dev = torch.as_tensor(shield, device=dev)
+    # pinned host inputs for `e2e`
+    eps_pinned = torch.from_numpy(np.ascontiguousarray(w.eps_cell)).pin_memory().numpy()
+    for t in terms:
+        t.nodes = torch.from_numpy(np.ascontiguousarray(t.nodes, dtype=np.int64)).pin_memory().numpy()
+
+    def step_device(precision):
+        op = D.DeviceOperator(grid, eps_dev)
+        C, qs, info = extract_capacitance(op, term_dev, wall_dev, shield_dev,
+                                          tol=TOL, precision=precision)
+        info["gpu_launches"] += 1 + 2  # mass build + plan setup kernels
+        return C, qs, info
+
+    def step_e2e(precision):
+        rep = {}
+        C = EX.capacitance_matrix(grid, eps_pinned, terms, bc, SolverConfig(tol=TOL),
+                                  report=rep, gpu=GPUConfig(precision=precision))
+        return C, rep
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            out = fn()
+        barrier()
+        torch.cuda.synchronize()
+        stream = torch.cuda.current_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        outs = []
+        e0.record(stream)
+        for _ in range(steps):
+            outs.append(fn())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, outs
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms_dev, outs = timed(lambda: step_device(args.precision), args.steps, args.warmup)
+    clocks = sampler.stop()
+    C, qs, info = outs[-1]
+    launches = sum(o[2]["gpu_launches"] for o in outs)
+    k_rhs = NBOX
+    n_solves_step = k_rhs * world
+    value = n_solves_step * args.steps / (ms_dev / 1000.0)
+
+    D.TRANSFERS.update(h2d=0, d2h=0)
+    ms_e2e, outs_e2e = timed(lambda: step_e2e(args.precision), args.steps, 1)
+    h2d = D.TRANSFERS["h2d"] / (args.steps + 1)
+    d2h = D.TRANSFERS["d2h"] / (args.steps + 1)
+    e2e_value = n_solves_step * args.steps / (ms_e2e / 1000.0)
+
+    variants = {}
+    if not args.no_variants:
+        other = "fp64" if args.precision == "mixed" else "mixed"
+        ms_o, outs_o = timed(lambda: step_device(other), max(2, args.steps // 2), 1)
+        Co = outs_o[-1][0]
+        variants[other] = {
+            "value": n_solves_step * max(2, args.steps // 2) / (ms_o / 1000.0),
+            "iterations": outs_o[-1][2]["iterations"],
+            "C_rel_diff_vs_default": float(np.abs(Co - C).max() / np.abs(np.diag(C)).max()),
+        }
+
+    if rank != 0:
+        return
+    N = int(np.prod(shape))
+    s = 4 if args.precision == "mixed" else 8
+    kb = kernel_bytes(N, 8, s)
+    km = info["kernel_ms"]
+    times = {"pupdate": km["pupdate_ms"], "stencil": km["stencil_ms"], "update": km["update_ms"]}
+    dom = max(times, key=times.get)
+    peak, peak_kind = measured_peaks()
+    gbs = {k: kb[k] / (times[k] * 1e-3) / 1e9 for k in times if times[k] > 0}
+    traffic = committed_traffic().get(f"{dom}_{args.precision}_bytes_per_node")
+    rep = capacitance_report(C, qs, info)
+    # parity against the committed full-size oracle result (same seed-0 input)
+    err_vs_oracle = None
+    if FULLSIZE_JSON.exists() and rank == 0 and shape == SHAPE:
+        ref = json.loads(FULLSIZE_JSON.read_text())
+        Cref = np.asarray(ref["C_tol1e-12_unsymmetrised"])
+        err_vs_oracle = float(np.abs(C - Cref).max() / np.abs(np.diag(Cref)).max())
+    line = {
+        "metric": "C solves/s @relres 1e-10 (256x256x128, 8 terminals)",
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_dev / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded layered dielectric + 8 conductor boxes per rank)",
+        "config": {
+            "workload": f"layered_boxes {shape[0]}x{shape[1]}x{shape[2]} nodes, "
+                        f"{NBOX} terminals, zlo grounded, seed=rank",
+            "nodes": N, "nrhs": NBOX, "tol": TOL, "precision": args.precision,
+            "preconditioner": "jacobi (equilibrated CG)",
+            "l2": "inputs larger than L2: every CG vector is N*8*4 B = 268 MB",
+            "parallelism": f"dp{world} (independent geometries)",
+        },
+        "e2e": {"value": e2e_value, "unit": "solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": ms_e2e / args.steps},
+        "roofline": {
+            "bound": "hbm", "kernel": dom, "achieved": gbs.get(dom), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": (gbs.get(dom) or 0.0) / peak,
+            "traffic": (traffic * N if traffic else None),
+            "algorithmic_bytes_per_launch": kb[dom],
+            "ms_per_launch": times[dom], "samples": km["samples"],
+            "all_kernels_gbs": gbs, "all_kernels_ms": times,
+        },
+        "stencil_gbs": gbs.get("stencil"),
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "iterations": info["iterations"],
+        "relres_fp64_max": info["residual"],
+        "asymmetry_rel": rep["asymmetry_rel"],
+        "C_err_vs_fp64_oracle": err_vs_oracle,
+        "variants": variants,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(shape, info["iterations"], args.cpu_sample_iters)
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle timing (cpu_baseline and the reference arm)
+# ---------------------------------------------------------------------------
+_CPU = {}
+
+
+def _cpu_setup(shape, seed=0):
+    from oracle import fs_oracle as O
+    from fieldspice_b200 import workloads as W
+    import scipy.sparse as sp
+    w = W.layered_boxes(shape, nbox=NBOX, seed=seed)
+    g = O.Grid(w.x, w.y, w.z)
+    t0 = time.perf_counter()
+    m = O.edge_mass_vector(g, O.cell_to_edge(g, w.eps_cell))
+    Lm = O.nodal_laplacian(g, m)
+    wall = O.wall_nodes(g, "zlo")
+    terms = [np.asarray(t, np.intp) for t in w.terminals]
+    fixed = np.unique(np.concatenate([wall] + terms))
+    A, _ = O.apply_dirichlet(Lm, np.zeros(g.n_nodes), fixed, 0.0)
+    ls = O.LinearSystemCPU(A, method="cg", tol=TOL)
+    t_setup = time.perf_counter() - t0
+    _CPU.update(Lm=Lm, ls=ls, terms=terms, fixed=fixed, n=g.n_nodes, t_setup=t_setup)
+    return t_setup
+
+
+def _cpu_iterate(j, iters):
+    """Run `iters` iterations of the reference's Jacobi CG on RHS j."""
+    import scipy.sparse.linalg as spla
+    Lm, ls, terms, fixed, n = (_CPU[k] for k in ("Lm", "ls", "terms", "fixed", "n"))
+    x0 = np.zeros(n)
+    x0[terms[j]] = 1.0
+    b = -(Lm @ x0)
+    b[fixed] = x0[fixed]
+    bs = (b[ls.free] if ls.split else b) * ls.dinv
+    t0 = time.perf_counter()
+    spla.cg(ls.A, bs, rtol=1e-30, atol=0.0, maxiter=iters, M=ls.M)
+    return (time.perf_counter() - t0) / iters
+
+
+def _reference_iterations(gpu_iters=None):
+    if FULLSIZE_JSON.exists():
+        d = json.loads(FULLSIZE_JSON.read_text())
+        return [int(v) for v in d["iterations_1e-10"]], "oracle full-size run (tests/golden)"
+    if gpu_iters:
+        return [int(v) for v in gpu_iters], "GPU solve of the same system"
+    return [1765] * NBOX, "survey measurement"
+
+
+def cpu_baseline(shape, gpu_iters, sample_iters):
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=1):
+        t_setup = _cpu_setup(shape)
+        t_iter = _cpu_iterate(0, sample_iters)
+    iters, src = _reference_iterations(gpu_iters)
+    t_ext = t_setup + sum(t_iter * it for it in iters)
+    return {"value": NBOX / t_ext, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": (f"CPU oracle (SciPy Jacobi-CG on the equilibrated system): "
+                       f"assembly ({t_setup:.2f} s) + {sample_iters} CG iterations on "
+                       f"RHS 0 of the same {shape} workload ({t_iter*1e3:.1f} ms/iter); "
+                       f"extraction time = assembly + sum over 8 RHS of ms/iter x "
+                       f"iterations to 1e-10 ({src}: {iters})"),
+            "seconds_per_extraction": t_ext}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    shape = tuple(int(v) for v in args.shape.split(","))
+    ncores = os.cpu_count() or 1
+    nproc = max(1, min(NBOX, ncores))
+    sample = max(5, args.cpu_sample_iters // 2)
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=1):
+        t_setup = _cpu_setup(shape)
+    iters, src = _reference_iterations()
+    ctx = mp.get_context("fork")  # no CUDA in this process
+    step_times = []
+    with threadpool_limits(limits=1), ctx.Pool(nproc) as pool:
+        for s in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            per = pool.starmap(_cpu_iterate, [(j, sample) for j in range(NBOX)])
+            wall = time.perf_counter() - t0
+            if s >= args.warmup:
+                # RHS run concurrently on nproc cores: the extraction takes the
+                # assembly plus the longest per-process chain of solves.
+                chains = [0.0] * nproc
+                for j in range(NBOX):
+                    chains[j % nproc] += per[j] * iters[j]
+                step_times.append(t_setup + max(chains))
+    t_ext = statistics.median(step_times)
+    value = NBOX / t_ext
+    line = {
+        "impl": "reference",
+        "metric": "C solves/s @relres 1e-10 (256x256x128, 8 terminals)",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ext * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded layered dielectric + 8 conductor boxes)",
+        "config": {"workload": f"layered_boxes {shape[0]}x{shape[1]}x{shape[2]} nodes, "
+                               f"{NBOX} terminals, zlo grounded, seed=0",
+                   "nodes": int(np.prod(shape)), "nrhs": NBOX, "tol": TOL,
+                   "precision": "fp64", "preconditioner": "jacobi (SciPy CG)"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nproc, "kind": "port",
+                         "sample": (f"CPU oracle (the reference's SciPy Jacobi-CG, restated): "
+                                    f"assembly ({t_setup:.2f} s) once, then per step {sample} "
+                                    f"CG iterations on each of the 8 RHS in {nproc} "
+                                    f"processes; extraction time = assembly + longest chain "
+                                    f"of (s/iter x iterations to 1e-10 [{src}: {iters}])")},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

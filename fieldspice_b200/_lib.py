@@ -1,0 +1,140 @@
+"""ctypes binding of the C ABI in ``include/fieldspice_b200.h``.
+
+The product path has no CPU fallback: if the shared library is missing, or
+no CUDA device is visible, every entry point raises.  Device memory and
+streams come from PyTorch (plumbing only); the library receives raw device
+pointers and a ``cudaStream_t``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import (POINTER, c_char_p, c_double, c_int, c_int32, c_longlong,
+                    c_size_t, c_void_p)
+
+from ._build import LIB_PATH
+
+__all__ = ["lib", "FsRhsStats", "check", "FsError", "stream_ptr", "ptr",
+           "FS_OK", "FS_NOT_CONVERGED", "FS_TIMEOUT", "FS_BAD_ARG", "FS_NAN",
+           "FS_CUDA_ERROR", "LABEL_FREE", "LABEL_FIXED", "LABEL_SOLO",
+           "LABEL_PINNED", "DTYPE_F64", "DTYPE_F32", "PRECISION_FP64",
+           "PRECISION_MIXED", "AVERAGE_PARALLEL", "AVERAGE_HARMONIC",
+           "EXPORTED_SYMBOLS", "load_library"]
+
+FS_OK, FS_NOT_CONVERGED, FS_TIMEOUT, FS_BAD_ARG, FS_NAN, FS_CUDA_ERROR = range(6)
+LABEL_FREE, LABEL_FIXED, LABEL_SOLO, LABEL_PINNED = range(4)
+DTYPE_F64, DTYPE_F32 = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+AVERAGE_PARALLEL, AVERAGE_HARMONIC = 0, 1
+
+
+class FsRhsStats(ctypes.Structure):
+    _fields_ = [("iterations", c_int32), ("status", c_int32),
+                ("relres", c_double), ("bnorm", c_double),
+                ("reliable_updates", c_int32), ("reserved", c_int32)]
+
+
+class FsError(RuntimeError):
+    """A library call returned a status other than FS_OK."""
+
+    def __init__(self, where: str, status: int, detail: str = ""):
+        self.status = status
+        msg = f"{where}: {_status_text(status)}"
+        if detail:
+            msg += f" [{detail}]"
+        super().__init__(msg)
+
+
+_SIGNATURES = {
+    "fs_version": (c_char_p, []),
+    "fs_status_string": (c_char_p, [c_int]),
+    "fs_last_error": (c_char_p, []),
+    "fs_build_masses": (c_int, [c_void_p] * 7 + [c_int] * 4 + [c_void_p] * 4),
+    "fs_combine_masses": (c_int, [c_void_p, c_void_p, c_double, c_double,
+                                  c_void_p, c_longlong, c_void_p]),
+    "fs_stencil_apply": (c_int, [c_void_p] * 6 + [c_int] * 5 + [c_void_p]),
+    "fs_fill_unit_excitation": (c_int, [c_void_p] * 3 + [c_int] * 4 + [c_void_p]),
+    "fs_set_dirichlet": (c_int, [c_void_p] * 4 + [c_int] * 3 + [c_void_p]),
+    "fs_pcg_workspace_bytes": (c_int, [c_int] * 5 + [POINTER(c_size_t)]),
+    "fs_pcg_plan_create": (c_int, [c_int] * 5 + [c_void_p] * 7 + [c_size_t,
+                                   POINTER(c_void_p), c_void_p]),
+    "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
+                                  POINTER(FsRhsStats), c_void_p]),
+    "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
+    "fs_pcg_plan_launches": (c_longlong, [c_void_p]),
+    "fs_pcg_plan_kernel_times": (c_int, [c_void_p, POINTER(c_double),
+                                         POINTER(c_longlong)]),
+    "fs_pcg_plan_destroy": (c_int, [c_void_p]),
+    "fs_group_apply_workspace_bytes": (c_int, [c_int, c_int, POINTER(c_size_t)]),
+    "fs_group_apply": (c_int, [c_void_p] * 10 + [c_int] * 5 + [c_void_p, c_void_p,
+                               c_size_t, c_void_p]),
+    "fs_quadform_workspace_bytes": (c_int, [c_int, POINTER(c_size_t)]),
+    "fs_quadform": (c_int, [c_void_p] * 4 + [c_int] * 4 + [c_void_p, c_void_p,
+                            c_size_t, c_void_p]),
+    "fs_apply_laplacian": (c_int, [c_void_p] * 6 + [c_int] * 4 + [c_void_p]),
+}
+
+#: Every symbol ``include/fieldspice_b200.h`` declares.
+EXPORTED_SYMBOLS = tuple(_SIGNATURES)
+
+_LIB: ctypes.CDLL | None = None
+
+
+def load_library(path=None) -> ctypes.CDLL:
+    """Load the shared library and declare its signatures (no GPU needed)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = LIB_PATH if path is None else path
+    if not p.exists():
+        raise RuntimeError(
+            f"the CUDA library {p} is not built; run "
+            "`python -c 'import __graft_entry__ as g; g.build()'` first. "
+            "fieldspice_b200 has no CPU fallback.")
+    dll = ctypes.CDLL(str(p))
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(dll, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _LIB = dll
+    return dll
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library, after checking that a CUDA device is present."""
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "fieldspice_b200 needs a CUDA device (sm_100a); none is visible and "
+            "there is no CPU fallback")
+    return load_library()
+
+
+def _status_text(status: int) -> str:
+    try:
+        return load_library().fs_status_string(status).decode()
+    except Exception:  # pragma: no cover - only when the library is absent
+        return f"status {status}"
+
+
+def check(where: str, status: int) -> None:
+    """Raise :class:`FsError` unless ``status`` is FS_OK."""
+    if status != FS_OK:
+        detail = ""
+        if status == FS_CUDA_ERROR:
+            detail = load_library().fs_last_error().decode()
+        raise FsError(where, status, detail)
+
+
+def stream_ptr(stream=None) -> c_void_p:
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return c_void_p(s.cuda_stream)
+
+
+def ptr(t) -> c_void_p:
+    """Raw device pointer of a tensor (``None`` -> NULL)."""
+    if t is None:
+        return c_void_p(0)
+    return c_void_p(t.data_ptr())

@@ -1,0 +1,140 @@
+"""Wall boundary conditions consumed by the elliptic path.
+
+Mirrors ``fieldspice/boundaries.py``: :func:`wall_nodes` (``:154-198``) and
+``BoundarySpec.dirichlet_nodes`` (``:963-1029``) with its precedence rule --
+among Dirichlet-like walls the later wall in ``xlo, xhi, ylo, yhi, zlo, zhi``
+wins on a shared node.  Dirichlet, homogeneous Neumann and symmetry walls
+are supported on the GPU path; the reference's own ``BoundarySpec`` objects
+are accepted as long as every wall is one of those (:func:`check_supported`).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable
+
+import numpy as np
+
+__all__ = ["WALLS", "Dirichlet", "Neumann", "BoundarySpec", "wall_nodes",
+           "dirichlet_nodes", "check_supported"]
+
+WALLS = ("xlo", "xhi", "ylo", "yhi", "zlo", "zhi")
+_AXIS = {"xlo": 0, "xhi": 0, "ylo": 1, "yhi": 1, "zlo": 2, "zhi": 2}
+
+
+@dataclass(frozen=True)
+class Dirichlet:
+    """Prescribed potential on a wall; ``value`` may be a callable of t."""
+    value: float | Callable[[float], float] = 0.0
+
+    is_dirichlet_like = True
+    is_natural = False
+
+    def prescribed_value(self, t: float = 0.0):
+        v = self.value
+        return np.asarray(v(t) if callable(v) else v, dtype=float)
+
+
+@dataclass(frozen=True)
+class Neumann:
+    """Prescribed outward normal flux; the GPU path supports flux = 0."""
+    flux: float = 0.0
+
+    is_dirichlet_like = False
+    is_natural = True
+
+    def prescribed_value(self, t: float = 0.0):
+        return None
+
+
+@dataclass
+class BoundarySpec:
+    """Six walls, homogeneous Neumann by default."""
+    xlo: object = field(default_factory=Neumann)
+    xhi: object = field(default_factory=Neumann)
+    ylo: object = field(default_factory=Neumann)
+    yhi: object = field(default_factory=Neumann)
+    zlo: object = field(default_factory=Neumann)
+    zhi: object = field(default_factory=Neumann)
+
+    @classmethod
+    def all_neumann(cls, grid=None) -> "BoundarySpec":
+        return cls()
+
+    def get(self, wall: str):
+        return getattr(self, wall)
+
+    def dirichlet_nodes(self, grid, t: float = 0.0):
+        return dirichlet_nodes(self, grid, t)
+
+
+def _wall(spec, w: str):
+    return spec.get(w) if hasattr(spec, "get") else getattr(spec, w)
+
+
+def wall_nodes(grid, wall: str) -> np.ndarray:
+    """Ascending flat indices of the nodes on one wall (boundaries.py:154-198)."""
+    if wall not in _AXIS:
+        raise ValueError(f"unknown wall {wall!r}; expected one of {WALLS}")
+    shape = tuple(int(s) for s in grid.shape_nodes)
+    strides = (shape[1] * shape[2], shape[2], 1)
+    axis = _AXIS[wall]
+    plane = 0 if wall.endswith("lo") else shape[axis] - 1
+    d0, d1 = [d for d in (0, 1, 2) if d != axis]
+    a = np.arange(shape[d0], dtype=np.intp) * strides[d0]
+    b = np.arange(shape[d1], dtype=np.intp) * strides[d1]
+    return (plane * strides[axis] + a[:, None] + b[None, :]).ravel()
+
+
+def check_supported(spec) -> None:
+    """Reject walls the GPU path does not implement, with a clear error.
+
+    Periodic walls need the node-merging reduction of
+    ``fieldspice/solvers/poisson.py:698-719``, absorbing walls have no
+    quasi-static meaning, and a Neumann wall with non-zero flux needs the
+    ``neumann_load`` right-hand side (``boundaries.py:1031-1085``).
+    """
+    for w in WALLS:
+        bc = _wall(spec, w)
+        kind = type(bc).__name__.lower()
+        if getattr(bc, "is_dirichlet_like", False):
+            continue  # Dirichlet, or a PEC symmetry wall at its value
+        if kind == "neumann":
+            flux = getattr(bc, "flux", 0.0)
+            if callable(flux) or np.any(np.asarray(flux, dtype=float) != 0.0):
+                raise NotImplementedError(
+                    f"wall {w}: driven Neumann flux is not supported on the GPU "
+                    "path; only homogeneous Neumann walls are")
+            continue
+        if getattr(bc, "is_natural", False) and kind != "periodic":
+            continue  # PMC symmetry: the natural zero-flux condition
+        raise NotImplementedError(
+            f"wall {w}: {type(bc).__name__} walls are not supported on the GPU "
+            "path (Dirichlet, Neumann and symmetry walls only)")
+
+
+def dirichlet_nodes(spec, grid, t: float = 0.0):
+    """Fixed wall nodes and values; the later wall wins on a shared node.
+
+    Same precedence as ``BoundarySpec.dirichlet_nodes``
+    (``fieldspice/boundaries.py:963-1029``): indices ascending and unique.
+    """
+    idx_parts, val_parts = [], []
+    for w in WALLS:
+        bc = _wall(spec, w)
+        if not getattr(bc, "is_dirichlet_like", False):
+            continue
+        v = bc.prescribed_value(t)
+        if v is None:
+            raise ValueError(f"wall {w}: {type(bc).__name__} claims to be "
+                             "Dirichlet-like but prescribes no value")
+        idx = wall_nodes(grid, w)
+        vals = np.broadcast_to(np.asarray(v, dtype=float), idx.shape).astype(float)
+        idx_parts.append(idx)
+        val_parts.append(vals)
+    if not idx_parts:
+        return np.empty(0, dtype=np.intp), np.empty(0, dtype=float)
+    idx_all = np.concatenate(idx_parts)
+    val_all = np.concatenate(val_parts)
+    uniq, first_in_rev = np.unique(idx_all[::-1], return_index=True)
+    return uniq.astype(np.intp, copy=False), val_all[::-1][first_in_rev]

@@ -1,0 +1,207 @@
+// Shared device helpers: grid indexing, RHS-interleaved vector access,
+// deterministic block/grid reductions and error bookkeeping.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "fieldspice_b200.h"
+
+namespace fs {
+
+constexpr int kBlock = 256;  // threads per block for every grid-stride kernel
+constexpr int kMaxRhs = 16;
+
+struct Dims {
+  int nx, ny, nz;
+  long long N;   // nodes
+  long long sx;  // stride of i (ny*nz)
+  int sy;        // stride of j (nz)
+};
+
+inline Dims make_dims(int nx, int ny, int nz) {
+  Dims d;
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.sy = nz;
+  d.sx = (long long)ny * nz;
+  d.N = (long long)nx * d.sx;
+  return d;
+}
+
+__device__ __forceinline__ void node_ijk(const Dims& d, long long n, int& i,
+                                         int& j, int& k) {
+  long long t = n / d.nz;
+  k = (int)(n - t * d.nz);
+  i = (int)(t / d.ny);
+  j = (int)(t - (long long)i * d.ny);
+}
+
+// ---- RHS-interleaved vector loads/stores (128-bit where the width allows) --
+template <typename T, int K>
+__device__ __forceinline__ void ldv(const T* __restrict__ base, long long n,
+                                    T (&v)[K]) {
+  const T* p = base + n * K;
+  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c) {
+      float4 t = reinterpret_cast<const float4*>(p)[c];
+      v[4 * c] = t.x;
+      v[4 * c + 1] = t.y;
+      v[4 * c + 2] = t.z;
+      v[4 * c + 3] = t.w;
+    }
+  } else if constexpr (std::is_same<T, float>::value && K == 2) {
+    float2 t = reinterpret_cast<const float2*>(p)[0];
+    v[0] = t.x;
+    v[1] = t.y;
+  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 2; ++c) {
+      double2 t = reinterpret_cast<const double2*>(p)[c];
+      v[2 * c] = t.x;
+      v[2 * c + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < K; ++c) v[c] = p[c];
+  }
+}
+
+// Read-only-path variant for arrays that no thread writes during the kernel.
+template <typename T, int K>
+__device__ __forceinline__ void ldv_ro(const T* __restrict__ base, long long n,
+                                       T (&v)[K]) {
+  const T* p = base + n * K;
+  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c) {
+      float4 t = __ldg(reinterpret_cast<const float4*>(p) + c);
+      v[4 * c] = t.x;
+      v[4 * c + 1] = t.y;
+      v[4 * c + 2] = t.z;
+      v[4 * c + 3] = t.w;
+    }
+  } else if constexpr (std::is_same<T, float>::value && K == 2) {
+    float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 2; ++c) {
+      double2 t = __ldg(reinterpret_cast<const double2*>(p) + c);
+      v[2 * c] = t.x;
+      v[2 * c + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < K; ++c) v[c] = __ldg(p + c);
+  }
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void stv(T* __restrict__ base, long long n,
+                                    const T (&v)[K]) {
+  T* p = base + n * K;
+  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c)
+      reinterpret_cast<float4*>(p)[c] =
+          make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+  } else if constexpr (std::is_same<T, float>::value && K == 2) {
+    reinterpret_cast<float2*>(p)[0] = make_float2(v[0], v[1]);
+  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 2; ++c)
+      reinterpret_cast<double2*>(p)[c] = make_double2(v[2 * c], v[2 * c + 1]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < K; ++c) p[c] = v[c];
+  }
+}
+
+// ---- deterministic reductions ---------------------------------------------
+// Each block reduces its per-thread FP64 accumulators in a fixed order
+// (warp shuffle tree, then warps in index order) and writes one partial per
+// value.  The last block to finish (atomic ticket) sums the partials over
+// blocks, again in a fixed order, so results do not depend on scheduling.
+template <int M>
+__device__ __forceinline__ void block_partials(double (&acc)[M],
+                                               double* __restrict__ partials) {
+  __shared__ double sm[kBlock / 32][M];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double v = acc[m];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) sm[warp][m] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < M) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kBlock / 32; ++w) s += sm[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * M + threadIdx.x] = s;
+  }
+}
+
+// Returns true in exactly one block: the last one to arrive.  That block
+// also resets the ticket so the next launch starts from zero.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == gridDim.x - 1);
+    if (is_last) *ticket = 0u;
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// Sum partials[b*M + m] over b in a fixed order; call from the last block.
+// Result is valid in out[m] for all threads after the call.
+template <int M>
+__device__ __forceinline__ void grid_total(const double* partials, int nblocks,
+                                           double (&out)[M]) {
+  __shared__ double red[kBlock];
+  for (int m = 0; m < M; ++m) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += kBlock)
+      s += __ldcg(partials + (size_t)b * M + m);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      __syncthreads();
+    }
+    out[m] = red[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace fs
+
+// ---- host-side error bookkeeping --------------------------------------------
+void fs_set_error(const char* where, cudaError_t err);
+int fs_cuda_status(const char* where, cudaError_t err);
+int fs_grid_blocks(const void* kernel, long long work_items);
+
+#define FS_CHECK(call)                                        \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return fs_cuda_status(#call, _e);  \
+  } while (0)
+
+#define FS_CHECK_LAUNCH(name)                                     \
+  do {                                                            \
+    cudaError_t _e = cudaGetLastError();                          \
+    if (_e != cudaSuccess) return fs_cuda_status(name, _e);       \
+  } while (0)

@@ -1,0 +1,297 @@
+// Stand-alone FP64/FP32 stencil applies and the FP64 post-processing
+// reductions: terminal charge / current integration and edge energies.
+#include "fs_common.cuh"
+
+using fs::Dims;
+
+namespace {
+
+// y = L x (optionally the eliminated operator: x read as 0 and y written 0
+// on non-free nodes).  Thread per node, all RHS per thread.
+template <typename T, int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_stencil(Dims d, const T* __restrict__ x, T* __restrict__ y,
+              const T* __restrict__ mx, const T* __restrict__ my,
+              const T* __restrict__ mz, const uint8_t* __restrict__ label,
+              const T* __restrict__ add) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T out[K];
+    if (label && label[n] != FS_LABEL_FREE) {
+#pragma unroll
+      for (int t = 0; t < K; ++t) out[t] = (T)0;
+      fs::stv<T, K>(y, n, out);
+      continue;
+    }
+    int i, j, k;
+    fs::node_ijk(d, n, i, j, k);
+    T xc[K];
+    fs::ldv_ro<T, K>(x, n, xc);
+#pragma unroll
+    for (int t = 0; t < K; ++t) out[t] = (T)0;
+    auto nbr = [&](T m, long long nb) {
+      T xn[K];
+      const bool zero = label && label[nb] != FS_LABEL_FREE;
+      if (zero) {
+#pragma unroll
+        for (int t = 0; t < K; ++t) xn[t] = (T)0;
+      } else {
+        fs::ldv_ro<T, K>(x, nb, xn);
+      }
+#pragma unroll
+      for (int t = 0; t < K; ++t) out[t] += m * (xc[t] - xn[t]);
+    };
+    if (i > 0) nbr(mx[n - d.sx], n - d.sx);
+    if (i < d.nx - 1) nbr(mx[n], n + d.sx);
+    if (j > 0) nbr(my[n - d.sy], n - d.sy);
+    if (j < d.ny - 1) nbr(my[n], n + d.sy);
+    if (k > 0) nbr(mz[n - 1], n - 1);
+    if (k < d.nz - 1) nbr(mz[n], n + 1);
+    if (add) {
+      T a[K];
+      fs::ldv_ro<T, K>(add, n, a);
+#pragma unroll
+      for (int t = 0; t < K; ++t) out[t] += a[t];
+    }
+    fs::stv<T, K>(y, n, out);
+  }
+}
+
+template <typename T>
+int launch_stencil(const Dims& d, int nrhs, const T* x, T* y, const T* mx,
+                   const T* my, const T* mz, const uint8_t* label, const T* add,
+                   cudaStream_t s) {
+#define FS_ST(KK)                                                           \
+  case KK: {                                                                \
+    int g = fs_grid_blocks((const void*)k_stencil<T, KK>, d.N);             \
+    k_stencil<T, KK><<<g, fs::kBlock, 0, s>>>(d, x, y, mx, my, mz, label,   \
+                                              add);                         \
+    FS_CHECK_LAUNCH("k_stencil");                                           \
+    return FS_OK;                                                           \
+  }
+  switch (nrhs) {
+    FS_ST(1)
+    FS_ST(2)
+    FS_ST(4)
+    FS_ST(8)
+    FS_ST(16)
+    default: return FS_BAD_ARG;
+  }
+#undef FS_ST
+}
+
+// Per-group sums of (L_A u - L_B w) over explicit node lists.  Grid: one row
+// of `chunks` blocks per group; each block reduces its slice of the group's
+// nodes, the last block sums the partials in a fixed order.
+template <int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_group_apply(Dims d, const double* __restrict__ ax,
+                  const double* __restrict__ ay, const double* __restrict__ az,
+                  const double* __restrict__ u, const double* __restrict__ bx,
+                  const double* __restrict__ by, const double* __restrict__ bz,
+                  const double* __restrict__ w,
+                  const long long* __restrict__ nodes,
+                  const long long* __restrict__ offsets, int ngroups,
+                  int chunks, double* __restrict__ partials,
+                  double* __restrict__ out, unsigned int* ticket) {
+  const int g = blockIdx.x / chunks, c = blockIdx.x % chunks;
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  const long long lo = offsets[g], hi = offsets[g + 1];
+  for (long long e = lo + (long long)c * blockDim.x + threadIdx.x; e < hi;
+       e += (long long)chunks * blockDim.x) {
+    const long long n = nodes[e];
+    if (n < 0 || n >= d.N) continue;  // host validates; never index out of range
+    int i, j, k;
+    fs::node_ijk(d, n, i, j, k);
+    auto apply = [&](const double* mx, const double* my, const double* mz,
+                     const double* v, double sign) {
+      double vc[K];
+#pragma unroll
+      for (int t = 0; t < K; ++t) vc[t] = v[n * K + t];
+      auto edge = [&](bool ok, double m, long long nb) {
+        if (!ok || m == 0.0) return;
+#pragma unroll
+        for (int t = 0; t < K; ++t) acc[t] += sign * m * (vc[t] - v[nb * K + t]);
+      };
+      edge(i > 0, i > 0 ? mx[n - d.sx] : 0.0, n - d.sx);
+      edge(i < d.nx - 1, mx[n], n + d.sx);
+      edge(j > 0, j > 0 ? my[n - d.sy] : 0.0, n - d.sy);
+      edge(j < d.ny - 1, my[n], n + d.sy);
+      edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
+      edge(k < d.nz - 1, mz[n], n + 1);
+    };
+    apply(ax, ay, az, u, 1.0);
+    if (bx) apply(bx, by, bz, w, -1.0);
+  }
+  fs::block_partials<K>(acc, partials);
+  if (fs::last_block(ticket)) {
+    // out[g][t] = sum over that group's chunks, in chunk order.
+    const int total = ngroups * K;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const int gg = idx / K, t = idx % K;
+      double s = 0.0;
+      for (int cc = 0; cc < chunks; ++cc)
+        s += __ldcg(partials + ((size_t)gg * chunks + cc) * K + t);
+      out[idx] = s;
+    }
+  }
+}
+
+// out[t] = sum_e m_e (u_head - u_tail)^2 per RHS.
+template <int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_quadform(Dims d, const double* __restrict__ mx,
+               const double* __restrict__ my, const double* __restrict__ mz,
+               const double* __restrict__ u, double* __restrict__ partials,
+               double* __restrict__ out, unsigned int* ticket) {
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    fs::node_ijk(d, n, i, j, k);
+    auto edge = [&](bool ok, double m, long long nb) {
+      if (!ok) return;
+#pragma unroll
+      for (int t = 0; t < K; ++t) {
+        const double df = u[nb * K + t] - u[n * K + t];
+        acc[t] += m * df * df;
+      }
+    };
+    edge(i < d.nx - 1, mx[n], n + d.sx);
+    edge(j < d.ny - 1, my[n], n + d.sy);
+    edge(k < d.nz - 1, mz[n], n + 1);
+  }
+  fs::block_partials<K>(acc, partials);
+  if (fs::last_block(ticket)) {
+    double tot[K];
+    fs::grid_total<K>(partials, gridDim.x, tot);
+    if (threadIdx.x < K) out[threadIdx.x] = tot[threadIdx.x];
+  }
+}
+
+constexpr int kGroupChunks = 32;
+constexpr int kQuadMaxBlocks = 4096;
+
+size_t group_ws(int ngroups, int nrhs) {
+  return 256 + (size_t)ngroups * kGroupChunks * nrhs * 8;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fs_stencil_apply(const void* x, void* y, const void* mx, const void* my,
+                     const void* mz, const uint8_t* label, int nx, int ny,
+                     int nz, int nrhs, int dtype, void* stream) {
+  if (!x || !y || !mx || !my || !mz || nx < 2 || ny < 2 || nz < 2)
+    return FS_BAD_ARG;
+  Dims d = fs::make_dims(nx, ny, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == FS_DTYPE_F64)
+    return launch_stencil<double>(d, nrhs, (const double*)x, (double*)y,
+                                  (const double*)mx, (const double*)my,
+                                  (const double*)mz, label, nullptr, s);
+  if (dtype == FS_DTYPE_F32)
+    return launch_stencil<float>(d, nrhs, (const float*)x, (float*)y,
+                                 (const float*)mx, (const float*)my,
+                                 (const float*)mz, label, nullptr, s);
+  return FS_BAD_ARG;
+}
+
+int fs_apply_laplacian(const double* mx, const double* my, const double* mz,
+                       const double* u, const double* add, double* out, int nx,
+                       int ny, int nz, int nrhs, void* stream) {
+  if (!mx || !my || !mz || !u || !out || nx < 2 || ny < 2 || nz < 2)
+    return FS_BAD_ARG;
+  Dims d = fs::make_dims(nx, ny, nz);
+  return launch_stencil<double>(d, nrhs, u, out, mx, my, mz, nullptr, add,
+                                (cudaStream_t)stream);
+}
+
+int fs_group_apply_workspace_bytes(int ngroups, int nrhs, size_t* bytes) {
+  if (ngroups < 1 || nrhs < 1 || nrhs > fs::kMaxRhs || !bytes) return FS_BAD_ARG;
+  *bytes = group_ws(ngroups, nrhs);
+  return FS_OK;
+}
+
+int fs_group_apply(const double* mAx, const double* mAy, const double* mAz,
+                   const double* u, const double* mBx, const double* mBy,
+                   const double* mBz, const double* w, const long long* nodes,
+                   const long long* offsets, int ngroups, int nx, int ny,
+                   int nz, int nrhs, double* out, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  if (!mAx || !mAy || !mAz || !u || !nodes || !offsets || !out || !workspace ||
+      ngroups < 1 || nx < 2 || ny < 2 || nz < 2)
+    return FS_BAD_ARG;
+  if (mBx && (!mBy || !mBz || !w)) return FS_BAD_ARG;
+  if (workspace_bytes < group_ws(ngroups, nrhs) || ((uintptr_t)workspace & 255))
+    return FS_BAD_ARG;
+  if ((long long)ngroups * kGroupChunks > 65535LL * 1024) return FS_BAD_ARG;
+  Dims d = fs::make_dims(nx, ny, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* ticket = (unsigned int*)workspace;
+  double* partials = (double*)((char*)workspace + 256);
+  FS_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  const int grid = ngroups * kGroupChunks;
+#define FS_GA(KK)                                                            \
+  case KK:                                                                   \
+    k_group_apply<KK><<<grid, fs::kBlock, 0, s>>>(                           \
+        d, mAx, mAy, mAz, u, mBx, mBy, mBz, w, nodes, offsets, ngroups,      \
+        kGroupChunks, partials, out, ticket);                                \
+    FS_CHECK_LAUNCH("k_group_apply");                                        \
+    return FS_OK;
+  switch (nrhs) {
+    FS_GA(1)
+    FS_GA(2)
+    FS_GA(4)
+    FS_GA(8)
+    FS_GA(16)
+    default: return FS_BAD_ARG;
+  }
+#undef FS_GA
+}
+
+int fs_quadform_workspace_bytes(int nrhs, size_t* bytes) {
+  if (nrhs < 1 || nrhs > fs::kMaxRhs || !bytes) return FS_BAD_ARG;
+  *bytes = 256 + (size_t)kQuadMaxBlocks * nrhs * 8;
+  return FS_OK;
+}
+
+int fs_quadform(const double* mx, const double* my, const double* mz,
+                const double* u, int nx, int ny, int nz, int nrhs, double* out,
+                void* workspace, size_t workspace_bytes, void* stream) {
+  size_t need = 0;
+  if (fs_quadform_workspace_bytes(nrhs, &need) != FS_OK) return FS_BAD_ARG;
+  if (!mx || !my || !mz || !u || !out || !workspace || workspace_bytes < need ||
+      nx < 2 || ny < 2 || nz < 2 || ((uintptr_t)workspace & 255))
+    return FS_BAD_ARG;
+  Dims d = fs::make_dims(nx, ny, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* ticket = (unsigned int*)workspace;
+  double* partials = (double*)((char*)workspace + 256);
+  FS_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+#define FS_QF(KK)                                                             \
+  case KK: {                                                                  \
+    int g = fs_grid_blocks((const void*)k_quadform<KK>, d.N);                 \
+    if (g > kQuadMaxBlocks) g = kQuadMaxBlocks;                               \
+    k_quadform<KK><<<g, fs::kBlock, 0, s>>>(d, mx, my, mz, u, partials, out,  \
+                                            ticket);                          \
+    FS_CHECK_LAUNCH("k_quadform");                                            \
+    return FS_OK;                                                             \
+  }
+  switch (nrhs) {
+    FS_QF(1)
+    FS_QF(2)
+    FS_QF(4)
+    FS_QF(8)
+    FS_QF(16)
+    default: return FS_BAD_ARG;
+  }
+#undef FS_QF
+}
+
+}  // extern "C"

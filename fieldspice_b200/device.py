@@ -1,0 +1,301 @@
+"""Device-resident operators and the eliminated CG system.
+
+:class:`DeviceOperator` holds the edge masses of one ``G^T diag(m) G`` in HBM
+(FP64, node-padded, see ``include/fieldspice_b200.h``) and offers the FP64
+applies, charge sums and energies.  :class:`EliminatedSystem` binds one
+operator, one Dirichlet label array and one potential buffer to a CG plan of
+the C library and solves in place.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+
+import numpy as np
+
+from . import _lib as L
+from .grid import grid_metric
+
+__all__ = ["DeviceOperator", "EliminatedSystem", "pad_rhs", "MAX_RHS",
+           "device", "h2d", "d2h", "TRANSFERS", "upload_groups"]
+
+#: Bytes moved between host and device by the product path (host arrays
+#: uploaded, results read back); the benchmark reads it per step.
+TRANSFERS = {"h2d": 0, "d2h": 0}
+
+
+def h2d(a, dtype, dev):
+    """Upload a host array (counted in ``TRANSFERS``)."""
+    import torch
+    arr = np.ascontiguousarray(a)
+    t = torch.as_tensor(arr).to(device=dev, dtype=dtype)
+    TRANSFERS["h2d"] += arr.nbytes
+    return t
+
+
+def d2h(t) -> np.ndarray:
+    """Read a device tensor back to a NumPy array (counted)."""
+    out = t.detach().cpu().numpy()
+    TRANSFERS["d2h"] += out.nbytes
+    return out
+
+MAX_RHS = 16
+_SUPPORTED_K = (1, 2, 4, 8, 16)
+
+
+def pad_rhs(k: int) -> int:
+    """Smallest supported RHS width (1, 2, 4, 8, 16) holding ``k`` columns."""
+    for s in _SUPPORTED_K:
+        if k <= s:
+            return s
+    raise ValueError(f"at most {MAX_RHS} right-hand sides per solve, got {k}")
+
+
+def device():
+    import torch
+    L.lib()  # raises without a GPU or without the library
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _as_dev(a, dtype, dev):
+    import torch
+    if isinstance(a, torch.Tensor):
+        return a.to(device=dev, dtype=dtype).contiguous()
+    return h2d(a, dtype, dev)
+
+
+class DeviceOperator:
+    """``G^T diag(m) G`` on one grid, masses resident on the GPU.
+
+    Build from a per-cell property with the reference's averaging
+    (``fieldspice/operators.py:144-237`` then ``:302-315``), or wrap masses
+    that already live on the device.
+    """
+
+    def __init__(self, grid, prop_cell=None, *, mode: str = "parallel",
+                 masses=None):
+        import torch
+        self.grid = grid
+        self.shape = tuple(int(s) for s in grid.shape_nodes)
+        self.N = int(np.prod(self.shape))
+        self.dev = device()
+        lib = L.lib()
+        if masses is not None:
+            self.m = masses
+            return
+        if mode not in ("parallel", "arithmetic", "harmonic", "series"):
+            raise ValueError(f"unknown averaging mode {mode!r}")
+        avg = L.AVERAGE_HARMONIC if mode in ("harmonic", "series") else L.AVERAGE_PARALLEL
+        (hx, hy, hz), (hxd, hyd, hzd) = grid_metric(grid)
+        hs = [_as_dev(a, torch.float64, self.dev) for a in (hx, hy, hz, hxd, hyd, hzd)]
+        prop = _as_dev(prop_cell, torch.float64, self.dev)
+        if prop.numel() != int(np.prod(grid.shape_cells)):
+            raise ValueError("prop_cell does not match the grid's cell shape")
+        self.m = torch.empty((3, self.N), dtype=torch.float64, device=self.dev)
+        nx, ny, nz = self.shape
+        st = lib.fs_build_masses(L.ptr(prop), *(L.ptr(h) for h in hs), nx, ny, nz,
+                                 avg, L.ptr(self.m[0]), L.ptr(self.m[1]),
+                                 L.ptr(self.m[2]), L.stream_ptr())
+        L.check("fs_build_masses", st)
+
+    # -- mass arrays ---------------------------------------------------------
+    @property
+    def mx(self):
+        return self.m[0]
+
+    @property
+    def my(self):
+        return self.m[1]
+
+    @property
+    def mz(self):
+        return self.m[2]
+
+    def combine(self, a: float, other: "DeviceOperator", b: float) -> "DeviceOperator":
+        """``a*self + b*other`` edge by edge (eqs.py:279-280)."""
+        import torch
+        out = torch.empty_like(self.m)
+        st = L.lib().fs_combine_masses(L.ptr(self.m), L.ptr(other.m), float(a),
+                                       float(b), L.ptr(out), self.m.numel(),
+                                       L.stream_ptr())
+        L.check("fs_combine_masses", st)
+        return DeviceOperator(self.grid, masses=out)
+
+    def edge_vector(self) -> np.ndarray:
+        """Masses in the reference's concatenated [x|y|z] edge order (host)."""
+        nx, ny, nz = self.shape
+        m = self.m.cpu().numpy().reshape(3, nx, ny, nz)
+        return np.concatenate([m[0, :-1].ravel(), m[1, :, :-1].ravel(),
+                               m[2, :, :, :-1].ravel()])
+
+    # -- FP64 applies ----------------------------------------------------------
+    def apply(self, u, nrhs: int = 1, add=None):
+        """``L u (+ add)`` in FP64 on the device (u: N*nrhs, RHS-interleaved)."""
+        import torch
+        out = torch.empty_like(u)
+        nx, ny, nz = self.shape
+        st = L.lib().fs_apply_laplacian(L.ptr(self.mx), L.ptr(self.my),
+                                        L.ptr(self.mz), L.ptr(u), L.ptr(add),
+                                        L.ptr(out), nx, ny, nz, nrhs,
+                                        L.stream_ptr())
+        L.check("fs_apply_laplacian", st)
+        return out
+
+    def quadform(self, u, nrhs: int = 1) -> np.ndarray:
+        """``u^T L u`` per RHS (FP64)."""
+        import torch
+        lib = L.lib()
+        nb = ctypes.c_size_t()
+        L.check("fs_quadform_workspace_bytes",
+                lib.fs_quadform_workspace_bytes(nrhs, ctypes.byref(nb)))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device=self.dev)
+        out = torch.empty(nrhs, dtype=torch.float64, device=self.dev)
+        nx, ny, nz = self.shape
+        st = lib.fs_quadform(L.ptr(self.mx), L.ptr(self.my), L.ptr(self.mz),
+                             L.ptr(u), nx, ny, nz, nrhs, L.ptr(out), L.ptr(ws),
+                             nb.value, L.stream_ptr())
+        L.check("fs_quadform", st)
+        return d2h(out)
+
+    def group_sums(self, u, groups, nrhs: int = 1, minus=None, w=None,
+                   nodes_dev=None) -> np.ndarray:
+        """``sum_{n in group} (L u - L_minus w)_n`` per group and RHS (FP64).
+
+        ``groups`` is a list of node-index arrays; ``nodes_dev`` may carry the
+        already-uploaded ``(nodes, offsets)`` pair to skip the copy.
+        """
+        import torch
+        lib = L.lib()
+        if nodes_dev is None:
+            nodes_dev = upload_groups(groups, self.dev)
+        nodes, offsets, ng = nodes_dev
+        nb = ctypes.c_size_t()
+        L.check("fs_group_apply_workspace_bytes",
+                lib.fs_group_apply_workspace_bytes(ng, nrhs, ctypes.byref(nb)))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device=self.dev)
+        out = torch.empty(ng * nrhs, dtype=torch.float64, device=self.dev)
+        nx, ny, nz = self.shape
+        mb = (None, None, None) if minus is None else (minus.mx, minus.my, minus.mz)
+        st = lib.fs_group_apply(L.ptr(self.mx), L.ptr(self.my), L.ptr(self.mz),
+                                L.ptr(u), *(L.ptr(t) for t in mb), L.ptr(w),
+                                L.ptr(nodes), L.ptr(offsets), ng, nx, ny, nz,
+                                nrhs, L.ptr(out), L.ptr(ws), nb.value,
+                                L.stream_ptr())
+        L.check("fs_group_apply", st)
+        return d2h(out).reshape(ng, nrhs)
+
+
+def upload_groups(groups, dev):
+    """Concatenate node lists into (nodes, offsets, ngroups) device arrays.
+
+    ``groups`` may hold host arrays or int64 device tensors."""
+    import torch
+    if groups and all(isinstance(g, torch.Tensor) for g in groups):
+        sizes = [int(g.numel()) for g in groups]
+        flat = torch.cat([g.reshape(-1).to(torch.int64) for g in groups])
+        offsets = np.zeros(len(groups) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum(sizes)
+        if flat.numel() == 0:
+            flat = torch.zeros(1, dtype=torch.int64, device=dev)
+        return flat, h2d(offsets, torch.int64, dev), len(groups)
+    groups = [np.asarray(g, dtype=np.int64).ravel() for g in groups]
+    offsets = np.zeros(len(groups) + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum([g.size for g in groups])
+    flat = np.concatenate(groups) if groups else np.zeros(0, np.int64)
+    if flat.size == 0:
+        flat = np.zeros(1, np.int64)
+    return h2d(flat, torch.int64, dev), h2d(offsets, torch.int64, dev), len(groups)
+
+
+class EliminatedSystem:
+    """One Dirichlet-eliminated system and its CG plan.
+
+    ``label``: uint8 device array (``FS_LABEL_FREE``/``FS_LABEL_FIXED`` per
+    node).  ``phi`` (N*k FP64) holds the Dirichlet values on fixed nodes and
+    receives the solution; ``f`` (optional, N*k) is the source term.
+    """
+
+    def __init__(self, op: DeviceOperator, label, nrhs: int, *,
+                 precision: str = "mixed", with_source: bool = False):
+        import torch
+        self.op = op
+        self.k = pad_rhs(nrhs)
+        self.nrhs = nrhs
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        self.precision = precision
+        prec = L.PRECISION_MIXED if precision == "mixed" else L.PRECISION_FP64
+        lib = L.lib()
+        dev = op.dev
+        N = op.N
+        self.label_in = label
+        self.phi = torch.zeros(N * self.k, dtype=torch.float64, device=dev)
+        self.f = (torch.zeros(N * self.k, dtype=torch.float64, device=dev)
+                  if with_source else None)
+        nb = ctypes.c_size_t()
+        nx, ny, nz = op.shape
+        L.check("fs_pcg_workspace_bytes",
+                lib.fs_pcg_workspace_bytes(nx, ny, nz, self.k, prec, ctypes.byref(nb)))
+        self.workspace = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+        if self.workspace.data_ptr() % 256:
+            raise RuntimeError("device allocation is not 256-byte aligned")
+        t0 = time.perf_counter()
+        plan = ctypes.c_void_p()
+        st = lib.fs_pcg_plan_create(nx, ny, nz, self.k, prec, L.ptr(op.mx),
+                                    L.ptr(op.my), L.ptr(op.mz), L.ptr(label),
+                                    L.ptr(self.phi), L.ptr(self.f),
+                                    L.ptr(self.workspace), nb.value,
+                                    ctypes.byref(plan), L.stream_ptr())
+        L.check("fs_pcg_plan_create", st)
+        self._plan = plan
+        # The classified labels are the first N bytes of the workspace.
+        lab_ptr = lib.fs_pcg_plan_labels(plan)
+        off = lab_ptr - self.workspace.data_ptr()
+        self.labels = self.workspace[off:off + N]
+        counts = torch.bincount(self.labels.to(torch.int64), minlength=4).cpu().numpy()
+        self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts[:4])
+        self.setup_time = time.perf_counter() - t0
+        self.launches = 0
+
+    def default_maxiter(self) -> int:
+        """The reference's cap ``max(500, 10*sqrt(n))`` (poisson.py:535-536)."""
+        return max(500, int(10 * math.sqrt(max(self.n_free, 1))))
+
+    def solve(self, tol: float, maxiter: int | None = None, *, warm: bool = False):
+        """Solve in place into ``phi``; returns (status, per-RHS stats dicts)."""
+        lib = L.lib()
+        stats = (L.FsRhsStats * self.k)()
+        mi = self.default_maxiter() if maxiter is None else int(maxiter)
+        st = lib.fs_pcg_plan_solve(self._plan, 1 if warm else 0, float(tol), mi,
+                                   stats, L.stream_ptr())
+        self.launches = int(lib.fs_pcg_plan_launches(self._plan))
+        if st not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN):
+            L.check("fs_pcg_plan_solve", st)
+        out = [{"iterations": s.iterations, "status": s.status, "relres": s.relres,
+                "bnorm": s.bnorm, "reliable_updates": s.reliable_updates}
+               for s in stats[:self.nrhs]]
+        return st, out
+
+    def kernel_times(self) -> dict:
+        """Per-kernel device time sampled during the last solve (ms per
+        launch): p-update, stencil (A~p, p.q) and update (x, r, r.r)."""
+        ms = (ctypes.c_double * 3)()
+        ns = ctypes.c_longlong()
+        L.check("fs_pcg_plan_kernel_times",
+                L.load_library().fs_pcg_plan_kernel_times(self._plan, ms, ctypes.byref(ns)))
+        n = max(ns.value, 1)
+        return {"samples": ns.value, "pupdate_ms": ms[0] / n, "stencil_ms": ms[1] / n,
+                "update_ms": ms[2] / n}
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) is not None and self._plan.value:
+            L.load_library().fs_pcg_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

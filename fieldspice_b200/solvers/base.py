@@ -1,0 +1,144 @@
+"""Problem and result types of the solve path.
+
+These mirror ``fieldspice/solvers/base.py`` (``ConvergenceError`` :35-48,
+``SolverConfig`` :51-82, ``Terminal`` :85-133, ``Result`` :136-202) so that a
+caller of the reference can pass the same objects.  The reference's own
+instances are accepted too: every function here reads them by attribute.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Any, Callable, Sequence
+
+import numpy as np
+
+__all__ = ["ConvergenceError", "SolverConfig", "GPUConfig", "Terminal", "Result"]
+
+
+class ConvergenceError(RuntimeError):
+    """An iterative solve ended above its tolerance.
+
+    ``history`` holds the final relative residuals; ``last_state`` the last
+    iterate when one is available (``fieldspice/solvers/base.py:35-48``).
+    """
+
+    def __init__(self, msg: str, history: Sequence[float] = (),
+                 last_state: np.ndarray | None = None):
+        super().__init__(msg)
+        self.history = list(history)
+        self.last_state = last_state
+
+
+@dataclass
+class SolverConfig:
+    """Shared solver knobs (same fields and defaults as the reference).
+
+    ``linear_solver`` is accepted for compatibility; the GPU path always runs
+    preconditioned CG on the eliminated system, so ``"direct"`` and ``"amg"``
+    select the same GPU solve.  ``tol`` is the relative residual of the
+    Jacobi-equilibrated free-node system, exactly SciPy's ``rtol`` in the
+    reference (``fieldspice/solvers/poisson.py:542``).
+    """
+    linear_solver: str = "auto"
+    tol: float = 1e-10
+    newton_tol: float = 1e-8
+    max_newton: int = 60
+    damping: float = 1.0
+    verbose: int = 0
+    store_every: int = 1
+    dtype: type = np.float64
+
+
+@dataclass
+class GPUConfig:
+    """GPU-only knobs, kept apart from :class:`SolverConfig`.
+
+    precision
+        ``"mixed"``: FP32 inner CG with FP64 reliable updates (the residual
+        that decides convergence is always FP64).  ``"fp64"``: every vector
+        in FP64, the plain method.
+    preconditioner
+        ``"jacobi"`` (CG on the equilibrated system, the reference's method)
+        or ``"mg"`` (geometric multigrid V-cycle inside flexible CG).
+    maxiter
+        Iteration cap; ``None`` uses the reference's ``max(500, 10*sqrt(n))``
+        (``poisson.py:535-536``).
+    """
+    precision: str = "mixed"
+    preconditioner: str = "jacobi"
+    maxiter: int | None = None
+
+
+@dataclass
+class Terminal:
+    """An electrode: a set of node indices held at a common potential.
+
+    Same contract as ``fieldspice/solvers/base.py:85-133``: ``nodes`` is made
+    unique and sorted, ``voltage`` or ``current`` may be a constant or a
+    callable of time.
+    """
+    name: str
+    nodes: np.ndarray
+    voltage: float | Callable[[float], float] | None = None
+    current: float | Callable[[float], float] | None = None
+    circuit_node: str | None = None
+
+    def __post_init__(self):
+        self.nodes = np.unique(np.asarray(self.nodes, dtype=np.intp).ravel())
+        if self.voltage is not None and self.current is not None:
+            raise ValueError(
+                f"terminal {self.name!r}: set voltage or current, not both")
+
+    def value_at(self, t: float) -> float | None:
+        src = self.voltage if self.voltage is not None else self.current
+        if src is None:
+            return None
+        return float(src(t)) if callable(src) else float(src)
+
+    @property
+    def driven(self) -> str:
+        if self.voltage is not None:
+            return "voltage"
+        if self.current is not None:
+            return "current"
+        return "float"
+
+
+@dataclass
+class Result:
+    """Uniform output container (``fieldspice/solvers/base.py:136-202``)."""
+    grid: Any
+    t: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    fields: dict[str, np.ndarray] = field(default_factory=dict)
+    terminals: dict[str, dict[str, np.ndarray]] = field(default_factory=dict)
+    scalars: dict[str, np.ndarray] = field(default_factory=dict)
+    meta: dict[str, Any] = field(default_factory=dict)
+
+    def v(self, terminal: str) -> np.ndarray:
+        return self.terminals[terminal]["v"]
+
+    def i(self, terminal: str) -> np.ndarray:
+        return self.terminals[terminal]["i"]
+
+    def field(self, name: str, step: int = -1) -> np.ndarray:
+        return self.fields[name][step]
+
+    def final(self, name: str) -> np.ndarray:
+        return self.fields[name][-1]
+
+
+def terminal_driven(t) -> str:
+    """``Terminal.driven`` for this module's or the reference's terminals."""
+    return t.driven
+
+
+class _Clock:
+    """Wall-clock bookkeeping for ``Result.meta`` (base.py:228-237)."""
+
+    def __init__(self):
+        self.t0 = time.perf_counter()
+
+    def elapsed(self) -> float:
+        return time.perf_counter() - self.t0

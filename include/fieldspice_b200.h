@@ -1,0 +1,194 @@
+/*
+ * fieldspice_b200 -- C ABI of the B200 elliptic-solve library.
+ *
+ * The library solves the finite-integration system  G^T M G phi = f  on a
+ * rectilinear node grid, matrix-free, with the Dirichlet rows eliminated
+ * symmetrically.  Every pointer below is DEVICE memory unless the comment says
+ * "host"; every function returns an FS_* status code and never throws.
+ *
+ * Node layout.  A grid has nx*ny*nz nodes stored in C order, z fastest:
+ *     n = (i*ny + j)*nz + k.
+ * A field with `nrhs` right-hand sides is stored RHS-interleaved, so value
+ * (n, r) sits at  n*nrhs + r.
+ *
+ * Edge masses.  The reference keeps one concatenated edge vector
+ * [x-edges (nx-1,ny,nz) | y-edges (nx,ny-1,nz) | z-edges (nx,ny,nz-1)]
+ * (fieldspice/grid.py:322-327).  Here each direction is padded to the node
+ * shape: mx[n] is the mass of the x-edge from node (i,j,k) to (i+1,j,k) and is
+ * 0 on the last x-plane; my and mz likewise.  This keeps all arrays in the
+ * node index space, so a kernel addresses masses and potentials alike.
+ *
+ * Labels.  One byte per node: FS_LABEL_FREE (unknown) or FS_LABEL_FIXED
+ * (Dirichlet, its value held in phi).  The solver further classifies free
+ * nodes that are coupled to no other free node as "solo" (solved directly,
+ * poisson.py:336-362) and free nodes with no incident mass as "pinned" to 0
+ * (poisson.py:282-295).
+ */
+#ifndef FIELDSPICE_B200_H
+#define FIELDSPICE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FS_OK 0
+#define FS_NOT_CONVERGED 1   /* iteration cap reached above tolerance        */
+#define FS_TIMEOUT 2         /* the device did not report completion          */
+#define FS_BAD_ARG 3         /* invalid size, pointer or option              */
+#define FS_NAN 4             /* a residual norm became NaN or Inf             */
+#define FS_CUDA_ERROR 5      /* a CUDA runtime call failed                    */
+
+/* ---- enumerations ------------------------------------------------------ */
+#define FS_LABEL_FREE 0
+#define FS_LABEL_FIXED 1
+#define FS_LABEL_SOLO 2
+#define FS_LABEL_PINNED 3
+
+#define FS_DTYPE_F64 0
+#define FS_DTYPE_F32 1
+
+#define FS_PRECISION_FP64 0  /* every vector and mass in FP64                 */
+#define FS_PRECISION_MIXED 1 /* FP32 inner CG, FP64 reliable updates          */
+
+#define FS_AVERAGE_PARALLEL 0 /* dual-area weighted arithmetic mean           */
+#define FS_AVERAGE_HARMONIC 1 /* dual-area weighted harmonic mean             */
+
+#define FS_PRECOND_JACOBI 0  /* CG on the Jacobi-equilibrated system          */
+#define FS_PRECOND_MG 1      /* geometric multigrid V-cycle (flexible CG)     */
+
+typedef struct fs_rhs_stats {
+  int32_t iterations;       /* CG iterations taken                            */
+  int32_t status;           /* FS_OK, FS_NOT_CONVERGED or FS_NAN              */
+  double relres;            /* final FP64 true relative residual              */
+  double bnorm;             /* ||D^-1/2 b_free||_2 of the eliminated system   */
+  int32_t reliable_updates; /* FP64 residual replacements performed           */
+  int32_t reserved;
+} fs_rhs_stats;
+
+typedef struct fs_pcg_plan fs_pcg_plan;
+
+/* ---- library ----------------------------------------------------------- */
+const char* fs_version(void);
+const char* fs_status_string(int status);
+/* Last CUDA error text recorded by a failing call on this thread (host).    */
+const char* fs_last_error(void);
+
+/* ---- a1-a3: material averaging and edge masses ----------------------------
+ * Replaces fieldspice/operators.py:144-237 (cell_to_edge) followed by
+ * operators.py:302-315 (edge_mass): for every edge the dual-area weighted
+ * mean of the (up to) four cells around it, times dual area over length.
+ * prop_cell: (nx-1)*(ny-1)*(nz-1) FP64 per-cell property, C order.
+ * h*, hd*: primal widths (n-1) and dual widths (n) per axis, FP64 device
+ * arrays, computed on the host exactly as fieldspice/grid.py:196-207.
+ * Writes padded node-shaped mx, my, mz (FP64).  The arithmetic order follows
+ * the reference so that the result is bit-identical to it.                  */
+int fs_build_masses(const double* prop_cell, const double* hx, const double* hy,
+                    const double* hz, const double* hxd, const double* hyd,
+                    const double* hzd, int nx, int ny, int nz, int mode,
+                    double* mx, double* my, double* mz, void* stream);
+
+/* out = a*m1 + b*m2 elementwise over n values (FP64).  Builds the EQS masses
+ * M_eps/dt + theta*M_sigma (fieldspice/solvers/eqs.py:279-280).            */
+int fs_combine_masses(const double* m1, const double* m2, double a, double b,
+                      double* out, long long n, void* stream);
+
+/* ---- a5: stencil apply ----------------------------------------------------
+ * y = (G^T M G) x, the operator of fieldspice/operators.py:340-351 applied
+ * matrix-free.  With `label` non-NULL the apply is the eliminated operator of
+ * operators.py:362-407: x is read as 0 on non-free nodes and y is written 0
+ * there.  dtype selects FP64 or FP32 for x, y and the masses.               */
+int fs_stencil_apply(const void* x, void* y, const void* mx, const void* my,
+                     const void* mz, const uint8_t* label, int nx, int ny,
+                     int nz, int nrhs, int dtype, void* stream);
+
+/* ---- a6/a10: Dirichlet excitation -------------------------------------------
+ * phi[n*nrhs + r] = (group[n] == r) ? 1 : 0 for every node whose label is
+ * fixed, and 0 on free nodes: the unit excitation of capacitance column r
+ * (fieldspice/solvers/poisson.py:1212-1217).  group: int16 per node, -1 for
+ * nodes in no terminal.                                                       */
+int fs_fill_unit_excitation(const int16_t* group, const uint8_t* label,
+                            double* phi, int nx, int ny, int nz, int nrhs,
+                            void* stream);
+
+/* phi[n] = values[group[n]] on fixed nodes with group[n] >= 0 (one RHS):
+ * the per-step Dirichlet values of fieldspice/solvers/eqs.py:108-129.        */
+int fs_set_dirichlet(const int16_t* group, const uint8_t* label,
+                     const double* values, double* phi, int nx, int ny, int nz,
+                     void* stream);
+
+/* ---- a7-a9: the eliminated CG solve ----------------------------------------
+ * Replaces LinearSystem (fieldspice/solvers/poisson.py:260-589) for the
+ * symmetric positive definite Dirichlet-eliminated system, with the
+ * reference's stopping rule: ||D^-1/2 (b - A x)||_2 < tol*||D^-1/2 b||_2 on
+ * the free nodes (SciPy CG on the equilibrated matrix, poisson.py:364-377,
+ * 533-552).  The plan is bound to one operator, one label array and one phi
+ * buffer (N*nrhs FP64, fixed values in place, the initial guess on free
+ * nodes) and an optional source f (N*nrhs FP64, may be NULL).
+ * nrhs must be 1, 2, 4, 8 or 16.  workspace must hold
+ * fs_pcg_workspace_bytes() bytes and stay alive until destroy.              */
+int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
+                           size_t* bytes);
+int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
+                       const double* mx, const double* my, const double* mz,
+                       const uint8_t* label_in, double* phi, const double* f,
+                       void* workspace, size_t workspace_bytes,
+                       fs_pcg_plan** plan, void* stream);
+/* Solve in place into phi.  warm_start != 0 keeps the free-node values of
+ * phi as the initial guess (the tolerance stays relative to ||b||, as in
+ * SciPy); otherwise the guess is 0.  stats: host array of nrhs entries.
+ * Returns FS_OK when every RHS converged, FS_NOT_CONVERGED if one hit
+ * maxiter, FS_NAN on breakdown.                                             */
+int fs_pcg_plan_solve(fs_pcg_plan* plan, int warm_start, double tol,
+                      int maxiter, fs_rhs_stats* stats, void* stream);
+/* Label array after classification (free / fixed / solo / pinned), device. */
+const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* plan);
+/* Number of kernel launches issued by the last solve (host count).          */
+long long fs_pcg_plan_launches(const fs_pcg_plan* plan);
+/* Device time of the p-update, stencil (A~p and p.q) and update kernels,
+ * summed over the samples taken during the last solve: the first CG
+ * iteration of every graph launch is bracketed by CUDA events.  ms: host
+ * array of 3.                                                               */
+int fs_pcg_plan_kernel_times(const fs_pcg_plan* plan, double* ms,
+                             long long* samples);
+int fs_pcg_plan_destroy(fs_pcg_plan* plan);
+
+/* ---- a10/a13: charge and current integration (FP64) -----------------------
+ * out[g*nrhs + r] = sum over nodes n of group g of
+ *                   (L_A u)[n, r] - (L_B w)[n, r]
+ * where L_A = G^T diag(mA) G and, when mBx is non-NULL, L_B likewise.  The
+ * groups are given as a concatenated node list `nodes` (int64) with
+ * offsets[0..ngroups].  With B absent this is the terminal charge
+ * C[i,j] = sum_{n in T_i} (L phi_j)_n of poisson.py:1219-1221; with
+ * A = K, B = Kexp it is the terminal current of eqs.py:328-340.
+ * workspace: fs_group_apply_workspace_bytes() bytes.                         */
+int fs_group_apply_workspace_bytes(int ngroups, int nrhs, size_t* bytes);
+int fs_group_apply(const double* mAx, const double* mAy, const double* mAz,
+                   const double* u, const double* mBx, const double* mBy,
+                   const double* mBz, const double* w, const long long* nodes,
+                   const long long* offsets, int ngroups, int nx, int ny,
+                   int nz, int nrhs, double* out, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* out[r] = sum over edges of m_e (u_head - u_tail)^2 = u^T L u per RHS: the
+ * stored energy 2*W of poisson.py:905-913 and eqs.py:342-348.               */
+int fs_quadform_workspace_bytes(int nrhs, size_t* bytes);
+int fs_quadform(const double* mx, const double* my, const double* mz,
+                const double* u, int nx, int ny, int nz, int nrhs,
+                double* out, void* workspace, size_t workspace_bytes,
+                void* stream);
+
+/* out = L u + add (add may be NULL), FP64, every node: the explicit part
+ * Kexp @ phi + inject of eqs.py:293.                                         */
+int fs_apply_laplacian(const double* mx, const double* my, const double* mz,
+                       const double* u, const double* add, double* out, int nx,
+                       int ny, int nz, int nrhs, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIELDSPICE_B200_H */

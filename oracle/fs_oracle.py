@@ -1,0 +1,536 @@
+"""CPU oracle of fieldspice's elliptic solve path -- TEST INFRASTRUCTURE ONLY.
+
+This module restates, in NumPy/SciPy, the reference algorithm of the path the
+GPU library replaces.  It is the checker: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may
+import it, and never as the thing measured or shipped.  The product path
+(``fieldspice_b200``) does not import it and has no CPU fallback.
+
+Parity pin: ``tests/golden/make_golden.py`` imported the reference package
+and recorded its outputs (masses, Laplacians, capacitance matrices, EQS
+currents) as ``tests/golden/*.npz``; ``tests/test_oracle_golden.py`` checks
+this restatement against every one of them.
+
+Every function cites the reference file:line it follows (paths inside the
+fieldspice project).  SciPy (the reference's own dependency, installed here
+at 1.18) provides the CSR products and ``cg``/``splu``, as in the reference.
+"""
+
+from __future__ import annotations
+
+import math
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+EPS0 = 1.0 / ((4e-7 * math.pi * 1.0000000000552) * 299_792_458.0 ** 2)  # units.py:20-26
+
+
+# ---------------------------------------------------------------------------
+# Grid metric -- fieldspice/grid.py:196-207 (_make_axis), :322-327, :398-420
+# ---------------------------------------------------------------------------
+@dataclass
+class Grid:
+    """Node coordinates per axis; metric arrays as in grid.py."""
+    xn: np.ndarray
+    yn: np.ndarray
+    zn: np.ndarray
+
+    @classmethod
+    def uniform(cls, extent, n):
+        # grid.py:533-546
+        axes = [np.linspace(e[0], e[1], int(k) + 1) for e, k in zip(extent, n)]
+        return cls(*axes)
+
+    @classmethod
+    def from_any(cls, g):
+        return cls(np.asarray(g.xn, float), np.asarray(g.yn, float),
+                   np.asarray(g.zn, float))
+
+    def _axis(self, a):
+        h = np.diff(a)
+        hd = np.empty(a.size)
+        hd[1:-1] = 0.5 * (h[:-1] + h[1:])
+        hd[0] = 0.5 * h[0]
+        hd[-1] = 0.5 * h[-1]
+        return h, hd
+
+    @property
+    def hx(self): return self._axis(self.xn)[0]
+    @property
+    def hy(self): return self._axis(self.yn)[0]
+    @property
+    def hz(self): return self._axis(self.zn)[0]
+    @property
+    def hxd(self): return self._axis(self.xn)[1]
+    @property
+    def hyd(self): return self._axis(self.yn)[1]
+    @property
+    def hzd(self): return self._axis(self.zn)[1]
+
+    @property
+    def shape_nodes(self):
+        return (self.xn.size, self.yn.size, self.zn.size)
+
+    @property
+    def shape_cells(self):
+        return (self.xn.size - 1, self.yn.size - 1, self.zn.size - 1)
+
+    @property
+    def shape_edges(self):
+        nx, ny, nz = self.shape_cells
+        return ((nx, ny + 1, nz + 1), (nx + 1, ny, nz + 1), (nx + 1, ny + 1, nz))
+
+    @property
+    def n_nodes(self):
+        return int(np.prod(self.shape_nodes))
+
+    @property
+    def n_edges(self):
+        return int(sum(np.prod(s) for s in self.shape_edges))
+
+    def node_volumes(self):
+        # grid.py:388-396
+        return (self.hxd[:, None, None] * self.hyd[None, :, None]
+                * self.hzd[None, None, :])
+
+    def edge_lengths(self):
+        # grid.py:398-405
+        sx, sy, sz = self.shape_edges
+        return (np.ascontiguousarray(np.broadcast_to(self.hx[:, None, None], sx)),
+                np.ascontiguousarray(np.broadcast_to(self.hy[None, :, None], sy)),
+                np.ascontiguousarray(np.broadcast_to(self.hz[None, None, :], sz)))
+
+    def edge_dual_areas(self):
+        # grid.py:407-420
+        sx, sy, sz = self.shape_edges
+        ax = np.broadcast_to(self.hyd[None, :, None] * self.hzd[None, None, :], sx)
+        ay = np.broadcast_to(self.hxd[:, None, None] * self.hzd[None, None, :], sy)
+        az = np.broadcast_to(self.hxd[:, None, None] * self.hyd[None, :, None], sz)
+        return (np.ascontiguousarray(ax), np.ascontiguousarray(ay),
+                np.ascontiguousarray(az))
+
+
+# ---------------------------------------------------------------------------
+# Incidence operators -- fieldspice/operators.py:59-138
+# ---------------------------------------------------------------------------
+def _ids(shape, offset=0):
+    return (offset + np.arange(int(np.prod(shape)))).reshape(shape)
+
+
+def _assemble(terms, shape):
+    # operators.py:63-68
+    rows = np.concatenate([np.asarray(r).ravel() for r, _, _ in terms])
+    cols = np.concatenate([np.asarray(c).ravel() for _, c, _ in terms])
+    vals = np.concatenate([np.full(np.asarray(c).size, v, dtype=np.float64)
+                           for _, c, v in terms])
+    return sp.coo_matrix((vals, (rows, cols)), shape=shape).tocsr()
+
+
+def grad_node_edge(g: Grid):
+    """``(G phi)_e = phi_head - phi_tail`` (operators.py:71-91)."""
+    nid = _ids(g.shape_nodes)
+    sx, sy, sz = g.shape_edges
+    nex, ney = int(np.prod(sx)), int(np.prod(sy))
+    ex, ey, ez = _ids(sx, 0), _ids(sy, nex), _ids(sz, nex + ney)
+    terms = [(ex, nid[1:, :, :], 1.0), (ex, nid[:-1, :, :], -1.0),
+             (ey, nid[:, 1:, :], 1.0), (ey, nid[:, :-1, :], -1.0),
+             (ez, nid[:, :, 1:], 1.0), (ez, nid[:, :, :-1], -1.0)]
+    return _assemble(terms, (g.n_edges, g.n_nodes))
+
+
+def _face_shapes(g: Grid):
+    nx, ny, nz = g.shape_cells
+    return ((nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1))
+
+
+def curl_edge_face(g: Grid):
+    """Right-handed face circulation (operators.py:94-119)."""
+    sx, sy, sz = g.shape_edges
+    fx, fy, fz = _face_shapes(g)
+    nex, ney = int(np.prod(sx)), int(np.prod(sy))
+    nfx, nfy = int(np.prod(fx)), int(np.prod(fy))
+    ex, ey, ez = _ids(sx, 0), _ids(sy, nex), _ids(sz, nex + ney)
+    Fx, Fy, Fz = _ids(fx, 0), _ids(fy, nfx), _ids(fz, nfx + nfy)
+    terms = [(Fx, ez[:, 1:, :], 1.0), (Fx, ez[:, :-1, :], -1.0),
+             (Fx, ey[:, :, :-1], 1.0), (Fx, ey[:, :, 1:], -1.0),
+             (Fy, ex[:, :, 1:], 1.0), (Fy, ex[:, :, :-1], -1.0),
+             (Fy, ez[:-1, :, :], 1.0), (Fy, ez[1:, :, :], -1.0),
+             (Fz, ey[1:, :, :], 1.0), (Fz, ey[:-1, :, :], -1.0),
+             (Fz, ex[:, :-1, :], 1.0), (Fz, ex[:, 1:, :], -1.0)]
+    nf = sum(int(np.prod(s)) for s in (fx, fy, fz))
+    return _assemble(terms, (nf, g.n_edges))
+
+
+def div_face_cell(g: Grid):
+    """Net outward flux per cell (operators.py:122-138)."""
+    fx, fy, fz = _face_shapes(g)
+    nfx, nfy = int(np.prod(fx)), int(np.prod(fy))
+    Fx, Fy, Fz = _ids(fx, 0), _ids(fy, nfx), _ids(fz, nfx + nfy)
+    cid = _ids(g.shape_cells)
+    terms = [(cid, Fx[1:, :, :], 1.0), (cid, Fx[:-1, :, :], -1.0),
+             (cid, Fy[:, 1:, :], 1.0), (cid, Fy[:, :-1, :], -1.0),
+             (cid, Fz[:, :, 1:], 1.0), (cid, Fz[:, :, :-1], -1.0)]
+    nf = sum(int(np.prod(s)) for s in (fx, fy, fz))
+    return _assemble(terms, (int(np.prod(g.shape_cells)), nf))
+
+
+# ---------------------------------------------------------------------------
+# Material averaging and masses -- fieldspice/operators.py:144-237, :302-315
+# ---------------------------------------------------------------------------
+def _combine(q, w, mode):
+    # operators.py:225-237: sums over the quadrant axis, left to right
+    wsum = w.sum(axis=0)
+    safe = np.where(wsum > 0, wsum, 1.0)
+    if mode in ("parallel", "arithmetic"):
+        return (q * w).sum(axis=0) / safe
+    if mode in ("harmonic", "series"):
+        qq = np.where(q > 0, q, np.finfo(float).tiny)
+        return safe / (w / qq).sum(axis=0)
+    raise ValueError(f"unknown averaging mode {mode!r}")
+
+
+def cell_to_edge(g: Grid, prop, mode="parallel"):
+    """Dual-area weighted mean of the four cells around each edge.
+
+    operators.py:144-222: cells are edge-padded at the walls; quadrants are
+    taken in the order (0,0), (0,1), (1,0), (1,1).
+    """
+    prop = np.asarray(prop, dtype=float)
+    if prop.shape != g.shape_cells:
+        raise ValueError(f"prop must have shape {g.shape_cells}, got {prop.shape}")
+    p = np.pad(prop, 1, mode="edge")
+
+    def halves(h):
+        return (np.concatenate([[0.0], 0.5 * h]), np.concatenate([0.5 * h, [0.0]]))
+
+    ylo, yhi = halves(g.hy)
+    zlo, zhi = halves(g.hz)
+    xlo, xhi = halves(g.hx)
+    combos = [(0, 0), (0, 1), (1, 0), (1, 1)]
+    out = []
+    sx = g.shape_edges[0]
+    q, w = np.empty((4,) + sx), np.empty((4,) + sx)
+    c = p[1:-1, :, :]
+    for m, (dj, dk) in enumerate(combos):
+        q[m] = c[:, dj:dj + sx[1], dk:dk + sx[2]]
+        wy = (ylo if dj == 0 else yhi)[None, :, None]
+        wz = (zlo if dk == 0 else zhi)[None, None, :]
+        w[m] = np.broadcast_to(wy * wz, sx)
+    out.append(_combine(q, w, mode))
+    sy = g.shape_edges[1]
+    q, w = np.empty((4,) + sy), np.empty((4,) + sy)
+    c = p[:, 1:-1, :]
+    for m, (di, dk) in enumerate(combos):
+        q[m] = c[di:di + sy[0], :, dk:dk + sy[2]]
+        wx = (xlo if di == 0 else xhi)[:, None, None]
+        wz = (zlo if dk == 0 else zhi)[None, None, :]
+        w[m] = np.broadcast_to(wx * wz, sy)
+    out.append(_combine(q, w, mode))
+    sz = g.shape_edges[2]
+    q, w = np.empty((4,) + sz), np.empty((4,) + sz)
+    c = p[:, :, 1:-1]
+    for m, (di, dj) in enumerate(combos):
+        q[m] = c[di:di + sz[0], dj:dj + sz[1], :]
+        wx = (xlo if di == 0 else xhi)[:, None, None]
+        wy = (ylo if dj == 0 else yhi)[None, :, None]
+        w[m] = np.broadcast_to(wx * wy, sz)
+    out.append(_combine(q, w, mode))
+    return np.concatenate([o.ravel() for o in out])
+
+
+def edge_mass_vector(g: Grid, prop_edge):
+    """``prop * A_dual / L`` per edge (operators.py:302-315)."""
+    prop_edge = np.asarray(prop_edge, dtype=float).ravel()
+    Lv = np.concatenate([a.ravel() for a in g.edge_lengths()])
+    A = np.concatenate([a.ravel() for a in g.edge_dual_areas()])
+    return prop_edge * A / Lv
+
+
+def nodal_laplacian(g: Grid, mass_edge):
+    """``G^T diag(m) G`` (operators.py:340-351)."""
+    G = grad_node_edge(g)
+    return sp.csr_matrix(G.T @ sp.diags(mass_edge, format="dia") @ G)
+
+
+def padded_masses(g: Grid, mass_edge):
+    """Edge vector -> three node-shaped arrays (0 on the last plane)."""
+    nx, ny, nz = g.shape_nodes
+    sx, sy, sz = g.shape_edges
+    n1, n2 = int(np.prod(sx)), int(np.prod(sy))
+    out = np.zeros((3, nx, ny, nz))
+    out[0, :-1] = mass_edge[:n1].reshape(sx)
+    out[1, :, :-1] = mass_edge[n1:n1 + n2].reshape(sy)
+    out[2, :, :, :-1] = mass_edge[n1 + n2:].reshape(sz)
+    return out.reshape(3, -1)
+
+
+def apply_dirichlet(A, b, fixed, values):
+    """Symmetric elimination (operators.py:362-407)."""
+    A = sp.csr_matrix(A, copy=True)
+    b = np.array(b, dtype=float, copy=True)
+    n = A.shape[0]
+    fixed = np.asarray(fixed)
+    idx = np.flatnonzero(fixed) if fixed.dtype == bool else fixed.astype(np.intp)
+    vals = np.broadcast_to(np.asarray(values, dtype=float), idx.shape)
+    x0 = np.zeros(n)
+    x0[idx] = vals
+    b -= A @ x0
+    mask = np.ones(n, dtype=bool)
+    mask[idx] = False
+    Dm = sp.diags(mask.astype(float))
+    A = Dm @ A @ Dm
+    A = A + sp.diags((~mask).astype(float))
+    b[idx] = vals
+    return sp.csr_matrix(A), b
+
+
+# ---------------------------------------------------------------------------
+# Walls -- fieldspice/boundaries.py:154-198, :963-1029
+# ---------------------------------------------------------------------------
+_AXIS = {"xlo": 0, "xhi": 0, "ylo": 1, "yhi": 1, "zlo": 2, "zhi": 2}
+WALLS = ("xlo", "xhi", "ylo", "yhi", "zlo", "zhi")
+
+
+def wall_nodes(g: Grid, wall: str):
+    shape = g.shape_nodes
+    strides = (shape[1] * shape[2], shape[2], 1)
+    axis = _AXIS[wall]
+    plane = 0 if wall.endswith("lo") else shape[axis] - 1
+    d0, d1 = [d for d in (0, 1, 2) if d != axis]
+    a = np.arange(shape[d0], dtype=np.intp) * strides[d0]
+    b = np.arange(shape[d1], dtype=np.intp) * strides[d1]
+    return (plane * strides[axis] + a[:, None] + b[None, :]).ravel()
+
+
+def dirichlet_nodes(g: Grid, walls: dict[str, float]):
+    """``walls``: {wall: value} of Dirichlet walls; later wall wins."""
+    idx_parts, val_parts = [], []
+    for w in WALLS:
+        if w not in walls:
+            continue
+        idx = wall_nodes(g, w)
+        idx_parts.append(idx)
+        val_parts.append(np.full(idx.size, float(walls[w])))
+    if not idx_parts:
+        return np.empty(0, np.intp), np.empty(0)
+    ia, va = np.concatenate(idx_parts), np.concatenate(val_parts)
+    u, first = np.unique(ia[::-1], return_index=True)
+    return u.astype(np.intp), va[::-1][first]
+
+
+def unique_last(idx, val):
+    # poisson.py:722-727
+    if idx.size == 0:
+        return idx.astype(np.intp), val.astype(float)
+    u, first = np.unique(idx[::-1], return_index=True)
+    return u.astype(np.intp), val[::-1][first]
+
+
+# ---------------------------------------------------------------------------
+# LinearSystem restated for the SPD eliminated system -- poisson.py:260-589
+# ---------------------------------------------------------------------------
+class LinearSystemCPU:
+    """Prepared eliminated system: solo split, equilibration, CG or LU.
+
+    Follows poisson.py:336-381 (decoupled rows split off, symmetric Jacobi
+    equilibration) and :487-589 (solve, un-scale, true residual).  ``method``
+    is "cg" (SciPy CG with the Jacobi preconditioner the reference falls back
+    to when its incomplete LU is unavailable, :477-484) or "direct" (SuperLU,
+    :457).  The default CG+ILU branch is not restated: it stalls on these
+    systems.
+    """
+
+    def __init__(self, A, method="cg", tol=1e-10, maxiter=None):
+        A = sp.csr_matrix(A)
+        self.n = A.shape[0]
+        self.tol = tol
+        d = A.diagonal()
+        row_abs = np.asarray(abs(A).sum(axis=1)).ravel()
+        solo = (row_abs <= np.abs(d)) & (d != 0)
+        self.solo = np.flatnonzero(solo)
+        self.free = np.flatnonzero(~solo)
+        self.solo_diag = d[self.solo]
+        self.split = bool(self.solo.size) and self.free.size > 0
+        if self.split:
+            A = sp.csr_matrix(A[self.free][:, self.free])
+        dreal = A.diagonal()
+        self.dhalf = np.sqrt(dreal)
+        self.dinv = 1.0 / self.dhalf
+        S = sp.diags(self.dinv)
+        self.A = sp.csr_matrix(S @ A @ S)
+        self.n_free = self.A.shape[0]
+        self.method = method
+        self.maxiter = maxiter
+        if method == "direct":
+            self.lu = spla.splu(self.A.tocsc(), permc_spec="MMD_AT_PLUS_A")
+        else:
+            dd = self.A.diagonal()
+            dd = np.where(np.abs(dd) > 0, dd, 1.0)
+            self.M = spla.LinearOperator(self.A.shape, lambda v: v / dd,
+                                         dtype=self.A.dtype)
+        self.info = {}
+
+    def solve(self, b, x0=None):
+        b = np.asarray(b, dtype=float).copy()
+        bf = b[self.free] if self.split else b
+        bs = bf * self.dinv
+        iters = 0
+        if self.method == "direct":
+            xs = self.lu.solve(bs)
+        else:
+            maxiter = self.maxiter or max(500, int(10 * np.sqrt(self.n_free)))
+            counter = {"n": 0}
+
+            def cb(_):
+                counter["n"] += 1
+            kw = {"rtol": self.tol, "atol": 0.0, "maxiter": maxiter, "M": self.M,
+                  "callback": cb}
+            if x0 is not None:
+                g0 = np.asarray(x0, float)
+                if self.split:
+                    g0 = g0[self.free]
+                kw["x0"] = g0 * self.dhalf
+            xs, flag = spla.cg(self.A, bs, **kw)
+            iters = counter["n"]
+            if flag != 0:
+                warnings.warn(f"cg flag {flag} after {iters} iterations",
+                              RuntimeWarning, stacklevel=2)
+        xf = xs * self.dinv
+        if self.split:
+            x = np.zeros(self.n)
+            x[self.free] = xf
+            x[self.solo] = b[self.solo] / self.solo_diag
+        else:
+            x = xf
+        rs = bs - self.A @ xs
+        nb = float(np.linalg.norm(bs))
+        self.info = {"iterations": iters,
+                     "relres": float(np.linalg.norm(rs) / nb) if nb > 0 else 0.0}
+        return x
+
+
+# ---------------------------------------------------------------------------
+# Capacitance extraction -- poisson.py:1100-1249
+# ---------------------------------------------------------------------------
+def capacitance_matrix(g: Grid, eps_cell, terminals, dirichlet_walls=None,
+                       method="cg", tol=1e-10, symmetrise=True, mode="parallel"):
+    """Maxwell C by unit excitation; returns (C, report).
+
+    ``terminals``: list of node-index arrays.  ``dirichlet_walls``: {wall:
+    value} (values are ignored, every Dirichlet wall is a grounded shield).
+    """
+    m = edge_mass_vector(g, cell_to_edge(g, eps_cell, mode))
+    Lmat = nodal_laplacian(g, m)
+    wall_idx, _ = dirichlet_nodes(g, dirichlet_walls or {})
+    terms = [np.unique(np.asarray(t, np.intp)) for t in terminals]
+    term_nodes = np.concatenate(terms)
+    fixed = np.concatenate([wall_idx, term_nodes]).astype(np.intp)
+    fixed, _ = unique_last(fixed, np.zeros(fixed.size))
+    shield = np.setdiff1d(wall_idx, term_nodes)
+    A_bc, _ = apply_dirichlet(Lmat, np.zeros(g.n_nodes), fixed, np.zeros(fixed.size))
+    ls = LinearSystemCPU(A_bc, method=method, tol=tol)
+    nt = len(terms)
+    C = np.zeros((nt, nt))
+    q_shield = np.zeros(nt)
+    iters, relres, phis = [], [], []
+    for j, tj in enumerate(terms):
+        x0 = np.zeros(g.n_nodes)
+        x0[tj] = 1.0
+        b = -(Lmat @ x0)
+        b[fixed] = x0[fixed]
+        phi = ls.solve(b)
+        phis.append(phi)
+        iters.append(ls.info["iterations"])
+        relres.append(ls.info["relres"])
+        q = Lmat @ phi
+        for i, ti in enumerate(terms):
+            C[i, j] = float(q[ti].sum())
+        if shield.size:
+            q_shield[j] = float(q[shield].sum())
+    scale = float(np.abs(np.diag(C)).max()) or 1.0
+    rep = {"asymmetry_abs": float(np.abs(C - C.T).max())}
+    rep["asymmetry_rel"] = rep["asymmetry_abs"] / scale
+    if symmetrise:
+        C = 0.5 * (C + C.T)
+    rows = C.sum(axis=1)
+    rep["row_sum"] = rows
+    rep["row_sum_rel"] = float(np.abs(rows).max() / scale)
+    off = C - np.diag(np.diag(C))
+    rep["max_offdiag"] = float(off.max()) if nt > 1 else 0.0
+    rep["shield_charge"] = q_shield
+    rep["iterations"] = iters
+    rep["relres"] = relres
+    rep["phis"] = phis
+    return C, rep
+
+
+# ---------------------------------------------------------------------------
+# EQS backward Euler / theta -- fieldspice/solvers/eqs.py:97-101, :176-195,
+# :229-323, :328-340
+# ---------------------------------------------------------------------------
+def eqs_transient(g: Grid, eps_cell, sigma_cell, fixed_groups, values_at,
+                  dt, nsteps, theta=1.0, method="cg", tol=1e-10,
+                  dirichlet_walls=None, t_start=0.0):
+    """Backward-Euler EQS with terminal currents.
+
+    ``fixed_groups``: list of node arrays (voltage-driven terminals);
+    ``values_at(t)``: their voltages at time t.  Dirichlet walls (values
+    fixed) come first, terminals after (eqs.py:108-129: a terminal listed
+    later wins).  Returns (phis, currents[nsteps+1, nterm]).
+    """
+    me = edge_mass_vector(g, cell_to_edge(g, eps_cell))
+    ms = edge_mass_vector(g, cell_to_edge(g, sigma_cell))
+    Le = nodal_laplacian(g, me)
+    Ls = nodal_laplacian(g, ms)
+    walls = dirichlet_walls or {}
+
+    def dirichlet(t):
+        idx, val = [], []
+        vt = values_at(t)
+        for grp, v in zip(fixed_groups, vt):
+            idx.append(np.asarray(grp, np.intp))
+            val.append(np.full(len(grp), float(v)))
+        widx, wval = dirichlet_nodes(g, walls)
+        if widx.size:
+            idx.append(widx)
+            val.append(wval)
+        fixed = np.concatenate(idx)
+        vals = np.concatenate(val)
+        u, last = np.unique(fixed[::-1], return_index=True)
+        return u, vals[::-1][last]
+
+    # consistent initial condition (eqs.py:176-195)
+    fixed, vals = dirichlet(t_start)
+    A0, b0 = apply_dirichlet(Le, np.zeros(g.n_nodes), fixed, vals)
+    phi = LinearSystemCPU(A0, method=method, tol=tol).solve(b0)
+    K = (Le / dt + theta * Ls).tocsr()
+    Kexp = (Le / dt - (1.0 - theta) * Ls).tocsr()
+    ls = None
+    phis = [phi.copy()]
+    for k in range(1, nsteps + 1):
+        t = t_start + dt * k
+        fixed, vals = dirichlet(t)
+        rhs = Kexp @ phi
+        A, b = apply_dirichlet(K, rhs, fixed, vals)
+        if ls is None:
+            ls = LinearSystemCPU(A, method=method, tol=tol)
+        phi = ls.solve(b)
+        phis.append(phi.copy())
+    cur = np.zeros((nsteps + 1, len(fixed_groups)))
+    for k in range(1, nsteps + 1):
+        resid = (Le @ (phis[k] - phis[k - 1]) / dt
+                 + Ls @ (theta * phis[k] + (1 - theta) * phis[k - 1]))
+        for j, grp in enumerate(fixed_groups):
+            cur[k, j] = float(resid[np.asarray(grp, np.intp)].sum())
+    if nsteps >= 1:
+        cur[0] = cur[1]
+    return phis, cur
+
+
+def laplacian_apply(g: Grid, mass_edge, x):
+    """``L @ x`` with the assembled CSR (reference arithmetic)."""
+    return nodal_laplacian(g, mass_edge) @ x

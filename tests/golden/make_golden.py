@@ -1,0 +1,217 @@
+"""Generate the golden fixtures by running the reference fieldspice package.
+
+Run in a container where the reference source tree is available:
+
+    FIELDSPICE_REF=/path/to/fieldspice python tests/golden/make_golden.py
+
+The reference is imported from that path and executed on small seeded
+inputs; its outputs are written next to this script as ``.npz`` files.  The
+tests never import the reference: they compare the CPU oracle and the GPU
+library against these recorded outputs.
+
+Iterative reference solves force SciPy's Jacobi branch of ``LinearSystem``
+(``fieldspice/solvers/poisson.py:472-484``) by making ``spilu`` raise: the
+default incomplete-LU branch stalls on these systems.
+"""
+
+from __future__ import annotations
+
+import contextlib
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = os.environ.get("FIELDSPICE_REF", "/root/reference")
+sys.path.insert(0, REF)
+sys.path.insert(0, str(HERE.parents[1]))
+
+import scipy.sparse.linalg as spla  # noqa: E402
+
+import fieldspice as fs  # noqa: E402
+from fieldspice import operators as ops  # noqa: E402
+from fieldspice.boundaries import BoundarySpec, Dirichlet  # noqa: E402
+from fieldspice.grid import RectilinearGrid, graded_1d  # noqa: E402
+from fieldspice.solvers.base import SolverConfig, Terminal  # noqa: E402
+from fieldspice.solvers.eqs import EQSSolver  # noqa: E402
+from fieldspice.solvers.poisson import PoissonSolver  # noqa: E402
+from fieldspice.units import eps0  # noqa: E402
+
+from fieldspice_b200 import workloads as W  # noqa: E402  (input generator only)
+
+
+@contextlib.contextmanager
+def jacobi_forced():
+    orig = spla.spilu
+
+    def _raise(*a, **k):
+        raise MemoryError("incomplete LU disabled: Jacobi branch forced")
+    spla.spilu = _raise
+    try:
+        yield
+    finally:
+        spla.spilu = orig
+
+
+def graded_grid():
+    # the awkward grid of tests/test_core.py:25-36 ("3d_graded")
+    return RectilinearGrid(graded_1d(0, 1e-3, 7, 1.3), graded_1d(0, 2e-3, 5, 0.8),
+                           graded_1d(0, 3e-4, 4, 1.5))
+
+
+def masses_fixture():
+    out = {}
+    rng = np.random.default_rng(1234)
+    for name, g in {"graded": graded_grid(),
+                    "uniform": RectilinearGrid.uniform([(0, 1), (0, 1), (0, 1)], [4, 3, 2]),
+                    "collapsed": RectilinearGrid(graded_1d(0, 1e-3, 7, 1.3),
+                                                 graded_1d(0, 2e-3, 5, 0.8), None),
+                    "wide": RectilinearGrid(np.sort(rng.uniform(0, 1, 12)),
+                                            np.sort(rng.uniform(0, 1, 9)),
+                                            np.sort(rng.uniform(0, 1, 7)))}.items():
+        prop = rng.uniform(1.0, 12.0, g.shape_cells) * eps0
+        pe = ops.cell_to_edge(g, prop, "parallel")
+        ph = ops.cell_to_edge(g, prop, "harmonic")
+        mp = ops.edge_mass(g, pe).diagonal()
+        mh = ops.edge_mass(g, ph).diagonal()
+        Lm = ops.nodal_laplacian(g, pe)
+        x = rng.standard_normal((g.n_nodes, 3))
+        y = Lm @ x
+        G = ops.grad_node_edge(g)
+        out.update({f"{name}_xn": g.xn, f"{name}_yn": g.yn, f"{name}_zn": g.zn,
+                    f"{name}_prop": prop, f"{name}_eps_edge": pe,
+                    f"{name}_mass_parallel": mp, f"{name}_mass_harmonic": mh,
+                    f"{name}_x": x, f"{name}_Lx": y,
+                    f"{name}_L_indptr": Lm.indptr, f"{name}_L_indices": Lm.indices,
+                    f"{name}_L_data": Lm.data,
+                    f"{name}_G_indptr": G.indptr, f"{name}_G_indices": G.indices,
+                    f"{name}_G_data": G.data})
+    np.savez_compressed(HERE / "masses.npz", **out)
+
+
+def readme_fixture():
+    w = W.parallel_plate()
+    g = RectilinearGrid(w.x, w.y, w.z)
+    terms = [Terminal("top", w.terminals[0], voltage=1.0),
+             Terminal("bottom", w.terminals[1], voltage=0.0)]
+    ps = PoissonSolver(g, w.eps_cell)
+    rep = {}
+    C = ps.capacitance_matrix(terms, report=rep)
+    res = ps.solve(terms)
+    np.savez_compressed(HERE / "readme.npz", C=C, asym=rep["asymmetry_rel"],
+                        row_sum_rel=rep["row_sum_rel"],
+                        phi=res.fields["phi"].ravel(),
+                        energy=res.scalars["energy"], q_top=res.terminals["top"]["q"])
+
+
+def layered_fixture(shape, seed, tol):
+    w = W.layered_boxes(shape, nbox=8, seed=seed)
+    g = RectilinearGrid(w.x, w.y, w.z)
+    terms = [Terminal(n, t) for n, t in zip(w.names, w.terminals)]
+    bc = BoundarySpec(zlo=Dirichlet(0.0))
+    rep = {}
+    with jacobi_forced():
+        ps = PoissonSolver(g, w.eps_cell, SolverConfig(linear_solver="cg", tol=tol))
+        C = ps.capacitance_matrix(terms, bc, report=rep)
+    tag = f"layered_{shape[0]}x{shape[1]}x{shape[2]}_s{seed}"
+    np.savez_compressed(HERE / f"{tag}.npz", C=C, x=w.x, y=w.y, z=w.z,
+                        eps_cell=w.eps_cell.astype(np.float64),
+                        boxes=np.asarray(w.boxes), shield=rep["shield_charge"],
+                        asym=rep["asymmetry_rel"], tol=tol,
+                        iterations=rep["linear"].get("iterations", -1))
+
+
+def rc_stack(n=60):
+    d, Wd, H = 4e-6, 3e-6, 2e-6
+    sigma1, er1, er2 = 1e3, 4.0, 2.0
+    g = RectilinearGrid(np.linspace(0, d, n + 1), np.linspace(0, Wd, 4),
+                        np.linspace(0, H, 3))
+    left = g.xc < d / 2
+    sig = np.zeros(g.shape_cells)
+    sig[left] = sigma1
+    eps = np.empty(g.shape_cells)
+    eps[left] = er1 * eps0
+    eps[~left] = er2 * eps0
+    return g, eps, sig
+
+
+def eqs_fixture():
+    # the RC stack of tests/test_quasistatic.py:24-59, direct path
+    g, eps, sig = rc_stack()
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    out = {"xn": g.xn, "yn": g.yn, "zn": g.zn, "eps": eps, "sig": sig}
+    from fieldspice import reference as ref
+    A = 3e-6 * 2e-6
+    R1 = 2e-6 / (1e3 * A)
+    C1 = ref.parallel_plate_capacitance(A, 2e-6, 4.0)
+    C2 = ref.parallel_plate_capacitance(A, 2e-6, 2.0)
+    tau = R1 * (C1 + C2)
+    out["tau"] = tau
+    for spt in (50, 100):
+        s = EQSSolver(g, eps, sig, SolverConfig(verbose=0))
+        hi = Terminal("hi", nid[0].ravel(), voltage=1.0)
+        lo = Terminal("lo", nid[-1].ravel(), voltage=0.0)
+        r = s.solve([hi, lo], t_end=8 * tau, dt=tau / spt, store=True)
+        out[f"spt{spt}_i_hi"] = r.i("hi")
+        out[f"spt{spt}_i_lo"] = r.i("lo")
+        out[f"spt{spt}_vm"] = r.fields["phi"][:, nid[30, 1, 1]]
+        out[f"spt{spt}_t"] = r.scalars["t_stored"]
+        out[f"spt{spt}_energy"] = r.scalars["energy_electric"]
+    # a small interconnect transient (CG path, Jacobi forced, tight tol)
+    w = W.eqs_interconnect((24, 24, 16), nbox=3, nports=2, seed=3, si_cells=4)
+    g2 = RectilinearGrid(w.x, w.y, w.z)
+    ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
+    terms = [Terminal("port0", w.terminals[0], voltage=ramp),
+             Terminal("port1", w.terminals[1], voltage=0.0)]
+    with jacobi_forced():
+        s2 = EQSSolver(g2, w.eps_cell, w.sigma_cell,
+                       SolverConfig(linear_solver="cg", tol=1e-12))
+        r2 = s2.solve(terms, t_end=20e-12, dt=1e-12,
+                      bc=BoundarySpec(zlo=Dirichlet(0.0)), store=True)
+    out.update({"ic_x": w.x, "ic_y": w.y, "ic_z": w.z, "ic_eps": w.eps_cell,
+                "ic_sig": w.sigma_cell, "ic_boxes": np.asarray(w.boxes),
+                "ic_i0": r2.i("port0"), "ic_i1": r2.i("port1"),
+                "ic_v0": r2.v("port0"), "ic_phi_last": r2.fields["phi"][-1],
+                "ic_energy": r2.scalars["energy_electric"],
+                "ic_dissipation": r2.scalars["dissipation"]})
+    np.savez_compressed(HERE / "eqs.npz", **out)
+
+
+def closed_forms():
+    # tests/test_core.py:236-297: series stack and graded plate, direct solves
+    from fieldspice import reference as ref
+    out = {}
+    er1, er2, d, Wd, H = 4.0, 2.0, 4e-6, 3e-6, 2e-6
+    g = RectilinearGrid(np.linspace(0, d, 41), np.linspace(0, Wd, 5), np.linspace(0, H, 4))
+    e = np.empty(g.shape_cells)
+    left = g.xc < d / 2
+    e[left] = er1 * eps0
+    e[~left] = er2 * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    C = PoissonSolver(g, e).capacitance_matrix(
+        [Terminal("lo", nid[0].ravel()), Terminal("hi", nid[-1].ravel())])
+    out["series_C"] = C
+    C1 = ref.parallel_plate_capacitance(Wd * H, d / 2, er1)
+    C2 = ref.parallel_plate_capacitance(Wd * H, d / 2, er2)
+    out["series_ref"] = C1 * C2 / (C1 + C2)
+    x = graded_1d(0, 2e-6, 30, 1.25)
+    g = RectilinearGrid(x, graded_1d(0, 5e-6, 9, 0.85), np.linspace(0, 4e-6, 7))
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    C = PoissonSolver(g, np.full(g.shape_cells, 3.9 * eps0)).capacitance_matrix(
+        [Terminal("lo", nid[0].ravel()), Terminal("hi", nid[-1].ravel())])
+    out["graded_C"] = C
+    out["graded_xn"], out["graded_yn"], out["graded_zn"] = g.xn, g.yn, g.zn
+    out["graded_ref"] = ref.parallel_plate_capacitance(20e-12, 2e-6, 3.9)
+    np.savez_compressed(HERE / "closed_forms.npz", **out)
+
+
+if __name__ == "__main__":
+    masses_fixture()
+    readme_fixture()
+    closed_forms()
+    layered_fixture((32, 32, 16), 0, 1e-12)
+    layered_fixture((48, 48, 24), 1, 1e-12)
+    eqs_fixture()
+    print("golden fixtures written to", HERE)

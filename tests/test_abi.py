@@ -1,0 +1,83 @@
+"""The C-ABI library loads and exports what ``include/*.h`` declares (CPU).
+
+No compute call is made here: only symbol lookup, status strings and the
+argument checks that return before any CUDA call.
+"""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from fieldspice_b200 import _lib as L
+from fieldspice_b200._build import LIB_PATH, build
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(fs_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def dll():
+    build()
+    return L.load_library()
+
+
+def test_every_declared_symbol_is_exported(dll):
+    names = declared_symbols()
+    assert len(names) >= 15
+    for n in sorted(names):
+        assert hasattr(dll, n), n
+    assert names == set(L.EXPORTED_SYMBOLS), names ^ set(L.EXPORTED_SYMBOLS)
+
+
+def test_status_strings(dll):
+    assert dll.fs_version().decode().startswith("fieldspice_b200")
+    assert dll.fs_status_string(L.FS_OK).decode() == "ok"
+    assert "converged" in dll.fs_status_string(L.FS_NOT_CONVERGED).decode()
+    assert dll.fs_status_string(99).decode() == "unknown status"
+
+
+def test_workspace_sizes_and_bad_arguments(dll):
+    nb = ctypes.c_size_t()
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_MIXED, ctypes.byref(nb)) == L.FS_OK
+    n = 32 * 32 * 16
+    # label + s64 + 3 FP32 masses + 4 FP32 vectors of 8 RHS
+    assert nb.value >= n * (1 + 8 + 12 + 4 * 8 * 4)
+    nb64 = ctypes.c_size_t()
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_FP64, ctypes.byref(nb64)) == L.FS_OK
+    assert nb64.value > nb.value
+    for k in (0, 3, 5, 17):
+        assert dll.fs_pcg_workspace_bytes(32, 32, 16, k, 1, ctypes.byref(nb)) == L.FS_BAD_ARG
+    assert dll.fs_pcg_workspace_bytes(1, 32, 16, 8, 1, ctypes.byref(nb)) == L.FS_BAD_ARG
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, 7, ctypes.byref(nb)) == L.FS_BAD_ARG
+    null = ctypes.c_void_p(0)
+    assert dll.fs_build_masses(*([null] * 7), 4, 4, 4, 0, null, null, null, null) == L.FS_BAD_ARG
+    plan = ctypes.c_void_p()
+    assert dll.fs_pcg_plan_create(8, 8, 8, 3, 1, *([null] * 7), 0, ctypes.byref(plan), null) == L.FS_BAD_ARG
+    assert dll.fs_pcg_plan_destroy(null) == L.FS_OK
+    assert dll.fs_group_apply_workspace_bytes(0, 8, ctypes.byref(nb)) == L.FS_BAD_ARG
+    assert dll.fs_quadform_workspace_bytes(17, ctypes.byref(nb)) == L.FS_BAD_ARG
+
+
+def test_library_is_sm100a_only():
+    # the build flags target sm_100a and nothing else
+    from fieldspice_b200 import _build
+    assert _build.ARCH_FLAGS == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert LIB_PATH.exists()
+
+
+def test_product_path_fails_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        L.lib()

@@ -1,0 +1,133 @@
+"""Pin the CPU oracle to the reference's recorded outputs (CPU only).
+
+The fixtures in ``tests/golden`` were produced by running the reference
+fieldspice package (``tests/golden/make_golden.py``).  The oracle restates
+the reference's algorithm; here it must reproduce every fixture: masses
+bit-for-bit, Laplacian applies to FP64 round-off, and the capacitance
+matrices and EQS currents to the tolerances the reference's own tests use.
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import fs_oracle as O
+
+GRIDS = ("graded", "uniform", "collapsed", "wide")
+
+
+def _grid(d, name):
+    return O.Grid(d[f"{name}_xn"], d[f"{name}_yn"], d[f"{name}_zn"])
+
+
+@pytest.mark.parametrize("name", GRIDS)
+def test_masses_bit_exact(golden, name):
+    d = golden("masses")
+    g = _grid(d, name)
+    prop = d[f"{name}_prop"]
+    pe = O.cell_to_edge(g, prop, "parallel")
+    assert np.array_equal(pe, d[f"{name}_eps_edge"])
+    assert np.array_equal(O.edge_mass_vector(g, pe), d[f"{name}_mass_parallel"])
+    ph = O.cell_to_edge(g, prop, "harmonic")
+    assert np.array_equal(O.edge_mass_vector(g, ph), d[f"{name}_mass_harmonic"])
+
+
+@pytest.mark.parametrize("name", GRIDS)
+def test_incidence_and_laplacian_match_reference(golden, name):
+    d = golden("masses")
+    g = _grid(d, name)
+    G = O.grad_node_edge(g)
+    assert np.array_equal(G.indptr, d[f"{name}_G_indptr"])
+    assert np.array_equal(G.indices, d[f"{name}_G_indices"])
+    assert np.array_equal(G.data, d[f"{name}_G_data"])
+    m = O.edge_mass_vector(g, O.cell_to_edge(g, d[f"{name}_prop"]))
+    L = O.nodal_laplacian(g, m)
+    Lref = sp.csr_matrix((d[f"{name}_L_data"], d[f"{name}_L_indices"],
+                          d[f"{name}_L_indptr"]), shape=L.shape)
+    assert abs(L - Lref).max() <= 1e-15 * abs(Lref).max()
+    y = L @ d[f"{name}_x"]
+    assert np.abs(y - d[f"{name}_Lx"]).max() <= 1e-14 * np.abs(d[f"{name}_Lx"]).max()
+
+
+@pytest.mark.parametrize("name", GRIDS)
+def test_topology_identities_exact(golden, name):
+    # tests/test_core.py:132-180 of the reference: C@G == 0 and D@C == 0
+    # exactly, entries are +-1.
+    g = _grid(golden("masses"), name)
+    G, C, D = O.grad_node_edge(g), O.curl_edge_face(g), O.div_face_cell(g)
+    CG, DC = C @ G, D @ C
+    assert CG.nnz == 0 or np.abs(CG.data).max() == 0.0
+    assert DC.nnz == 0 or np.abs(DC.data).max() == 0.0
+    for M in (G, C, D):
+        assert set(np.unique(M.data)).issubset({-1.0, 1.0})
+    assert np.abs(G @ np.ones(g.n_nodes)).max() == 0.0
+
+
+def test_readme_capacitor(golden):
+    from fieldspice_b200 import workloads as W
+    d = golden("readme")
+    w = W.parallel_plate()
+    g = O.Grid(w.x, w.y, w.z)
+    C, rep = O.capacitance_matrix(g, w.eps_cell, w.terminals, method="direct")
+    assert np.allclose(C, d["C"], rtol=1e-12, atol=0)
+    assert C[0, 0] == pytest.approx(w.meta["C_ref"], rel=1e-12)
+    # CG path too (Jacobi), at the README's 1e-12 requirement
+    C2, _ = O.capacitance_matrix(g, w.eps_cell, w.terminals, method="cg", tol=1e-13)
+    assert C2[0, 0] == pytest.approx(w.meta["C_ref"], rel=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["layered_32x32x16_s0", "layered_48x48x24_s1"])
+def test_layered_capacitance_matches_reference(golden, tag):
+    d = golden(tag)
+    g = O.Grid(d["x"], d["y"], d["z"])
+    nx, ny, nz = g.shape_nodes
+    nid = np.arange(g.n_nodes).reshape(nx, ny, nz)
+    terms = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    C, rep = O.capacitance_matrix(g, d["eps_cell"], terms, {"zlo": 0.0},
+                                  method="cg", tol=float(d["tol"]))
+    scale = np.abs(np.diag(d["C"])).max()
+    assert np.abs(C - d["C"]).max() / scale < 1e-11
+    assert np.abs(rep["shield_charge"] - d["shield"]).max() / scale < 1e-11
+
+
+def test_closed_forms(golden):
+    d = golden("closed_forms")
+    assert d["series_C"][0, 0] == pytest.approx(float(d["series_ref"]), rel=1e-10)
+    assert d["graded_C"][0, 0] == pytest.approx(float(d["graded_ref"]), rel=1e-10)
+    g = O.Grid(d["graded_xn"], d["graded_yn"], d["graded_zn"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    eps = np.full(g.shape_cells, 3.9 * O.EPS0)
+    C, _ = O.capacitance_matrix(g, eps, [nid[0].ravel(), nid[-1].ravel()], method="direct")
+    assert np.allclose(C, d["graded_C"], rtol=1e-12, atol=0)
+
+
+def test_eqs_interconnect_matches_reference(golden):
+    from fieldspice_b200 import workloads as W
+    d = golden("eqs")
+    g = O.Grid(d["ic_x"], d["ic_y"], d["ic_z"])
+    nx, ny, nz = g.shape_nodes
+    nid = np.arange(g.n_nodes).reshape(nx, ny, nz)
+    boxes = d["ic_boxes"]
+    ports = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in boxes[:2]]
+    ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
+    # terminals first, then the zlo wall: the wall wins on shared nodes
+    phis, cur = O.eqs_transient(g, d["ic_eps"], d["ic_sig"], ports,
+                                lambda t: (ramp(t), 0.0), 1e-12, 20, tol=1e-12,
+                                dirichlet_walls={"zlo": 0.0})
+    scale = np.abs(d["ic_i0"]).max()
+    assert np.abs(cur[:, 0] - d["ic_i0"]).max() / scale < 1e-8
+    assert np.abs(cur[:, 1] - d["ic_i1"]).max() / scale < 1e-8
+    assert np.abs(phis[-1] - d["ic_phi_last"]).max() < 1e-9
+
+
+def test_eqs_rc_stack_matches_reference(golden):
+    d = golden("eqs")
+    g = O.Grid(d["xn"], d["yn"], d["zn"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    tau = float(d["tau"])
+    phis, cur = O.eqs_transient(g, d["eps"], d["sig"], [nid[0].ravel(), nid[-1].ravel()],
+                                lambda t: (1.0, 0.0), tau / 50, 400, method="direct")
+    vm = np.array([p[nid[30, 1, 1]] for p in phis])
+    assert np.abs(vm - d["spt50_vm"]).max() < 1e-10
+    scale = np.abs(d["spt50_i_hi"]).max()
+    assert np.abs(cur[:, 0] - d["spt50_i_hi"]).max() / scale < 1e-8
