@@ -711,14 +711,16 @@ bool dispatch(fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
 
 // One CG iteration with event records between its kernels (captured into
 // the graph as event nodes).
+// A plain cudaEventRecord inside a capture only orders streams; the
+// External flag makes it an event-record node that executes with the graph.
 void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
-  cudaEventRecord(P->ev[0], s);
+  cudaEventRecordWithFlags(P->ev[0], s, cudaEventRecordExternal);
   dispatch(P, 5, s);  // K0
-  cudaEventRecord(P->ev[1], s);
+  cudaEventRecordWithFlags(P->ev[1], s, cudaEventRecordExternal);
   dispatch(P, 6, s);  // K1
-  cudaEventRecord(P->ev[2], s);
+  cudaEventRecordWithFlags(P->ev[2], s, cudaEventRecordExternal);
   dispatch(P, 7, s);  // K2
-  cudaEventRecord(P->ev[3], s);
+  cudaEventRecordWithFlags(P->ev[3], s, cudaEventRecordExternal);
   dispatch(P, 8, s);  // K3
 }
 
@@ -867,6 +869,8 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
         cudaEventElapsedTime(&ms[2], P->ev[2], P->ev[3]) == cudaSuccess) {
       for (int t = 0; t < 3; ++t) P->kernel_ms[t] += ms[t];
       P->kernel_samples += 1;
+    } else {
+      (void)cudaGetLastError();  // timing unavailable: not a solve failure
     }
     if (*P->h_flag) {
       timed_out = 0;

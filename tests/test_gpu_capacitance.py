@@ -137,7 +137,7 @@ def test_solve_potential_and_energy_match_reference(cuda, golden):
     assert np.abs(res.fields["phi"].ravel() - d["phi"]).max() < 1e-12
     assert res.scalars["energy"][0] == pytest.approx(float(d["energy"][0]), rel=1e-11)
     assert res.terminals["top"]["q"][0] == pytest.approx(float(d["q_top"][0]), rel=1e-11)
-    assert ps.energy(res.fields["phi"]) == pytest.approx(float(d["energy"][0]), rel=1e-11)
+    assert ps.energy(res.fields["phi"][0]) == pytest.approx(float(d["energy"][0]), rel=1e-11)
 
 
 def test_maxiter_raises_convergence_error(cuda):
