@@ -68,6 +68,8 @@ _SIGNATURES = {
     "fs_group_apply_workspace_bytes": (c_int, [c_int, c_int, POINTER(c_size_t)]),
     "fs_group_apply": (c_int, [c_void_p] * 10 + [c_int] * 5 + [c_void_p, c_void_p,
                                c_size_t, c_void_p]),
+    "fs_group_apply_noalloc": (c_int, [c_void_p] * 10 + [c_int] * 5 + [c_void_p,
+                                       c_void_p]),
     "fs_quadform_workspace_bytes": (c_int, [c_int, POINTER(c_size_t)]),
     "fs_quadform": (c_int, [c_void_p] * 4 + [c_int] * 4 + [c_void_p, c_void_p,
                             c_size_t, c_void_p]),

@@ -191,6 +191,7 @@ __device__ __forceinline__ void grid_total(const double* partials, int nblocks,
 
 // ---- host-side error bookkeeping --------------------------------------------
 void fs_set_error(const char* where, cudaError_t err);
+void fs_set_error_msg(const char* msg);
 int fs_cuda_status(const char* where, cudaError_t err);
 int fs_grid_blocks(const void* kernel, long long work_items);
 

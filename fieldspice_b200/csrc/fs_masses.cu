@@ -168,6 +168,10 @@ void fs_set_error(const char* where, cudaError_t err) {
            cudaGetErrorString(err), cudaGetErrorName(err));
 }
 
+void fs_set_error_msg(const char* msg) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
+
 int fs_cuda_status(const char* where, cudaError_t err) {
   fs_set_error(where, err);
   return FS_CUDA_ERROR;

@@ -1,5 +1,8 @@
 // Stand-alone FP64/FP32 stencil applies and the FP64 post-processing
 // reductions: terminal charge / current integration and edge energies.
+#include <mutex>
+#include <stdio.h>
+
 #include "fs_common.cuh"
 
 using fs::Dims;
@@ -176,6 +179,42 @@ __global__ void __launch_bounds__(fs::kBlock)
 constexpr int kGroupChunks = 32;
 constexpr int kQuadMaxBlocks = 4096;
 
+// ---- static scratch of fs_group_apply_noalloc ---------------------------------
+// One 256-byte slot for the completion ticket, then the per-block partial
+// sums: ngroups * kGroupChunks * nrhs doubles.  Every GPU that loads this
+// library holds one copy (512 KiB + 256 B) until the process exits.
+constexpr int kNoAllocMaxGroupRhs = 2048;  // limit on ngroups * nrhs
+constexpr size_t kNoAllocScratchBytes =
+    256 + (size_t)kNoAllocMaxGroupRhs * kGroupChunks * sizeof(double);
+static __device__ __align__(256) unsigned char
+    g_group_scratch[kNoAllocScratchBytes];
+
+// Host code may not pass `g_group_scratch` itself to a kernel: in host code
+// that name is a stand-in, not a device address.  The device address is
+// looked up once per device (with that device current) and cached.
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kMaxDevices] = {};
+
+int group_scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fs_cuda_status("cudaGetDevice", e);
+  if (dev < 0 || dev >= kMaxDevices) {
+    fs_set_error_msg("fs_group_apply_noalloc: device ordinal beyond 64");
+    return FS_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_group_scratch);
+    if (e != cudaSuccess) return fs_cuda_status("cudaGetSymbolAddress", e);
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return FS_OK;
+}
+
 size_t group_ws(int ngroups, int nrhs) {
   return 256 + (size_t)ngroups * kGroupChunks * nrhs * 8;
 }
@@ -292,6 +331,55 @@ int fs_quadform(const double* mx, const double* my, const double* mz,
     default: return FS_BAD_ARG;
   }
 #undef FS_QF
+}
+
+int fs_group_apply_noalloc(const double* mAx, const double* mAy,
+                           const double* mAz, const double* u,
+                           const double* mBx, const double* mBy,
+                           const double* mBz, const double* w,
+                           const long long* nodes, const long long* offsets,
+                           int ngroups, int nx, int ny, int nz, int nrhs,
+                           double* out, void* stream) {
+  if (!mAx || !mAy || !mAz || !u || !nodes || !offsets || !out ||
+      ngroups < 1 || nx < 2 || ny < 2 || nz < 2 || nrhs < 1)
+    return FS_BAD_ARG;
+  if (mBx && (!mBy || !mBz || !w)) return FS_BAD_ARG;
+  if ((long long)ngroups * nrhs > kNoAllocMaxGroupRhs) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "fs_group_apply_noalloc: ngroups*nrhs = %lld exceeds the static "
+             "scratch limit of %d",
+             (long long)ngroups * nrhs, kNoAllocMaxGroupRhs);
+    fs_set_error_msg(msg);
+    return FS_BAD_ARG;
+  }
+  void* scratch = nullptr;
+  int st = group_scratch_address(&scratch);
+  if (st != FS_OK) return st;
+  Dims d = fs::make_dims(nx, ny, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* ticket = (unsigned int*)scratch;
+  double* partials = (double*)((char*)scratch + 256);
+  // The array keeps whatever the previous call left; the ticket must start
+  // at zero (the partials are written before they are read).
+  FS_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  const int grid = ngroups * kGroupChunks;
+#define FS_GA(KK)                                                            \
+  case KK:                                                                   \
+    k_group_apply<KK><<<grid, fs::kBlock, 0, s>>>(                           \
+        d, mAx, mAy, mAz, u, mBx, mBy, mBz, w, nodes, offsets, ngroups,      \
+        kGroupChunks, partials, out, ticket);                                \
+    FS_CHECK_LAUNCH("k_group_apply");                                        \
+    return FS_OK;
+  switch (nrhs) {
+    FS_GA(1)
+    FS_GA(2)
+    FS_GA(4)
+    FS_GA(8)
+    FS_GA(16)
+    default: return FS_BAD_ARG;
+  }
+#undef FS_GA
 }
 
 }  // extern "C"

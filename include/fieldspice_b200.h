@@ -173,6 +173,30 @@ int fs_group_apply(const double* mAx, const double* mAy, const double* mAz,
                    int nz, int nrhs, double* out, void* workspace,
                    size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of fs_group_apply, for callers that cannot let a
+ * library allocate device memory: hosts that hand the library only their
+ * own input and output buffers from a pre-reserved pool (a Go or JVM
+ * application binding through cgo or JNI, a real-time time-stepping loop
+ * that must not stall on cudaMalloc), so there is no workspace argument.
+ * No counterpart in the reference (it allocates freely in NumPy); same
+ * arguments and result as fs_group_apply minus the workspace.
+ * Scratch is a static device array inside the library: 512 KiB + 256 B per
+ * GPU that loads the library, held until the process exits, so
+ * ngroups * nrhs must not exceed 2048 (larger sizes return FS_BAD_ARG with
+ * the reason in fs_last_error()).  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  Every call
+ * shares the one array and it keeps the previous call's contents: calls
+ * that overlap on the GPU (two streams, two host threads) race on it and
+ * must be serialised by the caller.  Never allocates or frees memory.     */
+int fs_group_apply_noalloc(const double* mAx, const double* mAy,
+                           const double* mAz, const double* u,
+                           const double* mBx, const double* mBy,
+                           const double* mBz, const double* w,
+                           const long long* nodes, const long long* offsets,
+                           int ngroups, int nx, int ny, int nz, int nrhs,
+                           double* out, void* stream);
+
 /* out[r] = sum over edges of m_e (u_head - u_tail)^2 = u^T L u per RHS: the
  * stored energy 2*W of poisson.py:905-913 and eqs.py:342-348.               */
 int fs_quadform_workspace_bytes(int nrhs, size_t* bytes);
