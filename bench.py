@@ -53,11 +53,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
     ap.add_argument("--shape", default=",".join(map(str, SHAPE)))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    ap.add_argument("--single", action="store_true",
+                    help="one device-resident extraction only (profiler runs)")
     return ap.parse_args()
 
 
@@ -142,7 +144,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def kernel_bytes(N: int, k: int, s: int) -> dict:
     """Algorithmic bytes per launch of the CG kernels (each array once)."""
-    return {"pupdate": 3 * N * k * s,                 # read r, p; write p
+    return {"pupdate": 3 * N * k * s,                 # read r, p_old; write p
             "stencil": N * (2 * k * s + 3 * s),       # read p, 3 masses; write q
             "update": 6 * N * k * s}                  # read p, q, x, r; write x, r
 
@@ -215,6 +217,16 @@ def run_ours(args, rank, world, local_rank):
             ms = float(t.item())
         return ms, outs
 
+    if args.single:
+        for _ in range(args.warmup + args.steps):
+            C, qs, info = step_device(args.precision)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"single": True, "shape": shape, "iterations": info["iterations"],
+                              "kernel_ms": info["kernel_ms"],
+                              "gpu_launches": info["gpu_launches"]}), flush=True)
+        return
+
     sampler = ClockSampler(local_rank)
     sampler.start()
     ms_dev, outs = timed(lambda: step_device(args.precision), args.steps, args.warmup)
@@ -233,7 +245,7 @@ def run_ours(args, rank, world, local_rank):
 
     variants = {}
     if not args.no_variants:
-        other = "fp64" if args.precision == "mixed" else "mixed"
+        other = "fp64" if args.precision != "fp64" else "mixed"
         ms_o, outs_o = timed(lambda: step_device(other), max(2, args.steps // 2), 1)
         Co = outs_o[-1][0]
         variants[other] = {
@@ -245,10 +257,11 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     N = int(np.prod(shape))
-    s = 4 if args.precision == "mixed" else 8
+    s = 8 if (args.precision == "fp64" or info.get("fp64_fallback")) else 4
     kb = kernel_bytes(N, 8, s)
     km = info["kernel_ms"]
-    times = {"pupdate": km["pupdate_ms"], "stencil": km["stencil_ms"], "update": km["update_ms"]}
+    times = {"pupdate": km["pupdate_ms"], "stencil": km["stencil_ms"],
+             "update": km["update_ms"]}
     dom = max(times, key=times.get)
     peak, peak_kind = measured_peaks()
     gbs = {k: kb[k] / (times[k] * 1e-3) / 1e9 for k in times if times[k] > 0}
@@ -271,12 +284,13 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "dtype": "f64" if s == 8 else "f32+f64",
         "data": "synthetic (seeded layered dielectric + 8 conductor boxes per rank)",
         "config": {
             "workload": f"layered_boxes {shape[0]}x{shape[1]}x{shape[2]} nodes, "
                         f"{NBOX} terminals, zlo grounded, seed=rank",
             "nodes": N, "nrhs": NBOX, "tol": TOL, "precision": args.precision,
+            "fp64_fallback": info.get("fp64_fallback"),
             "preconditioner": "jacobi (equilibrated CG)",
             "l2": "inputs larger than L2: every CG vector is N*8*4 B = 268 MB",
             "parallelism": f"dp{world} (independent geometries)",

@@ -16,15 +16,16 @@ from ._build import LIB_PATH
 
 __all__ = ["lib", "FsRhsStats", "check", "FsError", "stream_ptr", "ptr",
            "FS_OK", "FS_NOT_CONVERGED", "FS_TIMEOUT", "FS_BAD_ARG", "FS_NAN",
-           "FS_CUDA_ERROR", "LABEL_FREE", "LABEL_FIXED", "LABEL_SOLO",
+           "FS_CUDA_ERROR", "FS_STALLED", "LABEL_FREE", "LABEL_FIXED", "LABEL_SOLO",
            "LABEL_PINNED", "DTYPE_F64", "DTYPE_F32", "PRECISION_FP64",
-           "PRECISION_MIXED", "AVERAGE_PARALLEL", "AVERAGE_HARMONIC",
+           "PRECISION_MIXED", "PRECOND_JACOBI", "PRECOND_MG", "AVERAGE_PARALLEL", "AVERAGE_HARMONIC",
            "EXPORTED_SYMBOLS", "load_library"]
 
-FS_OK, FS_NOT_CONVERGED, FS_TIMEOUT, FS_BAD_ARG, FS_NAN, FS_CUDA_ERROR = range(6)
+FS_OK, FS_NOT_CONVERGED, FS_TIMEOUT, FS_BAD_ARG, FS_NAN, FS_CUDA_ERROR, FS_STALLED = range(7)
 LABEL_FREE, LABEL_FIXED, LABEL_SOLO, LABEL_PINNED = range(4)
 DTYPE_F64, DTYPE_F32 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECOND_JACOBI, PRECOND_MG = 0, 1
 AVERAGE_PARALLEL, AVERAGE_HARMONIC = 0, 1
 
 
@@ -55,8 +56,8 @@ _SIGNATURES = {
     "fs_stencil_apply": (c_int, [c_void_p] * 6 + [c_int] * 5 + [c_void_p]),
     "fs_fill_unit_excitation": (c_int, [c_void_p] * 3 + [c_int] * 4 + [c_void_p]),
     "fs_set_dirichlet": (c_int, [c_void_p] * 4 + [c_int] * 3 + [c_void_p]),
-    "fs_pcg_workspace_bytes": (c_int, [c_int] * 5 + [POINTER(c_size_t)]),
-    "fs_pcg_plan_create": (c_int, [c_int] * 5 + [c_void_p] * 7 + [c_size_t,
+    "fs_pcg_workspace_bytes": (c_int, [c_int] * 6 + [POINTER(c_size_t)]),
+    "fs_pcg_plan_create": (c_int, [c_int] * 6 + [c_void_p] * 7 + [c_size_t,
                                    POINTER(c_void_p), c_void_p]),
     "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
                                   POINTER(FsRhsStats), c_void_p]),

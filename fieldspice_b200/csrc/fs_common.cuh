@@ -128,10 +128,11 @@ __device__ __forceinline__ void stv(T* __restrict__ base, long long n,
 // (warp shuffle tree, then warps in index order) and writes one partial per
 // value.  The last block to finish (atomic ticket) sums the partials over
 // blocks, again in a fixed order, so results do not depend on scheduling.
-template <int M>
+template <int M, int NT = kBlock>
 __device__ __forceinline__ void block_partials(double (&acc)[M],
                                                double* __restrict__ partials) {
-  __shared__ double sm[kBlock / 32][M];
+  static_assert(NT % 32 == 0 && NT >= 32, "block size must be whole warps");
+  __shared__ double sm[NT / 32][M];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int m = 0; m < M; ++m) {
@@ -145,7 +146,7 @@ __device__ __forceinline__ void block_partials(double (&acc)[M],
   if (threadIdx.x < M) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < kBlock / 32; ++w) s += sm[w][threadIdx.x];
+    for (int w = 0; w < NT / 32; ++w) s += sm[w][threadIdx.x];
     partials[(size_t)blockIdx.x * M + threadIdx.x] = s;
   }
 }
@@ -166,19 +167,20 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
   return is_last;
 }
 
-// Sum partials[b*M + m] over b in a fixed order; call from the last block.
-// Result is valid in out[m] for all threads after the call.
-template <int M>
+// Sum partials[b*M + m] over b in a fixed order; call from the last block
+// (NT threads).  Result is valid in out[m] for all threads after the call.
+template <int M, int NT = kBlock>
 __device__ __forceinline__ void grid_total(const double* partials, int nblocks,
                                            double (&out)[M]) {
-  __shared__ double red[kBlock];
+  static_assert((NT & (NT - 1)) == 0, "block size must be a power of two");
+  __shared__ double red[NT];
   for (int m = 0; m < M; ++m) {
     double s = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += kBlock)
+    for (int b = threadIdx.x; b < nblocks; b += NT)
       s += __ldcg(partials + (size_t)b * M + m);
     red[threadIdx.x] = s;
     __syncthreads();
-    for (int w = kBlock / 2; w > 0; w >>= 1) {
+    for (int w = NT / 2; w > 0; w >>= 1) {
       if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
       __syncthreads();
     }

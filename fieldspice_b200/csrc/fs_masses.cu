@@ -209,6 +209,7 @@ const char* fs_status_string(int status) {
     case FS_BAD_ARG: return "bad argument";
     case FS_NAN: return "residual became NaN or Inf";
     case FS_CUDA_ERROR: return "CUDA error";
+    case FS_STALLED: return "mixed-precision iterations stalled";
     default: return "unknown status";
   }
 }

@@ -1,0 +1,288 @@
+// Geometric multigrid V-cycle for the equilibrated, Dirichlet-eliminated
+// system  A~ = S A S  (S = diag(A)^-1/2 on free nodes, 0 on fixed nodes).
+//
+// Levels.  Vertex-centred coarsening: coarse node I sits on fine node 2I, so
+// n_c = (n + 1) / 2 per axis.  The coarse operator is a rediscretisation of
+// the original Laplacian A: a coarse x-edge joins fine nodes 2I -> 2I+2, i.e.
+// two fine x-edges in series, and collects the 3 x 3 fine edge rows around
+// it with lateral weights (1/2, 1, 1/2) per direction, which reproduces the
+// coarse edge mass 2m of a uniform medium (twice the dual area over twice
+// the length) and the half dual areas at the walls.  A coarse node is fixed
+// when its fine node is.  Every level is then equilibrated the same way, so
+// every level's operator has unit diagonal and one stencil form
+//     (A~ u)_i = u_i - sum_e m~_e u_nbr(e).
+//
+// Transfers.  With trilinear P (weights 1, 1/2, 1/2 per axis; a last fine
+// node with no coarse partner takes weight 1 from its lower neighbour), the
+// equilibrated prolongation is P~ = S_f^-1 P S_c and restriction R~ = P~^T,
+// so that P~^T A~_f P~ = S_c (P^T A_f P) S_c ~ A~_c.  S^-1 is stored as
+// `sd` (sqrt(diag), 0 on fixed nodes) and S as `s`.
+//
+// Smoothing.  Chebyshev polynomials of A~ on [lo, 2]: 2 bounds the spectrum
+// of A~ (it is similar to D^-1 A, whose Gershgorin discs lie in [0, 2]).
+// Pre- and post-smoothing use the same polynomial and the coarsest level a
+// fixed higher-degree one, so the V-cycle is a symmetric linear operator and
+// plain PCG applies.
+#pragma once
+
+#include "fs_common.cuh"
+
+namespace fs {
+
+// ---- setup (FP64, original scale) ---------------------------------------------
+__device__ __forceinline__ double series2(double a, double b) {
+  return (a > 0.0 && b > 0.0) ? 1.0 / (1.0 / a + 1.0 / b) : 0.0;
+}
+
+// Coarse masses (padded node layout) and coarse "fixed" labels.
+__global__ void k_mg_coarsen(Dims f, Dims c, const double* __restrict__ fmx,
+                             const double* __restrict__ fmy,
+                             const double* __restrict__ fmz,
+                             const uint8_t* __restrict__ flabel,
+                             double* __restrict__ cmx, double* __restrict__ cmy,
+                             double* __restrict__ cmz,
+                             uint8_t* __restrict__ clabel) {
+  const double lat[3] = {0.5, 1.0, 0.5};
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int I, J, Kc;
+    node_ijk(c, n, I, J, Kc);
+    const int i = 2 * I, j = 2 * J, k = 2 * Kc;
+    const long long fn = ((long long)i * f.ny + j) * f.nz + k;
+    clabel[n] = flabel[fn] == FS_LABEL_FREE ? FS_LABEL_FREE : FS_LABEL_FIXED;
+    // x-edge I -> I+1: fine x-edges i -> i+1 -> i+2 in series, lateral j, k
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    if (I + 1 < c.nx) {
+      for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b) {
+          const int jj = j + a, kk = k + b;
+          if (jj < 0 || jj >= f.ny || kk < 0 || kk >= f.nz) continue;
+          const long long m0 = ((long long)i * f.ny + jj) * f.nz + kk;
+          sx += lat[a + 1] * lat[b + 1] * series2(fmx[m0], fmx[m0 + f.sx]);
+        }
+    }
+    if (J + 1 < c.ny) {
+      for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b) {
+          const int ii = i + a, kk = k + b;
+          if (ii < 0 || ii >= f.nx || kk < 0 || kk >= f.nz) continue;
+          const long long m0 = ((long long)ii * f.ny + j) * f.nz + kk;
+          sy += lat[a + 1] * lat[b + 1] * series2(fmy[m0], fmy[m0 + f.sy]);
+        }
+    }
+    if (Kc + 1 < c.nz) {
+      for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b) {
+          const int ii = i + a, jj = j + b;
+          if (ii < 0 || ii >= f.nx || jj < 0 || jj >= f.ny) continue;
+          const long long m0 = ((long long)ii * f.ny + jj) * f.nz + k;
+          sz += lat[a + 1] * lat[b + 1] * series2(fmz[m0], fmz[m0 + 1]);
+        }
+    }
+    cmx[n] = sx;
+    cmy[n] = sy;
+    cmz[n] = sz;
+  }
+}
+
+// s = diag^-1/2 and sd = diag^1/2 in T (both 0 on non-free nodes).
+template <typename T>
+__global__ void k_mg_scales(long long N, const double* __restrict__ s64,
+                            T* __restrict__ s, T* __restrict__ sd) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const double v = s64[n];
+    s[n] = (T)v;
+    sd[n] = (T)(v > 0.0 ? 1.0 / v : 0.0);
+  }
+}
+
+// ---- V-cycle kernels (T, K RHS interleaved) ---------------------------------------
+template <typename T, int K>
+__device__ __forceinline__ void apply_eq(const Dims& d, const T* __restrict__ ex,
+                                         const T* __restrict__ ey,
+                                         const T* __restrict__ ez,
+                                         const T* __restrict__ x, long long n,
+                                         T (&ax)[K]) {
+  int i, j, k;
+  node_ijk(d, n, i, j, k);
+  ldv_ro<T, K>(x, n, ax);
+  auto nbr = [&](T m, long long nb) {
+    T v[K];
+    ldv_ro<T, K>(x, nb, v);
+#pragma unroll
+    for (int t = 0; t < K; ++t) ax[t] -= m * v[t];
+  };
+  if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
+  if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
+  if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
+  if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
+  if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
+  if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+}
+
+// One Chebyshev step: d = cd*d + cr*(b - A~ x_in), x_out = x_in + d.
+// x_zero: x_in is identically zero (first pre-smoothing step).
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_cheb(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+              const T* __restrict__ ez, const T* __restrict__ xin,
+              T* __restrict__ xout, T* __restrict__ dv,
+              const T* __restrict__ b, T cd, T cr, int x_zero,
+              const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T r[K], bv[K], dd[K], xo[K];
+    ldv_ro<T, K>(b, n, bv);
+    if (x_zero) {
+#pragma unroll
+      for (int t = 0; t < K; ++t) {
+        r[t] = bv[t];
+        xo[t] = (T)0;
+      }
+    } else {
+      T ax[K];
+      apply_eq<T, K>(d, ex, ey, ez, xin, n, ax);
+      ldv_ro<T, K>(xin, n, xo);
+#pragma unroll
+      for (int t = 0; t < K; ++t) r[t] = bv[t] - ax[t];
+    }
+    if (cd != (T)0) {
+      ldv<T, K>(dv, n, dd);
+#pragma unroll
+      for (int t = 0; t < K; ++t) dd[t] = cd * dd[t] + cr * r[t];
+    } else {
+#pragma unroll
+      for (int t = 0; t < K; ++t) dd[t] = cr * r[t];
+    }
+#pragma unroll
+    for (int t = 0; t < K; ++t) xo[t] += dd[t];
+    stv<T, K>(dv, n, dd);
+    stv<T, K>(xout, n, xo);
+  }
+}
+
+// res = b - A~ x
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_residual(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+                  const T* __restrict__ ez, const T* __restrict__ x,
+                  const T* __restrict__ b, T* __restrict__ res,
+                  const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T ax[K], bv[K];
+    apply_eq<T, K>(d, ex, ey, ez, x, n, ax);
+    ldv_ro<T, K>(b, n, bv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) bv[t] -= ax[t];
+    stv<T, K>(res, n, bv);
+  }
+}
+
+// Per-axis trilinear weights of fine index i onto coarse index I (0 if none).
+__device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
+  const int dlt = i - 2 * I;
+  if (dlt == 0) return 1.0f;
+  if (dlt == 1) return (I + 1 < nc) ? 0.5f : 1.0f;  // last fine node: weight 1
+  if (dlt == -1) return 0.5f;
+  return 0.0f;
+}
+
+// b_c(I) = s_c(I) * sum_f P(f,I) sd(f) res(f)   (coarse-centric gather)
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_restrict(Dims f, Dims c, const T* __restrict__ res,
+                  const T* __restrict__ sdf, const T* __restrict__ sc,
+                  T* __restrict__ bc, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const T scale = sc[n];
+    T acc[K];
+#pragma unroll
+    for (int t = 0; t < K; ++t) acc[t] = (T)0;
+    if (scale != (T)0) {
+      int I, J, Kc;
+      node_ijk(c, n, I, J, Kc);
+      for (int a = -1; a <= 1; ++a) {
+        const int i = 2 * I + a;
+        if (i < 0 || i >= f.nx) continue;
+        const float wa = pw(i, I, f.nx, c.nx);
+        for (int b = -1; b <= 1; ++b) {
+          const int j = 2 * J + b;
+          if (j < 0 || j >= f.ny) continue;
+          const float wb = wa * pw(j, J, f.ny, c.ny);
+          for (int e = -1; e <= 1; ++e) {
+            const int k = 2 * Kc + e;
+            if (k < 0 || k >= f.nz) continue;
+            const long long fn = ((long long)i * f.ny + j) * f.nz + k;
+            const T w = (T)(wb * pw(k, Kc, f.nz, c.nz)) * __ldg(sdf + fn);
+            if (w == (T)0) continue;
+            T v[K];
+            ldv_ro<T, K>(res, fn, v);
+#pragma unroll
+            for (int t = 0; t < K; ++t) acc[t] += w * v[t];
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < K; ++t) acc[t] *= scale;
+    }
+    stv<T, K>(bc, n, acc);
+  }
+}
+
+// x_f += sd(f) * sum_I P(f,I) s_c(I) x_c(I)   (fine-centric, in place)
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_prolong(Dims f, Dims c, const T* __restrict__ xc,
+                 const T* __restrict__ sc, const T* __restrict__ sdf,
+                 T* __restrict__ xf, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < f.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const T scale = sdf[n];
+    if (scale == (T)0) continue;
+    int i, j, k;
+    node_ijk(f, n, i, j, k);
+    int ci[2], cj[2], ck[2];
+    float wi[2], wj[2], wk[2];
+    int ni, nj, nk;
+    auto axis = [](int x, int nc, int (&cx)[2], float (&wx)[2], int& cnt) {
+      if ((x & 1) == 0) {
+        cx[0] = x >> 1; wx[0] = 1.0f; cnt = 1;
+      } else if (((x + 1) >> 1) < nc) {
+        cx[0] = x >> 1; cx[1] = (x + 1) >> 1; wx[0] = wx[1] = 0.5f; cnt = 2;
+      } else {
+        cx[0] = x >> 1; wx[0] = 1.0f; cnt = 1;
+      }
+    };
+    axis(i, c.nx, ci, wi, ni);
+    axis(j, c.ny, cj, wj, nj);
+    axis(k, c.nz, ck, wk, nk);
+    T acc[K];
+#pragma unroll
+    for (int t = 0; t < K; ++t) acc[t] = (T)0;
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b)
+        for (int e = 0; e < nk; ++e) {
+          const long long cn = ((long long)ci[a] * c.ny + cj[b]) * c.nz + ck[e];
+          const T w = (T)(wi[a] * wj[b] * wk[e]) * __ldg(sc + cn);
+          if (w == (T)0) continue;
+          T v[K];
+          ldv_ro<T, K>(xc, cn, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) acc[t] += w * v[t];
+        }
+    T xv[K];
+    ldv<T, K>(xf, n, xv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) xv[t] += scale * acc[t];
+    stv<T, K>(xf, n, xv);
+  }
+}
+
+}  // namespace fs

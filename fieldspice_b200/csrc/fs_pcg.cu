@@ -22,9 +22,10 @@
 // whenever it has dropped by `delta` since the previous update.
 //
 // Each CG iteration is four kernels captured once in a CUDA graph:
-//   K0 p = r + beta p  (and, after a reliable update, phi += s x~, x~ = 0)
-//   K1 q = A~ p, partial p.q -> alpha           (stencil, FP64 dot)
-//   K2 x~ += alpha p, r -= alpha q, r.r -> beta (FP64 dot)
+//   K0 p = r + beta p_old                          (streaming, p double-buffered)
+//   K1 q = A~ p, p.q -> alpha                      (TMA-staged stencil, FP64 dot)
+//   K2 (phi += s x~, x~ = 0 after a reliable update) x~ += alpha p,
+//      r -= alpha q, r.r -> beta                    (FP64 dot)
 //   K3 reliable update when flagged (FP64 true residual)
 // Scalars live on the device; the host only polls an "all done" flag between
 // graph launches.  Reductions are deterministic (fixed-order block partials,
@@ -35,13 +36,18 @@
 #include <new>
 
 #include "fs_common.cuh"
+#include "fs_tma.cuh"
+#include "fs_mg.cuh"
+
+#include <cudaTypedefs.h>
 
 using fs::Dims;
 
 namespace {
 
 struct RhsState {
-  double gamma;      // r~.r~ of the current residual
+  double rr;         // r~.r~ of the current residual (convergence test)
+  double gamma;      // r~.z of the current residual (= rr without precond)
   double gamma_old;  // previous gamma
   double pq;
   double alpha, beta;
@@ -55,11 +61,17 @@ struct RhsState {
   int zero;          // b == 0: the solution on free nodes is 0 (SciPy)
   int status;
   int nru;
-  int pad;
+  int nstall;        // reliable updates since the true residual last halved
+  int fresh;         // preconditioned: next r.z starts the recurrence (beta 0)
+  int pad1;
+  double best;       // best true residual norm so far
 };
 
-enum { kTicketP = 0, kTicketApply, kTicketUpdate, kTicketRel, kTicketInit,
-       kTicketFin, kTickets };
+constexpr int kStallUpdates = 6;
+constexpr int kRefreshEvery = 64;
+
+enum { kTicketApply = 0, kTicketUpdate, kTicketRel, kTicketInit,
+       kTicketFin, kTicketRz, kTickets };
 
 struct Control {
   double tol;
@@ -68,6 +80,8 @@ struct Control {
   int all_done;
   int any_ru;
   int any_fold;
+  int error;    // a bounded wait expired (TMA stage never landed)
+  int precond;  // 0: CG on A~ (Jacobi), 1: multigrid-preconditioned CG
   unsigned int tickets[kTickets];
   unsigned int pad[2];
 };
@@ -148,7 +162,8 @@ __global__ void __launch_bounds__(fs::kBlock)
            const double* __restrict__ s64, double* __restrict__ phi,
            const double* __restrict__ f, int warm, T* __restrict__ x,
            T* __restrict__ r, T* __restrict__ p, double* __restrict__ partials,
-           RhsState* st, Control* ctl, double tol, int maxiter, double delta) {
+           RhsState* st, Control* ctl, double tol, int maxiter, double delta,
+           int precond) {
   double acc[2 * K];
 #pragma unroll
   for (int t = 0; t < 2 * K; ++t) acc[t] = 0.0;
@@ -222,13 +237,17 @@ __global__ void __launch_bounds__(fs::kBlock)
       RhsState& s = st[threadIdx.x];
       const double g = tot[threadIdx.x];
       const double bn = sqrt(tot[K + threadIdx.x]);
+      s.rr = g;
       s.gamma = g;
       s.gamma_old = g;
+      s.fresh = 1;
       s.pq = 0.0;
       s.alpha = 0.0;
       s.beta = 0.0;
       s.bnorm = bn;
       s.rmax = sqrt(g);
+      s.best = sqrt(g);
+      s.nstall = 0;
       s.iters = 0;
       s.ru = 0;
       s.fold = 0;
@@ -251,67 +270,284 @@ __global__ void __launch_bounds__(fs::kBlock)
       ctl->tol = tol;
       ctl->maxiter = maxiter;
       ctl->delta = delta;
+      ctl->precond = precond;
+      ctl->error = 0;
       ctl->any_fold = 0;
       refresh_done(st, ctl, K);
     }
   }
 }
 
-// ---- K0: fold pending corrections, p = r + beta p -----------------------------
+// ---- K1: q = A~ p and p.q (TMA-staged, 2.5-D tiled, persistent) --------------
+// The (z, y) plane is cut into TZ x TY tiles ("columns" along x).  The
+// column-planes are dealt out evenly to a persistent grid: each block gets
+// one contiguous run of x-planes, which spans at most a few columns.  Along
+// a run one thread issues a TMA tensor load per x-plane of the p tile plus
+// a one-node halo in y and z into an NS-deep ring of shared-memory stages
+// (mbarrier completion, two planes in flight); out-of-range halo nodes
+// arrive as zeros, which is the boundary of the eliminated operator.  The
+// stencil of plane x reads planes x-1, x, x+1 from the ring.
+constexpr long long kWaitBudget = 2000000000LL;  // ~1 s of SM clocks
+
 template <typename T, int K>
-__global__ void __launch_bounds__(fs::kBlock)
-    k_pupdate(Dims d, const double* __restrict__ s64, double* __restrict__ phi,
-              T* __restrict__ x, const T* __restrict__ r, T* __restrict__ p,
-              RhsState* st, Control* ctl) {
-  __shared__ T beta[K];
-  __shared__ int fold[K], act[K];
-  __shared__ int any_fold, done;
-  if (threadIdx.x == 0) {
-    any_fold = ctl->any_fold;
-    done = ctl->all_done;
-  }
-  if (threadIdx.x < K) {
-    beta[threadIdx.x] = (T)st[threadIdx.x].beta;
-    fold[threadIdx.x] = st[threadIdx.x].fold;
-    act[threadIdx.x] = st[threadIdx.x].active;
-  }
-  __syncthreads();
-  if (done && !any_fold) return;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
-       n += (long long)gridDim.x * blockDim.x) {
-    if (any_fold) {
-      const double s = s64[n];
-      if (s != 0.0) {
-        T xv[K];
-        fs::ldv<T, K>(x, n, xv);
-        bool touched = false;
+struct TmaTile {
+  static constexpr int B = K * (int)sizeof(T);       // bytes per node
+  static constexpr int TZ = 32;
+  static constexpr int TY = B <= 32 ? 16 : (B <= 64 ? 8 : 4);
+  static constexpr int NS = 5;                       // ring of x-planes
+  static constexpr int HY = TY + 2, HZ = TZ + 2;
+  static constexpr int BOX = HY * HZ * B;            // bytes of one plane
+  static constexpr int BOXP = (BOX + 127) / 128 * 128;
+  static constexpr int THREADS = TZ * TY;
+  static constexpr size_t SMEM = (size_t)NS * BOXP + NS * 8 + 128;
+  static constexpr bool OK = B >= 16;                // TMA row >= 16 B
+};
+
+template <typename T, int K>
+__device__ __forceinline__ void ld_smem(const T* p, T (&v)[K]) {
+  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
 #pragma unroll
-        for (int t = 0; t < K; ++t)
-          if (fold[t]) {
-            phi[n * K + t] += (double)xv[t] * s;
-            xv[t] = (T)0;
-            touched = true;
-          }
-        if (touched) fs::stv<T, K>(x, n, xv);
-      }
+    for (int c = 0; c < K / 4; ++c) {
+      float4 t = reinterpret_cast<const float4*>(p)[c];
+      v[4 * c] = t.x; v[4 * c + 1] = t.y; v[4 * c + 2] = t.z; v[4 * c + 3] = t.w;
     }
-    if (!done) {
-      T rv[K], pv[K];
-      fs::ldv<T, K>(r, n, rv);
-      fs::ldv<T, K>(p, n, pv);
+  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
 #pragma unroll
-      for (int t = 0; t < K; ++t)
-        if (act[t]) pv[t] = rv[t] + beta[t] * pv[t];
-      fs::stv<T, K>(p, n, pv);
+    for (int c = 0; c < K / 2; ++c) {
+      double2 t = reinterpret_cast<const double2*>(p)[c];
+      v[2 * c] = t.x; v[2 * c + 1] = t.y;
     }
-  }
-  if (any_fold && fs::last_block(&ctl->tickets[kTicketP])) {
-    if (threadIdx.x < K) st[threadIdx.x].fold = 0;
-    if (threadIdx.x == 0) ctl->any_fold = 0;
+  } else {
+#pragma unroll
+    for (int c = 0; c < K; ++c) v[c] = p[c];
   }
 }
 
-// ---- K1: q = A~ p and p.q -------------------------------------------------------
+template <typename T, int K, int NT>
+__device__ void finish_pq(double (&acc)[K], double* partials, RhsState* st,
+                          Control* ctl) {
+  fs::block_partials<K, NT>(acc, partials);
+  if (fs::last_block(&ctl->tickets[kTicketApply])) {
+    double tot[K];
+    fs::grid_total<K, NT>(partials, gridDim.x, tot);
+    if (threadIdx.x < K) {
+      RhsState& s = st[threadIdx.x];
+      s.pq = tot[threadIdx.x];
+      if (ctl->error) {
+        s.alpha = 0.0;
+        if (s.active) s.status = FS_TIMEOUT;
+        s.active = 0;
+      } else if (s.active) {
+        if (tot[threadIdx.x] > 0.0 && isfinite(tot[threadIdx.x])) {
+          s.alpha = s.gamma / tot[threadIdx.x];
+        } else {
+          s.alpha = 0.0;  // A~ is SPD: p.q <= 0 only through NaN/Inf
+          s.active = 0;
+          s.status = FS_NAN;
+        }
+      } else {
+        s.alpha = 0.0;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) refresh_done(st, ctl, K);
+  }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
+    k_stencil_tma(Dims d, const __grid_constant__ CUtensorMap tm_p,
+                  const T* __restrict__ ex, const T* __restrict__ ey,
+                  const T* __restrict__ ez, const T* __restrict__ p,
+                  T* __restrict__ q, double* __restrict__ partials,
+                  RhsState* st, Control* ctl) {
+  using C = TmaTile<T, K>;
+  if (ctl->all_done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base =
+      (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  T* ring = reinterpret_cast<T*>(base);                    // [NS][BOXP]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::NS * C::BOXP);
+  constexpr int BOXT = C::BOXP / (int)sizeof(T);
+
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const long long total = (long long)nbz * nby * d.nx;   // column-planes
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  long long u = (long long)blockIdx.x * per;
+  const long long u_end = min(u + per, total);
+
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  long long ticket = 0;  // planes issued so far by this block (ring position)
+  bool failed = false;
+
+  while (u < u_end && !failed) {
+    const long long col = u / d.nx;
+    const int xa = (int)(u % d.nx);
+    const int xb = (int)min((long long)d.nx, xa + (u_end - u));
+    const int bz = (int)(col % nbz), by = (int)(col / nbz);
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nplanes = (xb - xa) + 2;   // planes xa-1 .. xb
+    auto issue = [&](int j) {
+      const int s = (int)((ticket + j) % C::NS);
+      fs::mbar_arrive_expect_tx(&bar[s], C::BOX);
+      fs::tma_load_4d(ring + s * BOXT, &tm_p, &bar[s], 0, z0 - 1, y0 - 1,
+                      xa - 1 + j);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
+    for (int j = 0; j < nplanes; ++j) {
+      const long long tk = ticket + j;
+      const int s = (int)(tk % C::NS);
+      const bool ok = fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1),
+                                            kWaitBudget);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      if (j >= 2) {
+        if (inb) {
+          const int x = xa - 2 + j;
+          const long long n = ((long long)x * d.ny + y) * d.nz + z;
+          const T* pm = ring + (int)((tk - 2) % C::NS) * BOXT;
+          const T* pc = ring + (int)((tk - 1) % C::NS) * BOXT;
+          const T* pp = ring + s * BOXT;
+          const T mxm = x > 0 ? __ldg(ex + n - d.sx) : (T)0;
+          const T mxp = __ldg(ex + n);  // 0 on the last plane (padded)
+          const T mym = y > 0 ? __ldg(ey + n - d.sy) : (T)0;
+          const T myp = __ldg(ey + n);
+          const T mzm = z > 0 ? __ldg(ez + n - 1) : (T)0;
+          const T mzp = __ldg(ez + n);
+          T c[K], v[K], qv[K];
+          ld_smem<T, K>(pc + cpos * K, c);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] = c[t];
+          ld_smem<T, K>(pm + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
+          ld_smem<T, K>(pp + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
+          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
+          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            qv[t] -= mzp * v[t];
+            acc[t] += (double)c[t] * (double)qv[t];
+          }
+          fs::stv<T, K>(q, n, qv);
+        }
+        __syncthreads();  // plane j-2 no longer read: its stage may refill
+        if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
+      }
+    }
+    ticket += nplanes;
+    u += (xb - xa);
+  }
+  if (failed) {
+    // A staged load did not land in time.  Give copies still in flight a
+    // bounded chance to finish before the block exits, then report.
+    if (tid == 0) {
+      ctl->error = 1;
+      for (int s = 0; s < C::NS; ++s)
+        (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+  (void)p;
+  finish_pq<T, K, TmaTile<T, K>::THREADS>(acc, partials, st, ctl);
+}
+
+// ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
+template <typename T, int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_rz(Dims d, const T* __restrict__ r, const T* __restrict__ z,
+         double* __restrict__ partials, RhsState* st, Control* ctl) {
+  if (ctl->all_done) return;
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T rv[K], zv[K];
+    fs::ldv_ro<T, K>(r, n, rv);
+    fs::ldv_ro<T, K>(z, n, zv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) acc[t] += (double)rv[t] * (double)zv[t];
+  }
+  fs::block_partials<K>(acc, partials);
+  if (fs::last_block(&ctl->tickets[kTicketRz])) {
+    double tot[K];
+    fs::grid_total<K>(partials, gridDim.x, tot);
+    if (threadIdx.x < K) {
+      RhsState& s = st[threadIdx.x];
+      if (s.active) {
+        const double g = tot[threadIdx.x];
+        if (!(g > 0.0) || !isfinite(g)) {
+          // M is SPD: r.Mr <= 0 only through NaN/Inf (or r == 0)
+          s.active = 0;
+          s.status = (g == 0.0) ? FS_OK : FS_NAN;
+        } else if (s.fresh) {
+          s.gamma = g;
+          s.gamma_old = g;
+          s.beta = 0.0;
+          s.fresh = 0;
+        } else {
+          s.gamma_old = s.gamma;
+          s.gamma = g;
+          s.beta = g / s.gamma_old;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) refresh_done(st, ctl, K);
+  }
+}
+
+// ---- fallback for rows narrower than 16 B (float k <= 2, double k = 1) -----
+template <typename T, int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_pnew(Dims d, const T* __restrict__ r, const T* __restrict__ pold,
+           T* __restrict__ pnew, RhsState* st, Control* ctl) {
+  if (ctl->all_done) return;
+  __shared__ T beta[K];
+  __shared__ int act[K];
+  if (threadIdx.x < K) {
+    beta[threadIdx.x] = (T)st[threadIdx.x].beta;
+    act[threadIdx.x] = st[threadIdx.x].active;
+  }
+  __syncthreads();
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T rv[K], pv[K];
+    fs::ldv_ro<T, K>(r, n, rv);
+    fs::ldv_ro<T, K>(pold, n, pv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) pv[t] = act[t] ? rv[t] + beta[t] * pv[t] : pv[t];
+    fs::stv<T, K>(pnew, n, pv);
+  }
+}
+
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_apply_pq(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
@@ -346,39 +582,27 @@ __global__ void __launch_bounds__(fs::kBlock)
 #pragma unroll
     for (int t = 0; t < K; ++t) acc[t] += (double)pc[t] * (double)qv[t];
   }
-  fs::block_partials<K>(acc, partials);
-  if (fs::last_block(&ctl->tickets[kTicketApply])) {
-    double tot[K];
-    fs::grid_total<K>(partials, gridDim.x, tot);
-    if (threadIdx.x < K) {
-      RhsState& s = st[threadIdx.x];
-      s.pq = tot[threadIdx.x];
-      if (s.active) {
-        if (tot[threadIdx.x] > 0.0 && isfinite(tot[threadIdx.x])) {
-          s.alpha = s.gamma / tot[threadIdx.x];
-        } else {
-          s.alpha = 0.0;  // breakdown: A~ is SPD, so p.q <= 0 means NaN/Inf
-          s.active = 0;
-          s.status = FS_NAN;
-        }
-      } else {
-        s.alpha = 0.0;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) refresh_done(st, ctl, K);
-  }
+  finish_pq<T, K, fs::kBlock>(acc, partials, st, ctl);
 }
 
-// ---- K2: x~ += alpha p, r~ -= alpha q, r~.r~ ------------------------------------
+// ---- K2: fold a pending correction, x~ += alpha p, r~ -= alpha q, r~.r~ ---------
+// After a reliable update (K3 of the previous iteration) the correction x~
+// it verified is folded into phi here (phi += s x~) and x~ restarts at 0.
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_update(Dims d, const T* __restrict__ p, const T* __restrict__ q,
-             T* __restrict__ x, T* __restrict__ r, double* __restrict__ partials,
+             T* __restrict__ x, T* __restrict__ r, const double* __restrict__ s64,
+             double* __restrict__ phi, double* __restrict__ partials,
              RhsState* st, Control* ctl) {
   if (ctl->all_done) return;
   __shared__ T alpha[K];
-  if (threadIdx.x < K) alpha[threadIdx.x] = (T)st[threadIdx.x].alpha;
+  __shared__ int fold[K];
+  __shared__ int any_fold;
+  if (threadIdx.x < K) {
+    alpha[threadIdx.x] = (T)st[threadIdx.x].alpha;
+    fold[threadIdx.x] = st[threadIdx.x].fold;
+  }
+  if (threadIdx.x == 0) any_fold = ctl->any_fold;
   __syncthreads();
   double acc[K];
 #pragma unroll
@@ -390,6 +614,17 @@ __global__ void __launch_bounds__(fs::kBlock)
     fs::ldv_ro<T, K>(q, n, qv);
     fs::ldv<T, K>(x, n, xv);
     fs::ldv<T, K>(r, n, rv);
+    if (any_fold) {
+      const double s = s64[n];
+      if (s != 0.0) {
+#pragma unroll
+        for (int t = 0; t < K; ++t)
+          if (fold[t]) {
+            phi[n * K + t] += (double)xv[t] * s;
+            xv[t] = (T)0;
+          }
+      }
+    }
 #pragma unroll
     for (int t = 0; t < K; ++t) {
       xv[t] += alpha[t] * pv[t];
@@ -405,6 +640,7 @@ __global__ void __launch_bounds__(fs::kBlock)
     fs::grid_total<K>(partials, gridDim.x, tot);
     if (threadIdx.x < K) {
       RhsState& s = st[threadIdx.x];
+      s.fold = 0;
       if (s.active) {
         const double g = tot[threadIdx.x];
         s.iters += 1;
@@ -412,18 +648,28 @@ __global__ void __launch_bounds__(fs::kBlock)
           s.active = 0;
           s.status = FS_NAN;
         } else {
-          s.gamma_old = s.gamma;
-          s.gamma = g;
-          s.beta = g / s.gamma_old;
+          s.rr = g;
+          if (!ctl->precond) {
+            s.gamma_old = s.gamma;
+            s.gamma = g;
+            s.beta = g / s.gamma_old;
+          }
           const double rn = sqrt(g);
+          // Reliable update: to verify convergence, at the cap, and in mixed
+          // mode after a 1/delta drop or every kRefreshEvery iterations (so
+          // a stagnating low-precision recurrence is noticed).
           if (rn < ctl->tol * s.bnorm || s.iters >= ctl->maxiter ||
-              (ctl->delta > 0.0 && rn < ctl->delta * s.rmax))
+              (ctl->delta > 0.0 &&
+               (rn < ctl->delta * s.rmax || s.iters % kRefreshEvery == 0)))
             s.ru = 1;
         }
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) refresh_done(st, ctl, K);
+    if (threadIdx.x == 0) {
+      ctl->any_fold = 0;
+      refresh_done(st, ctl, K);
+    }
   }
 }
 
@@ -510,9 +756,25 @@ __global__ void __launch_bounds__(fs::kBlock)
           s.active = 0;
           s.status = FS_NOT_CONVERGED;
         } else {
-          s.gamma = g;
-          s.beta = g / s.gamma_old;
-          s.rmax = rn;
+          if (rn < 0.5 * s.best) {
+            s.best = rn;
+            s.nstall = 0;
+          } else {
+            s.nstall += 1;
+          }
+          if (ctl->delta > 0.0 && s.nstall >= kStallUpdates) {
+            // Low-precision iterations no longer reduce the FP64 residual
+            // (a mode below FP32 resolution): stop and report it.
+            s.active = 0;
+            s.status = FS_STALLED;
+          } else {
+            s.rr = g;
+            if (!ctl->precond) {
+              s.gamma = g;
+              s.beta = g / s.gamma_old;
+            }
+            s.rmax = rn;
+          }
         }
       }
     }
@@ -563,13 +825,72 @@ __global__ void k_finalize(Dims d, const uint8_t* __restrict__ label,
 
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// ---- multigrid hierarchy ---------------------------------------------------------
+constexpr int kMaxLevels = 12;
+constexpr int kSmoothDeg = 2;          // Chebyshev degree, pre and post
+constexpr double kSmoothLo = 0.3;      // smoothing interval [lo, 2] of A~
+constexpr int kCoarseDeg = 24;         // coarsest-level Chebyshev degree
+constexpr double kCoarseLo = 0.03;
+constexpr long long kCoarsestNodes = 512;
+
+struct MgLevel {
+  Dims d;
+  // level >= 1: original-scale FP64 masses, labels, scale (setup only)
+  double *m64[3], *s64;
+  uint8_t *label_in, *label;
+  void *em[3];       // equilibrated masses (T); level 0 uses the plan's
+  void *s, *sd;      // diag^-1/2, diag^1/2 (T), 0 on fixed nodes
+  void *x[2], *b, *dv, *res;  // K-interleaved vectors (T); level 0 b = r~
+  size_t off_m64[3], off_s64, off_label_in, off_label, off_em[3], off_s, off_sd,
+      off_x[2], off_b, off_dv, off_res;
+};
+
+int mg_dims(const Dims& fine, Dims* out) {
+  int nl = 0;
+  Dims d = fine;
+  out[nl++] = d;
+  while (nl < kMaxLevels && d.N > kCoarsestNodes && d.nx >= 5 && d.ny >= 5 &&
+         d.nz >= 5) {
+    d = fs::make_dims((d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2);
+    out[nl++] = d;
+  }
+  return nl;
+}
+
+// Chebyshev step coefficients (cd, cr) for degree `deg` on [lo, hi].
+void cheb_coeffs(int deg, double lo, double hi, double* cd, double* cr) {
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+  const double sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  cd[0] = 0.0;
+  cr[0] = 1.0 / theta;
+  for (int k = 1; k < deg; ++k) {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    cd[k] = rho * rho_old;
+    cr[k] = 2.0 * rho / delta;
+    rho_old = rho;
+  }
+}
+
 struct Layout {
-  size_t label, s64, ex, ey, ez, x, r, p, q, partials, st, ctl, total;
+  size_t label, s64, ex, ey, ez, x, r, p0, p1, q, partials, st, ctl, total;
+  int nlev;
+  MgLevel lev[kMaxLevels];
 };
 
 constexpr int kMaxBlocks = 4096;
 
-Layout make_layout(const Dims& d, int nrhs, int precision) {
+// Upper bound on the stencil grid over every tile shape (TY >= 2, XC = 32).
+long long fused_blocks(const Dims& d) {
+  return (long long)((d.nz + 31) / 32) * ((d.ny + 1) / 2) * ((d.nx + 31) / 32);
+}
+
+long long max_blocks(const Dims& d) {
+  long long f = fused_blocks(d);
+  return f > kMaxBlocks ? f : kMaxBlocks;
+}
+
+Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
   const size_t tb = precision == FS_PRECISION_MIXED ? 4 : 8;
   const size_t N = (size_t)d.N;
   Layout L;
@@ -581,11 +902,37 @@ Layout make_layout(const Dims& d, int nrhs, int precision) {
   L.ez = o; o = align_up(o + N * tb);
   L.x = o; o = align_up(o + N * nrhs * tb);
   L.r = o; o = align_up(o + N * nrhs * tb);
-  L.p = o; o = align_up(o + N * nrhs * tb);
+  L.p0 = o; o = align_up(o + N * nrhs * tb);
+  L.p1 = o; o = align_up(o + N * nrhs * tb);
   L.q = o; o = align_up(o + N * nrhs * tb);
-  L.partials = o; o = align_up(o + (size_t)kMaxBlocks * 2 * fs::kMaxRhs * 8);
+  L.partials = o;
+  o = align_up(o + (size_t)max_blocks(d) * 2 * fs::kMaxRhs * 8);
   L.st = o; o = align_up(o + sizeof(RhsState) * fs::kMaxRhs);
   L.ctl = o; o = align_up(o + sizeof(Control));
+  L.nlev = 0;
+  if (precond == FS_PRECOND_MG) {
+    Dims dl[kMaxLevels];
+    L.nlev = mg_dims(d, dl);
+    for (int l = 0; l < L.nlev; ++l) {
+      MgLevel& m = L.lev[l];
+      m = MgLevel{};
+      m.d = dl[l];
+      const size_t n = (size_t)dl[l].N;
+      if (l > 0) {
+        for (int a = 0; a < 3; ++a) { m.off_m64[a] = o; o = align_up(o + n * 8); }
+        m.off_s64 = o; o = align_up(o + n * 8);
+        m.off_label_in = o; o = align_up(o + n);
+        m.off_label = o; o = align_up(o + n);
+        for (int a = 0; a < 3; ++a) { m.off_em[a] = o; o = align_up(o + n * tb); }
+        m.off_b = o; o = align_up(o + n * nrhs * tb);
+      }
+      m.off_s = o; o = align_up(o + n * tb);
+      m.off_sd = o; o = align_up(o + n * tb);
+      for (int a = 0; a < 2; ++a) { m.off_x[a] = o; o = align_up(o + n * nrhs * tb); }
+      m.off_dv = o; o = align_up(o + n * nrhs * tb);
+      m.off_res = o; o = align_up(o + n * nrhs * tb);
+    }
+  }
   L.total = o;
   return L;
 }
@@ -596,42 +943,115 @@ bool valid_nrhs(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16;
 
 struct fs_pcg_plan {
   Dims d;
-  int nrhs, precision;
+  int nrhs, precision, precond;
+  int nlev;
+  MgLevel lev[kMaxLevels];
+  void* z;                 // preconditioned residual (level-0 V-cycle output)
+  int g_rz;
+  long long launches_per_iter;
   const double *mx, *my, *mz;
   double* phi;
   const double* f;
   uint8_t* label;
   double* s64;
-  void *ex, *ey, *ez, *x, *r, *p, *q;
+  void *ex, *ey, *ez, *x, *r, *p[2], *q;
   double* partials;
   RhsState* st;
   Control* ctl;
-  int g_init, g_p, g_apply, g_update, g_rel, g_fin;
+  int g_init, g_apply, g_pnew, g_update, g_rel, g_fin;
+  int use_tma;
+  CUtensorMap tm_p[2];
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
   int* h_flag;
   RhsState* h_st;
   long long launches;
-  // Event samples around K0, K1, K2 of the first iteration of every graph
+  // Event samples around the kernels of the first iteration of every graph
   // launch: live per-kernel durations for the roofline figures.
-  cudaEvent_t ev[4];
-  double kernel_ms[3];
+  cudaEvent_t ev[6];
+  double kernel_ms[5];
   long long kernel_samples;
 };
 
 namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    else
+      (void)cudaGetLastError();
+  }
+  return fn;
+}
 
 template <typename T, int K>
 struct Impl {
   static void grids(fs_pcg_plan* P) {
     const long long N = P->d.N;
     P->g_init = fs_grid_blocks((const void*)k_init<T, K>, N);
-    P->g_p = fs_grid_blocks((const void*)k_pupdate<T, K>, N);
-    P->g_apply = fs_grid_blocks((const void*)k_apply_pq<T, K>, N);
+    using C = TmaTile<T, K>;
+    P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
+    if constexpr (C::OK) {
+      cudaFuncSetAttribute(k_stencil_tma<T, K>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)C::SMEM);
+      int per_sm = 0, dev = 0, sms = 148;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &per_sm, k_stencil_tma<T, K>, C::THREADS, C::SMEM) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long cols = (long long)((P->d.nz + C::TZ - 1) / C::TZ) *
+                             ((P->d.ny + C::TY - 1) / C::TY) * P->d.nx;
+      long long g = (long long)sms * per_sm;
+      if (g > cols) g = cols;
+      P->g_apply = (int)g;
+    } else {
+      P->g_apply = fs_grid_blocks((const void*)k_apply_pq<T, K>, N);
+    }
     P->g_update = fs_grid_blocks((const void*)k_update<T, K>, N);
     P->g_rel = fs_grid_blocks((const void*)k_reliable<T, K>, N);
     P->g_fin = fs_grid_blocks((const void*)k_finalize<T, K>, N);
+    P->g_rz = fs_grid_blocks((const void*)k_rz<T, K>, N);
+  }
+  static int maps(fs_pcg_plan* P) {
+    using C = TmaTile<T, K>;
+    P->use_tma = C::OK ? 1 : 0;
+    if constexpr (!C::OK) return FS_OK;
+    auto encode = encode_fn();
+    if (!encode) {
+      fs_set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
+      return FS_CUDA_ERROR;
+    }
+    const cuuint64_t B = C::B;
+    cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)P->d.nz,
+                          (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
+    cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
+    cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)C::HZ, (cuuint32_t)C::HY, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUtensorMap* maps[2] = {&P->tm_p[0], &P->tm_p[1]};
+    void* bases[2] = {P->p[0], P->p[1]};
+    for (int m = 0; m < 2; ++m) {
+      CUresult rc = encode(maps[m], dt, 4, bases[m], dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rc != CUDA_SUCCESS) {
+        fs_set_error_msg("cuTensorMapEncodeTiled rejected the stencil tensor map");
+        return FS_CUDA_ERROR;
+      }
+    }
+    return FS_OK;
   }
   static void setup_masses(fs_pcg_plan* P, cudaStream_t s) {
     int g = fs_grid_blocks((const void*)k_eq_masses<T>, P->d.N);
@@ -642,28 +1062,39 @@ struct Impl {
                    double delta, cudaStream_t s) {
     k_init<T, K><<<P->g_init, fs::kBlock, 0, s>>>(
         P->d, P->mx, P->my, P->mz, P->label, P->s64, P->phi, P->f, warm,
-        (T*)P->x, (T*)P->r, (T*)P->p, P->partials, P->st, P->ctl, tol, maxiter,
-        delta);
+        (T*)P->x, (T*)P->r, (T*)P->p[0], P->partials, P->st, P->ctl, tol, maxiter,
+        delta, P->precond);
   }
-  static void iteration(fs_pcg_plan* P, cudaStream_t s) {
-    for (int w = 0; w < 4; ++w) kernel(P, w, s);
+  // Iteration with parity `par` reads p[par] and writes p[1 - par].
+  // Iteration with parity `par` reads p[par] and writes p[1 - par].
+  static void iteration(fs_pcg_plan* P, int par, cudaStream_t s) {
+    for (int w = 0; w < 4; ++w) kernel(P, w, par, s);
+    if (P->precond) precondition(P, s);
   }
-  static void kernel(fs_pcg_plan* P, int which, cudaStream_t s) {
+  static void kernel(fs_pcg_plan* P, int which, int par, cudaStream_t s) {
     switch (which) {
       case 0:
-        k_pupdate<T, K><<<P->g_p, fs::kBlock, 0, s>>>(
-            P->d, P->s64, P->phi, (T*)P->x, (const T*)P->r, (T*)P->p, P->st,
-            P->ctl);
+        k_pnew<T, K><<<P->g_pnew, fs::kBlock, 0, s>>>(
+            P->d, (const T*)(P->precond ? P->z : P->r), (const T*)P->p[par],
+            (T*)P->p[1 - par], P->st, P->ctl);
         break;
       case 1:
-        k_apply_pq<T, K><<<P->g_apply, fs::kBlock, 0, s>>>(
-            P->d, (const T*)P->ex, (const T*)P->ey, (const T*)P->ez,
-            (const T*)P->p, (T*)P->q, P->partials, P->st, P->ctl);
+        if constexpr (TmaTile<T, K>::OK) {
+          using C = TmaTile<T, K>;
+          k_stencil_tma<T, K><<<P->g_apply, C::THREADS, C::SMEM, s>>>(
+              P->d, P->tm_p[1 - par], (const T*)P->ex, (const T*)P->ey,
+              (const T*)P->ez, (const T*)P->p[1 - par], (T*)P->q, P->partials,
+              P->st, P->ctl);
+        } else {
+          k_apply_pq<T, K><<<P->g_apply, fs::kBlock, 0, s>>>(
+              P->d, (const T*)P->ex, (const T*)P->ey, (const T*)P->ez,
+              (const T*)P->p[1 - par], (T*)P->q, P->partials, P->st, P->ctl);
+        }
         break;
       case 2:
         k_update<T, K><<<P->g_update, fs::kBlock, 0, s>>>(
-            P->d, (const T*)P->p, (const T*)P->q, (T*)P->x, (T*)P->r,
-            P->partials, P->st, P->ctl);
+            P->d, (const T*)P->p[1 - par], (const T*)P->q, (T*)P->x, (T*)P->r,
+            P->s64, P->phi, P->partials, P->st, P->ctl);
         break;
       default:
         k_reliable<T, K><<<P->g_rel, fs::kBlock, 0, s>>>(
@@ -671,6 +1102,105 @@ struct Impl {
             (const T*)P->x, (T*)P->r, P->partials, P->st, P->ctl);
         break;
     }
+  }
+  // ---- multigrid ----------------------------------------------------------
+  static void mg_setup(fs_pcg_plan* P, cudaStream_t s) {
+    MgLevel& L0 = P->lev[0];
+    L0.em[0] = P->ex;
+    L0.em[1] = P->ey;
+    L0.em[2] = P->ez;
+    L0.b = P->r;
+    int g = fs_grid_blocks((const void*)fs::k_mg_scales<T>, P->d.N);
+    fs::k_mg_scales<T><<<g, fs::kBlock, 0, s>>>(P->d.N, P->s64, (T*)L0.s,
+                                                (T*)L0.sd);
+    for (int l = 1; l < P->nlev; ++l) {
+      MgLevel& f = P->lev[l - 1];
+      MgLevel& c = P->lev[l];
+      const double* fm[3] = {l == 1 ? P->mx : f.m64[0], l == 1 ? P->my : f.m64[1],
+                             l == 1 ? P->mz : f.m64[2]};
+      const uint8_t* flab = l == 1 ? P->label : f.label;
+      g = fs_grid_blocks((const void*)fs::k_mg_coarsen, c.d.N);
+      fs::k_mg_coarsen<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fm[0], fm[1], fm[2],
+                                                flab, c.m64[0], c.m64[1],
+                                                c.m64[2], c.label_in);
+      g = fs_grid_blocks((const void*)k_classify, c.d.N);
+      k_classify<<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
+                                          c.label_in, c.label, c.s64);
+      g = fs_grid_blocks((const void*)k_eq_masses<T>, c.d.N);
+      k_eq_masses<T><<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
+                                              c.s64, (T*)c.em[0], (T*)c.em[1],
+                                              (T*)c.em[2]);
+      g = fs_grid_blocks((const void*)fs::k_mg_scales<T>, c.d.N);
+      fs::k_mg_scales<T><<<g, fs::kBlock, 0, s>>>(c.d.N, c.s64, (T*)c.s,
+                                                  (T*)c.sd);
+    }
+  }
+  // Launch one V-cycle on level l for right-hand side b; returns the index
+  // of the level's x buffer that holds the result, and counts launches.
+  static int vcycle(fs_pcg_plan* P, int l, const T* b, cudaStream_t s,
+                    long long* nl, bool dry = false) {
+    MgLevel& L = P->lev[l];
+    const int* done = &P->ctl->all_done;
+    const bool last = l == P->nlev - 1;
+    const int deg = last ? kCoarseDeg : kSmoothDeg;
+    double cd[64], cr[64];
+    cheb_coeffs(deg, last ? kCoarseLo : kSmoothLo, 2.0, cd, cr);
+    const T *e0 = (const T*)L.em[0], *e1 = (const T*)L.em[1], *e2 = (const T*)L.em[2];
+    const int g = fs_grid_blocks((const void*)fs::k_mg_cheb<T, K>, L.d.N);
+    int cur = 0;
+    for (int k = 0; k < deg; ++k) {  // pre-smoothing (or coarse solve) from 0
+      const int out = k == 0 ? 0 : 1 - cur;
+      if (!dry)
+        fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
+            (T)cd[k], (T)cr[k], k == 0 ? 1 : 0, done);
+      cur = out;
+      ++*nl;
+    }
+    if (last) return cur;
+    MgLevel& C = P->lev[l + 1];
+    const int gc = fs_grid_blocks((const void*)fs::k_mg_restrict<T, K>, C.d.N);
+    if (!dry) {
+      fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
+          L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
+      fs::k_mg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
+          L.d, C.d, (const T*)L.res, (const T*)L.sd, (const T*)C.s, (T*)C.b,
+          done);
+    }
+    *nl += 2;
+    const int cc = vcycle(P, l + 1, (const T*)C.b, s, nl, dry);
+    if (!dry)
+      fs::k_mg_prolong<T, K><<<g, fs::kBlock, 0, s>>>(
+          L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd,
+          (T*)L.x[cur], done);
+    ++*nl;
+    for (int k = 0; k < deg; ++k) {  // post-smoothing from the corrected x
+      const int out = 1 - cur;
+      if (!dry)
+        fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
+            (T)cd[k], (T)cr[k], 0, done);
+      cur = out;
+      ++*nl;
+    }
+    return cur;
+  }
+  // Fix the level-0 output buffer (z) without launching anything; the graph
+  // captures kernels that read z before the first V-cycle of an iteration.
+  static void locate_z(fs_pcg_plan* P) {
+    long long nl = 0;
+    const int zi = vcycle(P, 0, (const T*)P->r, nullptr, &nl, true);
+    P->z = P->lev[0].x[zi];
+    P->launches_per_iter = nl + 1;
+  }
+  static long long precondition(fs_pcg_plan* P, cudaStream_t s) {
+    long long nl = 0;
+    const int zi = vcycle(P, 0, (const T*)P->r, s, &nl);
+    P->z = P->lev[0].x[zi];
+    k_rz<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r,
+                                              (const T*)P->z, P->partials,
+                                              P->st, P->ctl);
+    return nl + 1;
   }
   static void finalize(fs_pcg_plan* P, cudaStream_t s) {
     k_finalize<T, K><<<P->g_fin, fs::kBlock, 0, s>>>(P->d, P->label, P->s64,
@@ -681,15 +1211,18 @@ struct Impl {
 
 template <typename T>
 bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
-                double tol = 0, int maxiter = 0, double delta = 0) {
+                double tol = 0, int maxiter = 0, double delta = 0,
+                int par = 0) {
 #define FS_OP(KK)                                                   \
   case KK:                                                          \
     if (op == 0) Impl<T, KK>::grids(P);                             \
     if (op == 1) Impl<T, KK>::setup_masses(P, s);                   \
     if (op == 2) Impl<T, KK>::init(P, warm, tol, maxiter, delta, s); \
-    if (op == 3) Impl<T, KK>::iteration(P, s);                      \
+    if (op == 3) Impl<T, KK>::iteration(P, par, s);                 \
     if (op == 4) Impl<T, KK>::finalize(P, s);                       \
-    if (op >= 5 && op <= 8) Impl<T, KK>::kernel(P, op - 5, s);      \
+    if (op >= 5 && op <= 8) Impl<T, KK>::kernel(P, op - 5, par, s); \
+    if (op == 9) { Impl<T, KK>::mg_setup(P, s); Impl<T, KK>::locate_z(P); } \
+    if (op == 10) P->launches_per_iter = Impl<T, KK>::precondition(P, s); \
     return true;
   switch (k) {
     FS_OP(1)
@@ -702,11 +1235,28 @@ bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
 #undef FS_OP
 }
 
+template <typename T>
+int maps_k(int k, fs_pcg_plan* P) {
+  switch (k) {
+    case 1: return Impl<T, 1>::maps(P);
+    case 2: return Impl<T, 2>::maps(P);
+    case 4: return Impl<T, 4>::maps(P);
+    case 8: return Impl<T, 8>::maps(P);
+    case 16: return Impl<T, 16>::maps(P);
+    default: return FS_BAD_ARG;
+  }
+}
+
+int make_maps(fs_pcg_plan* P) {
+  return P->precision == FS_PRECISION_MIXED ? maps_k<float>(P->nrhs, P)
+                                            : maps_k<double>(P->nrhs, P);
+}
+
 bool dispatch(fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
-              double tol = 0, int maxiter = 0, double delta = 0) {
+              double tol = 0, int maxiter = 0, double delta = 0, int par = 0) {
   if (P->precision == FS_PRECISION_MIXED)
-    return dispatch_k<float>(P->nrhs, P, op, s, warm, tol, maxiter, delta);
-  return dispatch_k<double>(P->nrhs, P, op, s, warm, tol, maxiter, delta);
+    return dispatch_k<float>(P->nrhs, P, op, s, warm, tol, maxiter, delta, par);
+  return dispatch_k<double>(P->nrhs, P, op, s, warm, tol, maxiter, delta, par);
 }
 
 // One CG iteration with event records between its kernels (captured into
@@ -714,14 +1264,13 @@ bool dispatch(fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
 // A plain cudaEventRecord inside a capture only orders streams; the
 // External flag makes it an event-record node that executes with the graph.
 void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
-  cudaEventRecordWithFlags(P->ev[0], s, cudaEventRecordExternal);
-  dispatch(P, 5, s);  // K0
-  cudaEventRecordWithFlags(P->ev[1], s, cudaEventRecordExternal);
-  dispatch(P, 6, s);  // K1
-  cudaEventRecordWithFlags(P->ev[2], s, cudaEventRecordExternal);
-  dispatch(P, 7, s);  // K2
-  cudaEventRecordWithFlags(P->ev[3], s, cudaEventRecordExternal);
-  dispatch(P, 8, s);  // K3
+  for (int w = 0; w < 4; ++w) {
+    cudaEventRecordWithFlags(P->ev[w], s, cudaEventRecordExternal);
+    dispatch(P, 5 + w, s);  // K0 p update, K1 stencil, K2 update, K3 (parity 0)
+  }
+  cudaEventRecordWithFlags(P->ev[4], s, cudaEventRecordExternal);
+  if (P->precond) dispatch(P, 10, s);  // V-cycle and r.z
+  cudaEventRecordWithFlags(P->ev[5], s, cudaEventRecordExternal);
 }
 
 }  // namespace
@@ -729,23 +1278,24 @@ void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
 extern "C" {
 
 int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
-                           size_t* bytes) {
+                           int precond, size_t* bytes) {
   if (nx < 2 || ny < 2 || nz < 2 || !valid_nrhs(nrhs) || !bytes) return FS_BAD_ARG;
   if (precision != FS_PRECISION_FP64 && precision != FS_PRECISION_MIXED)
     return FS_BAD_ARG;
-  *bytes = make_layout(fs::make_dims(nx, ny, nz), nrhs, precision).total;
+  if (precond != FS_PRECOND_JACOBI && precond != FS_PRECOND_MG) return FS_BAD_ARG;
+  *bytes = make_layout(fs::make_dims(nx, ny, nz), nrhs, precision, precond).total;
   return FS_OK;
 }
 
 int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
-                       const double* mx, const double* my, const double* mz,
-                       const uint8_t* label_in, double* phi, const double* f,
-                       void* workspace, size_t workspace_bytes,
+                       int precond, const double* mx, const double* my,
+                       const double* mz, const uint8_t* label_in, double* phi,
+                       const double* f, void* workspace, size_t workspace_bytes,
                        fs_pcg_plan** plan, void* stream) {
   if (!plan) return FS_BAD_ARG;
   *plan = nullptr;
   size_t need = 0;
-  int st = fs_pcg_workspace_bytes(nx, ny, nz, nrhs, precision, &need);
+  int st = fs_pcg_workspace_bytes(nx, ny, nz, nrhs, precision, precond, &need);
   if (st != FS_OK) return st;
   if (!mx || !my || !mz || !label_in || !phi || !workspace ||
       workspace_bytes < need)
@@ -759,13 +1309,37 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   P->d = fs::make_dims(nx, ny, nz);
   P->nrhs = nrhs;
   P->precision = precision;
+  P->precond = precond == FS_PRECOND_MG ? 1 : 0;
+  P->launches_per_iter = 0;
   P->mx = mx;
   P->my = my;
   P->mz = mz;
   P->phi = phi;
   P->f = f;
-  Layout L = make_layout(P->d, nrhs, precision);
+  Layout L = make_layout(P->d, nrhs, precision, precond);
   char* w = (char*)workspace;
+  P->nlev = L.nlev;
+  for (int l = 0; l < L.nlev; ++l) {
+    MgLevel& m = P->lev[l];
+    m = L.lev[l];
+    if (l > 0) {
+      for (int a = 0; a < 3; ++a) {
+        m.m64[a] = (double*)(w + m.off_m64[a]);
+        m.em[a] = w + m.off_em[a];
+      }
+      m.s64 = (double*)(w + m.off_s64);
+      m.label_in = (uint8_t*)(w + m.off_label_in);
+      m.label = (uint8_t*)(w + m.off_label);
+      m.b = w + m.off_b;
+    }
+    m.s = w + m.off_s;
+    m.sd = w + m.off_sd;
+    m.x[0] = w + m.off_x[0];
+    m.x[1] = w + m.off_x[1];
+    m.dv = w + m.off_dv;
+    m.res = w + m.off_res;
+  }
+  P->z = nullptr;
   P->label = (uint8_t*)(w + L.label);
   P->s64 = (double*)(w + L.s64);
   P->ex = w + L.ex;
@@ -773,7 +1347,8 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   P->ez = w + L.ez;
   P->x = w + L.x;
   P->r = w + L.r;
-  P->p = w + L.p;
+  P->p[0] = w + L.p0;
+  P->p[1] = w + L.p1;
   P->q = w + L.q;
   P->partials = (double*)(w + L.partials);
   P->st = (RhsState*)(w + L.st);
@@ -784,14 +1359,14 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   P->h_st = nullptr;
   P->launches = 0;
   dispatch(P, 0, s);
-  const int gmax = P->g_init > P->g_apply ? P->g_init : P->g_apply;
-  if (gmax > kMaxBlocks || P->g_p > kMaxBlocks || P->g_update > kMaxBlocks ||
-      P->g_rel > kMaxBlocks || P->g_fin > kMaxBlocks) {
+  if (P->g_init > kMaxBlocks || P->g_apply > max_blocks(P->d) ||
+      P->g_update > kMaxBlocks || P->g_rel > kMaxBlocks ||
+      P->g_fin > kMaxBlocks) {
     delete P;
     return FS_BAD_ARG;
   }
-  for (int t = 0; t < 4; ++t) P->ev[t] = nullptr;
-  P->kernel_ms[0] = P->kernel_ms[1] = P->kernel_ms[2] = 0.0;
+  for (int t = 0; t < 6; ++t) P->ev[t] = nullptr;
+  for (int t = 0; t < 5; ++t) P->kernel_ms[t] = 0.0;
   P->kernel_samples = 0;
   auto fail = [&](const char* where, cudaError_t e) {
     fs_pcg_plan_destroy(P);
@@ -806,6 +1381,17 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   if ((e = cudaGetLastError()) != cudaSuccess) return fail("k_classify", e);
   dispatch(P, 1, s);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail("k_eq_masses", e);
+  {
+    int ms = make_maps(P);
+    if (ms != FS_OK) {
+      fs_pcg_plan_destroy(P);
+      return ms;
+    }
+  }
+  if (P->precond) {
+    dispatch(P, 9, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail("multigrid setup", e);
+  }
   if ((e = cudaMallocHost((void**)&P->h_flag, sizeof(int))) != cudaSuccess)
     return fail("cudaMallocHost", e);
   if ((e = cudaMallocHost((void**)&P->h_st, sizeof(RhsState) * fs::kMaxRhs)) !=
@@ -818,18 +1404,19 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   if ((e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking)) !=
       cudaSuccess)
     return fail("cudaStreamCreate", e);
-  for (int t = 0; t < 4; ++t)
+  for (int t = 0; t < 6; ++t)
     if ((e = cudaEventCreate(&P->ev[t])) != cudaSuccess)
       return fail("cudaEventCreate", e);
   cudaGraph_t graph = nullptr;
   if ((e = cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal)) !=
       cudaSuccess)
     return fail("cudaStreamBeginCapture", e);
+  // chunk is even, so every graph launch starts on parity 0 (p[0] = p_old)
   for (int it = 0; it < P->chunk; ++it) {
     if (it == 0) {
       dispatch_first(P, P->cap);
     } else {
-      dispatch(P, 3, P->cap);
+      dispatch(P, 3, P->cap, 0, 0, 0, 0, it & 1);
     }
   }
   e = cudaStreamEndCapture(P->cap, &graph);
@@ -850,24 +1437,30 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
   dispatch(P, 2, s, warm_start ? 1 : 0, tol, maxiter, delta);
   FS_CHECK_LAUNCH("k_init");
   long long launches = 1;
-  P->kernel_ms[0] = P->kernel_ms[1] = P->kernel_ms[2] = 0.0;
+  if (P->precond) {
+    dispatch(P, 10, s);  // z = M r and r.z for the first direction
+    FS_CHECK_LAUNCH("multigrid V-cycle");
+    launches += P->launches_per_iter;
+  }
+  for (int t = 0; t < 5; ++t) P->kernel_ms[t] = 0.0;
   P->kernel_samples = 0;
   const long long max_chunks = (long long)maxiter / P->chunk + 4;
   int timed_out = 1;
   for (long long c = 0; c < max_chunks; ++c) {
     if ((e = cudaGraphLaunch(P->exec, s)) != cudaSuccess)
       return fs_cuda_status("cudaGraphLaunch", e);
-    launches += 4LL * P->chunk;
+    launches += (4LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
     if ((e = cudaMemcpyAsync(P->h_flag, &P->ctl->all_done, sizeof(int),
                              cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return fs_cuda_status("cudaMemcpyAsync", e);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
       return fs_cuda_status("cudaStreamSynchronize", e);
-    float ms[3];
-    if (cudaEventElapsedTime(&ms[0], P->ev[0], P->ev[1]) == cudaSuccess &&
-        cudaEventElapsedTime(&ms[1], P->ev[1], P->ev[2]) == cudaSuccess &&
-        cudaEventElapsedTime(&ms[2], P->ev[2], P->ev[3]) == cudaSuccess) {
-      for (int t = 0; t < 3; ++t) P->kernel_ms[t] += ms[t];
+    float ms[5];
+    bool ok = true;
+    for (int t = 0; t < 5 && ok; ++t)
+      ok = cudaEventElapsedTime(&ms[t], P->ev[t], P->ev[t + 1]) == cudaSuccess;
+    if (ok) {
+      for (int t = 0; t < 5; ++t) P->kernel_ms[t] += ms[t];
       P->kernel_samples += 1;
     } else {
       (void)cudaGetLastError();  // timing unavailable: not a solve failure
@@ -898,7 +1491,9 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
       stats[t].reserved = 0;
     }
     if (h.status == FS_NAN) worst = FS_NAN;
+    else if (h.status == FS_STALLED && worst != FS_NAN) worst = FS_STALLED;
     else if (h.status == FS_NOT_CONVERGED && worst == FS_OK) worst = FS_NOT_CONVERGED;
+    else if (h.status == FS_TIMEOUT && worst == FS_OK) worst = FS_TIMEOUT;
   }
   if (timed_out) return FS_TIMEOUT;
   return worst;
@@ -915,14 +1510,14 @@ long long fs_pcg_plan_launches(const fs_pcg_plan* P) {
 int fs_pcg_plan_kernel_times(const fs_pcg_plan* P, double* ms,
                              long long* samples) {
   if (!P || !ms || !samples) return FS_BAD_ARG;
-  for (int t = 0; t < 3; ++t) ms[t] = P->kernel_ms[t];
+  for (int t = 0; t < 5; ++t) ms[t] = P->kernel_ms[t];
   *samples = P->kernel_samples;
   return FS_OK;
 }
 
 int fs_pcg_plan_destroy(fs_pcg_plan* P) {
   if (!P) return FS_OK;
-  for (int t = 0; t < 4; ++t)
+  for (int t = 0; t < 6; ++t)
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->cap) cudaStreamDestroy(P->cap);

@@ -215,84 +215,131 @@ class EliminatedSystem:
     ``label``: uint8 device array (``FS_LABEL_FREE``/``FS_LABEL_FIXED`` per
     node).  ``phi`` (N*k FP64) holds the Dirichlet values on fixed nodes and
     receives the solution; ``f`` (optional, N*k) is the source term.
+
+    ``precision``: ``"mixed"`` (FP32 inner CG, FP64 reliable updates),
+    ``"fp64"``, or ``"auto"``: mixed, and if a right-hand side stalls (a mode
+    below FP32 resolution, e.g. a floating copper island in oxide) the same
+    solve continues in FP64 from the mixed iterate; later solves of this
+    system then stay in FP64.
     """
 
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
-                 precision: str = "mixed", with_source: bool = False):
+                 precision: str = "auto", with_source: bool = False,
+                 preconditioner: str = "jacobi"):
         import torch
+        if precision not in ("auto", "mixed", "fp64"):
+            raise ValueError(f"precision must be 'auto', 'mixed' or 'fp64', got {precision!r}")
+        if preconditioner not in ("jacobi", "mg"):
+            raise ValueError(f"preconditioner must be 'jacobi' or 'mg', got {preconditioner!r}")
+        self.preconditioner = preconditioner
+        self._pc = L.PRECOND_MG if preconditioner == "mg" else L.PRECOND_JACOBI
         self.op = op
         self.k = pad_rhs(nrhs)
         self.nrhs = nrhs
-        if precision not in ("mixed", "fp64"):
-            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
-        self.precision = precision
-        prec = L.PRECISION_MIXED if precision == "mixed" else L.PRECISION_FP64
-        lib = L.lib()
+        self.mode = precision
+        self.precision = "fp64" if precision == "fp64" else "mixed"
         dev = op.dev
         N = op.N
         self.label_in = label
         self.phi = torch.zeros(N * self.k, dtype=torch.float64, device=dev)
         self.f = (torch.zeros(N * self.k, dtype=torch.float64, device=dev)
                   if with_source else None)
-        nb = ctypes.c_size_t()
-        nx, ny, nz = op.shape
-        L.check("fs_pcg_workspace_bytes",
-                lib.fs_pcg_workspace_bytes(nx, ny, nz, self.k, prec, ctypes.byref(nb)))
-        self.workspace = torch.empty(nb.value, dtype=torch.uint8, device=dev)
-        if self.workspace.data_ptr() % 256:
-            raise RuntimeError("device allocation is not 256-byte aligned")
         t0 = time.perf_counter()
-        plan = ctypes.c_void_p()
-        st = lib.fs_pcg_plan_create(nx, ny, nz, self.k, prec, L.ptr(op.mx),
-                                    L.ptr(op.my), L.ptr(op.mz), L.ptr(label),
-                                    L.ptr(self.phi), L.ptr(self.f),
-                                    L.ptr(self.workspace), nb.value,
-                                    ctypes.byref(plan), L.stream_ptr())
-        L.check("fs_pcg_plan_create", st)
-        self._plan = plan
+        self._plan, self.workspace = self._make_plan(self.precision)
+        self._fp64 = None
+        self.fell_back = False
         # The classified labels are the first N bytes of the workspace.
-        lab_ptr = lib.fs_pcg_plan_labels(plan)
+        lib = L.lib()
+        lab_ptr = lib.fs_pcg_plan_labels(self._plan)
         off = lab_ptr - self.workspace.data_ptr()
         self.labels = self.workspace[off:off + N]
         counts = torch.bincount(self.labels.to(torch.int64), minlength=4).cpu().numpy()
         self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts[:4])
         self.setup_time = time.perf_counter() - t0
         self.launches = 0
+        self._last_plan = self._plan
+
+    def _make_plan(self, precision: str):
+        import torch
+        lib = L.lib()
+        op = self.op
+        prec = L.PRECISION_MIXED if precision == "mixed" else L.PRECISION_FP64
+        nb = ctypes.c_size_t()
+        nx, ny, nz = op.shape
+        L.check("fs_pcg_workspace_bytes",
+                lib.fs_pcg_workspace_bytes(nx, ny, nz, self.k, prec, self._pc,
+                                           ctypes.byref(nb)))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device=op.dev)
+        if ws.data_ptr() % 256:
+            raise RuntimeError("device allocation is not 256-byte aligned")
+        plan = ctypes.c_void_p()
+        st = lib.fs_pcg_plan_create(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
+                                    L.ptr(op.my), L.ptr(op.mz), L.ptr(self.label_in),
+                                    L.ptr(self.phi), L.ptr(self.f), L.ptr(ws),
+                                    nb.value, ctypes.byref(plan), L.stream_ptr())
+        L.check("fs_pcg_plan_create", st)
+        return plan, ws
 
     def default_maxiter(self) -> int:
         """The reference's cap ``max(500, 10*sqrt(n))`` (poisson.py:535-536)."""
         return max(500, int(10 * math.sqrt(max(self.n_free, 1))))
 
-    def solve(self, tol: float, maxiter: int | None = None, *, warm: bool = False):
-        """Solve in place into ``phi``; returns (status, per-RHS stats dicts)."""
+    def _run(self, plan, tol, maxiter, warm):
         lib = L.lib()
         stats = (L.FsRhsStats * self.k)()
-        mi = self.default_maxiter() if maxiter is None else int(maxiter)
-        st = lib.fs_pcg_plan_solve(self._plan, 1 if warm else 0, float(tol), mi,
+        st = lib.fs_pcg_plan_solve(plan, 1 if warm else 0, float(tol), maxiter,
                                    stats, L.stream_ptr())
-        self.launches = int(lib.fs_pcg_plan_launches(self._plan))
-        if st not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN):
+        self.launches += int(lib.fs_pcg_plan_launches(plan))
+        if st not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN, L.FS_STALLED):
             L.check("fs_pcg_plan_solve", st)
-        out = [{"iterations": s.iterations, "status": s.status, "relres": s.relres,
-                "bnorm": s.bnorm, "reliable_updates": s.reliable_updates}
-               for s in stats[:self.nrhs]]
-        return st, out
+        self._last_plan = plan
+        return st, [{"iterations": s.iterations, "status": s.status,
+                     "relres": s.relres, "bnorm": s.bnorm,
+                     "reliable_updates": s.reliable_updates}
+                    for s in stats[:self.nrhs]]
+
+    def solve(self, tol: float, maxiter: int | None = None, *, warm: bool = False):
+        """Solve in place into ``phi``; returns (status, per-RHS stats dicts)."""
+        mi = self.default_maxiter() if maxiter is None else int(maxiter)
+        self.launches = 0
+        if self.fell_back:
+            return self._run(self._fp64[0], tol, mi, warm)
+        st, stats = self._run(self._plan, tol, mi, warm)
+        bad = any(s["status"] in (L.FS_NOT_CONVERGED, L.FS_STALLED) for s in stats)
+        if self.mode == "auto" and bad:
+            if self._fp64 is None:
+                self._fp64 = self._make_plan("fp64")
+            self.fell_back = True
+            st, stats2 = self._run(self._fp64[0], tol, mi, True)
+            for a, b in zip(stats, stats2):
+                b["iterations"] += a["iterations"]
+                b["reliable_updates"] += a["reliable_updates"]
+                b["fp64_fallback"] = True
+            stats = stats2
+        return st, stats
 
     def kernel_times(self) -> dict:
         """Per-kernel device time sampled during the last solve (ms per
-        launch): p-update, stencil (A~p, p.q) and update (x, r, r.r)."""
-        ms = (ctypes.c_double * 3)()
+        launch): p update, stencil (A~p, p.q), update (x, r, r.r), reliable
+        update, and the preconditioner (V-cycle + r.z)."""
+        ms = (ctypes.c_double * 5)()
         ns = ctypes.c_longlong()
         L.check("fs_pcg_plan_kernel_times",
-                L.load_library().fs_pcg_plan_kernel_times(self._plan, ms, ctypes.byref(ns)))
+                L.load_library().fs_pcg_plan_kernel_times(self._last_plan, ms,
+                                                          ctypes.byref(ns)))
         n = max(ns.value, 1)
         return {"samples": ns.value, "pupdate_ms": ms[0] / n, "stencil_ms": ms[1] / n,
-                "update_ms": ms[2] / n}
+                "update_ms": ms[2] / n, "reliable_ms": ms[3] / n,
+                "precond_ms": ms[4] / n}
 
     def close(self) -> None:
-        if getattr(self, "_plan", None) is not None and self._plan.value:
-            L.load_library().fs_pcg_plan_destroy(self._plan)
-            self._plan = None
+        lib = L.load_library()
+        for plan in (getattr(self, "_plan", None),
+                     (getattr(self, "_fp64", None) or (None,))[0]):
+            if plan is not None and plan.value:
+                lib.fs_pcg_plan_destroy(plan)
+        self._plan = None
+        self._fp64 = None
 
     def __del__(self):
         try:

@@ -58,15 +58,18 @@ class GPUConfig:
     precision
         ``"mixed"``: FP32 inner CG with FP64 reliable updates (the residual
         that decides convergence is always FP64).  ``"fp64"``: every vector
-        in FP64, the plain method.
+        in FP64, the plain method.  ``"auto"`` (default): mixed, continuing
+        in FP64 if the FP32 iterations stall on a mode below FP32 resolution
+        (extreme conductivity contrast).
     preconditioner
         ``"jacobi"`` (CG on the equilibrated system, the reference's method)
-        or ``"mg"`` (geometric multigrid V-cycle inside flexible CG).
+        or ``"mg"`` (a geometric-multigrid V-cycle as the CG preconditioner;
+        same FP64 stopping rule).
     maxiter
         Iteration cap; ``None`` uses the reference's ``max(500, 10*sqrt(n))``
         (``poisson.py:535-536``).
     """
-    precision: str = "mixed"
+    precision: str = "auto"
     preconditioner: str = "jacobi"
     maxiter: int | None = None
 

@@ -218,7 +218,8 @@ class PoissonSolver:
         shield_dev = h2d(shield.astype(np.int64), torch.int64, dev)
         C, q_shield, info = extract_capacitance(
             self.op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
-            precision=self.gpu.precision, maxiter=self.gpu.maxiter)
+            precision=self.gpu.precision, maxiter=self.gpu.maxiter,
+            preconditioner=self.gpu.preconditioner)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         rep["terminals"] = tuple(t.name for t in terms)
@@ -290,7 +291,8 @@ class PoissonSolver:
         label[fixed_d] = L.LABEL_FIXED
         with_src = rho_node is not None
         system = EliminatedSystem(self.op, label, 1, precision=self.gpu.precision,
-                                  with_source=with_src)
+                                  with_source=with_src,
+                                  preconditioner=self.gpu.preconditioner)
         system.phi.zero_()
         system.phi[fixed_d] = torch.as_tensor(vals, dtype=torch.float64, device=dev)
         if with_src:
@@ -337,8 +339,8 @@ class PoissonSolver:
 
 
 def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
-                        tol: float, precision: str = "mixed",
-                        maxiter: int | None = None):
+                        tol: float, precision: str = "auto",
+                        maxiter: int | None = None, preconditioner: str = "jacobi"):
     """Device core of the extraction: inputs already in HBM.
 
     ``term_dev``: sorted unique int64 node tensors, one per terminal;
@@ -373,7 +375,8 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         if system is None or system.k != k:
             if system is not None:
                 system.close()
-            system = EliminatedSystem(op, label, kb, precision=precision)
+            system = EliminatedSystem(op, label, kb, precision=precision,
+                                      preconditioner=preconditioner)
             setup_time += system.setup_time
         system.nrhs = kb
         group.fill_(-1)
@@ -394,7 +397,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
             if has_shield:
                 q_shield[j] = Q[nt, c]
     info = {
-        "method": f"gpu-cg-jacobi-{precision}",
+        "method": f"gpu-cg-{preconditioner}-{precision}",
         "n": N,
         "n_factorised": system.n_free,
         "n_decoupled": system.n_fixed + system.n_solo,
@@ -409,6 +412,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         "residual": max(s["relres"] for s in stats_all),
         "relres_fp64": [s["relres"] for s in stats_all],
         "reliable_updates": [s["reliable_updates"] for s in stats_all],
+        "fp64_fallback": bool(system.fell_back),
         "gpu_launches": launches,
         "kernel_ms": system.kernel_times(),
         "notes": (),

@@ -41,6 +41,9 @@ extern "C" {
 #define FS_BAD_ARG 3         /* invalid size, pointer or option              */
 #define FS_NAN 4             /* a residual norm became NaN or Inf             */
 #define FS_CUDA_ERROR 5      /* a CUDA runtime call failed                    */
+#define FS_STALLED 6         /* mixed precision: FP32 iterations stopped
+                                reducing the FP64 residual (solve again in
+                                FS_PRECISION_FP64, warm-started)               */
 
 /* ---- enumerations ------------------------------------------------------ */
 #define FS_LABEL_FREE 0
@@ -58,11 +61,11 @@ extern "C" {
 #define FS_AVERAGE_HARMONIC 1 /* dual-area weighted harmonic mean             */
 
 #define FS_PRECOND_JACOBI 0  /* CG on the Jacobi-equilibrated system          */
-#define FS_PRECOND_MG 1      /* geometric multigrid V-cycle (flexible CG)     */
+#define FS_PRECOND_MG 1      /* geometric multigrid V-cycle preconditioner    */
 
 typedef struct fs_rhs_stats {
   int32_t iterations;       /* CG iterations taken                            */
-  int32_t status;           /* FS_OK, FS_NOT_CONVERGED or FS_NAN              */
+  int32_t status;           /* FS_OK, FS_NOT_CONVERGED, FS_STALLED, FS_NAN    */
   double relres;            /* final FP64 true relative residual              */
   double bnorm;             /* ||D^-1/2 b_free||_2 of the eliminated system   */
   int32_t reliable_updates; /* FP64 residual replacements performed           */
@@ -128,30 +131,35 @@ int fs_set_dirichlet(const int16_t* group, const uint8_t* label,
  * 533-552).  The plan is bound to one operator, one label array and one phi
  * buffer (N*nrhs FP64, fixed values in place, the initial guess on free
  * nodes) and an optional source f (N*nrhs FP64, may be NULL).
- * nrhs must be 1, 2, 4, 8 or 16.  workspace must hold
+ * nrhs must be 1, 2, 4, 8 or 16.  precond: FS_PRECOND_JACOBI (CG on the
+ * equilibrated system, the reference's method) or FS_PRECOND_MG (a
+ * geometric-multigrid V-cycle with Chebyshev smoothing as the
+ * preconditioner; same stopping rule).  workspace must hold
  * fs_pcg_workspace_bytes() bytes and stay alive until destroy.              */
 int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
-                           size_t* bytes);
+                           int precond, size_t* bytes);
 int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
-                       const double* mx, const double* my, const double* mz,
-                       const uint8_t* label_in, double* phi, const double* f,
-                       void* workspace, size_t workspace_bytes,
+                       int precond, const double* mx, const double* my,
+                       const double* mz, const uint8_t* label_in, double* phi,
+                       const double* f, void* workspace, size_t workspace_bytes,
                        fs_pcg_plan** plan, void* stream);
 /* Solve in place into phi.  warm_start != 0 keeps the free-node values of
  * phi as the initial guess (the tolerance stays relative to ||b||, as in
  * SciPy); otherwise the guess is 0.  stats: host array of nrhs entries.
  * Returns FS_OK when every RHS converged, FS_NOT_CONVERGED if one hit
- * maxiter, FS_NAN on breakdown.                                             */
+ * maxiter, FS_STALLED if a mixed-precision RHS stopped making progress,
+ * FS_NAN on breakdown, FS_TIMEOUT if a staged load never arrived.           */
 int fs_pcg_plan_solve(fs_pcg_plan* plan, int warm_start, double tol,
                       int maxiter, fs_rhs_stats* stats, void* stream);
 /* Label array after classification (free / fixed / solo / pinned), device. */
 const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* plan);
 /* Number of kernel launches issued by the last solve (host count).          */
 long long fs_pcg_plan_launches(const fs_pcg_plan* plan);
-/* Device time of the p-update, stencil (A~p and p.q) and update kernels,
- * summed over the samples taken during the last solve: the first CG
- * iteration of every graph launch is bracketed by CUDA events.  ms: host
- * array of 3.                                                               */
+/* Device time of the CG kernels -- p update (p = r + beta p), stencil
+ * (A~p, p.q), update (x, r, r.r), reliable update, and the preconditioner
+ * (V-cycle and r.z; 0 without one) -- summed over the samples taken during
+ * the last solve: the first CG iteration of every graph launch is bracketed
+ * by CUDA events.  ms: host array of 5.                                     */
 int fs_pcg_plan_kernel_times(const fs_pcg_plan* plan, double* ms,
                              long long* samples);
 int fs_pcg_plan_destroy(fs_pcg_plan* plan);

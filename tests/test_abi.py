@@ -48,21 +48,26 @@ def test_status_strings(dll):
 
 def test_workspace_sizes_and_bad_arguments(dll):
     nb = ctypes.c_size_t()
-    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_MIXED, ctypes.byref(nb)) == L.FS_OK
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_MIXED, 0, ctypes.byref(nb)) == L.FS_OK
     n = 32 * 32 * 16
     # label + s64 + 3 FP32 masses + 4 FP32 vectors of 8 RHS
     assert nb.value >= n * (1 + 8 + 12 + 4 * 8 * 4)
     nb64 = ctypes.c_size_t()
-    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_FP64, ctypes.byref(nb64)) == L.FS_OK
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_FP64, 0, ctypes.byref(nb64)) == L.FS_OK
     assert nb64.value > nb.value
+    nbmg = ctypes.c_size_t()
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, L.PRECISION_MIXED, L.PRECOND_MG,
+                                      ctypes.byref(nbmg)) == L.FS_OK
+    assert nbmg.value > nb.value
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, 1, 7, ctypes.byref(nb)) == L.FS_BAD_ARG
     for k in (0, 3, 5, 17):
-        assert dll.fs_pcg_workspace_bytes(32, 32, 16, k, 1, ctypes.byref(nb)) == L.FS_BAD_ARG
-    assert dll.fs_pcg_workspace_bytes(1, 32, 16, 8, 1, ctypes.byref(nb)) == L.FS_BAD_ARG
-    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, 7, ctypes.byref(nb)) == L.FS_BAD_ARG
+        assert dll.fs_pcg_workspace_bytes(32, 32, 16, k, 1, 0, ctypes.byref(nb)) == L.FS_BAD_ARG
+    assert dll.fs_pcg_workspace_bytes(1, 32, 16, 8, 1, 0, ctypes.byref(nb)) == L.FS_BAD_ARG
+    assert dll.fs_pcg_workspace_bytes(32, 32, 16, 8, 7, 0, ctypes.byref(nb)) == L.FS_BAD_ARG
     null = ctypes.c_void_p(0)
     assert dll.fs_build_masses(*([null] * 7), 4, 4, 4, 0, null, null, null, null) == L.FS_BAD_ARG
     plan = ctypes.c_void_p()
-    assert dll.fs_pcg_plan_create(8, 8, 8, 3, 1, *([null] * 7), 0, ctypes.byref(plan), null) == L.FS_BAD_ARG
+    assert dll.fs_pcg_plan_create(8, 8, 8, 3, 1, 0, *([null] * 7), 0, ctypes.byref(plan), null) == L.FS_BAD_ARG
     assert dll.fs_pcg_plan_destroy(null) == L.FS_OK
     assert dll.fs_group_apply_workspace_bytes(0, 8, ctypes.byref(nb)) == L.FS_BAD_ARG
     assert dll.fs_quadform_workspace_bytes(17, ctypes.byref(nb)) == L.FS_BAD_ARG
