@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
+    ap.add_argument("--preconditioner", default="mg", choices=["mg", "jacobi"])
     ap.add_argument("--shape", default=",".join(map(str, SHAPE)))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
@@ -144,9 +145,10 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def kernel_bytes(N: int, k: int, s: int) -> dict:
     """Algorithmic bytes per launch of the CG kernels (each array once)."""
-    return {"pupdate": 3 * N * k * s,                 # read r, p_old; write p
+    return {"pupdate": 3 * N * k * s,                 # read r|z, p_old; write p
             "stencil": N * (2 * k * s + 3 * s),       # read p, 3 masses; write q
-            "update": 6 * N * k * s}                  # read p, q, x, r; write x, r
+            "update": 6 * N * k * s,                  # read p, q, x, r; write x, r
+            "smoother": N * (5 * k * s + 3 * s)}      # read x, d, b, masses; write x, d
 
 
 def run_ours(args, rank, world, local_rank):
@@ -178,17 +180,19 @@ def run_ours(args, rank, world, local_rank):
     for t in terms:
         t.nodes = torch.from_numpy(np.ascontiguousarray(t.nodes, dtype=np.int64)).pin_memory().numpy()
 
-    def step_device(precision):
+    def step_device(precision, pc=args.preconditioner):
         op = D.DeviceOperator(grid, eps_dev)
         C, qs, info = extract_capacitance(op, term_dev, wall_dev, shield_dev,
-                                          tol=TOL, precision=precision)
+                                          tol=TOL, precision=precision,
+                                          preconditioner=pc)
         info["gpu_launches"] += 1 + 2  # mass build + plan setup kernels
         return C, qs, info
 
     def step_e2e(precision):
         rep = {}
         C = EX.capacitance_matrix(grid, eps_pinned, terms, bc, SolverConfig(tol=TOL),
-                                  report=rep, gpu=GPUConfig(precision=precision))
+                                  report=rep, gpu=GPUConfig(precision=precision,
+                                                            preconditioner=args.preconditioner))
         return C, rep
 
     def barrier():
@@ -245,14 +249,22 @@ def run_ours(args, rank, world, local_rank):
 
     variants = {}
     if not args.no_variants:
+        nv = max(2, args.steps // 2)
+        runs = []
+        if args.preconditioner == "mg":
+            runs.append(("plain_pcg_jacobi", args.precision, "jacobi"))
         other = "fp64" if args.precision != "fp64" else "mixed"
-        ms_o, outs_o = timed(lambda: step_device(other), max(2, args.steps // 2), 1)
-        Co = outs_o[-1][0]
-        variants[other] = {
-            "value": n_solves_step * max(2, args.steps // 2) / (ms_o / 1000.0),
-            "iterations": outs_o[-1][2]["iterations"],
-            "C_rel_diff_vs_default": float(np.abs(Co - C).max() / np.abs(np.diag(C)).max()),
-        }
+        runs.append((f"{args.preconditioner}_{other}", other, args.preconditioner))
+        for name, prec, pc in runs:
+            ms_o, outs_o = timed(lambda: step_device(prec, pc), nv, 1)
+            Co = outs_o[-1][0]
+            variants[name] = {
+                "value": n_solves_step * nv / (ms_o / 1000.0),
+                "ms_per_step": ms_o / nv,
+                "precision": prec, "preconditioner": pc,
+                "iterations": outs_o[-1][2]["iterations"],
+                "C_rel_diff_vs_default": float(np.abs(Co - C).max() / np.abs(np.diag(C)).max()),
+            }
 
     if rank != 0:
         return
@@ -262,6 +274,8 @@ def run_ours(args, rank, world, local_rank):
     km = info["kernel_ms"]
     times = {"pupdate": km["pupdate_ms"], "stencil": km["stencil_ms"],
              "update": km["update_ms"]}
+    if args.preconditioner == "mg":
+        times["smoother"] = km["smoother_ms"]
     dom = max(times, key=times.get)
     peak, peak_kind = measured_peaks()
     gbs = {k: kb[k] / (times[k] * 1e-3) / 1e9 for k in times if times[k] > 0}
@@ -291,7 +305,8 @@ def run_ours(args, rank, world, local_rank):
                         f"{NBOX} terminals, zlo grounded, seed=rank",
             "nodes": N, "nrhs": NBOX, "tol": TOL, "precision": args.precision,
             "fp64_fallback": info.get("fp64_fallback"),
-            "preconditioner": "jacobi (equilibrated CG)",
+            "preconditioner": ("mg (geometric multigrid V-cycle, Chebyshev smoothing)"
+                               if args.preconditioner == "mg" else "jacobi (equilibrated CG)"),
             "l2": "inputs larger than L2: every CG vector is N*8*4 B = 268 MB",
             "parallelism": f"dp{world} (independent geometries)",
         },
@@ -306,6 +321,7 @@ def run_ours(args, rank, world, local_rank):
             "algorithmic_bytes_per_launch": kb[dom],
             "ms_per_launch": times[dom], "samples": km["samples"],
             "all_kernels_gbs": gbs, "all_kernels_ms": times,
+            "precond_ms_per_iteration": km.get("precond_ms"),
         },
         "stencil_gbs": gbs.get("stencil"),
         "gpu_launches": int(launches),

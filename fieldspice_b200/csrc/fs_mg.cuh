@@ -285,4 +285,76 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// Prolongation, coarse-cell-centric: the thread of coarse node (I, J, Kc)
+// writes the fine nodes 2I+a, 2J+b, 2Kc+c (a, b, c in {0, 1}) that it owns,
+// interpolating from the up to 8 coarse corners it loads once:
+//   x_f += sd(f) * sum_I P(f, I) s_c(I) x_c(I).
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_prolong_cell(Dims f, Dims c, const T* __restrict__ xc,
+                      const T* __restrict__ sc, const T* __restrict__ sdf,
+                      T* __restrict__ xf, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int I, J, Kc;
+    node_ijk(c, n, I, J, Kc);
+    const bool hx = I + 1 < c.nx, hy = J + 1 < c.ny, hz = Kc + 1 < c.nz;
+    // corner values v[a][b][e] = s_c x_c at (I+a, J+b, Kc+e); absent -> 0
+    T v[2][2][2][K];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const bool ok = (a == 0 || hx) && (b == 0 || hy) && (e == 0 || hz);
+          if (ok) {
+            const long long cn = n + a * c.sx + b * c.sy + e;
+            const T w = __ldg(sc + cn);
+            ldv_ro<T, K>(xc, cn, v[a][b][e]);
+#pragma unroll
+            for (int t = 0; t < K; ++t) v[a][b][e][t] *= w;
+          } else {
+#pragma unroll
+            for (int t = 0; t < K; ++t) v[a][b][e][t] = (T)0;
+          }
+        }
+    // per-axis weights for fine offset 0 (coarse node itself) and 1 (midpoint
+    // or, on a last fine node with no upper partner, weight 1 from below)
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      const int i = 2 * I + a;
+      if (i >= f.nx) continue;
+      const T wa0 = a == 0 ? (T)1 : (hx ? (T)0.5 : (T)1), wa1 = a == 0 ? (T)0 : (hx ? (T)0.5 : (T)0);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int j = 2 * J + b;
+        if (j >= f.ny) continue;
+        const T wb0 = b == 0 ? (T)1 : (hy ? (T)0.5 : (T)1), wb1 = b == 0 ? (T)0 : (hy ? (T)0.5 : (T)0);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int k = 2 * Kc + e;
+          if (k >= f.nz) continue;
+          const T we0 = e == 0 ? (T)1 : (hz ? (T)0.5 : (T)1), we1 = e == 0 ? (T)0 : (hz ? (T)0.5 : (T)0);
+          const long long fn = ((long long)i * f.ny + j) * f.nz + k;
+          const T scale = __ldg(sdf + fn);
+          if (scale == (T)0) continue;
+          T xv[K];
+          ldv<T, K>(xf, fn, xv);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            const T y0 = wb0 * (we0 * v[0][0][0][t] + we1 * v[0][0][1][t]) +
+                         wb1 * (we0 * v[0][1][0][t] + we1 * v[0][1][1][t]);
+            const T y1 = wb0 * (we0 * v[1][0][0][t] + we1 * v[1][0][1][t]) +
+                         wb1 * (we0 * v[1][1][0][t] + we1 * v[1][1][1][t]);
+            xv[t] += scale * (wa0 * y0 + wa1 * y1);
+          }
+          stv<T, K>(xf, fn, xv);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace fs

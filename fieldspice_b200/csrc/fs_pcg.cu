@@ -19,7 +19,8 @@
 // f - L phi with the FP64 masses, so convergence is always decided on an FP64
 // residual.  Updates trigger when the iterated residual falls below
 // tol*||b~|| (to verify convergence), at the iteration cap, and in mixed mode
-// whenever it has dropped by `delta` since the previous update.
+// whenever it has dropped by a factor `delta` since the previous update (and
+// every kRefreshEvery iterations, which also feeds the stall detector).
 //
 // Each CG iteration is four kernels captured once in a CUDA graph:
 //   K0 p = r + beta p_old                          (streaming, p double-buffered)
@@ -57,7 +58,6 @@ struct RhsState {
   int iters;
   int active;
   int ru;            // reliable update requested
-  int fold;          // x~ must be folded into phi
   int zero;          // b == 0: the solution on free nodes is 0 (SciPy)
   int status;
   int nru;
@@ -79,7 +79,6 @@ struct Control {
   int maxiter;
   int all_done;
   int any_ru;
-  int any_fold;
   int error;    // a bounded wait expired (TMA stage never landed)
   int precond;  // 0: CG on A~ (Jacobi), 1: multigrid-preconditioned CG
   unsigned int tickets[kTickets];
@@ -250,7 +249,6 @@ __global__ void __launch_bounds__(fs::kBlock)
       s.nstall = 0;
       s.iters = 0;
       s.ru = 0;
-      s.fold = 0;
       s.nru = 0;
       s.zero = 0;
       s.status = FS_OK;
@@ -272,7 +270,6 @@ __global__ void __launch_bounds__(fs::kBlock)
       ctl->delta = delta;
       ctl->precond = precond;
       ctl->error = 0;
-      ctl->any_fold = 0;
       refresh_done(st, ctl, K);
     }
   }
@@ -585,24 +582,15 @@ __global__ void __launch_bounds__(fs::kBlock)
   finish_pq<T, K, fs::kBlock>(acc, partials, st, ctl);
 }
 
-// ---- K2: fold a pending correction, x~ += alpha p, r~ -= alpha q, r~.r~ ---------
-// After a reliable update (K3 of the previous iteration) the correction x~
-// it verified is folded into phi here (phi += s x~) and x~ restarts at 0.
+// ---- K2: x~ += alpha p, r~ -= alpha q, r~.r~ --------------------------------------
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_update(Dims d, const T* __restrict__ p, const T* __restrict__ q,
-             T* __restrict__ x, T* __restrict__ r, const double* __restrict__ s64,
-             double* __restrict__ phi, double* __restrict__ partials,
+             T* __restrict__ x, T* __restrict__ r, double* __restrict__ partials,
              RhsState* st, Control* ctl) {
   if (ctl->all_done) return;
   __shared__ T alpha[K];
-  __shared__ int fold[K];
-  __shared__ int any_fold;
-  if (threadIdx.x < K) {
-    alpha[threadIdx.x] = (T)st[threadIdx.x].alpha;
-    fold[threadIdx.x] = st[threadIdx.x].fold;
-  }
-  if (threadIdx.x == 0) any_fold = ctl->any_fold;
+  if (threadIdx.x < K) alpha[threadIdx.x] = (T)st[threadIdx.x].alpha;
   __syncthreads();
   double acc[K];
 #pragma unroll
@@ -614,17 +602,6 @@ __global__ void __launch_bounds__(fs::kBlock)
     fs::ldv_ro<T, K>(q, n, qv);
     fs::ldv<T, K>(x, n, xv);
     fs::ldv<T, K>(r, n, rv);
-    if (any_fold) {
-      const double s = s64[n];
-      if (s != 0.0) {
-#pragma unroll
-        for (int t = 0; t < K; ++t)
-          if (fold[t]) {
-            phi[n * K + t] += (double)xv[t] * s;
-            xv[t] = (T)0;
-          }
-      }
-    }
 #pragma unroll
     for (int t = 0; t < K; ++t) {
       xv[t] += alpha[t] * pv[t];
@@ -640,7 +617,6 @@ __global__ void __launch_bounds__(fs::kBlock)
     fs::grid_total<K>(partials, gridDim.x, tot);
     if (threadIdx.x < K) {
       RhsState& s = st[threadIdx.x];
-      s.fold = 0;
       if (s.active) {
         const double g = tot[threadIdx.x];
         s.iters += 1;
@@ -666,23 +642,46 @@ __global__ void __launch_bounds__(fs::kBlock)
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      ctl->any_fold = 0;
-      refresh_done(st, ctl, K);
-    }
+    if (threadIdx.x == 0) refresh_done(st, ctl, K);
   }
 }
 
-// ---- K3: reliable update: true FP64 residual of phi + s x~ -----------------------
+// ---- K3a/K3b: reliable update ---------------------------------------------------
+// K3a folds the correction accumulated since the last update into the FP64
+// solution (phi += s x~, x~ = 0) for the flagged right-hand sides; K3b then
+// recomputes their TRUE residual r = f - L phi with the FP64 masses, replaces
+// the recurrence residual with it and decides convergence on it.
+template <typename T, int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_fold(Dims d, const double* __restrict__ s64, double* __restrict__ phi,
+           T* __restrict__ x, RhsState* st, Control* ctl) {
+  if (!ctl->any_ru) return;
+  __shared__ int ru[K];
+  if (threadIdx.x < K) ru[threadIdx.x] = st[threadIdx.x].ru;
+  __syncthreads();
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const double s = s64[n];
+    if (s == 0.0) continue;  // x~ is 0 off the free nodes
+    T xv[K];
+    fs::ldv<T, K>(x, n, xv);
+#pragma unroll
+    for (int t = 0; t < K; ++t)
+      if (ru[t]) {
+        phi[n * K + t] += (double)xv[t] * s;
+        xv[t] = (T)0;
+      }
+    fs::stv<T, K>(x, n, xv);
+  }
+}
+
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_reliable(Dims d, const double* __restrict__ mx,
                const double* __restrict__ my, const double* __restrict__ mz,
-               const uint8_t* __restrict__ label,
                const double* __restrict__ s64, const double* __restrict__ phi,
-               const double* __restrict__ f, const T* __restrict__ x,
-               T* __restrict__ r, double* __restrict__ partials, RhsState* st,
-               Control* ctl) {
+               const double* __restrict__ f, T* __restrict__ r,
+               double* __restrict__ partials, RhsState* st, Control* ctl) {
   if (!ctl->any_ru) return;
   __shared__ int ru[K];
   if (threadIdx.x < K) ru[threadIdx.x] = st[threadIdx.x].ru;
@@ -692,28 +691,24 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (int t = 0; t < K; ++t) acc[t] = 0.0;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
-    if (label[n] != FS_LABEL_FREE) continue;
+    const double sc = s64[n];
+    if (sc == 0.0) continue;  // only free nodes carry a residual
     int i, j, k;
     fs::node_ijk(d, n, i, j, k);
-    const double sc = s64[n];
     double c[K], res[K];
-    {
-      T xv[K];
-      fs::ldv_ro<T, K>(x, n, xv);
+    fs::ldv_ro<double, K>(phi, n, c);
+    if (f) {
+      fs::ldv_ro<double, K>(f, n, res);
+    } else {
 #pragma unroll
-      for (int t = 0; t < K; ++t) {
-        c[t] = phi[n * K + t] + (double)xv[t] * sc;
-        res[t] = f ? f[n * K + t] : 0.0;
-      }
+      for (int t = 0; t < K; ++t) res[t] = 0.0;
     }
     auto edge = [&](bool ok, double m, long long nb) {
       if (!ok || m == 0.0) return;
-      const double snb = s64[nb];
-      T xv[K];
-      fs::ldv_ro<T, K>(x, nb, xv);
+      double v[K];
+      fs::ldv_ro<double, K>(phi, nb, v);
 #pragma unroll
-      for (int t = 0; t < K; ++t)
-        res[t] -= m * (c[t] - (phi[nb * K + t] + (double)xv[t] * snb));
+      for (int t = 0; t < K; ++t) res[t] -= m * (c[t] - v[t]);
     };
     edge(i > 0, i > 0 ? mx[n - d.sx] : 0.0, n - d.sx);
     edge(i < d.nx - 1, mx[n], n + d.sx);
@@ -743,7 +738,6 @@ __global__ void __launch_bounds__(fs::kBlock)
         const double g = tot[threadIdx.x];
         const double rn = sqrt(g);
         s.nru += 1;
-        s.fold = 1;
         s.ru = 0;
         s.relres = rn / s.bnorm;
         if (!isfinite(g)) {
@@ -779,10 +773,7 @@ __global__ void __launch_bounds__(fs::kBlock)
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      ctl->any_fold = 1;
-      refresh_done(st, ctl, K);
-    }
+    if (threadIdx.x == 0) refresh_done(st, ctl, K);
   }
 }
 
@@ -792,11 +783,8 @@ __global__ void k_finalize(Dims d, const uint8_t* __restrict__ label,
                            const double* __restrict__ s64,
                            double* __restrict__ phi, T* __restrict__ x,
                            RhsState* st, Control* ctl) {
-  __shared__ int fold[K], zero[K];
-  if (threadIdx.x < K) {
-    fold[threadIdx.x] = st[threadIdx.x].fold;
-    zero[threadIdx.x] = st[threadIdx.x].zero;
-  }
+  __shared__ int zero[K];
+  if (threadIdx.x < K) zero[threadIdx.x] = st[threadIdx.x].zero;
   __syncthreads();
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
@@ -806,20 +794,14 @@ __global__ void k_finalize(Dims d, const uint8_t* __restrict__ label,
     fs::ldv<T, K>(x, n, xv);
 #pragma unroll
     for (int t = 0; t < K; ++t) {
-      if (fold[t]) {
-        phi[n * K + t] += (double)xv[t] * s;
-        xv[t] = (T)0;
-      }
+      phi[n * K + t] += (double)xv[t] * s;  // correction since the last fold
+      xv[t] = (T)0;
       if (zero[t]) phi[n * K + t] = 0.0;
     }
     fs::stv<T, K>(x, n, xv);
   }
   if (fs::last_block(&ctl->tickets[kTicketFin])) {
-    if (threadIdx.x < K) {
-      st[threadIdx.x].fold = 0;
-      st[threadIdx.x].zero = 0;
-    }
-    if (threadIdx.x == 0) ctl->any_fold = 0;
+    if (threadIdx.x < K) st[threadIdx.x].zero = 0;
   }
 }
 
@@ -958,7 +940,7 @@ struct fs_pcg_plan {
   double* partials;
   RhsState* st;
   Control* ctl;
-  int g_init, g_apply, g_pnew, g_update, g_rel, g_fin;
+  int g_init, g_apply, g_pnew, g_update, g_rel, g_fin, g_fold;
   int use_tma;
   CUtensorMap tm_p[2];
   int chunk;
@@ -969,8 +951,9 @@ struct fs_pcg_plan {
   long long launches;
   // Event samples around the kernels of the first iteration of every graph
   // launch: live per-kernel durations for the roofline figures.
-  cudaEvent_t ev[6];
-  double kernel_ms[5];
+  cudaEvent_t ev[8];
+  double kernel_ms[6];
+  int trace;               // record ev[6..7] around fine-level post-smoothing
   long long kernel_samples;
 };
 
@@ -1019,6 +1002,7 @@ struct Impl {
     }
     P->g_update = fs_grid_blocks((const void*)k_update<T, K>, N);
     P->g_rel = fs_grid_blocks((const void*)k_reliable<T, K>, N);
+    P->g_fold = fs_grid_blocks((const void*)k_fold<T, K>, N);
     P->g_fin = fs_grid_blocks((const void*)k_finalize<T, K>, N);
     P->g_rz = fs_grid_blocks((const void*)k_rz<T, K>, N);
   }
@@ -1094,12 +1078,14 @@ struct Impl {
       case 2:
         k_update<T, K><<<P->g_update, fs::kBlock, 0, s>>>(
             P->d, (const T*)P->p[1 - par], (const T*)P->q, (T*)P->x, (T*)P->r,
-            P->s64, P->phi, P->partials, P->st, P->ctl);
+            P->partials, P->st, P->ctl);
         break;
       default:
+        k_fold<T, K><<<P->g_fold, fs::kBlock, 0, s>>>(P->d, P->s64, P->phi,
+                                                      (T*)P->x, P->st, P->ctl);
         k_reliable<T, K><<<P->g_rel, fs::kBlock, 0, s>>>(
-            P->d, P->mx, P->my, P->mz, P->label, P->s64, P->phi, P->f,
-            (const T*)P->x, (T*)P->r, P->partials, P->st, P->ctl);
+            P->d, P->mx, P->my, P->mz, P->s64, P->phi, P->f, (T*)P->r,
+            P->partials, P->st, P->ctl);
         break;
     }
   }
@@ -1169,11 +1155,15 @@ struct Impl {
     }
     *nl += 2;
     const int cc = vcycle(P, l + 1, (const T*)C.b, s, nl, dry);
-    if (!dry)
-      fs::k_mg_prolong<T, K><<<g, fs::kBlock, 0, s>>>(
+    if (!dry) {
+      const int gp = fs_grid_blocks((const void*)fs::k_mg_prolong_cell<T, K>, C.d.N);
+      fs::k_mg_prolong_cell<T, K><<<gp, fs::kBlock, 0, s>>>(
           L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd,
           (T*)L.x[cur], done);
+    }
     ++*nl;
+    const bool tr = !dry && l == 0 && P->trace;
+    if (tr) cudaEventRecordWithFlags(P->ev[6], s, cudaEventRecordExternal);
     for (int k = 0; k < deg; ++k) {  // post-smoothing from the corrected x
       const int out = 1 - cur;
       if (!dry)
@@ -1183,6 +1173,7 @@ struct Impl {
       cur = out;
       ++*nl;
     }
+    if (tr) cudaEventRecordWithFlags(P->ev[7], s, cudaEventRecordExternal);
     return cur;
   }
   // Fix the level-0 output buffer (z) without launching anything; the graph
@@ -1269,7 +1260,9 @@ void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
     dispatch(P, 5 + w, s);  // K0 p update, K1 stencil, K2 update, K3 (parity 0)
   }
   cudaEventRecordWithFlags(P->ev[4], s, cudaEventRecordExternal);
+  P->trace = 1;
   if (P->precond) dispatch(P, 10, s);  // V-cycle and r.z
+  P->trace = 0;
   cudaEventRecordWithFlags(P->ev[5], s, cudaEventRecordExternal);
 }
 
@@ -1365,8 +1358,9 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
     delete P;
     return FS_BAD_ARG;
   }
-  for (int t = 0; t < 6; ++t) P->ev[t] = nullptr;
-  for (int t = 0; t < 5; ++t) P->kernel_ms[t] = 0.0;
+  for (int t = 0; t < 8; ++t) P->ev[t] = nullptr;
+  for (int t = 0; t < 6; ++t) P->kernel_ms[t] = 0.0;
+  P->trace = 0;
   P->kernel_samples = 0;
   auto fail = [&](const char* where, cudaError_t e) {
     fs_pcg_plan_destroy(P);
@@ -1404,7 +1398,7 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   if ((e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking)) !=
       cudaSuccess)
     return fail("cudaStreamCreate", e);
-  for (int t = 0; t < 6; ++t)
+  for (int t = 0; t < 8; ++t)
     if ((e = cudaEventCreate(&P->ev[t])) != cudaSuccess)
       return fail("cudaEventCreate", e);
   cudaGraph_t graph = nullptr;
@@ -1432,7 +1426,11 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
                       fs_rhs_stats* stats, void* stream) {
   if (!P || !(tol > 0.0) || maxiter < 1) return FS_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  const double delta = P->precision == FS_PRECISION_MIXED ? 0.1 : 0.0;
+  // Mixed precision: refresh the residual after a 10x drop under Jacobi CG
+  // (hundreds of FP32 iterations per decade) and after a 1000x drop under
+  // multigrid (a decade every ~2 iterations, so little FP32 drift).
+  const double delta = P->precision != FS_PRECISION_MIXED ? 0.0
+                       : (P->precond ? 1e-3 : 0.1);
   cudaError_t e;
   dispatch(P, 2, s, warm_start ? 1 : 0, tol, maxiter, delta);
   FS_CHECK_LAUNCH("k_init");
@@ -1442,25 +1440,28 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
     FS_CHECK_LAUNCH("multigrid V-cycle");
     launches += P->launches_per_iter;
   }
-  for (int t = 0; t < 5; ++t) P->kernel_ms[t] = 0.0;
+  for (int t = 0; t < 6; ++t) P->kernel_ms[t] = 0.0;
   P->kernel_samples = 0;
   const long long max_chunks = (long long)maxiter / P->chunk + 4;
   int timed_out = 1;
   for (long long c = 0; c < max_chunks; ++c) {
     if ((e = cudaGraphLaunch(P->exec, s)) != cudaSuccess)
       return fs_cuda_status("cudaGraphLaunch", e);
-    launches += (4LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
+    launches += (5LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
     if ((e = cudaMemcpyAsync(P->h_flag, &P->ctl->all_done, sizeof(int),
                              cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return fs_cuda_status("cudaMemcpyAsync", e);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
       return fs_cuda_status("cudaStreamSynchronize", e);
-    float ms[5];
+    float ms[6] = {0, 0, 0, 0, 0, 0};
     bool ok = true;
     for (int t = 0; t < 5 && ok; ++t)
       ok = cudaEventElapsedTime(&ms[t], P->ev[t], P->ev[t + 1]) == cudaSuccess;
+    if (ok && P->precond)
+      ok = cudaEventElapsedTime(&ms[5], P->ev[6], P->ev[7]) == cudaSuccess;
     if (ok) {
-      for (int t = 0; t < 5; ++t) P->kernel_ms[t] += ms[t];
+      ms[5] /= (float)kSmoothDeg;  // per launch
+      for (int t = 0; t < 6; ++t) P->kernel_ms[t] += ms[t];
       P->kernel_samples += 1;
     } else {
       (void)cudaGetLastError();  // timing unavailable: not a solve failure
@@ -1510,14 +1511,14 @@ long long fs_pcg_plan_launches(const fs_pcg_plan* P) {
 int fs_pcg_plan_kernel_times(const fs_pcg_plan* P, double* ms,
                              long long* samples) {
   if (!P || !ms || !samples) return FS_BAD_ARG;
-  for (int t = 0; t < 5; ++t) ms[t] = P->kernel_ms[t];
+  for (int t = 0; t < 6; ++t) ms[t] = P->kernel_ms[t];
   *samples = P->kernel_samples;
   return FS_OK;
 }
 
 int fs_pcg_plan_destroy(fs_pcg_plan* P) {
   if (!P) return FS_OK;
-  for (int t = 0; t < 6; ++t)
+  for (int t = 0; t < 8; ++t)
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->cap) cudaStreamDestroy(P->cap);

@@ -321,8 +321,9 @@ class EliminatedSystem:
     def kernel_times(self) -> dict:
         """Per-kernel device time sampled during the last solve (ms per
         launch): p update, stencil (A~p, p.q), update (x, r, r.r), reliable
-        update, and the preconditioner (V-cycle + r.z)."""
-        ms = (ctypes.c_double * 5)()
+        update, the preconditioner (V-cycle + r.z) and one fine-level
+        multigrid smoothing step."""
+        ms = (ctypes.c_double * 6)()
         ns = ctypes.c_longlong()
         L.check("fs_pcg_plan_kernel_times",
                 L.load_library().fs_pcg_plan_kernel_times(self._last_plan, ms,
@@ -330,7 +331,7 @@ class EliminatedSystem:
         n = max(ns.value, 1)
         return {"samples": ns.value, "pupdate_ms": ms[0] / n, "stencil_ms": ms[1] / n,
                 "update_ms": ms[2] / n, "reliable_ms": ms[3] / n,
-                "precond_ms": ms[4] / n}
+                "precond_ms": ms[4] / n, "smoother_ms": ms[5] / n}
 
     def close(self) -> None:
         lib = L.load_library()

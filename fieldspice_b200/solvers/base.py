@@ -14,7 +14,8 @@ from typing import Any, Callable, Sequence
 
 import numpy as np
 
-__all__ = ["ConvergenceError", "SolverConfig", "GPUConfig", "Terminal", "Result"]
+__all__ = ["ConvergenceError", "SolverConfig", "GPUConfig", "Terminal", "Result",
+           "resolve_preconditioner"]
 
 
 class ConvergenceError(RuntimeError):
@@ -62,16 +63,37 @@ class GPUConfig:
         in FP64 if the FP32 iterations stall on a mode below FP32 resolution
         (extreme conductivity contrast).
     preconditioner
-        ``"jacobi"`` (CG on the equilibrated system, the reference's method)
-        or ``"mg"`` (a geometric-multigrid V-cycle as the CG preconditioner;
-        same FP64 stopping rule).
+        ``"jacobi"`` (CG on the equilibrated system, the reference's CG
+        method), ``"mg"`` (a geometric-multigrid V-cycle as the CG
+        preconditioner; same FP64 stopping rule), or ``None``: chosen from
+        ``SolverConfig.linear_solver`` (:func:`resolve_preconditioner`).
     maxiter
         Iteration cap; ``None`` uses the reference's ``max(500, 10*sqrt(n))``
         (``poisson.py:535-536``).
     """
     precision: str = "auto"
-    preconditioner: str = "jacobi"
+    preconditioner: str | None = None
     maxiter: int | None = None
+
+
+def resolve_preconditioner(cfg, gpu) -> str:
+    """GPU preconditioner for a reference ``SolverConfig.linear_solver``.
+
+    ``"cg"`` is the reference's Jacobi-preconditioned CG; ``"auto"``,
+    ``"amg"`` and ``"direct"`` map to multigrid-preconditioned CG (the
+    reference's ``"auto"`` path on large 3-D systems is AMG-preconditioned
+    CG, ``fieldspice/solvers/poisson.py:391-398``).  An explicit
+    ``GPUConfig.preconditioner`` wins.
+    """
+    if gpu is not None and gpu.preconditioner is not None:
+        if gpu.preconditioner not in ("jacobi", "mg"):
+            raise ValueError(f"unknown preconditioner {gpu.preconditioner!r}")
+        return gpu.preconditioner
+    want = getattr(cfg, "linear_solver", "auto")
+    if want not in ("auto", "direct", "cg", "amg"):
+        raise ValueError(f"unknown linear_solver {want!r}; expected one of "
+                         "'auto', 'direct', 'cg', 'amg'")
+    return "jacobi" if want == "cg" else "mg"
 
 
 @dataclass

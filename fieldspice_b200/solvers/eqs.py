@@ -29,7 +29,7 @@ import numpy as np
 from .. import _lib as L
 from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes
 from ..device import DeviceOperator, EliminatedSystem, d2h, h2d, upload_groups
-from .base import GPUConfig, Result, SolverConfig
+from .base import GPUConfig, Result, SolverConfig, resolve_preconditioner
 from .poisson import check_terminals, raise_on_status
 
 __all__ = ["EQSSolver"]
@@ -128,7 +128,7 @@ class EQSSolver:
             label[h2d(fixed.astype(np.int64), torch.int64, dev)] = L.LABEL_FIXED
         system = EliminatedSystem(op, label, 1, precision=self.gpu.precision,
                                   with_source=rhs_dev is not None,
-                                  preconditioner=self.gpu.preconditioner)
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
         if fixed.size:
             system.phi[h2d(fixed.astype(np.int64), torch.int64, dev)] = \
                 h2d(vals, torch.float64, dev)
@@ -211,7 +211,7 @@ class EQSSolver:
             label[fixed_d] = L.LABEL_FIXED
         system = EliminatedSystem(K, label, 1, precision=self.gpu.precision,
                                   with_source=True,
-                                  preconditioner=self.gpu.preconditioner)
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
         system.phi.copy_(h2d(phi0, torch.float64, dev))
         prev = system.phi.clone()
 

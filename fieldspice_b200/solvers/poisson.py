@@ -21,7 +21,7 @@ from .. import _lib as L
 from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes
 from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d,
                       pad_rhs, upload_groups)
-from .base import ConvergenceError, GPUConfig, Result, SolverConfig
+from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
 
 __all__ = ["PoissonSolver", "check_terminals", "as_cell_array", "raise_on_status"]
 
@@ -219,7 +219,7 @@ class PoissonSolver:
         C, q_shield, info = extract_capacitance(
             self.op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,
-            preconditioner=self.gpu.preconditioner)
+            preconditioner=resolve_preconditioner(self.cfg, self.gpu))
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         rep["terminals"] = tuple(t.name for t in terms)
@@ -292,7 +292,7 @@ class PoissonSolver:
         with_src = rho_node is not None
         system = EliminatedSystem(self.op, label, 1, precision=self.gpu.precision,
                                   with_source=with_src,
-                                  preconditioner=self.gpu.preconditioner)
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
         system.phi.zero_()
         system.phi[fixed_d] = torch.as_tensor(vals, dtype=torch.float64, device=dev)
         if with_src:

@@ -156,10 +156,11 @@ const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* plan);
 /* Number of kernel launches issued by the last solve (host count).          */
 long long fs_pcg_plan_launches(const fs_pcg_plan* plan);
 /* Device time of the CG kernels -- p update (p = r + beta p), stencil
- * (A~p, p.q), update (x, r, r.r), reliable update, and the preconditioner
- * (V-cycle and r.z; 0 without one) -- summed over the samples taken during
- * the last solve: the first CG iteration of every graph launch is bracketed
- * by CUDA events.  ms: host array of 5.                                     */
+ * (A~p, p.q), update (x, r, r.r), reliable update, the preconditioner
+ * (V-cycle and r.z; 0 without one) and one fine-level multigrid smoothing
+ * step (average over the post-smoothing launches) -- summed over the samples
+ * taken during the last solve: the first CG iteration of every graph launch
+ * is bracketed by CUDA events.  ms: host array of 6.                        */
 int fs_pcg_plan_kernel_times(const fs_pcg_plan* plan, double* ms,
                              long long* samples);
 int fs_pcg_plan_destroy(fs_pcg_plan* plan);

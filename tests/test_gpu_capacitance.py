@@ -24,8 +24,9 @@ def _layered(d):
     return g, terms
 
 
+@pytest.mark.parametrize("preconditioner", ["jacobi", "mg"])
 @pytest.mark.parametrize("precision", PRECISIONS)
-def test_readme_capacitor(cuda, golden, precision):
+def test_readme_capacitor(cuda, golden, precision, preconditioner):
     from fieldspice_b200 import extraction as EX
     from fieldspice_b200 import workloads as W
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
@@ -35,7 +36,8 @@ def test_readme_capacitor(cuda, golden, precision):
     rep = {}
     C = EX.capacitance_matrix(w.grid(), w.eps_cell, terms,
                               config=SolverConfig(tol=1e-13), report=rep,
-                              gpu=GPUConfig(precision=precision))
+                              gpu=GPUConfig(precision=precision,
+                                            preconditioner=preconditioner))
     assert C[0, 0] == pytest.approx(w.meta["C_ref"], rel=1e-12)
     assert np.allclose(C, golden("readme")["C"], rtol=1e-12, atol=0)
     assert rep["asymmetry_rel"] < 1e-9 and rep["row_sum_rel"] < 1e-9
@@ -43,16 +45,17 @@ def test_readme_capacitor(cuda, golden, precision):
     assert max(rep["linear"]["relres_fp64"]) < 1e-13
 
 
+@pytest.mark.parametrize("preconditioner", ["jacobi", "mg"])
 @pytest.mark.parametrize("precision", PRECISIONS)
 @pytest.mark.parametrize("tag", ["layered_32x32x16_s0", "layered_48x48x24_s1"])
-def test_layered_matches_reference(cuda, golden, tag, precision):
+def test_layered_matches_reference(cuda, golden, tag, precision, preconditioner):
     from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
     from fieldspice_b200.solvers.poisson import PoissonSolver
     d = golden(tag)
     g, terms = _layered(d)
     ps = PoissonSolver(g, d["eps_cell"], SolverConfig(tol=1e-10),
-                       gpu=GPUConfig(precision=precision))
+                       gpu=GPUConfig(precision=precision, preconditioner=preconditioner))
     rep = {}
     C = ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)), report=rep)
     ref = d["C"]
@@ -63,6 +66,24 @@ def test_layered_matches_reference(cuda, golden, tag, precision):
     assert max(rep["linear"]["relres_fp64"]) < 1e-10
     assert rep["max_offdiag"] <= 0.0
     assert rep["asymmetry_rel"] < 1e-8
+
+
+def test_multigrid_cuts_iterations(cuda, golden):
+    """The multigrid V-cycle must pay for itself: >5x fewer iterations than
+    Jacobi CG on the same system, same answer."""
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
+    from fieldspice_b200.solvers.poisson import PoissonSolver
+    d = golden("layered_48x48x24_s1")
+    g, terms = _layered(d)
+    its = {}
+    for pc in ("jacobi", "mg"):
+        ps = PoissonSolver(g, d["eps_cell"], SolverConfig(tol=1e-10),
+                           gpu=GPUConfig(preconditioner=pc))
+        rep = {}
+        ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)), report=rep)
+        its[pc] = max(rep["linear"]["iterations"])
+    assert its["mg"] * 5 < its["jacobi"], its
 
 
 def test_many_terminals_and_padding(cuda):

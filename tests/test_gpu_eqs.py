@@ -88,8 +88,9 @@ def test_terminal_currents_conserve(cuda, precision):
     assert np.abs(total).max() / scale < 1e-8
 
 
+@pytest.mark.parametrize("preconditioner", ["mg", "jacobi"])
 @pytest.mark.parametrize("precision", ["auto", "fp64"])
-def test_interconnect_ramp_matches_reference(cuda, golden, precision):
+def test_interconnect_ramp_matches_reference(cuda, golden, precision, preconditioner):
     """Copper next to oxide: the floating copper box is an eigenvalue of
     1.5e-7 of the equilibrated operator, below FP32 resolution, so "auto"
     must notice the stall and finish in FP64."""
@@ -106,7 +107,7 @@ def test_interconnect_ramp_matches_reference(cuda, golden, precision):
     ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
     terms = [Terminal("port0", ports[0], voltage=ramp), Terminal("port1", ports[1], voltage=0.0)]
     s = EQSSolver(g, d["ic_eps"], d["ic_sig"], SolverConfig(tol=1e-12),
-                  gpu=GPUConfig(precision=precision))
+                  gpu=GPUConfig(precision=precision, preconditioner=preconditioner))
     r = s.solve(terms, t_end=20e-12, dt=1e-12, bc=BoundarySpec(zlo=Dirichlet(0.0)), store=True)
     scale = np.abs(d["ic_i0"]).max()
     assert np.abs(r.i("port0") - d["ic_i0"]).max() / scale < 1e-7

@@ -130,3 +130,14 @@ def test_prepare_bc_defaults_to_neumann():
 def test_solver_config_defaults_match_reference():
     c = SolverConfig()
     assert c.tol == 1e-10 and c.linear_solver == "auto"
+
+
+def test_preconditioner_follows_linear_solver():
+    from fieldspice_b200.solvers.base import GPUConfig, resolve_preconditioner
+    assert resolve_preconditioner(SolverConfig(linear_solver="cg"), None) == "jacobi"
+    for ls in ("auto", "amg", "direct"):
+        assert resolve_preconditioner(SolverConfig(linear_solver=ls), None) == "mg"
+    assert resolve_preconditioner(SolverConfig(linear_solver="cg"),
+                                  GPUConfig(preconditioner="mg")) == "mg"
+    with pytest.raises(ValueError):
+        resolve_preconditioner(SolverConfig(linear_solver="lu"), None)
