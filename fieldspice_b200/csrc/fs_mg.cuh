@@ -182,6 +182,77 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// Degree-2 pre-smoothing from x = 0 in residual form.  The Chebyshev steps
+//   x1 = c0 b,  d1 = cd1 x1 + cr1 (b - A~ x1),  x2 = x1 + d1
+// need r1 = b - A~ x1 and r2 = r1 - A~ d1 for the restriction; carrying the
+// residual along saves the separate residual pass over x2.
+// pre0: x1 = c0 b, r1 = b - c0 A~ b.
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_pre0(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+              const T* __restrict__ ez, const T* __restrict__ b,
+              T* __restrict__ x1, T* __restrict__ r1, T c0,
+              const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T ab[K], bv[K], xo[K];
+    apply_eq<T, K>(d, ex, ey, ez, b, n, ab);
+    ldv_ro<T, K>(b, n, bv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      xo[t] = c0 * bv[t];
+      ab[t] = bv[t] - c0 * ab[t];
+    }
+    stv<T, K>(x1, n, xo);
+    stv<T, K>(r1, n, ab);
+  }
+}
+
+// pre1: d1 = cd x1 + cr r1 (formed at the node and its six neighbours),
+// x2 = x1 + d1, r2 = r1 - A~ d1.
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_pre1(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+              const T* __restrict__ ez, const T* __restrict__ x1,
+              const T* __restrict__ r1, T* __restrict__ x2, T* __restrict__ r2,
+              T cd, T cr, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_ijk(d, n, i, j, k);
+    T xv[K], rv[K], dc[K], ad[K];
+    ldv_ro<T, K>(x1, n, xv);
+    ldv_ro<T, K>(r1, n, rv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      dc[t] = cd * xv[t] + cr * rv[t];
+      ad[t] = dc[t];
+    }
+    auto nbr = [&](T m, long long nb) {
+      T a[K], c[K];
+      ldv_ro<T, K>(x1, nb, a);
+      ldv_ro<T, K>(r1, nb, c);
+#pragma unroll
+      for (int t = 0; t < K; ++t) ad[t] -= m * (cd * a[t] + cr * c[t]);
+    };
+    if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
+    if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
+    if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
+    if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
+    if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
+    if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      xv[t] += dc[t];
+      rv[t] -= ad[t];
+    }
+    stv<T, K>(x2, n, xv);
+    stv<T, K>(r2, n, rv);
+  }
+}
+
 // Per-axis trilinear weights of fine index i onto coarse index I (0 if none).
 __device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
   const int dlt = i - 2 * I;

@@ -809,11 +809,18 @@ size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // ---- multigrid hierarchy ---------------------------------------------------------
 constexpr int kMaxLevels = 12;
-constexpr int kSmoothDeg = 2;          // Chebyshev degree, pre and post
-constexpr double kSmoothLo = 0.3;      // smoothing interval [lo, 2] of A~
-constexpr int kCoarseDeg = 24;         // coarsest-level Chebyshev degree
-constexpr double kCoarseLo = 0.03;
-constexpr long long kCoarsestNodes = 512;
+// Multigrid parameters (process-wide; a plan copies them when created).
+// Defaults from a sweep on the 256x256x128 8-terminal extraction: degree-2
+// smoothing on [0.3, 2] and a degree-32 Chebyshev solve on a coarsest level
+// of at most 4096 nodes gave the shortest extraction (20-21 iterations).
+struct MgParams {
+  int smooth_deg = 2;          // Chebyshev degree, pre and post
+  double smooth_lo = 0.3;      // smoothing interval [lo, 2] of A~
+  int coarse_deg = 32;         // coarsest-level Chebyshev degree
+  double coarse_lo = 0.03;
+  long long coarsest_nodes = 4096;
+};
+MgParams g_mg;
 
 struct MgLevel {
   Dims d;
@@ -827,11 +834,11 @@ struct MgLevel {
       off_x[2], off_b, off_dv, off_res;
 };
 
-int mg_dims(const Dims& fine, Dims* out) {
+int mg_dims(const Dims& fine, long long coarsest, Dims* out) {
   int nl = 0;
   Dims d = fine;
   out[nl++] = d;
-  while (nl < kMaxLevels && d.N > kCoarsestNodes && d.nx >= 5 && d.ny >= 5 &&
+  while (nl < kMaxLevels && d.N > coarsest && d.nx >= 5 && d.ny >= 5 &&
          d.nz >= 5) {
     d = fs::make_dims((d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2);
     out[nl++] = d;
@@ -894,7 +901,7 @@ Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
   L.nlev = 0;
   if (precond == FS_PRECOND_MG) {
     Dims dl[kMaxLevels];
-    L.nlev = mg_dims(d, dl);
+    L.nlev = mg_dims(d, g_mg.coarsest_nodes, dl);
     for (int l = 0; l < L.nlev; ++l) {
       MgLevel& m = L.lev[l];
       m = MgLevel{};
@@ -931,6 +938,7 @@ struct fs_pcg_plan {
   void* z;                 // preconditioned residual (level-0 V-cycle output)
   int g_rz;
   long long launches_per_iter;
+  MgParams mg;
   const double *mx, *my, *mz;
   double* phi;
   const double* f;
@@ -1128,32 +1136,49 @@ struct Impl {
     MgLevel& L = P->lev[l];
     const int* done = &P->ctl->all_done;
     const bool last = l == P->nlev - 1;
-    const int deg = last ? kCoarseDeg : kSmoothDeg;
+    const int deg = last ? P->mg.coarse_deg : P->mg.smooth_deg;
     double cd[64], cr[64];
-    cheb_coeffs(deg, last ? kCoarseLo : kSmoothLo, 2.0, cd, cr);
+    cheb_coeffs(deg, last ? P->mg.coarse_lo : P->mg.smooth_lo, 2.0, cd, cr);
     const T *e0 = (const T*)L.em[0], *e1 = (const T*)L.em[1], *e2 = (const T*)L.em[2];
     const int g = fs_grid_blocks((const void*)fs::k_mg_cheb<T, K>, L.d.N);
     int cur = 0;
-    for (int k = 0; k < deg; ++k) {  // pre-smoothing (or coarse solve) from 0
-      const int out = k == 0 ? 0 : 1 - cur;
-      if (!dry)
-        fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
-            L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
-            (T)cd[k], (T)cr[k], k == 0 ? 1 : 0, done);
-      cur = out;
-      ++*nl;
+    // Degree-2 pre-smoothing carries its residual along (x in x[1], the
+    // residual in dv); otherwise Chebyshev steps then a residual pass.
+    const bool resform = !last && deg == 2;
+    const T* rfine = (const T*)L.res;
+    if (resform) {
+      if (!dry) {
+        fs::k_mg_pre0<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, b, (T*)L.x[0], (T*)L.res, (T)cr[0], done);
+        fs::k_mg_pre1<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[0], (const T*)L.res, (T*)L.x[1],
+            (T*)L.dv, (T)cd[1], (T)cr[1], done);
+      }
+      cur = 1;
+      rfine = (const T*)L.dv;
+      *nl += 2;
+    } else {
+      for (int k = 0; k < deg; ++k) {  // pre-smoothing (or coarse solve) from 0
+        const int out = k == 0 ? 0 : 1 - cur;
+        if (!dry)
+          fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
+              L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
+              (T)cd[k], (T)cr[k], k == 0 ? 1 : 0, done);
+        cur = out;
+        ++*nl;
+      }
     }
     if (last) return cur;
     MgLevel& C = P->lev[l + 1];
     const int gc = fs_grid_blocks((const void*)fs::k_mg_restrict<T, K>, C.d.N);
     if (!dry) {
-      fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
-          L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
+      if (!resform)
+        fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
       fs::k_mg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
-          L.d, C.d, (const T*)L.res, (const T*)L.sd, (const T*)C.s, (T*)C.b,
-          done);
+          L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
     }
-    *nl += 2;
+    *nl += resform ? 1 : 2;
     const int cc = vcycle(P, l + 1, (const T*)C.b, s, nl, dry);
     if (!dry) {
       const int gp = fs_grid_blocks((const void*)fs::k_mg_prolong_cell<T, K>, C.d.N);
@@ -1270,6 +1295,20 @@ void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
 
 extern "C" {
 
+int fs_mg_set_params(int smooth_deg, double smooth_lo, int coarse_deg,
+                     double coarse_lo, long long coarsest_nodes) {
+  if (smooth_deg < 1 || smooth_deg > 16 || coarse_deg < 1 || coarse_deg > 64 ||
+      !(smooth_lo > 0.0 && smooth_lo < 2.0) || !(coarse_lo > 0.0 && coarse_lo < 2.0) ||
+      coarsest_nodes < 8)
+    return FS_BAD_ARG;
+  g_mg.smooth_deg = smooth_deg;
+  g_mg.smooth_lo = smooth_lo;
+  g_mg.coarse_deg = coarse_deg;
+  g_mg.coarse_lo = coarse_lo;
+  g_mg.coarsest_nodes = coarsest_nodes;
+  return FS_OK;
+}
+
 int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
                            int precond, size_t* bytes) {
   if (nx < 2 || ny < 2 || nz < 2 || !valid_nrhs(nrhs) || !bytes) return FS_BAD_ARG;
@@ -1303,6 +1342,7 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   P->nrhs = nrhs;
   P->precision = precision;
   P->precond = precond == FS_PRECOND_MG ? 1 : 0;
+  P->mg = g_mg;
   P->launches_per_iter = 0;
   P->mx = mx;
   P->my = my;
@@ -1460,7 +1500,7 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
     if (ok && P->precond)
       ok = cudaEventElapsedTime(&ms[5], P->ev[6], P->ev[7]) == cudaSuccess;
     if (ok) {
-      ms[5] /= (float)kSmoothDeg;  // per launch
+      ms[5] /= (float)P->mg.smooth_deg;  // per launch
       for (int t = 0; t < 6; ++t) P->kernel_ms[t] += ms[t];
       P->kernel_samples += 1;
     } else {

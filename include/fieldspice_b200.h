@@ -151,6 +151,13 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
  * FS_NAN on breakdown, FS_TIMEOUT if a staged load never arrived.           */
 int fs_pcg_plan_solve(fs_pcg_plan* plan, int warm_start, double tol,
                       int maxiter, fs_rhs_stats* stats, void* stream);
+/* Multigrid parameters for plans created after the call (process-wide):
+ * Chebyshev smoothing degree (pre and post) and the lower end of its
+ * interval [smooth_lo, 2] on the unit-diagonal level operators, the
+ * coarsest level's degree and interval, and the node count at or below
+ * which coarsening stops.  Defaults: 2, 0.3, 32, 0.03, 4096.               */
+int fs_mg_set_params(int smooth_deg, double smooth_lo, int coarse_deg,
+                     double coarse_lo, long long coarsest_nodes);
 /* Label array after classification (free / fixed / solo / pinned), device. */
 const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* plan);
 /* Number of kernel launches issued by the last solve (host count).          */

@@ -73,6 +73,16 @@ def test_workspace_sizes_and_bad_arguments(dll):
     assert dll.fs_quadform_workspace_bytes(17, ctypes.byref(nb)) == L.FS_BAD_ARG
 
 
+def test_multigrid_parameters_are_validated(dll):
+    # host-only setter: checks its arguments, touches no device
+    assert dll.fs_mg_set_params(0, 0.3, 32, 0.03, 4096) == L.FS_BAD_ARG
+    assert dll.fs_mg_set_params(2, 2.0, 32, 0.03, 4096) == L.FS_BAD_ARG
+    assert dll.fs_mg_set_params(2, 0.3, 65, 0.03, 4096) == L.FS_BAD_ARG
+    assert dll.fs_mg_set_params(2, 0.3, 32, 0.0, 4096) == L.FS_BAD_ARG
+    assert dll.fs_mg_set_params(2, 0.3, 32, 0.03, 4) == L.FS_BAD_ARG
+    assert dll.fs_mg_set_params(2, 0.3, 32, 0.03, 4096) == L.FS_OK
+
+
 def test_library_is_sm100a_only():
     # the build flags target sm_100a and nothing else
     from fieldspice_b200 import _build

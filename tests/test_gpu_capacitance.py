@@ -86,6 +86,30 @@ def test_multigrid_cuts_iterations(cuda, golden):
     assert its["mg"] * 5 < its["jacobi"], its
 
 
+@pytest.mark.parametrize("params", [(3, 0.3, 24, 0.03, 512), (1, 0.5, 8, 0.05, 64)])
+def test_multigrid_parameters(cuda, golden, params):
+    """Non-default smoothing degrees (the plain Chebyshev pre-smoothing path,
+    not the degree-2 residual form) and coarsest sizes give the same C."""
+    from fieldspice_b200 import _lib as L
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
+    from fieldspice_b200.solvers.poisson import PoissonSolver
+    d = golden("layered_48x48x24_s1")
+    g, terms = _layered(d)
+    L.check("fs_mg_set_params", L.lib().fs_mg_set_params(*params))
+    try:
+        ps = PoissonSolver(g, d["eps_cell"], SolverConfig(tol=1e-10),
+                           gpu=GPUConfig(preconditioner="mg"))
+        rep = {}
+        C = ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)), report=rep)
+    finally:
+        L.check("fs_mg_set_params", L.lib().fs_mg_set_params(2, 0.3, 32, 0.03, 4096))
+    scale = np.abs(np.diag(d["C"])).max()
+    assert np.abs(C - d["C"]).max() / scale <= 1e-9
+    assert max(rep["linear"]["relres_fp64"]) < 1e-10
+    assert max(rep["linear"]["iterations"]) < 100
+
+
 def test_many_terminals_and_padding(cuda):
     """19 terminals: one 16-RHS block plus a padded 4-RHS block; matches the
     oracle run on the same inputs."""

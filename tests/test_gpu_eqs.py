@@ -59,8 +59,11 @@ def test_initial_condition_is_the_capacitive_divider(cuda):
 
 
 def test_matches_reference_rc_transient(cuda, golden):
+    # the reference factorises this small system (exact solve); the GPU
+    # iterates to relres 1e-13 so that 400 steps of accumulated solver error
+    # stay inside 1e-9 V
     d = golden("eqs")
-    r, vm, ana, _, _ = _run(50)
+    r, vm, ana, _, _ = _run(50, tol=1e-13)
     assert np.abs(vm - d["spt50_vm"]).max() < 1e-9
     scale = np.abs(d["spt50_i_hi"]).max()
     assert np.abs(r.i("hi") - d["spt50_i_hi"]).max() / scale < 1e-7
@@ -81,8 +84,9 @@ def test_backward_euler_is_first_order_and_matches_analytic(cuda):
 @pytest.mark.parametrize("precision", ["auto", "fp64"])
 def test_terminal_currents_conserve(cuda, precision):
     # The imbalance equals the summed free-node residual, so it tracks the
-    # CG tolerance (the reference factorises this case directly): tol 1e-13.
-    r, *_ = _run(100, tol=1e-13, precision=precision)
+    # CG tolerance (the reference factorises this case directly): with the
+    # step's right-hand side ~1e5 x the current, tol 1e-14 keeps it < 1e-8.
+    r, *_ = _run(100, tol=1e-14, precision=precision)
     total = r.i("hi") + r.i("lo")
     scale = max(np.abs(r.i("hi")).max(), 1e-30)
     assert np.abs(total).max() / scale < 1e-8
