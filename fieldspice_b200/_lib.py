@@ -61,6 +61,14 @@ _SIGNATURES = {
                                    POINTER(c_void_p), c_void_p]),
     "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
                                   POINTER(FsRhsStats), c_void_p]),
+    "fs_pcg_plans_solve": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p), c_int,
+                                   c_double, c_int, POINTER(POINTER(FsRhsStats)),
+                                   POINTER(c_int)]),
+    "fs_conv3d_pack_weights": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "fs_conv3d_bf16": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p,
+                               c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
+                               c_int, c_int, c_int, c_int, c_int, c_int, c_void_p,
+                               c_void_p]),
     "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
     "fs_pcg_plan_launches": (c_longlong, [c_void_p]),

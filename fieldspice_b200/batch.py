@@ -1,0 +1,232 @@
+"""Capacitance extraction of many independent geometries at once.
+
+The reference extracts one geometry per ``capacitance_matrix`` call
+(``fieldspice/extraction.py:41-56`` -> ``solvers/poisson.py:1100-1249``).
+:func:`capacitance_matrices` takes a batch of uneven geometries, builds one
+CG plan per geometry (all of its terminals as one block of right-hand sides)
+and hands every plan to ``fs_pcg_plans_solve``, which runs them together on a
+pool of CUDA streams: one graph chunk per unfinished geometry per round, so
+the iterations of small geometries overlap those of large ones.  Charges are
+integrated per geometry in FP64 exactly as in a single extraction.
+
+With a process group of several ranks (one per GPU), the geometries are
+shared out by estimated cost (nodes x padded RHS, longest first onto the
+least-loaded rank), every rank extracts its share, and one all-gather of the
+small C matrices returns the whole batch, in input order, on every rank.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Any, Callable, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from .boundaries import dirichlet_nodes
+from .device import DeviceOperator, EliminatedSystem, MAX_RHS, h2d, pad_rhs, upload_groups
+from .solvers.base import GPUConfig, SolverConfig, resolve_preconditioner
+from .solvers.poisson import (PoissonSolver, as_cell_array, capacitance_report,
+                              check_terminals, prepare_bc, raise_on_status)
+
+__all__ = ["capacitance_matrices", "shard_by_cost", "problem_cost"]
+
+
+def problem_cost(problem) -> float:
+    """Work estimate of one extraction: nodes x padded RHS width."""
+    grid, _, terms = problem[:3]
+    return float(np.prod(grid.shape_nodes)) * pad_rhs(min(len(terms), MAX_RHS))
+
+
+def shard_by_cost(costs: Sequence[float], world: int) -> list[list[int]]:
+    """Longest-processing-time assignment of items to ``world`` ranks.
+
+    Returns, per rank, the item indices it owns (ascending).  Ties go to the
+    lower rank, so every rank computes the same assignment.
+    """
+    if world < 1:
+        raise ValueError("world size must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda w: (load[w], w))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(o) for o in out]
+
+
+class _Extraction:
+    """One geometry's eliminated system, excitations and charge groups."""
+
+    def __init__(self, grid, eps_cell, terminals, bc, cfg, gcfg):
+        import torch
+        self.grid = grid
+        eps = as_cell_array(eps_cell, grid, "eps_cell")
+        if np.any(eps <= 0.0):
+            raise ValueError("eps_cell must be strictly positive [F/m]")
+        if float(eps.min()) >= 1e-6:
+            raise ValueError("eps_cell looks like a RELATIVE permittivity; "
+                             "pass the absolute value in F/m")
+        self.terms = check_terminals(terminals, grid)
+        nt = len(self.terms)
+        if nt == 0:
+            raise ValueError("capacitance extraction needs at least one terminal")
+        bc = prepare_bc(bc, grid)
+        self.op = DeviceOperator(grid, eps)
+        dev = self.op.dev
+        wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
+        term_nodes = [np.asarray(t.nodes, np.int64) for t in self.terms]
+        shield = np.setdiff1d(wall_idx, np.concatenate(term_nodes))
+        term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
+        label = torch.zeros(self.op.N, dtype=torch.uint8, device=dev)
+        if wall_idx.size:
+            label[h2d(wall_idx.astype(np.int64), torch.int64, dev)] = L.LABEL_FIXED
+        for n in term_dev:
+            label[n] = L.LABEL_FIXED
+        self.has_shield = shield.size > 0
+        groups = term_dev + ([h2d(shield.astype(np.int64), torch.int64, dev)]
+                             if self.has_shield else [])
+        self.groups = groups
+        self.gdev = upload_groups(groups, dev)
+        self.tol = float(cfg.tol)
+        self.system = EliminatedSystem(
+            self.op, label, nt, precision=gcfg.precision,
+            preconditioner=resolve_preconditioner(cfg, gcfg))
+        self.maxiter = (self.system.default_maxiter() if gcfg.maxiter is None
+                        else int(gcfg.maxiter))
+        group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)
+        for c, n in enumerate(term_dev):
+            group[n] = c
+        nx, ny, nz = self.op.shape
+        L.check("fs_fill_unit_excitation", L.lib().fs_fill_unit_excitation(
+            L.ptr(group), L.ptr(self.system.label_in), L.ptr(self.system.phi),
+            nx, ny, nz, self.system.k, L.stream_ptr()))
+
+    def collect(self, stats: list[dict]) -> tuple[np.ndarray, dict]:
+        nt = len(self.terms)
+        k = self.system.k
+        Q = self.op.group_sums(self.system.phi, self.groups, nrhs=k, nodes_dev=self.gdev)
+        C = np.array(Q[:nt, :nt], dtype=float)
+        q_shield = np.array(Q[nt, :nt]) if self.has_shield else np.zeros(nt)
+        info = {"method": f"gpu-cg-{self.system.preconditioner}-{self.system.mode}",
+                "n": self.op.N, "iterations": [s["iterations"] for s in stats],
+                "relres_fp64": [s["relres"] for s in stats],
+                "residual": max(s["relres"] for s in stats),
+                "fp64_fallback": bool(self.system.fell_back),
+                "symmetric": True, "equilibrated": True}
+        rep = capacitance_report(C, q_shield, info)
+        rep["terminals"] = tuple(t.name for t in self.terms)
+        return 0.5 * (C + C.T), rep
+
+    def close(self):
+        self.system.close()
+
+
+def _stats_list(arr, n):
+    return [{"iterations": s.iterations, "status": s.status, "relres": s.relres,
+             "bnorm": s.bnorm, "reliable_updates": s.reliable_updates}
+            for s in arr[:n]]
+
+
+def _extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
+    """Extract every problem on this GPU; returns the list of C matrices."""
+    import torch
+    out: list[Any] = [None] * len(problems)
+    batchable, singles = [], []
+    for i, p in enumerate(problems):
+        (batchable if len(p[2]) <= MAX_RHS else singles).append(i)
+    for i in singles:  # more terminals than one RHS block: the plain path
+        grid, eps, terms = problems[i][:3]
+        bc = problems[i][3] if len(problems[i]) > 3 else None
+        rep: dict = {}
+        out[i] = PoissonSolver(grid, eps, cfg, gpu=gcfg).capacitance_matrix(
+            terms, bc, report=rep)
+        if reports is not None:
+            reports[i] = rep
+    if not batchable:
+        return out
+    ex = {}
+    try:
+        for i in batchable:
+            p = problems[i]
+            ex[i] = _Extraction(p[0], p[1], p[2], p[3] if len(p) > 3 else None, cfg, gcfg)
+        torch.cuda.synchronize()  # plan set-up and excitations are on this stream
+        pool = [torch.cuda.Stream() for _ in range(max(1, min(streams, len(batchable))))]
+        n = len(batchable)
+        plans = (ctypes.c_void_p * n)(*[ex[i].system.plan.value for i in batchable])
+        strm = (ctypes.c_void_p * n)(*[pool[j % len(pool)].cuda_stream for j in range(n)])
+        stat_arrays = [(L.FsRhsStats * ex[i].system.k)() for i in batchable]
+        sp = (ctypes.POINTER(L.FsRhsStats) * n)(
+            *[ctypes.cast(a, ctypes.POINTER(L.FsRhsStats)) for a in stat_arrays])
+        status = (ctypes.c_int * n)()
+        tol = float(cfg.tol)
+        maxiter = max(ex[i].maxiter for i in batchable)
+        st = L.lib().fs_pcg_plans_solve(plans, n, strm, 0, tol, maxiter, sp, status)
+        if st == L.FS_CUDA_ERROR or st == L.FS_BAD_ARG:
+            L.check("fs_pcg_plans_solve", st)
+        for j, i in enumerate(batchable):
+            e = ex[i]
+            stats = _stats_list(stat_arrays[j], e.system.nrhs)
+            if status[j] not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN, L.FS_STALLED):
+                L.check("fs_pcg_plans_solve", status[j])
+            _, stats = e.system.finish_auto(status[j], stats, tol, e.maxiter)
+            raise_on_status(stats, tol, "gpu-cg")
+            out[i], rep = e.collect(stats)
+            if reports is not None:
+                reports[i] = rep
+    finally:
+        for e in ex.values():
+            e.close()
+    return out
+
+
+def capacitance_matrices(problems: Sequence, config: SolverConfig | None = None, *,
+                         gpu: GPUConfig | None = None, streams: int = 16,
+                         reports: list | None = None, group=None,
+                         local: Callable | None = None) -> list[np.ndarray]:
+    """Maxwell capacitance matrices of a batch of independent geometries.
+
+    ``problems``: sequence of ``(grid, eps_cell, terminals)`` or
+    ``(grid, eps_cell, terminals, bc)`` -- the arguments of
+    ``extraction.capacitance_matrix`` per geometry.  Returns the symmetrised
+    C matrices in input order.  ``reports``: optional list, filled with one
+    report dict per geometry (the keys of a single extraction's report).
+
+    ``group``: a ``torch.distributed`` process group (or ``None`` for the
+    default group when one is initialised): geometries are sharded by cost
+    over its ranks and the results all-gathered.  ``local``: the per-rank
+    extraction, ``local(problems, config, gpu, streams, reports)``
+    (defaults to the GPU one).
+    """
+    cfg = config or SolverConfig()
+    gcfg = gpu or GPUConfig()
+    problems = list(problems)
+    run = local or _extract_local
+    t0 = time.perf_counter()
+    import torch.distributed as dist
+    world, rank = 1, 0
+    if dist.is_available() and dist.is_initialized():
+        world = dist.get_world_size(group)
+        rank = dist.get_rank(group)
+    if world == 1:
+        return run(problems, cfg, gcfg, streams, reports)
+    shards = shard_by_cost([problem_cost(p) for p in problems], world)
+    mine = shards[rank]
+    my_reports = [None] * len(mine) if reports is not None else None
+    res = run([problems[i] for i in mine], cfg, gcfg, streams, my_reports)
+    gathered: list[Any] = [None] * world
+    payload = (mine, [np.asarray(c) for c in res], my_reports)
+    dist.all_gather_object(gathered, payload, group=group)
+    out: list[Any] = [None] * len(problems)
+    for idx, mats, reps in gathered:
+        for j, i in enumerate(idx):
+            out[i] = mats[j]
+            if reports is not None and reps is not None:
+                reports[i] = reps[j]
+    if reports is not None:
+        for r in reports:
+            if isinstance(r, dict):
+                r.setdefault("batch_time", time.perf_counter() - t0)
+    return out

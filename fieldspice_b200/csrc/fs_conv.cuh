@@ -1,0 +1,249 @@
+// 3x3x3 convolution on 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Activations are BF16, channels-last, on a zero halo of one voxel:
+//   x[b][i][j][k][c], i in [0, X+2), j in [0, Y+2), k in [0, Z+2),
+// flattened to rows r = ((b*Xp + i)*Yp + j)*Zp + k of C_total channels.
+// In that layout the input row of tap (dx, dy, dz) for output row r is
+// r + dx*Yp*Zp + dy*Zp + dz, so the convolution is an implicit GEMM
+//   D[r][co] = sum_taps sum_ci X[r + off_t][ci] * W[t][co][ci]
+// whose A operand for a tap is a contiguous window of rows shifted by off_t.
+//
+// One CTA computes T tiles of 128 consecutive output rows.  Per x-offset dx
+// it stages, with 2-D TMA tensor loads (no multicast), the window of rows
+// [m0 + dx*S - Zp - 1, m0 + 128T + dx*S + Zp + 1) of the C_in channels,
+// 8 channels (16 B) per column, so every (dy, dz) tap of that dx is the same
+// window at a row offset: a descriptor start address +16 B per row.  Weights
+// arrive pre-packed in their shared-memory image with one bulk copy.  One
+// thread issues tcgen05.mma (M = 128, N = C_out, K = 16, BF16 x BF16 -> FP32)
+// into tensor memory, commits to an mbarrier, and the four warps read the
+// accumulators back (tcgen05.ld), add the bias, apply ReLU and/or a ReLU
+// mask, zero the halo rows and store BF16.  Output halo rows are always
+// written as zeros, which keeps the zero-halo invariant for the next layer.
+//
+// Small layers keep all 27 taps' operands resident (one phase); large ones
+// run three phases, one per dx, reusing the shared memory.  Every wait is
+// bounded; on a timeout the CTA records an error, waits again (bounded) for
+// its own transfers, frees its tensor memory and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fs_tc.cuh"
+#include "fs_tma.cuh"
+
+namespace fs {
+
+struct ConvGeom {
+  int X, Y, Z;          // interior voxels per batch element
+  int Xp, Yp, Zp;       // padded (X + 2, ...)
+  long long S;          // Yp * Zp (row distance of dx = 1)
+  long long V;          // Xp * Yp * Zp (rows per batch element)
+  long long R;          // batch * V
+};
+
+struct ConvArgs {
+  ConvGeom g;
+  int cin, cin_off;     // channels read from the input buffer
+  int cout;             // output channels (multiple of 16, <= 128)
+  const uint16_t* wpack;  // BF16 image [27][cin/8][cout][8]
+  const float* bias;      // [cout] or null
+  __nv_bfloat16* out;
+  int out_stride, out_off;
+  const __nv_bfloat16* mask;  // optional: result *= (mask > 0)
+  int mask_stride, mask_off;
+  int relu;
+  int accumulate;       // out += result
+  int T;                // 128-row tiles per CTA
+  int W;                // staged window rows (a multiple of BR)
+  int BR;               // rows per TMA box (<= 256, multiple of 8)
+  int phases;           // 1: all taps resident; 3: one dx per phase
+  int* error;
+};
+
+constexpr long long kConvBudget = 4000000000LL;  // ~2 s of SM clocks
+
+__device__ __forceinline__ uint32_t tmem_cols(int n) {
+  uint32_t c = 32;
+  while ((int)c < n) c <<= 1;
+  return c;
+}
+
+__global__ void __launch_bounds__(128)
+    k_conv3d_tc(const __grid_constant__ CUtensorMap xmap, ConvArgs a) {
+  extern __shared__ uint8_t conv_smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)conv_smem_raw + 1023) & ~(uintptr_t)1023);
+  const int nch = a.cin >> 3;
+  const int ndx = a.phases == 1 ? 3 : 1;  // windows resident per phase
+  const uint32_t colb = (uint32_t)a.W * 16u;
+  uint8_t* A = smem;
+  uint8_t* Bw = A + (size_t)ndx * nch * colb;
+  const uint32_t wtap = (uint32_t)nch * a.cout * 16u;  // one tap's weights
+  const int ntap_res = a.phases == 1 ? 27 : 9;
+  uint64_t* bars = (uint64_t*)(Bw + (size_t)ntap_res * wtap);
+  uint32_t* tslot = (uint32_t*)(bars + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long m0 = (long long)blockIdx.x * 128LL * a.T;
+  const uint32_t ncols = tmem_cols(a.T * a.cout);
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc_alloc(tslot, ncols);
+    tc_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(128, a.cout);
+  const int nseg = a.W / a.BR;
+  bool ok = true;
+  int issued = 0;  // phases whose loads were issued (thread 0)
+  int mmas = 0;    // phases whose MMAs were committed (thread 0)
+  for (int ph = 0; ph < a.phases && ok; ++ph) {
+    if (tid == 0) {
+      const int dx0 = a.phases == 1 ? 0 : ph;
+      mbar_arrive_expect_tx(&bars[0], (uint32_t)ndx * nch * colb + ntap_res * wtap);
+      bulk_load(Bw, a.wpack + (size_t)(a.phases == 1 ? 0 : ph * 9) * (wtap / 2),
+                ntap_res * wtap, &bars[0]);
+      for (int w = 0; w < ndx; ++w) {
+        const long long r0 = m0 + (long long)(dx0 + w - 1) * a.g.S - a.g.Zp - 1;
+        for (int c = 0; c < nch; ++c)
+          for (int sg = 0; sg < nseg; ++sg)
+            tma_load_2d(A + (size_t)(w * nch + c) * colb + (size_t)sg * a.BR * 16, &xmap,
+                        &bars[0], a.cin_off + 8 * c, (int)(r0 + (long long)sg * a.BR));
+      }
+      issued = ph + 1;
+    }
+    ok = mbar_wait_bounded(&bars[0], ph & 1, kConvBudget);
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t abase = smem_u32(A), bbase = smem_u32(Bw);
+      for (int j = 0; j < a.T; ++j) {
+        for (int tl = 0; tl < ntap_res; ++tl) {
+          const int t = a.phases == 1 ? tl : ph * 9 + tl;
+          const int w = a.phases == 1 ? t / 9 : 0;
+          const int dy = (t / 3) % 3, dz = t % 3;
+          const uint32_t rowoff = (uint32_t)(j * 128 + dy * a.g.Zp + dz) * 16u;
+          for (int s = 0; s < (a.cin >> 4); ++s) {
+            const uint64_t ad =
+                umma_desc(abase + (uint32_t)(w * nch + 2 * s) * colb + rowoff, colb, 128);
+            const uint64_t bd =
+                umma_desc(bbase + (uint32_t)tl * wtap + (uint32_t)(2 * s * a.cout) * 16u,
+                          (uint32_t)a.cout * 16u, 128);
+            const uint32_t acc = (ph > 0 || tl > 0 || s > 0) ? 1u : 0u;
+            tc_mma_bf16(tbase + (uint32_t)(j * a.cout), ad, bd, idesc, acc);
+          }
+        }
+      }
+      tc_commit(&bars[1]);
+      mmas = ph + 1;
+    }
+    // the operands of this phase stay in use until its MMAs complete
+    ok = mbar_wait_bounded(&bars[1], ph & 1, kConvBudget);
+    ok = __syncthreads_and(ok);
+    tc_fence_after();
+  }
+  if (ok) {
+    for (int j = 0; j < a.T; ++j) {
+      const long long row = m0 + (long long)j * 128 + warp * 32 + lane;
+      bool interior = false;
+      if (row < a.g.R) {
+        const long long rr = row % a.g.V;
+        const int k = (int)(rr % a.g.Zp);
+        const int jj = (int)((rr / a.g.Zp) % a.g.Yp);
+        const int i = (int)(rr / a.g.S);
+        interior = k >= 1 && k <= a.g.Z && jj >= 1 && jj <= a.g.Y && i >= 1 && i <= a.g.X;
+      }
+      for (int q = 0; q < (a.cout >> 4); ++q) {
+        float v[16];
+        tc_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * a.cout + q * 16), v);
+        if (row >= a.g.R) continue;
+        __nv_bfloat16* dst = a.out + row * a.out_stride + a.out_off + q * 16;
+        if (!interior) {
+          if (!a.accumulate) {
+            uint4 z = make_uint4(0, 0, 0, 0);
+            ((uint4*)dst)[0] = z;
+            ((uint4*)dst)[1] = z;
+          }
+          continue;
+        }
+        if (a.bias) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] += __ldg(a.bias + q * 16 + e);
+        }
+        if (a.relu) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] = fmaxf(v[e], 0.0f);
+        }
+        if (a.mask) {
+          const __nv_bfloat16* mp = a.mask + row * a.mask_stride + a.mask_off + q * 16;
+          uint4 mraw[2];
+          mraw[0] = ((const uint4*)mp)[0];
+          mraw[1] = ((const uint4*)mp)[1];
+          const __nv_bfloat16* mv = (const __nv_bfloat16*)mraw;
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            if (!(__bfloat162float(mv[e]) > 0.0f)) v[e] = 0.0f;
+        }
+        if (a.accumulate) {
+          uint4 oraw[2];
+          oraw[0] = ((const uint4*)dst)[0];
+          oraw[1] = ((const uint4*)dst)[1];
+          const __nv_bfloat16* ov = (const __nv_bfloat16*)oraw;
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] += __bfloat162float(ov[e]);
+        }
+        uint4 packed[2];
+        __nv_bfloat16* pv = (__nv_bfloat16*)packed;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) pv[e] = __float2bfloat16_rn(v[e]);
+        ((uint4*)dst)[0] = packed[0];
+        ((uint4*)dst)[1] = packed[1];
+      }
+    }
+  } else {
+    // bounded second wait for this CTA's own transfers and MMAs in flight
+    if (tid == 0) {
+      if (issued > 0) (void)mbar_wait_bounded(&bars[0], (issued - 1) & 1, kConvBudget);
+      if (mmas > 0) (void)mbar_wait_bounded(&bars[1], (mmas - 1) & 1, kConvBudget);
+    }
+    if (tid == 0 && a.error) atomicExch(a.error, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc_dealloc(tbase, ncols);
+}
+
+// Pack FP32 weights w[27][cout][cin] into the BF16 shared-memory image
+// [27][cin/8][cout][8]; flip != 0 packs the data-gradient operator instead:
+// taps reversed and the channel roles swapped (image [27][cout/8][cin][8]).
+__global__ void k_pack_weights(const float* __restrict__ w, int cin, int cout, int flip,
+                               uint16_t* __restrict__ out) {
+  const long long n = 27LL * cin * cout;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(idx / ((long long)cin * cout));
+    const int rem = (int)(idx % ((long long)cin * cout));
+    const int co = rem / cin, ci = rem % cin;
+    const float v = w[idx];
+    long long dst;
+    if (!flip) {
+      dst = (((long long)t * (cin / 8) + ci / 8) * cout + co) * 8 + (ci & 7);
+    } else {
+      // operator with K = cout_f channels, N = cin_f rows, tap 26 - t
+      dst = (((long long)(26 - t) * (cout / 8) + co / 8) * cin + ci) * 8 + (co & 7);
+    }
+    __nv_bfloat16 b = __float2bfloat16_rn(v);
+    out[dst] = *(uint16_t*)&b;
+  }
+}
+
+}  // namespace fs

@@ -98,6 +98,13 @@ __global__ void k_mg_scales(long long N, const double* __restrict__ s64,
 }
 
 // ---- V-cycle kernels (T, K RHS interleaved) ---------------------------------------
+// Three resident blocks per SM where the per-node state is small enough to
+// keep in registers (FP32, up to 8 RHS); wider nodes keep the register room.
+template <typename T, int K>
+constexpr int mg_min_blocks() {
+  return sizeof(T) * K <= 32 ? 3 : 1;
+}
+
 template <typename T, int K>
 __device__ __forceinline__ void apply_eq(const Dims& d, const T* __restrict__ ex,
                                          const T* __restrict__ ey,
@@ -124,7 +131,7 @@ __device__ __forceinline__ void apply_eq(const Dims& d, const T* __restrict__ ex
 // One Chebyshev step: d = cd*d + cr*(b - A~ x_in), x_out = x_in + d.
 // x_zero: x_in is identically zero (first pre-smoothing step).
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     k_mg_cheb(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
               const T* __restrict__ ez, const T* __restrict__ xin,
               T* __restrict__ xout, T* __restrict__ dv,
@@ -165,7 +172,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // res = b - A~ x
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     k_mg_residual(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
                   const T* __restrict__ ez, const T* __restrict__ x,
                   const T* __restrict__ b, T* __restrict__ res,
@@ -188,7 +195,7 @@ __global__ void __launch_bounds__(kBlock)
 // residual along saves the separate residual pass over x2.
 // pre0: x1 = c0 b, r1 = b - c0 A~ b.
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     k_mg_pre0(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
               const T* __restrict__ ez, const T* __restrict__ b,
               T* __restrict__ x1, T* __restrict__ r1, T c0,
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(kBlock)
 // pre1: d1 = cd x1 + cr r1 (formed at the node and its six neighbours),
 // x2 = x1 + d1, r2 = r1 - A~ d1.
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     k_mg_pre1(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
               const T* __restrict__ ez, const T* __restrict__ x1,
               const T* __restrict__ r1, T* __restrict__ x2, T* __restrict__ r2,

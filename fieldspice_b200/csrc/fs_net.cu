@@ -1,0 +1,202 @@
+// Learned coarse-level preconditioner: a small BF16 3-D U-Net on tcgen05.
+//
+// This file holds the host side of the tensor-core convolution (fs_conv.cuh)
+// -- launch planning, TMA tensor maps -- and the C-ABI entry points that run
+// one convolution on caller buffers (used by the tests and by the network).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "fieldspice_b200.h"
+#include "fs_common.cuh"
+#include "fs_conv.cuh"
+#include "fs_net.cuh"
+
+namespace fs {
+
+PFN_cuTensorMapEncodeTiled_v12000 net_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    else
+      (void)cudaGetLastError();
+  }
+  return fn;
+}
+
+ConvGeom conv_geom(int batch, int X, int Y, int Z) {
+  ConvGeom g;
+  g.X = X;
+  g.Y = Y;
+  g.Z = Z;
+  g.Xp = X + 2;
+  g.Yp = Y + 2;
+  g.Zp = Z + 2;
+  g.S = (long long)g.Yp * g.Zp;
+  g.V = (long long)g.Xp * g.S;
+  g.R = (long long)batch * g.V;
+  return g;
+}
+
+bool conv_config(const ConvGeom& g, int cin, int cout, ConvCfg* c) {
+  const int nch = cin / 8;
+  const int phase_opts[2] = {1, 3};
+  const int t_opts[3] = {4, 2, 1};
+  for (int pi = 0; pi < 2; ++pi) {
+    for (int ti = 0; ti < 3; ++ti) {
+      const int phases = phase_opts[pi], T = t_opts[ti];
+      if (T * cout > 256) continue;
+      const long long need = 128LL * T + 2LL * g.Zp + 2;
+      const int nseg = (int)((need + 255) / 256);
+      const int BR = (int)(((need + nseg - 1) / nseg + 7) / 8 * 8);
+      const int W = nseg * BR;
+      const int ndx = phases == 1 ? 3 : 1, ntap = phases == 1 ? 27 : 9;
+      const size_t smem = 1024 + (size_t)ndx * nch * W * 16 + (size_t)ntap * nch * cout * 16 + 64;
+      if (smem <= 227u * 1024u) {
+        c->T = T;
+        c->W = W;
+        c->BR = BR;
+        c->phases = phases;
+        c->smem = smem;
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
+int act_map(CUtensorMap* map, const void* base, int ctot, long long rows, int box_rows) {
+  auto encode = net_encode_fn();
+  if (!encode) {
+    fs_set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
+    return FS_CUDA_ERROR;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)ctot, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ctot * 2};
+  cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                      strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    fs_set_error_msg("cuTensorMapEncodeTiled rejected an activation tensor map");
+    return FS_CUDA_ERROR;
+  }
+  return FS_OK;
+}
+
+int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
+  if (io.cin < 16 || io.cin % 16 || io.cout < 16 || io.cout % 16 || io.cout > 128 ||
+      io.cin_off % 8 || io.ctot_in % 8 || io.out_off % 8 || io.ctot_out % 8 ||
+      io.cin_off + io.cin > io.ctot_in || io.out_off + io.cout > io.ctot_out || !io.x ||
+      !io.out || !io.wpack || ((uintptr_t)io.x & 15) || ((uintptr_t)io.out & 15) ||
+      ((uintptr_t)io.wpack & 15) || g.X < 1 || g.Y < 1 || g.Z < 1 || g.R <= 0) {
+    fs_set_error_msg("conv3d: bad channel counts, offsets, alignment or dims");
+    return FS_BAD_ARG;
+  }
+  if (io.mask && (io.mask_off % 8 || io.ctot_mask % 8 || ((uintptr_t)io.mask & 15) ||
+                  io.mask_off + io.cout > io.ctot_mask)) {
+    fs_set_error_msg("conv3d: bad mask layout");
+    return FS_BAD_ARG;
+  }
+  ConvCfg c;
+  if (!conv_config(g, io.cin, io.cout, &c)) {
+    fs_set_error_msg("conv3d: layer does not fit in shared memory");
+    return FS_BAD_ARG;
+  }
+  CUtensorMap map;
+  int st = act_map(&map, io.x, io.ctot_in, g.R, c.BR);
+  if (st != FS_OK) return st;
+  ConvArgs a;
+  a.g = g;
+  a.cin = io.cin;
+  a.cin_off = io.cin_off;
+  a.cout = io.cout;
+  a.wpack = (const uint16_t*)io.wpack;
+  a.bias = io.bias;
+  a.out = (__nv_bfloat16*)io.out;
+  a.out_stride = io.ctot_out;
+  a.out_off = io.out_off;
+  a.mask = (const __nv_bfloat16*)io.mask;
+  a.mask_stride = io.ctot_mask;
+  a.mask_off = io.mask_off;
+  a.relu = io.relu;
+  a.accumulate = io.accumulate;
+  a.T = c.T;
+  a.W = c.W;
+  a.BR = c.BR;
+  a.phases = c.phases;
+  a.error = io.error;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e != cudaSuccess) return fs_cuda_status("cudaFuncSetAttribute(conv)", e);
+    attr_set = true;
+  }
+  const long long tiles = (g.R + 128LL * c.T - 1) / (128LL * c.T);
+  if (tiles > 0x7fffffffLL) {
+    fs_set_error_msg("conv3d: volume too large");
+    return FS_BAD_ARG;
+  }
+  k_conv3d_tc<<<(unsigned)tiles, 128, c.smem, s>>>(map, a);
+  FS_CHECK_LAUNCH("k_conv3d_tc");
+  return FS_OK;
+}
+
+int pack_weights(const float* w, int cin, int cout, int flip, void* out, cudaStream_t s) {
+  if (!w || !out || cin < 16 || cin % 16 || cout < 16 || cout % 16) {
+    fs_set_error_msg("pack_weights: channel counts must be multiples of 16");
+    return FS_BAD_ARG;
+  }
+  const long long n = 27LL * cin * cout;
+  const int blocks = (int)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024);
+  k_pack_weights<<<blocks, 256, 0, s>>>(w, cin, cout, flip, (uint16_t*)out);
+  FS_CHECK_LAUNCH("k_pack_weights");
+  return FS_OK;
+}
+
+}  // namespace fs
+
+extern "C" {
+
+int fs_conv3d_pack_weights(const float* w, int cin, int cout, int flip, void* wpack,
+                           void* stream) {
+  return fs::pack_weights(w, cin, cout, flip, wpack, (cudaStream_t)stream);
+}
+
+int fs_conv3d_bf16(const void* x, int ctot_in, int cin_off, int cin, const void* wpack,
+                   const float* bias, void* y, int ctot_out, int cout_off, int cout,
+                   const void* mask, int ctot_mask, int mask_off, int batch, int X, int Y,
+                   int Z, int relu, int accumulate, int* error, void* stream) {
+  if (batch < 1) return FS_BAD_ARG;
+  fs::ConvIO io;
+  io.x = x;
+  io.ctot_in = ctot_in;
+  io.cin_off = cin_off;
+  io.cin = cin;
+  io.wpack = wpack;
+  io.bias = bias;
+  io.out = y;
+  io.ctot_out = ctot_out;
+  io.out_off = cout_off;
+  io.cout = cout;
+  io.mask = mask;
+  io.ctot_mask = ctot_mask;
+  io.mask_off = mask_off;
+  io.relu = relu;
+  io.accumulate = accumulate;
+  io.error = error;
+  return fs::conv_launch(fs::conv_geom(batch, X, Y, Z), io, (cudaStream_t)stream);
+}
+
+}  // extern "C"

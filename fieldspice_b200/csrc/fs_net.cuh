@@ -1,0 +1,38 @@
+// Host-side declarations shared by the network sources.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "fs_conv.cuh"
+
+namespace fs {
+
+struct ConvCfg {
+  int T, W, BR, phases;
+  size_t smem;
+};
+
+// One convolution's buffers: input channels [cin_off, cin_off + cin) of a
+// ctot_in-channel volume, output channels [out_off, out_off + cout) of a
+// ctot_out-channel volume, optional ReLU mask channels of a third volume.
+struct ConvIO {
+  const void* x = nullptr;
+  int ctot_in = 0, cin_off = 0, cin = 0;
+  const void* wpack = nullptr;
+  const float* bias = nullptr;
+  void* out = nullptr;
+  int ctot_out = 0, out_off = 0, cout = 0;
+  const void* mask = nullptr;
+  int ctot_mask = 0, mask_off = 0;
+  int relu = 0, accumulate = 0;
+  int* error = nullptr;
+};
+
+ConvGeom conv_geom(int batch, int X, int Y, int Z);
+bool conv_config(const ConvGeom& g, int cin, int cout, ConvCfg* c);
+int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s);
+int pack_weights(const float* w, int cin, int cout, int flip, void* out, cudaStream_t s);
+
+}  // namespace fs

@@ -35,6 +35,7 @@
 #include <string.h>
 
 #include <new>
+#include <vector>
 
 #include "fs_common.cuh"
 #include "fs_tma.cuh"
@@ -397,6 +398,20 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
     const int z = z0 + tz, y = y0 + ty;
     const bool inb = z < d.nz && y < d.ny;
     const int nplanes = (xb - xa) + 2;   // planes xa-1 .. xb
+    // The six masses of the next plane's node are loaded one plane ahead,
+    // so their latency hides behind this plane's arithmetic.
+    T nm0 = 0, nm1 = 0, nm2 = 0, nm3 = 0, nm4 = 0, nm5 = 0;
+#define FS_LOAD_MASSES(xx)                                       \
+  do {                                                          \
+    const long long nn = ((long long)(xx) * d.ny + y) * d.nz + z; \
+    nm0 = (xx) > 0 ? __ldg(ex + nn - d.sx) : (T)0;              \
+    nm1 = __ldg(ex + nn); /* 0 on the last plane (padded) */    \
+    nm2 = y > 0 ? __ldg(ey + nn - d.sy) : (T)0;                 \
+    nm3 = __ldg(ey + nn);                                       \
+    nm4 = z > 0 ? __ldg(ez + nn - 1) : (T)0;                    \
+    nm5 = __ldg(ez + nn);                                       \
+  } while (0)
+    if (inb) FS_LOAD_MASSES(xa);
     auto issue = [&](int j) {
       const int s = (int)((ticket + j) % C::NS);
       fs::mbar_arrive_expect_tx(&bar[s], C::BOX);
@@ -421,12 +436,8 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
           const T* pm = ring + (int)((tk - 2) % C::NS) * BOXT;
           const T* pc = ring + (int)((tk - 1) % C::NS) * BOXT;
           const T* pp = ring + s * BOXT;
-          const T mxm = x > 0 ? __ldg(ex + n - d.sx) : (T)0;
-          const T mxp = __ldg(ex + n);  // 0 on the last plane (padded)
-          const T mym = y > 0 ? __ldg(ey + n - d.sy) : (T)0;
-          const T myp = __ldg(ey + n);
-          const T mzm = z > 0 ? __ldg(ez + n - 1) : (T)0;
-          const T mzp = __ldg(ez + n);
+          const T mxm = nm0, mxp = nm1, mym = nm2, myp = nm3, mzm = nm4, mzp = nm5;
+          if (x + 1 < xb) FS_LOAD_MASSES(x + 1);
           T c[K], v[K], qv[K];
           ld_smem<T, K>(pc + cpos * K, c);
 #pragma unroll
@@ -461,6 +472,7 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
     ticket += nplanes;
     u += (xb - xa);
   }
+#undef FS_LOAD_MASSES
   if (failed) {
     // A staged load did not land in time.  Give copies still in flight a
     // bounded chance to finish before the block exits, then report.
@@ -1462,10 +1474,13 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   return FS_OK;
 }
 
-int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
-                      fs_rhs_stats* stats, void* stream) {
-  if (!P || !(tol > 0.0) || maxiter < 1) return FS_BAD_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
+}  // extern "C"
+
+namespace {
+
+// Start a solve on stream s: k_init, then (preconditioned) z = M r and r.z.
+int solve_begin(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
+                cudaStream_t s) {
   // Mixed precision: refresh the residual after a 10x drop under Jacobi CG
   // (hundreds of FP32 iterations per decade) and after a 1000x drop under
   // multigrid (a decade every ~2 iterations, so little FP32 drift).
@@ -1474,52 +1489,60 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
   cudaError_t e;
   dispatch(P, 2, s, warm_start ? 1 : 0, tol, maxiter, delta);
   FS_CHECK_LAUNCH("k_init");
-  long long launches = 1;
+  P->launches = 1;
   if (P->precond) {
     dispatch(P, 10, s);  // z = M r and r.z for the first direction
     FS_CHECK_LAUNCH("multigrid V-cycle");
-    launches += P->launches_per_iter;
+    P->launches += P->launches_per_iter;
   }
   for (int t = 0; t < 6; ++t) P->kernel_ms[t] = 0.0;
   P->kernel_samples = 0;
-  const long long max_chunks = (long long)maxiter / P->chunk + 4;
-  int timed_out = 1;
-  for (long long c = 0; c < max_chunks; ++c) {
-    if ((e = cudaGraphLaunch(P->exec, s)) != cudaSuccess)
-      return fs_cuda_status("cudaGraphLaunch", e);
-    launches += (5LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
-    if ((e = cudaMemcpyAsync(P->h_flag, &P->ctl->all_done, sizeof(int),
-                             cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-      return fs_cuda_status("cudaMemcpyAsync", e);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
-      return fs_cuda_status("cudaStreamSynchronize", e);
-    float ms[6] = {0, 0, 0, 0, 0, 0};
-    bool ok = true;
-    for (int t = 0; t < 5 && ok; ++t)
-      ok = cudaEventElapsedTime(&ms[t], P->ev[t], P->ev[t + 1]) == cudaSuccess;
-    if (ok && P->precond)
-      ok = cudaEventElapsedTime(&ms[5], P->ev[6], P->ev[7]) == cudaSuccess;
-    if (ok) {
-      ms[5] /= (float)P->mg.smooth_deg;  // per launch
-      for (int t = 0; t < 6; ++t) P->kernel_ms[t] += ms[t];
-      P->kernel_samples += 1;
-    } else {
-      (void)cudaGetLastError();  // timing unavailable: not a solve failure
-    }
-    if (*P->h_flag) {
-      timed_out = 0;
-      break;
-    }
+  return FS_OK;
+}
+
+// Enqueue one graph chunk and the copy of the all-done flag.
+int solve_chunk(fs_pcg_plan* P, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaGraphLaunch(P->exec, s)) != cudaSuccess)
+    return fs_cuda_status("cudaGraphLaunch", e);
+  P->launches += (5LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
+  if ((e = cudaMemcpyAsync(P->h_flag, &P->ctl->all_done, sizeof(int),
+                           cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return fs_cuda_status("cudaMemcpyAsync", e);
+  return FS_OK;
+}
+
+// After the chunk's stream has drained: accumulate the kernel timings of
+// its first iteration; returns 1 when every RHS is done.
+int solve_check(fs_pcg_plan* P) {
+  float ms[6] = {0, 0, 0, 0, 0, 0};
+  bool ok = true;
+  for (int t = 0; t < 5 && ok; ++t)
+    ok = cudaEventElapsedTime(&ms[t], P->ev[t], P->ev[t + 1]) == cudaSuccess;
+  if (ok && P->precond)
+    ok = cudaEventElapsedTime(&ms[5], P->ev[6], P->ev[7]) == cudaSuccess;
+  if (ok) {
+    ms[5] /= (float)P->mg.smooth_deg;  // per launch
+    for (int t = 0; t < 6; ++t) P->kernel_ms[t] += ms[t];
+    P->kernel_samples += 1;
+  } else {
+    (void)cudaGetLastError();  // timing unavailable: not a solve failure
   }
+  return *P->h_flag ? 1 : 0;
+}
+
+// k_finalize, copy the per-RHS state back and fold it into a status.
+int solve_finish(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats,
+                 cudaStream_t s) {
+  cudaError_t e;
   dispatch(P, 4, s);
   FS_CHECK_LAUNCH("k_finalize");
-  launches += 1;
+  P->launches += 1;
   if ((e = cudaMemcpyAsync(P->h_st, P->st, sizeof(RhsState) * P->nrhs,
                            cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return fs_cuda_status("cudaMemcpyAsync", e);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fs_cuda_status("cudaStreamSynchronize", e);
-  P->launches = launches;
   int worst = FS_OK;
   for (int t = 0; t < P->nrhs; ++t) {
     const RhsState& h = P->h_st[t];
@@ -1537,6 +1560,79 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
     else if (h.status == FS_TIMEOUT && worst == FS_OK) worst = FS_TIMEOUT;
   }
   if (timed_out) return FS_TIMEOUT;
+  return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
+                      fs_rhs_stats* stats, void* stream) {
+  if (!P || !(tol > 0.0) || maxiter < 1) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = solve_begin(P, warm_start, tol, maxiter, s);
+  if (st != FS_OK) return st;
+  const long long max_chunks = (long long)maxiter / P->chunk + 4;
+  int timed_out = 1;
+  cudaError_t e;
+  for (long long c = 0; c < max_chunks; ++c) {
+    if ((st = solve_chunk(P, s)) != FS_OK) return st;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return fs_cuda_status("cudaStreamSynchronize", e);
+    if (solve_check(P)) {
+      timed_out = 0;
+      break;
+    }
+  }
+  return solve_finish(P, timed_out, stats, s);
+}
+
+int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
+                       void* const* streams, int warm_start, double tol,
+                       int maxiter, fs_rhs_stats* const* stats, int* status) {
+  if (!plans || nplans < 1 || !streams || !status || !(tol > 0.0) || maxiter < 1)
+    return FS_BAD_ARG;
+  for (int i = 0; i < nplans; ++i)
+    if (!plans[i]) return FS_BAD_ARG;
+  std::vector<int> active(nplans, 1);
+  std::vector<long long> chunks(nplans, 0);
+  int st;
+  cudaError_t e;
+  for (int i = 0; i < nplans; ++i) {
+    status[i] = FS_TIMEOUT;
+    if ((st = solve_begin(plans[i], warm_start, tol, maxiter,
+                          (cudaStream_t)streams[i])) != FS_OK)
+      return st;
+  }
+  // Round robin: one chunk per unfinished plan on its own stream, so the
+  // chunks of small systems overlap those of large ones, then a check of
+  // each; a plan leaves the rotation when all its RHS are done.
+  int left = nplans;
+  while (left > 0) {
+    for (int i = 0; i < nplans; ++i) {
+      if (!active[i]) continue;
+      if ((st = solve_chunk(plans[i], (cudaStream_t)streams[i])) != FS_OK) return st;
+      ++chunks[i];
+    }
+    for (int i = 0; i < nplans; ++i) {
+      if (!active[i]) continue;
+      fs_pcg_plan* P = plans[i];
+      if ((e = cudaStreamSynchronize((cudaStream_t)streams[i])) != cudaSuccess)
+        return fs_cuda_status("cudaStreamSynchronize", e);
+      const int done = solve_check(P);
+      const bool out = chunks[i] >= (long long)maxiter / P->chunk + 4;
+      if (done || out) {
+        active[i] = 0;
+        --left;
+        status[i] = solve_finish(P, done ? 0 : 1, stats ? stats[i] : nullptr,
+                                 (cudaStream_t)streams[i]);
+      }
+    }
+  }
+  int worst = FS_OK;
+  for (int i = 0; i < nplans; ++i)
+    if (status[i] != FS_OK && (worst == FS_OK || status[i] == FS_CUDA_ERROR)) worst = status[i];
   return worst;
 }
 

@@ -305,18 +305,28 @@ class EliminatedSystem:
         if self.fell_back:
             return self._run(self._fp64[0], tol, mi, warm)
         st, stats = self._run(self._plan, tol, mi, warm)
+        return self.finish_auto(st, stats, tol, mi)
+
+    def finish_auto(self, st: int, stats: list, tol: float, maxiter: int):
+        """In ``"auto"`` mode, continue a mixed solve whose RHS stalled or hit
+        ``maxiter`` in FP64 from its iterate (this system then stays FP64)."""
         bad = any(s["status"] in (L.FS_NOT_CONVERGED, L.FS_STALLED) for s in stats)
-        if self.mode == "auto" and bad:
+        if self.mode == "auto" and bad and not self.fell_back:
             if self._fp64 is None:
                 self._fp64 = self._make_plan("fp64")
             self.fell_back = True
-            st, stats2 = self._run(self._fp64[0], tol, mi, True)
+            st, stats2 = self._run(self._fp64[0], tol, maxiter, True)
             for a, b in zip(stats, stats2):
                 b["iterations"] += a["iterations"]
                 b["reliable_updates"] += a["reliable_updates"]
                 b["fp64_fallback"] = True
             stats = stats2
         return st, stats
+
+    @property
+    def plan(self):
+        """The CG plan the next solve runs (the FP64 one after a fallback)."""
+        return self._fp64[0] if self.fell_back else self._plan
 
     def kernel_times(self) -> dict:
         """Per-kernel device time sampled during the last solve (ms per

@@ -151,6 +151,14 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
  * FS_NAN on breakdown, FS_TIMEOUT if a staged load never arrived.           */
 int fs_pcg_plan_solve(fs_pcg_plan* plan, int warm_start, double tol,
                       int maxiter, fs_rhs_stats* stats, void* stream);
+/* Solve several independent plans (a batch of geometries) together: plan i
+ * runs on streams[i], one graph chunk per unfinished plan per round, so the
+ * iterations of small systems overlap those of large ones.  stats[i]: host
+ * array of plan i's nrhs entries (or NULL); status[i]: plan i's result as
+ * fs_pcg_plan_solve would return it.  Returns FS_OK when every plan is.    */
+int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
+                       void* const* streams, int warm_start, double tol,
+                       int maxiter, fs_rhs_stats* const* stats, int* status);
 /* Multigrid parameters for plans created after the call (process-wide):
  * Chebyshev smoothing degree (pre and post) and the lower end of its
  * interval [smooth_lo, 2] on the unit-diagonal level operators, the
@@ -226,6 +234,27 @@ int fs_quadform(const double* mx, const double* my, const double* mz,
 int fs_apply_laplacian(const double* mx, const double* my, const double* mz,
                        const double* u, const double* add, double* out, int nx,
                        int ny, int nz, int nrhs, void* stream);
+
+
+/* ---- Learned preconditioner: BF16 3-D convolution on tensor cores ------ *
+ * Activations: BF16, channels-last on a one-voxel zero halo,
+ * [batch][X+2][Y+2][Z+2][ctot] (a 16-byte aligned base, ctot a multiple of
+ * 8).  Weights: FP32 w[27][cout][cin], taps ordered (dx, dy, dz) with z
+ * fastest, offsets -1..1 (the cross-correlation of a padded conv3d).
+ * fs_conv3d_pack_weights writes their BF16 tensor-core image (27*cin*cout
+ * elements); flip != 0 packs the data-gradient operator (taps reversed,
+ * channel roles swapped) for a convolution from cout to cin channels.
+ * fs_conv3d_bf16: y[.., cout_off + co] = act(bias + sum W x[.., cin_off + ci]),
+ * act = ReLU when relu != 0, times (mask > 0) channel-wise when mask is not
+ * NULL, added to y when accumulate != 0; halo rows of y are written as 0
+ * (left untouched when accumulating).  cin, cout: multiples of 16, cout
+ * <= 128.  error: optional device int set to 1 if a staged load timed out. */
+int fs_conv3d_pack_weights(const float* w, int cin, int cout, int flip, void* wpack,
+                           void* stream);
+int fs_conv3d_bf16(const void* x, int ctot_in, int cin_off, int cin, const void* wpack,
+                   const float* bias, void* y, int ctot_out, int cout_off, int cout,
+                   const void* mask, int ctot_mask, int mask_off, int batch, int X, int Y,
+                   int Z, int relu, int accumulate, int* error, void* stream);
 
 #ifdef __cplusplus
 }

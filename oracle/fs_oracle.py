@@ -348,8 +348,16 @@ class LinearSystemCPU:
         A = sp.csr_matrix(A)
         self.n = A.shape[0]
         self.tol = tol
-        d = A.diagonal()
+        # empty rows (a zero-conductivity region no terminal reaches) are
+        # pinned to zero with an identity row, poisson.py:286-325,600-611
         row_abs = np.asarray(abs(A).sum(axis=1)).ravel()
+        self.empty = np.flatnonzero(row_abs == 0.0)
+        if self.empty.size:
+            keep = np.ones(self.n)
+            keep[self.empty] = 0.0
+            A = sp.csr_matrix(sp.diags(keep) @ A @ sp.diags(keep) + sp.diags(1.0 - keep))
+            row_abs = np.asarray(abs(A).sum(axis=1)).ravel()
+        d = A.diagonal()
         solo = (row_abs <= np.abs(d)) & (d != 0)
         self.solo = np.flatnonzero(solo)
         self.free = np.flatnonzero(~solo)
@@ -376,6 +384,7 @@ class LinearSystemCPU:
 
     def solve(self, b, x0=None):
         b = np.asarray(b, dtype=float).copy()
+        b[self.empty] = 0.0
         bf = b[self.free] if self.split else b
         bs = bf * self.dinv
         iters = 0
@@ -472,6 +481,38 @@ def capacitance_matrix(g: Grid, eps_cell, terminals, dirichlet_walls=None,
 # EQS backward Euler / theta -- fieldspice/solvers/eqs.py:97-101, :176-195,
 # :229-323, :328-340
 # ---------------------------------------------------------------------------
+def resistance_matrix(g: Grid, sigma_cell, terminals, method="cg", tol=1e-10,
+                      mode="parallel"):
+    """DC resistance matrix [ohm] (``fieldspice/extraction.py:59-87``).
+
+    Unit excitation of every terminal with all terminal nodes fixed and every
+    wall insulating; ``Y[i, j] = sum_{n in T_i} (L_sigma phi_j)_n``,
+    symmetrised, then the pseudo-inverse (``Y`` is singular: the all-ones
+    vector drives no current).  Returns ``(R, Y_unsymmetrised)``.
+    """
+    terms = [np.unique(np.asarray(t, np.intp)) for t in terminals]
+    if len(terms) < 2:
+        raise ValueError("resistance extraction needs at least two terminals")
+    m = edge_mass_vector(g, cell_to_edge(g, np.asarray(sigma_cell, float), mode))
+    Lmat = nodal_laplacian(g, m)
+    fixed = np.concatenate(terms)
+    nt = len(terms)
+    Y = np.zeros((nt, nt))
+    A_bc, _ = apply_dirichlet(Lmat, np.zeros(g.n_nodes), fixed, np.zeros(fixed.size))
+    ls = LinearSystemCPU(A_bc, method=method, tol=tol)
+    for j, tj in enumerate(terms):
+        x0 = np.zeros(g.n_nodes)
+        x0[tj] = 1.0
+        b = -(Lmat @ x0)
+        b[fixed] = x0[fixed]
+        phi = ls.solve(b)
+        q = Lmat @ phi
+        for i, ti in enumerate(terms):
+            Y[i, j] = float(q[ti].sum())
+    Ys = 0.5 * (Y + Y.T)
+    return np.linalg.pinv(Ys), Y
+
+
 def eqs_transient(g: Grid, eps_cell, sigma_cell, fixed_groups, values_at,
                   dt, nsteps, theta=1.0, method="cg", tol=1e-10,
                   dirichlet_walls=None, t_start=0.0):

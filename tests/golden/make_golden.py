@@ -123,6 +123,27 @@ def layered_fixture(shape, seed, tol):
                         iterations=rep["linear"].get("iterations", -1))
 
 
+def resistance_fixture():
+    """extraction.py:59-87 on a seeded conductor network: a doped-silicon
+    slab, two copper straps on it, insulating oxide (sigma = 0) above, three
+    terminals; small enough that the reference factorises it directly."""
+    from fieldspice.extraction import resistance_matrix
+    rng = np.random.default_rng(7)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 4e-6, 22)), np.linspace(0, 3e-6, 17),
+                        np.linspace(0, 1e-6, 11))
+    sig = np.zeros(g.shape_cells)
+    sig[:, :, :4] = 1e2
+    sig[2:19, 3:6, 4:6] = 5.8e7
+    sig[2:19, 10:13, 4:6] = 5.8e7
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(0, 0, 0, 21, 16, 0), (2, 3, 5, 3, 6, 6), (18, 10, 5, 19, 13, 6)]
+    terms = [Terminal(f"t{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(boxes)]
+    R = resistance_matrix(g, sig, terms)
+    np.savez_compressed(HERE / "resistance.npz", R=R, x=g.xn, y=g.yn, z=g.zn,
+                        sigma=sig, boxes=np.asarray(boxes))
+
+
 def rc_stack(n=60):
     d, Wd, H = 4e-6, 3e-6, 2e-6
     sigma1, er1, er2 = 1e3, 4.0, 2.0
@@ -214,4 +235,5 @@ if __name__ == "__main__":
     layered_fixture((32, 32, 16), 0, 1e-12)
     layered_fixture((48, 48, 24), 1, 1e-12)
     eqs_fixture()
+    resistance_fixture()
     print("golden fixtures written to", HERE)

@@ -1,0 +1,93 @@
+"""Multi-rank batch extraction, host side (CPU, gloo, world size 2).
+
+The batch path shards geometries over ranks by cost and all-gathers the C
+matrices (no data-path collective).  Here two gloo ranks run the sharding and
+the gather with the oracle standing in for the per-GPU extraction; every rank
+must end with the whole batch, in input order, equal to a one-rank run.
+"""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from fieldspice_b200.batch import capacitance_matrices, problem_cost, shard_by_cost
+
+
+def test_shard_by_cost_is_balanced_and_deterministic():
+    rng = np.random.default_rng(0)
+    costs = np.exp(rng.uniform(np.log(32 ** 3), np.log(160 * 160 * 96), 64)) * rng.integers(2, 17, 64)
+    for world in (1, 2, 4, 8):
+        sh = shard_by_cost(costs, world)
+        assert sorted(i for s in sh for i in s) == list(range(64))
+        loads = [costs[s].sum() for s in sh]
+        # LPT bound: max load <= mean + largest item
+        assert max(loads) <= np.mean(loads) + costs.max() + 1e-6
+        assert sh == shard_by_cost(list(costs), world)
+    assert shard_by_cost([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        shard_by_cost([1.0], 0)
+
+
+def _problems():
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.solvers.base import Terminal
+    out = []
+    for s, shape in enumerate([(10, 9, 8), (12, 10, 8), (9, 9, 9), (14, 8, 7), (8, 8, 10)]):
+        w = W.layered_boxes(shape, nbox=2 + s % 3, seed=s, ext_xy=(16, 48), ext_z=(16, 30))
+        terms = [Terminal(n, t) for n, t in zip(w.names, w.terminals)]
+        out.append((w.grid(), w.eps_cell, terms))
+    return out
+
+
+def _oracle_local(problems, cfg, gcfg, streams, reports):
+    from oracle import fs_oracle as O
+    res = []
+    for grid, eps, terms in problems:
+        g = O.Grid(grid.xn, grid.yn, grid.zn)
+        C, _ = O.capacitance_matrix(g, eps, [t.nodes for t in terms], method="direct")
+        res.append(C)
+    return res
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out = capacitance_matrices(_problems(), local=_oracle_local)
+        q.put((rank, [np.asarray(c) for c in out]))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_ranks_gather_the_whole_batch_in_order():
+    import torch.multiprocessing as mp
+    probs = _problems()
+    want = _oracle_local(probs, None, None, 1, None)
+    assert len(shard_by_cost([problem_cost(p) for p in probs], 2)[0]) > 0
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in procs:
+        r, mats = q.get(timeout=120)
+        got[r] = mats
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in (0, 1):
+        assert len(got[r]) == len(want)
+        for a, b in zip(got[r], want):
+            assert np.array_equal(a, b)

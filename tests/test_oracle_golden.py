@@ -131,3 +131,22 @@ def test_eqs_rc_stack_matches_reference(golden):
     assert np.abs(vm - d["spt50_vm"]).max() < 1e-10
     scale = np.abs(d["spt50_i_hi"]).max()
     assert np.abs(cur[:, 0] - d["spt50_i_hi"]).max() / scale < 1e-8
+
+
+def _projected(R):
+    n = R.shape[0]
+    P = np.eye(n) - np.ones((n, n)) / n
+    return P @ R @ P
+
+
+def test_resistance_matrix_matches_reference(golden):
+    # extraction.py:59-87: pinv keeps the round-off-null all-ones direction,
+    # so only P R P (resistance differences) is reproducible
+    d = golden("resistance")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    R, Y = O.resistance_matrix(g, d["sigma"], terms, method="direct")
+    want = _projected(d["R"])
+    assert np.abs(_projected(R) - want).max() <= 1e-9 * np.abs(want).max()
+    assert np.abs(Y.sum(axis=1)).max() <= 1e-9 * np.abs(np.diag(Y)).max()
