@@ -9,7 +9,7 @@ pointers and a ``cudaStream_t``.
 from __future__ import annotations
 
 import ctypes
-from ctypes import (POINTER, c_char_p, c_double, c_int, c_int32, c_longlong,
+from ctypes import (POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_longlong,
                     c_size_t, c_void_p)
 
 from ._build import LIB_PATH
@@ -69,6 +69,27 @@ _SIGNATURES = {
                                c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
                                c_int, c_int, c_int, c_int, c_int, c_int, c_void_p,
                                c_void_p]),
+    "fs_unet_param_count": (c_int, [POINTER(c_longlong)]),
+    "fs_unet_layer": (c_int, [c_int, POINTER(c_int), POINTER(c_int), POINTER(c_longlong),
+                              POINTER(c_longlong)]),
+    "fs_unet_workspace_bytes": (c_int, [c_int] * 5 + [POINTER(c_size_t)]),
+    "fs_unet_create": (c_int, [c_int] * 5 + [c_void_p, c_void_p, c_size_t, POINTER(c_void_p),
+                                             c_void_p]),
+    "fs_unet_sync": (c_int, [c_void_p, c_void_p]),
+    "fs_unet_forward": (c_int, [c_void_p, c_void_p, c_longlong, c_longlong, c_void_p, c_longlong,
+                                c_void_p, c_longlong, c_void_p, c_longlong, c_longlong, c_void_p]),
+    "fs_unet_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
+                                   c_void_p, c_void_p]),
+    "fs_unet_gradient": (c_int, [c_void_p] * 8),
+    "fs_unet_error": (c_int, [c_void_p, POINTER(c_int), c_void_p]),
+    "fs_unet_destroy": (c_int, [c_void_p]),
+    "fs_eq_apply": (c_int, [c_void_p] * 6 + [c_int] * 4 + [c_void_p]),
+    "fs_pcg_plan_levels": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "fs_pcg_plan_level_data": (c_int, [c_void_p, c_int, POINTER(c_void_p), POINTER(c_void_p),
+                                       POINTER(c_void_p)]),
+    "fs_pcg_plan_unet_workspace_bytes": (c_int, [c_void_p, c_int, POINTER(c_size_t)]),
+    "fs_pcg_plan_set_unet": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "fs_pcg_plan_sync_unet": (c_int, [c_void_p, c_void_p]),
     "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
     "fs_pcg_plan_launches": (c_longlong, [c_void_p]),

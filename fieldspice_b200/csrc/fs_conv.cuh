@@ -71,6 +71,8 @@ __device__ __forceinline__ uint32_t tmem_cols(int n) {
   return c;
 }
 
+// The kernels are defined in exactly one translation unit (fs_net.cu).
+#ifdef FS_CONV_DEFINE_KERNELS
 __global__ void __launch_bounds__(128)
     k_conv3d_tc(const __grid_constant__ CUtensorMap xmap, ConvArgs a) {
   extern __shared__ uint8_t conv_smem_raw[];
@@ -245,5 +247,6 @@ __global__ void k_pack_weights(const float* __restrict__ w, int cin, int cout, i
     out[dst] = *(uint16_t*)&b;
   }
 }
+#endif  // FS_CONV_DEFINE_KERNELS
 
 }  // namespace fs

@@ -12,6 +12,7 @@
 
 #include "fieldspice_b200.h"
 #include "fs_common.cuh"
+#define FS_CONV_DEFINE_KERNELS
 #include "fs_conv.cuh"
 #include "fs_net.cuh"
 

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <stdint.h>
+
+#include "fieldspice_b200.h"
 #include "fs_conv.cuh"
 
 namespace fs {
@@ -36,3 +39,12 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s);
 int pack_weights(const float* w, int cin, int cout, int flip, void* out, cudaStream_t s);
 
 }  // namespace fs
+
+// The U-Net forward pass on caller buffers (defined in fs_unet.cu): rhs and
+// out in any (node, sample) strides, the level's three mass arrays and
+// labels with a per-sample stride (0: shared by every sample).
+int unet_forward(fs_unet* U, const float* rhs, long long rhs_sn, long long rhs_sb,
+                 const float* emx, const float* emy, const float* emz, long long em_sb,
+                 const uint8_t* lab, long long lab_sb, float* out, long long out_sn,
+                 long long out_sb, bool normalised, cudaStream_t s);
+long long unet_forward_launches();

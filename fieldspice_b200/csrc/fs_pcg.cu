@@ -40,6 +40,7 @@
 #include "fs_common.cuh"
 #include "fs_tma.cuh"
 #include "fs_mg.cuh"
+#include "fs_net.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -533,6 +534,59 @@ __global__ void __launch_bounds__(fs::kBlock)
   }
 }
 
+// ---- flexible CG (nonlinear preconditioner): gamma = r~.z and
+// beta = -(z . A~p_old) / (p_old . A~p_old), the A~-orthogonalisation of the
+// new direction against the previous one (FCG with one stored direction).
+// q still holds A~p_old from this iteration's stencil, pq its p.q.
+template <typename T, int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_rz_flex(Dims d, const T* __restrict__ r, const T* __restrict__ z,
+              const T* __restrict__ q, double* __restrict__ partials, RhsState* st,
+              Control* ctl) {
+  if (ctl->all_done) return;
+  double acc[2 * K];
+#pragma unroll
+  for (int t = 0; t < 2 * K; ++t) acc[t] = 0.0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T rv[K], zv[K], qv[K];
+    fs::ldv_ro<T, K>(r, n, rv);
+    fs::ldv_ro<T, K>(z, n, zv);
+    fs::ldv_ro<T, K>(q, n, qv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      acc[t] += (double)rv[t] * (double)zv[t];
+      acc[K + t] += (double)zv[t] * (double)qv[t];
+    }
+  }
+  fs::block_partials<2 * K>(acc, partials);
+  if (fs::last_block(&ctl->tickets[kTicketRz])) {
+    double tot[2 * K];
+    fs::grid_total<2 * K>(partials, gridDim.x, tot);
+    if (threadIdx.x < K) {
+      RhsState& s = st[threadIdx.x];
+      if (s.active) {
+        const double g = tot[threadIdx.x], zq = tot[K + threadIdx.x];
+        if (!isfinite(g) || !isfinite(zq)) {
+          s.active = 0;
+          s.status = FS_NAN;
+        } else if (s.fresh || !(s.pq > 0.0)) {
+          s.gamma = g;
+          s.gamma_old = g;
+          s.beta = 0.0;
+          s.fresh = 0;
+        } else {
+          s.gamma_old = s.gamma;
+          s.gamma = g;
+          s.beta = -zq / s.pq;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) refresh_done(st, ctl, K);
+  }
+}
+
 // ---- fallback for rows narrower than 16 B (float k <= 2, double k = 1) -----
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
@@ -975,6 +1029,12 @@ struct fs_pcg_plan {
   double kernel_ms[6];
   int trace;               // record ev[6..7] around fine-level post-smoothing
   long long kernel_samples;
+  // Learned preconditioner: the V-cycle stops at level `learned` and the
+  // U-Net maps that level's right-hand side to its correction; CG becomes
+  // flexible.  -1: plain multigrid.
+  int learned = -1;
+  fs_unet* net = nullptr;
+  int net_status = FS_OK;
 };
 
 namespace {
@@ -1147,6 +1207,20 @@ struct Impl {
                     long long* nl, bool dry = false) {
     MgLevel& L = P->lev[l];
     const int* done = &P->ctl->all_done;
+    if constexpr (std::is_same<T, float>::value) {
+      if (l == P->learned && P->net) {
+        // x[0] = U-Net(b): rhs and output K-interleaved, geometry shared
+        if (!dry) {
+          const float* em[3] = {(const float*)(l ? L.em[0] : P->ex), (const float*)(l ? L.em[1] : P->ey),
+                                (const float*)(l ? L.em[2] : P->ez)};
+          const int st = unet_forward(P->net, b, K, 1, em[0], em[1], em[2], 0,
+                                      l ? L.label : P->label, 0, (float*)L.x[0], K, 1, false, s);
+          if (st != FS_OK) P->net_status = st;
+        }
+        *nl += unet_forward_launches();
+        return 0;
+      }
+    }
     const bool last = l == P->nlev - 1;
     const int deg = last ? P->mg.coarse_deg : P->mg.smooth_deg;
     double cd[64], cr[64];
@@ -1225,9 +1299,14 @@ struct Impl {
     long long nl = 0;
     const int zi = vcycle(P, 0, (const T*)P->r, s, &nl);
     P->z = P->lev[0].x[zi];
-    k_rz<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r,
-                                              (const T*)P->z, P->partials,
-                                              P->st, P->ctl);
+    if (P->learned >= 0)
+      k_rz_flex<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r, (const T*)P->z,
+                                                     (const T*)P->q, P->partials, P->st,
+                                                     P->ctl);
+    else
+      k_rz<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r,
+                                                (const T*)P->z, P->partials,
+                                                P->st, P->ctl);
     return nl + 1;
   }
   static void finalize(fs_pcg_plan* P, cudaStream_t s) {
@@ -1251,6 +1330,7 @@ bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
     if (op >= 5 && op <= 8) Impl<T, KK>::kernel(P, op - 5, par, s); \
     if (op == 9) { Impl<T, KK>::mg_setup(P, s); Impl<T, KK>::locate_z(P); } \
     if (op == 10) P->launches_per_iter = Impl<T, KK>::precondition(P, s); \
+    if (op == 11) Impl<T, KK>::locate_z(P);                        \
     return true;
   switch (k) {
     FS_OP(1)
@@ -1301,6 +1381,39 @@ void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
   if (P->precond) dispatch(P, 10, s);  // V-cycle and r.z
   P->trace = 0;
   cudaEventRecordWithFlags(P->ev[5], s, cudaEventRecordExternal);
+}
+
+void locate_z_all(fs_pcg_plan* P) { dispatch(P, 11, nullptr); }
+
+// (Re)capture the graph of `chunk` CG iterations on the plan's capture
+// stream; chunk is even, so every launch starts on parity 0 (p[0] = p_old).
+int capture_graph(fs_pcg_plan* P) {
+  cudaError_t e;
+  if (P->exec) {
+    cudaGraphExecDestroy(P->exec);
+    P->exec = nullptr;
+  }
+  if (P->precond) locate_z_all(P);
+  cudaGraph_t graph = nullptr;
+  if ((e = cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return fs_cuda_status("cudaStreamBeginCapture", e);
+  for (int it = 0; it < P->chunk; ++it) {
+    if (it == 0) {
+      dispatch_first(P, P->cap);
+    } else {
+      dispatch(P, 3, P->cap, 0, 0, 0, 0, it & 1);
+    }
+  }
+  e = cudaStreamEndCapture(P->cap, &graph);
+  if (e != cudaSuccess) return fs_cuda_status("cudaStreamEndCapture", e);
+  if (P->net_status != FS_OK) {
+    cudaGraphDestroy(graph);
+    return P->net_status;
+  }
+  e = cudaGraphInstantiate(&P->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fs_cuda_status("cudaGraphInstantiate", e);
+  return FS_OK;
 }
 
 }  // namespace
@@ -1453,23 +1566,11 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   for (int t = 0; t < 8; ++t)
     if ((e = cudaEventCreate(&P->ev[t])) != cudaSuccess)
       return fail("cudaEventCreate", e);
-  cudaGraph_t graph = nullptr;
-  if ((e = cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal)) !=
-      cudaSuccess)
-    return fail("cudaStreamBeginCapture", e);
-  // chunk is even, so every graph launch starts on parity 0 (p[0] = p_old)
-  for (int it = 0; it < P->chunk; ++it) {
-    if (it == 0) {
-      dispatch_first(P, P->cap);
-    } else {
-      dispatch(P, 3, P->cap, 0, 0, 0, 0, it & 1);
-    }
+  const int cst = capture_graph(P);
+  if (cst != FS_OK) {
+    fs_pcg_plan_destroy(P);
+    return cst;
   }
-  e = cudaStreamEndCapture(P->cap, &graph);
-  if (e != cudaSuccess) return fail("cudaStreamEndCapture", e);
-  e = cudaGraphInstantiate(&P->exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) return fail("cudaGraphInstantiate", e);
   *plan = P;
   return FS_OK;
 }
@@ -1636,6 +1737,122 @@ int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
   return worst;
 }
 
+}  // extern "C"
+
+namespace {
+
+// y = A~ x on free nodes (unit diagonal, equilibrated masses), 0 elsewhere.
+template <int K>
+__global__ void __launch_bounds__(fs::kBlock)
+    k_eq_apply(Dims d, const float* __restrict__ ex, const float* __restrict__ ey,
+               const float* __restrict__ ez, const uint8_t* __restrict__ label,
+               const float* __restrict__ x, float* __restrict__ y) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    float ax[K];
+    fs::apply_eq<float, K>(d, ex, ey, ez, x, n, ax);
+    if (label[n] != FS_LABEL_FREE)
+#pragma unroll
+      for (int t = 0; t < K; ++t) ax[t] = 0.0f;
+    fs::stv<float, K>(y, n, ax);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, const float* ez,
+                const uint8_t* label, int nx, int ny, int nz, int nrhs, void* stream) {
+  if (!x || !y || !ex || !ey || !ez || !label || nx < 1 || ny < 1 || nz < 1) return FS_BAD_ARG;
+  const Dims d = fs::make_dims(nx, ny, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+#define FS_EQ(KK)                                                                  \
+  case KK: {                                                                       \
+    const int g = fs_grid_blocks((const void*)k_eq_apply<KK>, d.N);                \
+    k_eq_apply<KK><<<g, fs::kBlock, 0, s>>>(d, ex, ey, ez, label, x, y);           \
+    break;                                                                         \
+  }
+  switch (nrhs) {
+    FS_EQ(1)
+    FS_EQ(2)
+    FS_EQ(4)
+    FS_EQ(8)
+    FS_EQ(16)
+    default:
+      return FS_BAD_ARG;
+  }
+#undef FS_EQ
+  FS_CHECK_LAUNCH("k_eq_apply");
+  return FS_OK;
+}
+
+int fs_pcg_plan_levels(const fs_pcg_plan* P, int* nlev, int* dims) {
+  if (!P || !nlev) return FS_BAD_ARG;
+  *nlev = P->precond ? P->nlev : 1;
+  if (dims)
+    for (int l = 0; l < *nlev; ++l) {
+      const Dims& d = P->precond ? P->lev[l].d : P->d;
+      dims[3 * l] = d.nx;
+      dims[3 * l + 1] = d.ny;
+      dims[3 * l + 2] = d.nz;
+    }
+  return FS_OK;
+}
+
+int fs_pcg_plan_level_data(const fs_pcg_plan* P, int level, const void** em, const uint8_t** label,
+                           const void** scale) {
+  if (!P || !P->precond || level < 0 || level >= P->nlev || !em || !label) return FS_BAD_ARG;
+  const MgLevel& L = P->lev[level];
+  em[0] = level ? L.em[0] : P->ex;
+  em[1] = level ? L.em[1] : P->ey;
+  em[2] = level ? L.em[2] : P->ez;
+  *label = level ? L.label : P->label;
+  if (scale) *scale = level ? (const void*)L.s : nullptr;
+  return FS_OK;
+}
+
+int fs_pcg_plan_unet_workspace_bytes(const fs_pcg_plan* P, int level, size_t* bytes) {
+  if (!P || !bytes || !P->precond || P->precision != FS_PRECISION_MIXED || level < 0 ||
+      level >= P->nlev)
+    return FS_BAD_ARG;
+  const Dims& d = P->lev[level].d;
+  return fs_unet_workspace_bytes(d.nx, d.ny, d.nz, P->nrhs, 0, bytes);
+}
+
+int fs_pcg_plan_set_unet(fs_pcg_plan* P, int level, float* theta, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  if (!P || !P->precond || P->precision != FS_PRECISION_MIXED || level < -1 ||
+      level >= P->nlev) {
+    fs_set_error_msg("learned preconditioner: needs a mixed-precision multigrid plan and a valid level");
+    return FS_BAD_ARG;
+  }
+  if (P->net) {
+    fs_unet_destroy(P->net);
+    P->net = nullptr;
+  }
+  P->learned = -1;
+  P->net_status = FS_OK;
+  if (level >= 0) {
+    if (!theta) return FS_BAD_ARG;
+    const Dims& d = P->lev[level].d;
+    fs_unet* net = nullptr;
+    const int st = fs_unet_create(d.nx, d.ny, d.nz, P->nrhs, 0, theta, workspace, workspace_bytes,
+                                  &net, stream);
+    if (st != FS_OK) return st;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return fs_cuda_status("cudaStreamSynchronize", e);
+    P->net = net;
+    P->learned = level;
+  }
+  return capture_graph(P);
+}
+
+int fs_pcg_plan_sync_unet(fs_pcg_plan* P, void* stream) {
+  if (!P || !P->net) return FS_BAD_ARG;
+  return fs_unet_sync(P->net, stream);
+}
+
 const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* P) {
   return P ? P->label : nullptr;
 }
@@ -1654,6 +1871,7 @@ int fs_pcg_plan_kernel_times(const fs_pcg_plan* P, double* ms,
 
 int fs_pcg_plan_destroy(fs_pcg_plan* P) {
   if (!P) return FS_OK;
+  if (P->net) fs_unet_destroy(P->net);
   for (int t = 0; t < 8; ++t)
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
   if (P->exec) cudaGraphExecDestroy(P->exec);

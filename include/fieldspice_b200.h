@@ -256,6 +256,66 @@ int fs_conv3d_bf16(const void* x, int ctot_in, int cin_off, int cin, const void*
                    const void* mask, int ctot_mask, int mask_off, int batch, int X, int Y,
                    int Z, int relu, int accumulate, int* error, void* stream);
 
+
+/* ---- Learned preconditioner: the U-Net --------------------------------- *
+ * A 4-level BF16 3-D U-Net (channels 16/32/48/64, fourteen 3x3x3
+ * convolutions on tensor cores, ReLU, average pooling, nearest upsampling
+ * with skip concatenation, a 1x1 FP32 head) mapping a level residual and the
+ * level's equilibrated masses and fixed flags to an error estimate.
+ * Parameters: one caller-owned FP32 device vector theta of
+ * fs_unet_param_count() entries; fs_unet_layer(l) gives layer l's channels
+ * and the offsets of its weights [27][cout][cin] and bias (l = 14: the head,
+ * 16 weights then 1 bias).  train != 0 adds gradients and Adam state.      */
+typedef struct fs_unet fs_unet;
+int fs_unet_param_count(long long* n);
+int fs_unet_layer(int l, int* cin, int* cout, long long* woff, long long* boff);
+int fs_unet_workspace_bytes(int X, int Y, int Z, int batch, int train, size_t* bytes);
+int fs_unet_create(int X, int Y, int Z, int batch, int train, float* theta, void* workspace,
+                   size_t workspace_bytes, fs_unet** net, void* stream);
+/* Re-pack the tensor-core weight images after theta changed on the host side. */
+int fs_unet_sync(fs_unet* net, void* stream);
+/* out[b*out_sb + n*out_sn] = network(rhs_b, em_b, label_b) in rhs units, 0 on
+ * fixed nodes.  rhs[b*rhs_sb + n*rhs_sn]; em: sample b's +x, +y, +z masses at
+ * em + b*em_sb + {0, N, 2N} (FP32); label[b*label_sb + n] (FS_LABEL_*).      */
+int fs_unet_forward(fs_unet* net, const float* rhs, long long rhs_sn, long long rhs_sb,
+                    const float* em, long long em_sb, const uint8_t* label, long long label_sb,
+                    float* out, long long out_sn, long long out_sb, void* stream);
+/* One Adam step on the relative squared error of the network's output
+ * against target (planar [batch][N] inputs, em [batch][3][N]); loss: device
+ * float receiving the batch loss before the step (or NULL).                */
+int fs_unet_train_step(fs_unet* net, const float* rhs, const float* em, const uint8_t* label,
+                       const float* target, float lr, float* loss, void* stream);
+/* The same loss and its gradient dL/dtheta (device, theta-sized), no update. */
+int fs_unet_gradient(fs_unet* net, const float* rhs, const float* em, const uint8_t* label,
+                     const float* target, float* grad, float* loss, void* stream);
+/* Host int: 1 if a staged load of a network convolution timed out.        */
+int fs_unet_error(const fs_unet* net, int* flag, void* stream);
+int fs_unet_destroy(fs_unet* net);
+
+
+/* ---- Learned preconditioner inside a CG plan --------------------------- *
+ * A mixed-precision multigrid plan can stop its V-cycle at `level` and ask
+ * the U-Net (parameters theta, caller-owned, read at every application) for
+ * that level's correction instead of recursing: smoothing on the levels
+ * above, the network below.  The preconditioner is then nonlinear, so the
+ * plan switches to flexible CG (beta = -z.Ap / p.Ap).  level = -1 restores
+ * plain multigrid.  fs_pcg_plan_levels: the level count and dims (3 ints
+ * per level); fs_pcg_plan_level_data: a level's equilibrated masses (FP32 in
+ * a mixed plan), labels and diag^-1/2 (NULL on level 0).                   */
+int fs_pcg_plan_levels(const fs_pcg_plan* plan, int* nlev, int* dims);
+/* y = A~ x for an equilibrated level operator (FP32, nrhs-interleaved,
+ * unit diagonal, masses ex/ey/ez of fs_pcg_plan_level_data); 0 on nodes
+ * whose label is not FS_LABEL_FREE.                                         */
+int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, const float* ez,
+                const uint8_t* label, int nx, int ny, int nz, int nrhs, void* stream);
+int fs_pcg_plan_level_data(const fs_pcg_plan* plan, int level, const void** em,
+                           const uint8_t** label, const void** scale);
+int fs_pcg_plan_unet_workspace_bytes(const fs_pcg_plan* plan, int level, size_t* bytes);
+int fs_pcg_plan_set_unet(fs_pcg_plan* plan, int level, float* theta, void* workspace,
+                         size_t workspace_bytes, void* stream);
+/* Re-pack the plan's network weights after theta changed.                  */
+int fs_pcg_plan_sync_unet(fs_pcg_plan* plan, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,12 +32,13 @@ def test_resistance_matrix_matches_reference(cuda, golden, precision, preconditi
              for i, (a0, b0, c0, a1, b1, c1) in enumerate(d["boxes"])]
     rep = {}
     with pytest.warns(RuntimeWarning, match="coupled to nothing"):
-        R = EX.resistance_matrix(g, d["sigma"], terms, config=SolverConfig(tol=1e-12),
+        R = EX.resistance_matrix(g, d["sigma"], terms, config=SolverConfig(tol=1e-14),
                                  report=rep,
                                  gpu=GPUConfig(precision=precision,
                                                preconditioner=preconditioner))
     # the conductances themselves against the oracle (pinned to the reference
-    # in tests/test_oracle_golden.py) at the solve's accuracy
+    # in tests/test_oracle_golden.py); copper next to silicon makes the system
+    # stiff (contrast 6e5), so the solve runs to relres 1e-14 for 1e-9 here
     from oracle import fs_oracle as O
     og = O.Grid(d["x"], d["y"], d["z"])
     _, Yo = O.resistance_matrix(og, d["sigma"], [t.nodes for t in terms], method="direct")
