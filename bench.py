@@ -180,11 +180,11 @@ def run_ours(args, rank, world, local_rank):
     for t in terms:
         t.nodes = torch.from_numpy(np.ascontiguousarray(t.nodes, dtype=np.int64)).pin_memory().numpy()
 
-    def step_device(precision, pc=args.preconditioner):
+    def step_device(precision, pc=args.preconditioner, learned=None):
         op = D.DeviceOperator(grid, eps_dev)
         C, qs, info = extract_capacitance(op, term_dev, wall_dev, shield_dev,
                                           tol=TOL, precision=precision,
-                                          preconditioner=pc)
+                                          preconditioner=pc, learned=learned)
         info["gpu_launches"] += 1 + 2  # mass build + plan setup kernels
         return C, qs, info
 
@@ -274,6 +274,7 @@ def run_ours(args, rank, world, local_rank):
 
     if not args.no_variants and world == 1:
         variants["batch64"] = batch_variant(timed)
+        variants["learned_fcg"] = learned_variant(timed, step_device, C, args)
 
     if rank != 0:
         return
@@ -344,6 +345,45 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(shape, info["iterations"], args.cpu_sample_iters)
     print(json.dumps(line), flush=True)
+
+
+def learned_variant(timed, step_device, C_default, args):
+    """The learned preconditioner (U-Net coarse-level correction inside
+    flexible CG) on this workload: trained here on 4096 residual-to-error
+    pairs from Jacobi-PCG iterates on 64 seeded 128^3 geometries of the same
+    family (seeds disjoint from the timed one), then timed like the default
+    extraction.  Reports solves/s, iterations, training cost, and the same
+    extraction with the network's output zeroed (what the network gains)."""
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.learned import LearnedPreconditioner
+    t0 = time.perf_counter()
+    train = [W.layered_boxes((128, 128, 128), nbox=NBOX, seed=1000 + s) for s in range(64)]
+    net = LearnedPreconditioner.train(train, level=2, epochs=3, batch=8, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    nv = max(2, args.steps // 2)
+    ms, outs = timed(lambda: step_device("mixed", "learned", net), nv, 1)
+    Cl, _, info = outs[-1]
+    ms0, outs0 = timed(lambda: step_device("mixed", "learned", net.zero()), 1, 0)
+    scale = float(np.abs(np.diag(C_default)).max())
+    err = None
+    if FULLSIZE_JSON.exists() and tuple(int(v) for v in args.shape.split(",")) == SHAPE:
+        ref = json.loads(FULLSIZE_JSON.read_text())
+        Cref = np.asarray(ref["C_tol1e-12_unsymmetrised"])
+        err = float(np.abs(Cl - Cref).max() / np.abs(np.diag(Cref)).max())
+    return {"value": NBOX / (ms / nv / 1000.0), "ms_per_step": ms / nv,
+            "iterations": info["iterations"], "learned_fallback": info.get("learned_fallback"),
+            "relres_fp64_max": info["residual"],
+            "C_err_vs_fp64_oracle": err,
+            "C_rel_diff_vs_default": float(np.abs(Cl - C_default).max() / scale),
+            "kernel_ms": info["kernel_ms"],
+            "network_zeroed": {"value": NBOX / (ms0 / 1000.0),
+                               "iterations": outs0[-1][2]["iterations"]},
+            "training": {"pairs": net.pairs, "geometries": len(train), "shape": [128, 128, 128],
+                         "level": net.level, "epochs": 3, "batch": 8,
+                         "data_seconds": net.data_time, "fit_seconds": net.train_time,
+                         "total_seconds": t_train,
+                         "loss_first": net.history[0] if net.history else None,
+                         "loss_last": net.history[-1] if net.history else None}}
 
 
 def batch_variant(timed):

@@ -93,7 +93,7 @@ class _Extraction:
         self.tol = float(cfg.tol)
         self.system = EliminatedSystem(
             self.op, label, nt, precision=gcfg.precision,
-            preconditioner=resolve_preconditioner(cfg, gcfg))
+            preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned)
         self.maxiter = (self.system.default_maxiter() if gcfg.maxiter is None
                         else int(gcfg.maxiter))
         group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)
@@ -171,7 +171,10 @@ def _extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
             stats = _stats_list(stat_arrays[j], e.system.nrhs)
             if status[j] not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN, L.FS_STALLED):
                 L.check("fs_pcg_plans_solve", status[j])
-            _, stats = e.system.finish_auto(status[j], stats, tol, e.maxiter)
+            stj = status[j]
+            if e.system.preconditioner == "learned":
+                stj, stats = e.system.finish_learned(stj, stats, tol, e.maxiter)
+            _, stats = e.system.finish_auto(stj, stats, tol, e.maxiter)
             raise_on_status(stats, tol, "gpu-cg")
             out[i], rep = e.collect(stats)
             if reports is not None:

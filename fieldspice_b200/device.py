@@ -225,14 +225,21 @@ class EliminatedSystem:
 
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
                  precision: str = "auto", with_source: bool = False,
-                 preconditioner: str = "jacobi"):
+                 preconditioner: str = "jacobi", learned=None):
         import torch
         if precision not in ("auto", "mixed", "fp64"):
             raise ValueError(f"precision must be 'auto', 'mixed' or 'fp64', got {precision!r}")
-        if preconditioner not in ("jacobi", "mg"):
-            raise ValueError(f"preconditioner must be 'jacobi' or 'mg', got {preconditioner!r}")
+        if preconditioner not in ("jacobi", "mg", "learned"):
+            raise ValueError(f"preconditioner must be 'jacobi', 'mg' or 'learned', "
+                             f"got {preconditioner!r}")
+        if preconditioner == "learned":
+            if learned is None:
+                raise ValueError("preconditioner='learned' needs a trained network")
+            if precision == "fp64":
+                raise ValueError("the learned preconditioner runs in mixed precision")
         self.preconditioner = preconditioner
-        self._pc = L.PRECOND_MG if preconditioner == "mg" else L.PRECOND_JACOBI
+        self.learned = learned
+        self._pc = L.PRECOND_JACOBI if preconditioner == "jacobi" else L.PRECOND_MG
         self.op = op
         self.k = pad_rhs(nrhs)
         self.nrhs = nrhs
@@ -255,6 +262,11 @@ class EliminatedSystem:
         self.labels = self.workspace[off:off + N]
         counts = torch.bincount(self.labels.to(torch.int64), minlength=4).cpu().numpy()
         self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts[:4])
+        self._net_ws = None
+        self.learned_level = None
+        self.learned_fallback = False
+        if preconditioner == "learned":
+            self.learned_level = learned.attach(self._plan, self)
         self.setup_time = time.perf_counter() - t0
         self.launches = 0
         self._last_plan = self._plan
@@ -305,7 +317,25 @@ class EliminatedSystem:
         if self.fell_back:
             return self._run(self._fp64[0], tol, mi, warm)
         st, stats = self._run(self._plan, tol, mi, warm)
+        if self.preconditioner == "learned":
+            st, stats = self.finish_learned(st, stats, tol, mi)
         return self.finish_auto(st, stats, tol, mi)
+
+    def finish_learned(self, st: int, stats: list, tol: float, maxiter: int):
+        """If flexible CG with the network stalled or hit ``maxiter``, detach
+        the network (plain multigrid PCG) and continue from the iterate."""
+        bad = any(s["status"] in (L.FS_NOT_CONVERGED, L.FS_STALLED, L.FS_NAN) for s in stats)
+        if not bad:
+            return st, stats
+        L.check("fs_pcg_plan_set_unet", L.lib().fs_pcg_plan_set_unet(
+            self._plan, -1, None, None, 0, L.stream_ptr()))
+        self.learned_fallback = True
+        st, stats2 = self._run(self._plan, tol, maxiter, True)
+        for a, b in zip(stats, stats2):
+            b["iterations"] += a["iterations"]
+            b["reliable_updates"] += a["reliable_updates"]
+            b["learned_fallback"] = True
+        return st, stats2
 
     def finish_auto(self, st: int, stats: list, tol: float, maxiter: int):
         """In ``"auto"`` mode, continue a mixed solve whose RHS stalled or hit

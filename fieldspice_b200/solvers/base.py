@@ -67,13 +67,20 @@ class GPUConfig:
         method), ``"mg"`` (a geometric-multigrid V-cycle as the CG
         preconditioner; same FP64 stopping rule), or ``None``: chosen from
         ``SolverConfig.linear_solver`` (:func:`resolve_preconditioner`).
+        ``"learned"``: the multigrid V-cycle with its lower levels replaced
+        by a trained U-Net (``learned``, a
+        :class:`fieldspice_b200.learned.LearnedPreconditioner`) inside
+        flexible CG, falling back to plain multigrid if FCG stalls.
     maxiter
         Iteration cap; ``None`` uses the reference's ``max(500, 10*sqrt(n))``
         (``poisson.py:535-536``).
+    learned
+        The trained network for ``preconditioner="learned"``.
     """
     precision: str = "auto"
     preconditioner: str | None = None
     maxiter: int | None = None
+    learned: object | None = None
 
 
 def resolve_preconditioner(cfg, gpu) -> str:
@@ -86,8 +93,11 @@ def resolve_preconditioner(cfg, gpu) -> str:
     ``GPUConfig.preconditioner`` wins.
     """
     if gpu is not None and gpu.preconditioner is not None:
-        if gpu.preconditioner not in ("jacobi", "mg"):
+        if gpu.preconditioner not in ("jacobi", "mg", "learned"):
             raise ValueError(f"unknown preconditioner {gpu.preconditioner!r}")
+        if gpu.preconditioner == "learned" and getattr(gpu, "learned", None) is None:
+            raise ValueError("preconditioner='learned' needs GPUConfig.learned "
+                             "(a trained LearnedPreconditioner)")
         return gpu.preconditioner
     want = getattr(cfg, "linear_solver", "auto")
     if want not in ("auto", "direct", "cg", "amg"):

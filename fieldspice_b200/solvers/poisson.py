@@ -219,7 +219,8 @@ class PoissonSolver:
         C, q_shield, info = extract_capacitance(
             self.op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,
-            preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+            preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+            learned=self.gpu.learned)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         rep["terminals"] = tuple(t.name for t in terms)
@@ -340,7 +341,8 @@ class PoissonSolver:
 
 def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                         tol: float, precision: str = "auto",
-                        maxiter: int | None = None, preconditioner: str = "jacobi"):
+                        maxiter: int | None = None, preconditioner: str = "jacobi",
+                        learned=None):
     """Device core of the extraction: inputs already in HBM.
 
     ``term_dev``: sorted unique int64 node tensors, one per terminal;
@@ -376,7 +378,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
             if system is not None:
                 system.close()
             system = EliminatedSystem(op, label, kb, precision=precision,
-                                      preconditioner=preconditioner)
+                                      preconditioner=preconditioner, learned=learned)
             setup_time += system.setup_time
         system.nrhs = kb
         group.fill_(-1)
@@ -413,6 +415,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         "relres_fp64": [s["relres"] for s in stats_all],
         "reliable_updates": [s["reliable_updates"] for s in stats_all],
         "fp64_fallback": bool(system.fell_back),
+        "learned_fallback": bool(system.learned_fallback),
         "gpu_launches": launches,
         "kernel_ms": system.kernel_times(),
         "notes": (),
