@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    ap.add_argument("--unet-forward", action="store_true",
+                    help="time the U-Net forward pass alone at the learned level of the "
+                         "256x256x128 workload (64x64x32 nodes, 8 RHS), random weights")
     ap.add_argument("--single", action="store_true",
                     help="one device-resident extraction only (profiler runs)")
     return ap.parse_args()
@@ -275,6 +278,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_variants and world == 1:
         variants["batch64"] = batch_variant(timed)
         variants["learned_fcg"] = learned_variant(timed, step_device, C, args)
+        variants["eqs_transient"] = eqs_variant()
 
     if rank != 0:
         return
@@ -347,6 +351,9 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+EPOCHS = 5
+
+
 def learned_variant(timed, step_device, C_default, args):
     """The learned preconditioner (U-Net coarse-level correction inside
     flexible CG) on this workload: trained here on 4096 residual-to-error
@@ -358,12 +365,15 @@ def learned_variant(timed, step_device, C_default, args):
     from fieldspice_b200.learned import LearnedPreconditioner
     t0 = time.perf_counter()
     train = [W.layered_boxes((128, 128, 128), nbox=NBOX, seed=1000 + s) for s in range(64)]
-    net = LearnedPreconditioner.train(train, level=2, epochs=3, batch=8, lr=1e-3, seed=0)
+    net = LearnedPreconditioner.train(train, level=2, epochs=EPOCHS, batch=8, lr=1e-3, seed=0)
     t_train = time.perf_counter() - t0
     nv = max(2, args.steps // 2)
     ms, outs = timed(lambda: step_device("mixed", "learned", net), nv, 1)
     Cl, _, info = outs[-1]
     ms0, outs0 = timed(lambda: step_device("mixed", "learned", net.zero()), 1, 0)
+    rnet = net.with_mode("replace")
+    msr, outsr = timed(lambda: step_device("mixed", "learned", rnet), 1, 1)
+    msr0, outsr0 = timed(lambda: step_device("mixed", "learned", rnet.zero()), 1, 0)
     scale = float(np.abs(np.diag(C_default)).max())
     err = None
     if FULLSIZE_JSON.exists() and tuple(int(v) for v in args.shape.split(",")) == SHAPE:
@@ -376,14 +386,60 @@ def learned_variant(timed, step_device, C_default, args):
             "C_err_vs_fp64_oracle": err,
             "C_rel_diff_vs_default": float(np.abs(Cl - C_default).max() / scale),
             "kernel_ms": info["kernel_ms"],
+            "mode": "hybrid: network guess at level 2 + V-cycle on its residual",
             "network_zeroed": {"value": NBOX / (ms0 / 1000.0),
                                "iterations": outs0[-1][2]["iterations"]},
+            "replace_mode": {"value": NBOX / (msr / 1000.0),
+                             "iterations": outsr[-1][2]["iterations"],
+                             "network_zeroed_value": NBOX / (msr0 / 1000.0),
+                             "network_zeroed_iterations": outsr0[-1][2]["iterations"]},
             "training": {"pairs": net.pairs, "geometries": len(train), "shape": [128, 128, 128],
-                         "level": net.level, "epochs": 3, "batch": 8,
+                         "level": net.level, "epochs": EPOCHS, "batch": 8,
                          "data_seconds": net.data_time, "fit_seconds": net.train_time,
                          "total_seconds": t_train,
                          "loss_first": net.history[0] if net.history else None,
                          "loss_last": net.history[-1] if net.history else None}}
+
+
+def eqs_variant(shape=(192, 192, 96), steps=200):
+    """Backward-Euler EQS transient: copper boxes in oxide over doped
+    silicon, two ports driven by a 1 V ramp (10 ps rise), dt = 1 ps, 200
+    steps.  The default path (mixed precision, multigrid, warm-started steps)
+    against the same transient in FP64 at relres 1e-12 (the FP64 reference
+    method): per-step port-current error and time per step."""
+    import torch
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    from fieldspice_b200.solvers.eqs import EQSSolver
+    w = W.eqs_interconnect(shape, nbox=6, nports=2, seed=0)
+    g = w.grid()
+    ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
+    terms = [Terminal("port0", w.terminals[0], voltage=ramp),
+             Terminal("port1", w.terminals[1], voltage=0.0)]
+    bc = BoundarySpec(zlo=Dirichlet(0.0))
+
+    def run(precision, tol):
+        s = EQSSolver(g, w.eps_cell, w.sigma_cell, SolverConfig(tol=tol),
+                      gpu=GPUConfig(precision=precision, preconditioner="mg"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = s.solve(terms, t_end=steps * 1e-12, dt=1e-12, bc=bc)
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+    r, t = run("auto", TOL)
+    rf, tf = run("fp64", 1e-12)
+    i0, i1 = np.asarray(r.i("port0")), np.asarray(r.i("port1"))
+    f0, f1 = np.asarray(rf.i("port0")), np.asarray(rf.i("port1"))
+    scale = max(np.abs(f0).max(), np.abs(f1).max())
+    err = np.maximum(np.abs(i0 - f0), np.abs(i1 - f1)) / scale
+    return {"metric": "EQS steps/s (192x192x96, 200 steps, dt 1 ps)",
+            "value": steps / t, "seconds": t, "fp64_seconds": tf,
+            "nodes": int(np.prod(shape)),
+            "current_err_vs_fp64_max": float(err.max()),
+            "current_err_vs_fp64_final": float(err[-1]),
+            "per_step_err_quantiles": [float(np.quantile(err, q)) for q in (0.5, 0.9, 1.0)],
+            "precision": "auto (mixed, FP64 continuation on stall)", "tol": TOL}
 
 
 def batch_variant(timed):
@@ -535,6 +591,56 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_unet_forward(args, dims=(64, 64, 32), batch=8):
+    """U-Net forward timing (CUDA events) and its tensor-core FLOP rate."""
+    import ctypes
+    import torch
+    from fieldspice_b200 import _lib as L
+    from fieldspice_b200.learned import CIN, COUT, init_theta
+    lib = L.lib()
+    dev = torch.device("cuda", 0)
+    N = int(np.prod(dims))
+    th = torch.as_tensor(init_theta(0), device=dev)
+    nb = ctypes.c_size_t()
+    L.check("ws", lib.fs_unet_workspace_bytes(*dims, batch, 0, ctypes.byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    net = ctypes.c_void_p()
+    L.check("create", lib.fs_unet_create(*dims, batch, 0, L.ptr(th), L.ptr(ws), nb.value,
+                                         ctypes.byref(net), L.stream_ptr()))
+    g = torch.Generator(device=dev).manual_seed(0)
+    rhs = torch.randn((batch, N), device=dev, generator=g)
+    em = torch.rand((batch, 3, N), device=dev, generator=g) * 0.16
+    lab = (torch.rand((batch, N), device=dev, generator=g) < 0.05).to(torch.uint8)
+    out = torch.empty((batch, N), device=dev)
+
+    def fwd():
+        L.check("fwd", lib.fs_unet_forward(net, L.ptr(rhs), 1, N, L.ptr(em), 3 * N, L.ptr(lab), N,
+                                           L.ptr(out), 1, N, L.stream_ptr()))
+    for _ in range(args.warmup):
+        fwd()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fwd()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flops = 0.0
+    X, Y, Z = dims
+    vox = []
+    for l in range(4):
+        vox.append(X * Y * Z * batch)
+        X, Y, Z = (X + 1) // 2, (Y + 1) // 2, (Z + 1) // 2
+    lev = (0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0)
+    for l in range(14):
+        flops += 2.0 * 27 * CIN[l] * COUT[l] * vox[lev[l]]
+    lib.fs_unet_destroy(net)
+    print(json.dumps({"unet_forward": True, "dims": dims, "batch": batch, "ms": ms,
+                      "conv_tflop": flops / 1e12, "tflops": flops / (ms * 1e-3) / 1e12}),
+          flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -542,6 +648,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.unet_forward:
+        run_unet_forward(args)
         return
     import torch
     if world > 1:

@@ -88,7 +88,8 @@ _SIGNATURES = {
     "fs_pcg_plan_level_data": (c_int, [c_void_p, c_int, POINTER(c_void_p), POINTER(c_void_p),
                                        POINTER(c_void_p)]),
     "fs_pcg_plan_unet_workspace_bytes": (c_int, [c_void_p, c_int, POINTER(c_size_t)]),
-    "fs_pcg_plan_set_unet": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "fs_pcg_plan_set_unet": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_size_t,
+                                     c_void_p]),
     "fs_pcg_plan_sync_unet": (c_int, [c_void_p, c_void_p]),
     "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),

@@ -260,6 +260,22 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
   }
 }
 
+// x += u (the learned level's guess added to the V-cycle's correction).
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_mg_add(Dims d, T* __restrict__ x, const T* __restrict__ u, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T xv[K], uv[K];
+    ldv<T, K>(x, n, xv);
+    ldv_ro<T, K>(u, n, uv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) xv[t] += uv[t];
+    stv<T, K>(x, n, xv);
+  }
+}
+
 // Per-axis trilinear weights of fine index i onto coarse index I (0 if none).
 __device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
   const int dlt = i - 2 * I;

@@ -88,12 +88,19 @@ struct Control {
 };
 
 __device__ void refresh_done(RhsState* st, Control* ctl, int nrhs) {
-  // Called by thread 0 of a last block after the per-RHS updates.
+  // Called by thread 0 of a last block after the per-RHS updates.  A
+  // reliable update streams every RHS column anyway (the vectors are
+  // interleaved), so when one RHS asks for it every active RHS takes it:
+  // the RHS stay in step and the update passes happen once, not once per
+  // RHS at scattered iterations.
   int done = 1, ru = 0;
   for (int t = 0; t < nrhs; ++t) {
     done &= !st[t].active;
     ru |= st[t].ru;
   }
+  if (ru)
+    for (int t = 0; t < nrhs; ++t)
+      if (st[t].active && !st[t].ru) st[t].ru = 2;  // 2: taken along, not asked
   ctl->all_done = done;
   ctl->any_ru = ru;
 }
@@ -803,6 +810,7 @@ __global__ void __launch_bounds__(fs::kBlock)
       if (s.ru) {
         const double g = tot[threadIdx.x];
         const double rn = sqrt(g);
+        const bool own = s.ru == 1;
         s.nru += 1;
         s.ru = 0;
         s.relres = rn / s.bnorm;
@@ -819,8 +827,8 @@ __global__ void __launch_bounds__(fs::kBlock)
           if (rn < 0.5 * s.best) {
             s.best = rn;
             s.nstall = 0;
-          } else {
-            s.nstall += 1;
+          } else if (own) {
+            s.nstall += 1;  // only updates this RHS asked for count as stalls
           }
           if (ctl->delta > 0.0 && s.nstall >= kStallUpdates) {
             // Low-precision iterations no longer reduce the FP64 residual
@@ -1033,7 +1041,9 @@ struct fs_pcg_plan {
   // U-Net maps that level's right-hand side to its correction; CG becomes
   // flexible.  -1: plain multigrid.
   int learned = -1;
+  int learned_mode = 0;    // 0: network only, 1: network + V-cycle on its residual
   fs_unet* net = nullptr;
+  void *net_u = nullptr, *net_r = nullptr;  // level vectors of mode 1
   int net_status = FS_OK;
 };
 
@@ -1203,24 +1213,45 @@ struct Impl {
   }
   // Launch one V-cycle on level l for right-hand side b; returns the index
   // of the level's x buffer that holds the result, and counts launches.
+  // One V-cycle on level l; at the learned level the network takes over:
+  // mode 0 returns its output as the level's correction, mode 1 adds a
+  // V-cycle on the residual of that output (network guess + multigrid
+  // cleanup).  Returns the index of the level's x buffer holding the result.
   static int vcycle(fs_pcg_plan* P, int l, const T* b, cudaStream_t s,
                     long long* nl, bool dry = false) {
-    MgLevel& L = P->lev[l];
-    const int* done = &P->ctl->all_done;
     if constexpr (std::is_same<T, float>::value) {
       if (l == P->learned && P->net) {
-        // x[0] = U-Net(b): rhs and output K-interleaved, geometry shared
+        MgLevel& L = P->lev[l];
+        const int* done = &P->ctl->all_done;
+        float* u = P->learned_mode ? (float*)P->net_u : (float*)L.x[0];
         if (!dry) {
-          const float* em[3] = {(const float*)(l ? L.em[0] : P->ex), (const float*)(l ? L.em[1] : P->ey),
-                                (const float*)(l ? L.em[2] : P->ez)};
-          const int st = unet_forward(P->net, b, K, 1, em[0], em[1], em[2], 0,
-                                      l ? L.label : P->label, 0, (float*)L.x[0], K, 1, false, s);
+          // rhs and output K-interleaved, geometry shared by the K samples
+          const int st = unet_forward(P->net, b, K, 1, (const float*)L.em[0],
+                                      (const float*)L.em[1], (const float*)L.em[2], 0,
+                                      l ? L.label : P->label, 0, u, K, 1, false, s);
           if (st != FS_OK) P->net_status = st;
         }
         *nl += unet_forward_launches();
-        return 0;
+        if (!P->learned_mode) return 0;
+        const int g = fs_grid_blocks((const void*)fs::k_mg_residual<T, K>, L.d.N);
+        if (!dry)
+          fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
+              L.d, (const T*)L.em[0], (const T*)L.em[1], (const T*)L.em[2], (const T*)u, b,
+              (T*)P->net_r, done);
+        ++*nl;
+        const int cur = vcycle_plain(P, l, (const T*)P->net_r, s, nl, dry);
+        if (!dry)
+          fs::k_mg_add<T, K><<<g, fs::kBlock, 0, s>>>(L.d, (T*)L.x[cur], (const T*)u, done);
+        ++*nl;
+        return cur;
       }
     }
+    return vcycle_plain(P, l, b, s, nl, dry);
+  }
+  static int vcycle_plain(fs_pcg_plan* P, int l, const T* b, cudaStream_t s,
+                          long long* nl, bool dry = false) {
+    MgLevel& L = P->lev[l];
+    const int* done = &P->ctl->all_done;
     const bool last = l == P->nlev - 1;
     const int deg = last ? P->mg.coarse_deg : P->mg.smooth_deg;
     double cd[64], cr[64];
@@ -1817,14 +1848,19 @@ int fs_pcg_plan_unet_workspace_bytes(const fs_pcg_plan* P, int level, size_t* by
       level >= P->nlev)
     return FS_BAD_ARG;
   const Dims& d = P->lev[level].d;
-  return fs_unet_workspace_bytes(d.nx, d.ny, d.nz, P->nrhs, 0, bytes);
+  size_t nb = 0;
+  const int st = fs_unet_workspace_bytes(d.nx, d.ny, d.nz, P->nrhs, 0, &nb);
+  if (st != FS_OK) return st;
+  const size_t vec = ((size_t)d.N * P->nrhs * sizeof(float) + 255) & ~(size_t)255;
+  *bytes = ((nb + 255) & ~(size_t)255) + 2 * vec;
+  return FS_OK;
 }
 
-int fs_pcg_plan_set_unet(fs_pcg_plan* P, int level, float* theta, void* workspace,
+int fs_pcg_plan_set_unet(fs_pcg_plan* P, int level, int mode, float* theta, void* workspace,
                          size_t workspace_bytes, void* stream) {
   if (!P || !P->precond || P->precision != FS_PRECISION_MIXED || level < -1 ||
-      level >= P->nlev) {
-    fs_set_error_msg("learned preconditioner: needs a mixed-precision multigrid plan and a valid level");
+      level >= P->nlev || mode < 0 || mode > 1) {
+    fs_set_error_msg("learned preconditioner: needs a mixed-precision multigrid plan, a valid level and mode");
     return FS_BAD_ARG;
   }
   if (P->net) {
@@ -1832,18 +1868,32 @@ int fs_pcg_plan_set_unet(fs_pcg_plan* P, int level, float* theta, void* workspac
     P->net = nullptr;
   }
   P->learned = -1;
+  P->net_u = P->net_r = nullptr;
   P->net_status = FS_OK;
   if (level >= 0) {
-    if (!theta) return FS_BAD_ARG;
+    if (!theta || !workspace || ((uintptr_t)workspace & 255)) return FS_BAD_ARG;
     const Dims& d = P->lev[level].d;
+    size_t need = 0, nb = 0;
+    int st = fs_pcg_plan_unet_workspace_bytes(P, level, &need);
+    if (st != FS_OK) return st;
+    if (workspace_bytes < need) {
+      fs_set_error_msg("learned preconditioner: workspace too small");
+      return FS_BAD_ARG;
+    }
+    st = fs_unet_workspace_bytes(d.nx, d.ny, d.nz, P->nrhs, 0, &nb);
+    if (st != FS_OK) return st;
+    nb = (nb + 255) & ~(size_t)255;
+    const size_t vec = ((size_t)d.N * P->nrhs * sizeof(float) + 255) & ~(size_t)255;
     fs_unet* net = nullptr;
-    const int st = fs_unet_create(d.nx, d.ny, d.nz, P->nrhs, 0, theta, workspace, workspace_bytes,
-                                  &net, stream);
+    st = fs_unet_create(d.nx, d.ny, d.nz, P->nrhs, 0, theta, workspace, nb, &net, stream);
     if (st != FS_OK) return st;
     cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
     if (e != cudaSuccess) return fs_cuda_status("cudaStreamSynchronize", e);
     P->net = net;
+    P->net_u = (uint8_t*)workspace + nb;
+    P->net_r = (uint8_t*)workspace + nb + vec;
     P->learned = level;
+    P->learned_mode = mode;
   }
   return capture_graph(P);
 }

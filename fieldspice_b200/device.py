@@ -328,7 +328,7 @@ class EliminatedSystem:
         if not bad:
             return st, stats
         L.check("fs_pcg_plan_set_unet", L.lib().fs_pcg_plan_set_unet(
-            self._plan, -1, None, None, 0, L.stream_ptr()))
+            self._plan, -1, 0, None, None, 0, L.stream_ptr()))
         self.learned_fallback = True
         st, stats2 = self._run(self._plan, tol, maxiter, True)
         for a, b in zip(stats, stats2):

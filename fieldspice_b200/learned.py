@@ -176,7 +176,7 @@ class LearnedPreconditioner:
     V-cycle level whose correction the network computes.
     """
 
-    def __init__(self, theta=None, level: int = 2, seed: int = 0):
+    def __init__(self, theta=None, level: int = 2, seed: int = 0, mode: str = "hybrid"):
         import torch
         dev = device()
         th = init_theta(seed) if theta is None else theta
@@ -184,7 +184,11 @@ class LearnedPreconditioner:
                                      else th, dtype=torch.float32, device=dev).contiguous()
         if self.theta.numel() != param_count():
             raise ValueError(f"theta must have {param_count()} entries")
+        if mode not in ("hybrid", "replace"):
+            raise ValueError("mode must be 'hybrid' (network + V-cycle on its residual) "
+                             "or 'replace' (network only)")
         self.level = int(level)
+        self.mode = mode
         self.history: list[float] = []
         self.train_time = 0.0
 
@@ -192,7 +196,13 @@ class LearnedPreconditioner:
         """A network whose output is identically 0 (no coarse correction):
         the same V-cycle truncated at ``level`` without the learned part."""
         import torch
-        return LearnedPreconditioner(torch.zeros_like(self.theta), self.level)
+        return LearnedPreconditioner(torch.zeros_like(self.theta), self.level, mode=self.mode)
+
+    def with_mode(self, mode: str) -> "LearnedPreconditioner":
+        """The same network (shared parameters) used in another mode."""
+        other = LearnedPreconditioner(self.theta, self.level, mode=mode)
+        other.history = self.history
+        return other
 
     # -- training ------------------------------------------------------------
     def fit(self, data, *, epochs: int = 3, batch: int = 8, lr: float = 1e-3, seed: int = 0,
@@ -252,12 +262,13 @@ class LearnedPreconditioner:
 
     @classmethod
     def train(cls, workloads, *, level: int = 2, epochs: int = 3, batch: int = 8,
-              lr: float = 1e-3, seed: int = 0, log=None) -> "LearnedPreconditioner":
+              lr: float = 1e-3, seed: int = 0, mode: str = "hybrid",
+              log=None) -> "LearnedPreconditioner":
         """Generate the pairs from ``workloads`` and fit a fresh network."""
         t0 = time.perf_counter()
         data = training_pairs(workloads, level=level, log=log)
         gen = time.perf_counter() - t0
-        net = cls(level=level, seed=seed)
+        net = cls(level=level, seed=seed, mode=mode)
         net.fit(data, epochs=epochs, batch=batch, lr=lr, seed=seed, log=log)
         net.data_time = gen
         net.pairs = int(data["rhs"].shape[0])
@@ -278,7 +289,8 @@ class LearnedPreconditioner:
                 lib.fs_pcg_plan_unet_workspace_bytes(plan, level, ctypes.byref(nb)))
         system._net_ws = torch.empty(nb.value, dtype=torch.uint8, device=self.theta.device)
         L.check("fs_pcg_plan_set_unet", lib.fs_pcg_plan_set_unet(
-            plan, level, L.ptr(self.theta), L.ptr(system._net_ws), nb.value, L.stream_ptr()))
+            plan, level, 1 if self.mode == "hybrid" else 0, L.ptr(self.theta),
+            L.ptr(system._net_ws), nb.value, L.stream_ptr()))
         return level
 
     def state(self) -> np.ndarray:

@@ -298,8 +298,10 @@ int fs_unet_destroy(fs_unet* net);
  * the U-Net (parameters theta, caller-owned, read at every application) for
  * that level's correction instead of recursing: smoothing on the levels
  * above, the network below.  The preconditioner is then nonlinear, so the
- * plan switches to flexible CG (beta = -z.Ap / p.Ap).  level = -1 restores
- * plain multigrid.  fs_pcg_plan_levels: the level count and dims (3 ints
+ * plan switches to flexible CG (beta = -z.Ap / p.Ap).  mode 0: the network's
+ * output is the level's correction; mode 1: the network's output plus a
+ * V-cycle from that level on its residual.  level = -1 restores plain
+ * multigrid.  fs_pcg_plan_levels: the level count and dims (3 ints
  * per level); fs_pcg_plan_level_data: a level's equilibrated masses (FP32 in
  * a mixed plan), labels and diag^-1/2 (NULL on level 0).                   */
 int fs_pcg_plan_levels(const fs_pcg_plan* plan, int* nlev, int* dims);
@@ -311,7 +313,7 @@ int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, cons
 int fs_pcg_plan_level_data(const fs_pcg_plan* plan, int level, const void** em,
                            const uint8_t** label, const void** scale);
 int fs_pcg_plan_unet_workspace_bytes(const fs_pcg_plan* plan, int level, size_t* bytes);
-int fs_pcg_plan_set_unet(fs_pcg_plan* plan, int level, float* theta, void* workspace,
+int fs_pcg_plan_set_unet(fs_pcg_plan* plan, int level, int mode, float* theta, void* workspace,
                          size_t workspace_bytes, void* stream);
 /* Re-pack the plan's network weights after theta changed.                  */
 int fs_pcg_plan_sync_unet(fs_pcg_plan* plan, void* stream);

@@ -73,21 +73,35 @@ def test_training_reduces_the_loss(cuda, trained):
     assert h[-1] < 0.5 * h[0], h
 
 
-def test_learned_fcg_matches_multigrid_and_beats_no_network(cuda, trained):
-    from fieldspice_b200.learned import LearnedPreconditioner
+@pytest.mark.parametrize("mode", ["hybrid", "replace"])
+def test_learned_fcg_matches_fp64_multigrid(cuda, trained, mode):
     from fieldspice_b200.solvers.base import GPUConfig
     w = _workloads([999])[0]                      # held out
     Cref, _ = _extract(w, GPUConfig(precision="fp64", preconditioner="mg"), tol=1e-12)
-    C, rep = _extract(w, GPUConfig(preconditioner="learned", learned=trained))
+    C, rep = _extract(w, GPUConfig(preconditioner="learned", learned=trained.with_mode(mode)))
     scale = np.abs(np.diag(Cref)).max()
     assert np.abs(C - Cref).max() / scale <= 1e-9
     assert max(rep["linear"]["relres_fp64"]) < 1e-10
     assert not rep["linear"]["learned_fallback"]
-    it_learned = max(rep["linear"]["iterations"])
-    _, rep0 = _extract(w, GPUConfig(preconditioner="learned", learned=trained.zero()))
-    it_zero = max(rep0["linear"]["iterations"])
-    _, rep_r = _extract(w, GPUConfig(preconditioner="learned",
-                                     learned=LearnedPreconditioner(level=2, seed=5)))
-    it_rand = max(rep_r["linear"]["iterations"])
+
+
+def test_trained_network_gains_over_the_method_without_it(cuda, trained):
+    """'replace': the V-cycle truncated at the network's level, with the
+    trained network, with its output zeroed (no coarse correction) and with
+    an untrained network; 'hybrid': network guess + V-cycle on its residual
+    against the plain V-cycle (the network zeroed)."""
+    from fieldspice_b200.learned import LearnedPreconditioner
+    from fieldspice_b200.solvers.base import GPUConfig
+    w = _workloads([999])[0]
+
+    def iters(net):
+        _, rep = _extract(w, GPUConfig(preconditioner="learned", learned=net))
+        return max(rep["linear"]["iterations"])
+    rep_net = trained.with_mode("replace")
+    it_learned, it_zero = iters(rep_net), iters(rep_net.zero())
+    it_rand = iters(LearnedPreconditioner(level=2, seed=5, mode="replace"))
     assert it_learned * 2 <= it_zero, (it_learned, it_zero)
     assert it_learned < it_rand, (it_learned, it_rand)
+    hyb = trained.with_mode("hybrid")
+    it_h, it_mg = iters(hyb), iters(hyb.zero())
+    assert it_h <= it_mg + 2, (it_h, it_mg)
