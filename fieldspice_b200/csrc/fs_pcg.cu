@@ -32,6 +32,7 @@
 // graph launches.  Reductions are deterministic (fixed-order block partials,
 // reduced by the last block to finish).  No kernel waits on another block.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <new>
@@ -347,9 +348,11 @@ __device__ void finish_pq(double (&acc)[K], double* partials, RhsState* st,
         if (tot[threadIdx.x] > 0.0 && isfinite(tot[threadIdx.x])) {
           s.alpha = s.gamma / tot[threadIdx.x];
         } else {
-          s.alpha = 0.0;  // A~ is SPD: p.q <= 0 only through NaN/Inf
+          // A~ is SPD: a finite p.q <= 0 is round-off of a low-precision
+          // direction (a stall); NaN/Inf is a breakdown.
+          s.alpha = 0.0;
           s.active = 0;
-          s.status = FS_NAN;
+          s.status = isfinite(tot[threadIdx.x]) ? FS_STALLED : FS_NAN;
         }
       } else {
         s.alpha = 0.0;
@@ -521,9 +524,12 @@ __global__ void __launch_bounds__(fs::kBlock)
       if (s.active) {
         const double g = tot[threadIdx.x];
         if (!(g > 0.0) || !isfinite(g)) {
-          // M is SPD: r.Mr <= 0 only through NaN/Inf (or r == 0)
+          // M is SPD: r.Mr = 0 means r = 0; r.Mr < 0 means the FP32
+          // preconditioner lost definiteness on a mode below its resolution
+          // (reported as a stall, so "auto" continues in FP64); NaN/Inf is a
+          // breakdown.
           s.active = 0;
-          s.status = (g == 0.0) ? FS_OK : FS_NAN;
+          s.status = (g == 0.0) ? FS_OK : (isfinite(g) ? FS_STALLED : FS_NAN);
         } else if (s.fresh) {
           s.gamma = g;
           s.gamma_old = g;
@@ -619,7 +625,7 @@ __global__ void __launch_bounds__(fs::kBlock)
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(fs::kBlock)
+__global__ void __launch_bounds__(fs::kBlock, fs::mg_min_blocks<T, K>())
     k_apply_pq(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
                const T* __restrict__ ez, const T* __restrict__ p,
                T* __restrict__ q, double* __restrict__ partials, RhsState* st,
@@ -824,11 +830,16 @@ __global__ void __launch_bounds__(fs::kBlock)
           s.active = 0;
           s.status = FS_NOT_CONVERGED;
         } else {
-          if (rn < 0.5 * s.best) {
-            s.best = rn;
-            s.nstall = 0;
-          } else if (own) {
-            s.nstall += 1;  // only updates this RHS asked for count as stalls
+          // Progress is judged on the updates this RHS asked for; one taken
+          // along with another RHS neither counts as a stall nor moves the
+          // reference point.
+          if (own) {
+            if (rn < 0.5 * s.best) {
+              s.best = rn;
+              s.nstall = 0;
+            } else {
+              s.nstall += 1;
+            }
           }
           if (ctl->delta > 0.0 && s.nstall >= kStallUpdates) {
             // Low-precision iterations no longer reduce the FP64 residual
@@ -1049,6 +1060,13 @@ struct fs_pcg_plan {
 
 namespace {
 
+// The TMA-staged stencil is the default; FS_STENCIL=plain selects the
+// cached-load kernel (the same arithmetic) for comparison.
+bool plain_stencil() {
+  const char* sel = getenv("FS_STENCIL");
+  return sel && strcmp(sel, "plain") == 0;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -1071,7 +1089,7 @@ struct Impl {
     P->g_init = fs_grid_blocks((const void*)k_init<T, K>, N);
     using C = TmaTile<T, K>;
     P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
-    if constexpr (C::OK) {
+    if (C::OK && !plain_stencil()) {
       cudaFuncSetAttribute(k_stencil_tma<T, K>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)C::SMEM);
@@ -1098,7 +1116,7 @@ struct Impl {
   }
   static int maps(fs_pcg_plan* P) {
     using C = TmaTile<T, K>;
-    P->use_tma = C::OK ? 1 : 0;
+    P->use_tma = (C::OK && !plain_stencil()) ? 1 : 0;
     if constexpr (!C::OK) return FS_OK;
     auto encode = encode_fn();
     if (!encode) {
@@ -1154,6 +1172,12 @@ struct Impl {
         break;
       case 1:
         if constexpr (TmaTile<T, K>::OK) {
+          if (!P->use_tma) {
+            k_apply_pq<T, K><<<P->g_apply, fs::kBlock, 0, s>>>(
+                P->d, (const T*)P->ex, (const T*)P->ey, (const T*)P->ez,
+                (const T*)P->p[1 - par], (T*)P->q, P->partials, P->st, P->ctl);
+            break;
+          }
           using C = TmaTile<T, K>;
           k_stencil_tma<T, K><<<P->g_apply, C::THREADS, C::SMEM, s>>>(
               P->d, P->tm_p[1 - par], (const T*)P->ex, (const T*)P->ey,
