@@ -59,6 +59,8 @@ _SIGNATURES = {
     "fs_pcg_workspace_bytes": (c_int, [c_int] * 6 + [POINTER(c_size_t)]),
     "fs_pcg_plan_create": (c_int, [c_int] * 6 + [c_void_p] * 7 + [c_size_t,
                                    POINTER(c_void_p), c_void_p]),
+    "fs_pcg_plan_create_diag": (c_int, [c_int] * 6 + [c_void_p] * 8 + [c_size_t,
+                                        POINTER(c_void_p), c_void_p]),
     "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
                                   POINTER(FsRhsStats), c_void_p]),
     "fs_pcg_plans_solve": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p), c_int,

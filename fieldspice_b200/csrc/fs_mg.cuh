@@ -285,6 +285,35 @@ __device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
   return 0.0f;
 }
 
+// Coarse node diagonal term (heat capacity / dt, convection): the row-sum
+// lumping of P^T D_f P, i.e. d_c(I) = sum_f P(f, I) d_f(f) (P 1 = 1).
+__global__ void k_mg_coarsen_diag(Dims f, Dims c, const double* __restrict__ fd,
+                                  double* __restrict__ cd) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int I, J, Kc;
+    node_ijk(c, n, I, J, Kc);
+    double acc = 0.0;
+    for (int a = -1; a <= 1; ++a) {
+      const int i = 2 * I + a;
+      if (i < 0 || i >= f.nx) continue;
+      const double wa = pw(i, I, f.nx, c.nx);
+      for (int b = -1; b <= 1; ++b) {
+        const int j = 2 * J + b;
+        if (j < 0 || j >= f.ny) continue;
+        const double wb = wa * pw(j, J, f.ny, c.ny);
+        for (int e = -1; e <= 1; ++e) {
+          const int k = 2 * Kc + e;
+          if (k < 0 || k >= f.nz) continue;
+          const double w = wb * pw(k, Kc, f.nz, c.nz);
+          if (w != 0.0) acc += w * fd[((long long)i * f.ny + j) * f.nz + k];
+        }
+      }
+    }
+    cd[n] = acc;
+  }
+}
+
 // b_c(I) = s_c(I) * sum_f P(f,I) sd(f) res(f)   (coarse-centric gather)
 template <typename T, int K>
 __global__ void __launch_bounds__(kBlock)

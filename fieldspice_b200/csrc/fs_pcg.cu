@@ -110,6 +110,7 @@ __device__ void refresh_done(RhsState* st, Control* ctl, int nrhs) {
 __global__ void k_classify(Dims d, const double* __restrict__ mx,
                            const double* __restrict__ my,
                            const double* __restrict__ mz,
+                           const double* __restrict__ dgn,
                            const uint8_t* __restrict__ label_in,
                            uint8_t* __restrict__ label,
                            double* __restrict__ s64) {
@@ -120,7 +121,9 @@ __global__ void k_classify(Dims d, const double* __restrict__ mx,
     if (lab == FS_LABEL_FREE) {
       int i, j, k;
       fs::node_ijk(d, n, i, j, k);
-      double dg = 0.0, sfree = 0.0;
+      // diagonal = sum of incident masses + the node's own term (heat
+      // capacity / dt, convection), if any
+      double dg = dgn ? dgn[n] : 0.0, sfree = 0.0;
       auto edge = [&](bool ok, double m, long long nb) {
         if (!ok) return;
         dg += m;
@@ -167,7 +170,8 @@ __global__ void k_eq_masses(Dims d, const double* __restrict__ mx,
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_init(Dims d, const double* __restrict__ mx, const double* __restrict__ my,
-           const double* __restrict__ mz, const uint8_t* __restrict__ label,
+           const double* __restrict__ mz, const double* __restrict__ dgn,
+           const uint8_t* __restrict__ label,
            const double* __restrict__ s64, double* __restrict__ phi,
            const double* __restrict__ f, int warm, T* __restrict__ x,
            T* __restrict__ r, T* __restrict__ p, double* __restrict__ partials,
@@ -216,6 +220,12 @@ __global__ void __launch_bounds__(fs::kBlock)
     edge(j < d.ny - 1, my[n], n + d.sy);
     edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
     edge(k < d.nz - 1, mz[n], n + 1);
+    if (dgn) {
+      const double dd = dgn[n];
+      dg += dd;
+#pragma unroll
+      for (int t = 0; t < K; ++t) res[t] -= dd * c[t];
+    }
 
     if (lab == FS_LABEL_FREE) {
       const double s = s64[n];
@@ -758,6 +768,7 @@ template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_reliable(Dims d, const double* __restrict__ mx,
                const double* __restrict__ my, const double* __restrict__ mz,
+               const double* __restrict__ dgn,
                const double* __restrict__ s64, const double* __restrict__ phi,
                const double* __restrict__ f, T* __restrict__ r,
                double* __restrict__ partials, RhsState* st, Control* ctl) {
@@ -795,6 +806,11 @@ __global__ void __launch_bounds__(fs::kBlock)
     edge(j < d.ny - 1, my[n], n + d.sy);
     edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
     edge(k < d.nz - 1, mz[n], n + 1);
+    if (dgn) {
+      const double dd = dgn[n];
+#pragma unroll
+      for (int t = 0; t < K; ++t) res[t] -= dd * c[t];
+    }
     T rv[K];
     fs::ldv<T, K>(r, n, rv);
 #pragma unroll
@@ -910,12 +926,12 @@ MgParams g_mg;
 struct MgLevel {
   Dims d;
   // level >= 1: original-scale FP64 masses, labels, scale (setup only)
-  double *m64[3], *s64;
+  double *m64[3], *s64, *d64;
   uint8_t *label_in, *label;
   void *em[3];       // equilibrated masses (T); level 0 uses the plan's
   void *s, *sd;      // diag^-1/2, diag^1/2 (T), 0 on fixed nodes
   void *x[2], *b, *dv, *res;  // K-interleaved vectors (T); level 0 b = r~
-  size_t off_m64[3], off_s64, off_label_in, off_label, off_em[3], off_s, off_sd,
+  size_t off_d64, off_m64[3], off_s64, off_label_in, off_label, off_em[3], off_s, off_sd,
       off_x[2], off_b, off_dv, off_res;
 };
 
@@ -994,6 +1010,7 @@ Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
       const size_t n = (size_t)dl[l].N;
       if (l > 0) {
         for (int a = 0; a < 3; ++a) { m.off_m64[a] = o; o = align_up(o + n * 8); }
+        m.off_d64 = o; o = align_up(o + n * 8);
         m.off_s64 = o; o = align_up(o + n * 8);
         m.off_label_in = o; o = align_up(o + n);
         m.off_label = o; o = align_up(o + n);
@@ -1025,6 +1042,7 @@ struct fs_pcg_plan {
   long long launches_per_iter;
   MgParams mg;
   const double *mx, *my, *mz;
+  const double* dg;        // node diagonal term (NULL: pure Laplacian)
   double* phi;
   const double* f;
   uint8_t* label;
@@ -1153,7 +1171,7 @@ struct Impl {
   static void init(fs_pcg_plan* P, int warm, double tol, int maxiter,
                    double delta, cudaStream_t s) {
     k_init<T, K><<<P->g_init, fs::kBlock, 0, s>>>(
-        P->d, P->mx, P->my, P->mz, P->label, P->s64, P->phi, P->f, warm,
+        P->d, P->mx, P->my, P->mz, P->dg, P->label, P->s64, P->phi, P->f, warm,
         (T*)P->x, (T*)P->r, (T*)P->p[0], P->partials, P->st, P->ctl, tol, maxiter,
         delta, P->precond);
   }
@@ -1198,7 +1216,7 @@ struct Impl {
         k_fold<T, K><<<P->g_fold, fs::kBlock, 0, s>>>(P->d, P->s64, P->phi,
                                                       (T*)P->x, P->st, P->ctl);
         k_reliable<T, K><<<P->g_rel, fs::kBlock, 0, s>>>(
-            P->d, P->mx, P->my, P->mz, P->s64, P->phi, P->f, (T*)P->r,
+            P->d, P->mx, P->my, P->mz, P->dg, P->s64, P->phi, P->f, (T*)P->r,
             P->partials, P->st, P->ctl);
         break;
     }
@@ -1223,9 +1241,15 @@ struct Impl {
       fs::k_mg_coarsen<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fm[0], fm[1], fm[2],
                                                 flab, c.m64[0], c.m64[1],
                                                 c.m64[2], c.label_in);
+      if (P->dg) {
+        g = fs_grid_blocks((const void*)fs::k_mg_coarsen_diag, c.d.N);
+        fs::k_mg_coarsen_diag<<<g, fs::kBlock, 0, s>>>(f.d, c.d, l == 1 ? P->dg : f.d64,
+                                                       c.d64);
+      }
       g = fs_grid_blocks((const void*)k_classify, c.d.N);
       k_classify<<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
-                                          c.label_in, c.label, c.s64);
+                                          P->dg ? c.d64 : nullptr, c.label_in, c.label,
+                                          c.s64);
       g = fs_grid_blocks((const void*)k_eq_masses<T>, c.d.N);
       k_eq_masses<T><<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
                                               c.s64, (T*)c.em[0], (T*)c.em[1],
@@ -1504,6 +1528,16 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
                        const double* mz, const uint8_t* label_in, double* phi,
                        const double* f, void* workspace, size_t workspace_bytes,
                        fs_pcg_plan** plan, void* stream) {
+  return fs_pcg_plan_create_diag(nx, ny, nz, nrhs, precision, precond, mx, my, mz, nullptr,
+                                 label_in, phi, f, workspace, workspace_bytes, plan, stream);
+}
+
+int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
+                            int precond, const double* mx, const double* my,
+                            const double* mz, const double* diag,
+                            const uint8_t* label_in, double* phi,
+                            const double* f, void* workspace, size_t workspace_bytes,
+                            fs_pcg_plan** plan, void* stream) {
   if (!plan) return FS_BAD_ARG;
   *plan = nullptr;
   size_t need = 0;
@@ -1525,6 +1559,7 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   P->mg = g_mg;
   P->launches_per_iter = 0;
   P->mx = mx;
+  P->dg = diag;
   P->my = my;
   P->mz = mz;
   P->phi = phi;
@@ -1541,6 +1576,7 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
         m.em[a] = w + m.off_em[a];
       }
       m.s64 = (double*)(w + m.off_s64);
+      m.d64 = (double*)(w + m.off_d64);
       m.label_in = (uint8_t*)(w + m.off_label_in);
       m.label = (uint8_t*)(w + m.off_label);
       m.b = w + m.off_b;
@@ -1590,7 +1626,7 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
   if ((e = cudaMemsetAsync(w + L.st, 0, L.total - L.st, s)) != cudaSuccess)
     return fail("memset state", e);
   int g = fs_grid_blocks((const void*)k_classify, P->d.N);
-  k_classify<<<g, fs::kBlock, 0, s>>>(P->d, mx, my, mz, label_in, P->label,
+  k_classify<<<g, fs::kBlock, 0, s>>>(P->d, mx, my, mz, P->dg, label_in, P->label,
                                       P->s64);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail("k_classify", e);
   dispatch(P, 1, s);

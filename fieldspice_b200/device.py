@@ -225,7 +225,7 @@ class EliminatedSystem:
 
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
                  precision: str = "auto", with_source: bool = False,
-                 preconditioner: str = "jacobi", learned=None):
+                 preconditioner: str = "jacobi", learned=None, diag=None):
         import torch
         if precision not in ("auto", "mixed", "fp64"):
             raise ValueError(f"precision must be 'auto', 'mixed' or 'fp64', got {precision!r}")
@@ -239,6 +239,9 @@ class EliminatedSystem:
                 raise ValueError("the learned preconditioner runs in mixed precision")
         self.preconditioner = preconditioner
         self.learned = learned
+        # optional FP64 node-diagonal term of the operator (kept alive here)
+        self.diag = (None if diag is None else
+                     torch.as_tensor(diag, dtype=torch.float64, device=op.dev).contiguous())
         self._pc = L.PRECOND_JACOBI if preconditioner == "jacobi" else L.PRECOND_MG
         self.op = op
         self.k = pad_rhs(nrhs)
@@ -285,10 +288,11 @@ class EliminatedSystem:
         if ws.data_ptr() % 256:
             raise RuntimeError("device allocation is not 256-byte aligned")
         plan = ctypes.c_void_p()
-        st = lib.fs_pcg_plan_create(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
-                                    L.ptr(op.my), L.ptr(op.mz), L.ptr(self.label_in),
-                                    L.ptr(self.phi), L.ptr(self.f), L.ptr(ws),
-                                    nb.value, ctypes.byref(plan), L.stream_ptr())
+        st = lib.fs_pcg_plan_create_diag(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
+                                         L.ptr(op.my), L.ptr(op.mz), L.ptr(self.diag),
+                                         L.ptr(self.label_in), L.ptr(self.phi), L.ptr(self.f),
+                                         L.ptr(ws), nb.value, ctypes.byref(plan),
+                                         L.stream_ptr())
         L.check("fs_pcg_plan_create", st)
         return plan, ws
 

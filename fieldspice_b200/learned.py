@@ -96,7 +96,7 @@ def _level_tensors(plan, system, level):
     return d, ems, labels, scale
 
 
-def training_pairs(workloads, *, level: int = 2, snapshots=(4, 8, 16, 32, 64, 128, 256, 512),
+def training_pairs(workloads, *, level: int = 3, snapshots=(4, 8, 16, 32, 64, 128, 256, 512),
                    tol: float = 1e-10, log=None):
     """(rhs, em, label, target) device tensors of every pair, planar:
     rhs/target [S][N_l] FP32, em [S][3][N_l] FP32, label [S][N_l] uint8."""
@@ -176,7 +176,7 @@ class LearnedPreconditioner:
     V-cycle level whose correction the network computes.
     """
 
-    def __init__(self, theta=None, level: int = 2, seed: int = 0, mode: str = "hybrid"):
+    def __init__(self, theta=None, level: int = 3, seed: int = 0, mode: str = "replace"):
         import torch
         dev = device()
         th = init_theta(seed) if theta is None else theta
@@ -261,8 +261,8 @@ class LearnedPreconditioner:
         return hist
 
     @classmethod
-    def train(cls, workloads, *, level: int = 2, epochs: int = 3, batch: int = 8,
-              lr: float = 1e-3, seed: int = 0, mode: str = "hybrid",
+    def train(cls, workloads, *, level: int = 3, epochs: int = 3, batch: int = 8,
+              lr: float = 1e-3, seed: int = 0, mode: str = "replace",
               log=None) -> "LearnedPreconditioner":
         """Generate the pairs from ``workloads`` and fit a fresh network."""
         t0 = time.perf_counter()

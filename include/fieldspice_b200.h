@@ -143,6 +143,16 @@ int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
                        const double* mz, const uint8_t* label_in, double* phi,
                        const double* f, void* workspace, size_t workspace_bytes,
                        fs_pcg_plan** plan, void* stream);
+/* The same system plus a node-diagonal term: A = G^T M G + diag(d), d >= 0
+ * (FP64, one value per node; the heat capacity / dt and convective wall
+ * terms of ThermalSolver, thermal.py:140-160,200-290).  The array must stay
+ * valid for the plan's lifetime.                                           */
+int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
+                            int precond, const double* mx, const double* my,
+                            const double* mz, const double* diag,
+                            const uint8_t* label_in, double* phi,
+                            const double* f, void* workspace, size_t workspace_bytes,
+                            fs_pcg_plan** plan, void* stream);
 /* Solve in place into phi.  warm_start != 0 keeps the free-node values of
  * phi as the initial guess (the tolerance stays relative to ||b||, as in
  * SciPy); otherwise the guess is 0.  stats: host array of nrhs entries.

@@ -513,6 +513,95 @@ def resistance_matrix(g: Grid, sigma_cell, terminals, method="cg", tol=1e-10,
     return np.linalg.pinv(Ys), Y
 
 
+# ---------------------------------------------------------------------------
+# Heat conduction -- solvers/thermal.py:104-300
+# ---------------------------------------------------------------------------
+def node_volumes(g: Grid):
+    """Dual (box) volumes, flat C order (grid.py:388-396)."""
+    return (g.hxd[:, None, None] * g.hyd[None, :, None] * g.hzd[None, None, :]).ravel()
+
+
+def cell_to_node(g: Grid, prop):
+    """Dual-volume-weighted average of a cell property onto nodes, cells
+    edge-padded (operators.py:270-296)."""
+    prop = np.asarray(prop, dtype=float)
+    p = np.pad(prop, 1, mode="edge")
+    nx, ny, nz = g.shape_nodes
+    acc = np.zeros((nx, ny, nz))
+    wacc = np.zeros((nx, ny, nz))
+    halves = [(np.concatenate([[0.0], 0.5 * h]), np.concatenate([0.5 * h, [0.0]]))
+              for h in (g.hx, g.hy, g.hz)]
+    for di in (0, 1):
+        for dj in (0, 1):
+            for dk in (0, 1):
+                q = p[di:di + nx, dj:dj + ny, dk:dk + nz]
+                w = (halves[0][di][:, None, None] * halves[1][dj][None, :, None]
+                     * halves[2][dk][None, None, :])
+                acc += q * w
+                wacc += w
+    return acc / np.where(wacc > 0, wacc, 1.0)
+
+
+def wall_dual_areas(g: Grid, wall: str):
+    """Dual face area of every node on a wall, ordered as wall_nodes
+    (boundaries.py:200-218)."""
+    axis = {"x": 0, "y": 1, "z": 2}[wall[0]]
+    duals = (g.hxd, g.hyd, g.hzd)
+    d0, d1 = [d for d in (0, 1, 2) if d != axis]
+    return (duals[d0][:, None] * duals[d1][None, :]).ravel()
+
+
+def _thermal_walls(g: Grid, convection):
+    diag = np.zeros(g.n_nodes)
+    rhs = np.zeros(g.n_nodes)
+    for wall, (h, t_inf) in (convection or {}).items():
+        nodes = wall_nodes(g, wall)
+        area = wall_dual_areas(g, wall)
+        diag[nodes] += float(h) * area
+        rhs[nodes] += float(h) * area * float(t_inf)
+    return diag, rhs
+
+
+def thermal_steady(g: Grid, kappa_cell, q_node, dirichlet=None, convection=None,
+                   method="cg", tol=1e-10):
+    """Steady temperature: (K + diag(h A)) T = q + h A T_inf, fixed-temperature
+    walls eliminated (thermal.py:200-245)."""
+    K = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, kappa_cell)))
+    diag, rhs = _thermal_walls(g, convection)
+    A = sp.csr_matrix(K + sp.diags(diag))
+    b = np.broadcast_to(np.asarray(q_node, float), (g.n_nodes,)).copy() + rhs
+    idx, val = dirichlet_nodes(g, dirichlet or {})
+    if idx.size:
+        A, b = apply_dirichlet(A, b, idx, val)
+    return LinearSystemCPU(A, method=method, tol=tol).solve(b)
+
+
+def thermal_transient(g: Grid, kappa_cell, rho_cp_cell, q_node, t_end, dt, T0,
+                      dirichlet=None, convection=None, theta=1.0, method="cg", tol=1e-10):
+    """theta-scheme transient (thermal.py:247-300): (C/dt + theta K) T+ =
+    (C/dt - (1 - theta) K) T + q + h A T_inf.  Returns the list of T."""
+    K = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, kappa_cell)))
+    diag, wall_rhs = _thermal_walls(g, convection)
+    Kc = sp.csr_matrix(K + sp.diags(diag))
+    C = cell_to_node(g, rho_cp_cell).ravel() * node_volumes(g)
+    A_imp = sp.csr_matrix(sp.diags(C / dt) + theta * Kc)
+    A_exp = sp.csr_matrix(sp.diags(C / dt) - (1.0 - theta) * Kc)
+    n = int(np.ceil(t_end / dt))
+    T = np.full(g.n_nodes, float(T0)) if np.isscalar(T0) else np.asarray(T0, float).copy()
+    q = np.broadcast_to(np.asarray(q_node, float), (g.n_nodes,))
+    idx, val = dirichlet_nodes(g, dirichlet or {})
+    A, _ = apply_dirichlet(A_imp, np.zeros(g.n_nodes), idx, val) if idx.size else (A_imp, None)
+    ls = LinearSystemCPU(A, method=method, tol=tol)
+    out = [T.copy()]
+    for _ in range(n):
+        b = A_exp @ T + q + wall_rhs
+        if idx.size:
+            _, b = apply_dirichlet(A_imp, b, idx, val)
+        T = ls.solve(b)
+        out.append(T.copy())
+    return out
+
+
 def eqs_transient(g: Grid, eps_cell, sigma_cell, fixed_groups, values_at,
                   dt, nsteps, theta=1.0, method="cg", tol=1e-10,
                   dirichlet_walls=None, t_start=0.0):

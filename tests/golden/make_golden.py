@@ -144,6 +144,34 @@ def resistance_fixture():
                         sigma=sig, boxes=np.asarray(boxes))
 
 
+def thermal_fixture():
+    """solvers/thermal.py: steady (Dirichlet heat sink + convective top),
+    theta-scheme transients (theta 1 and 0.5) and a thermal resistance, on a
+    seeded graded grid with silicon/oxide conductivities."""
+    from fieldspice.solvers.thermal import ThermalSolver
+    rng = np.random.default_rng(11)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 20e-6, 15)), np.sort(rng.uniform(0, 16e-6, 12)),
+                        np.sort(rng.uniform(0, 8e-6, 10)))
+    kappa = np.where(rng.random(g.shape_cells) < 0.5, 150.0, 1.4)
+    rho_cp = rng.uniform(1.6e6, 2.1e6, g.shape_cells)
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    src = nid[5:9, 4:7, 7:9].ravel()
+    q = np.zeros(g.n_nodes)
+    q[src] = 2e-4
+    bc = BoundarySpec(zlo=Dirichlet(300.0))
+    conv = {"zhi": (2e4, 310.0), "xlo": (5e3, 295.0)}
+    th = ThermalSolver(g, kappa, rho_cp)
+    steady = th.steady(q, bc=bc, convection=conv).fields["T"][0]
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "kappa": kappa, "rho_cp": rho_cp, "q": q,
+           "src": src, "T_steady": steady}
+    for theta in (1.0, 0.5):
+        r = th.transient(q, t_end=2e-5, dt=1e-6, T0=300.0, bc=bc, convection=conv,
+                         theta=theta, store=True)
+        out[f"T_transient_theta{theta:g}"] = r.fields["T"]
+    out["R_th"] = th.thermal_resistance(src, bc=bc, convection=conv, power=1e-3)
+    np.savez_compressed(HERE / "thermal.npz", **out)
+
+
 def rc_stack(n=60):
     d, Wd, H = 4e-6, 3e-6, 2e-6
     sigma1, er1, er2 = 1e3, 4.0, 2.0
@@ -236,4 +264,5 @@ if __name__ == "__main__":
     layered_fixture((48, 48, 24), 1, 1e-12)
     eqs_fixture()
     resistance_fixture()
+    thermal_fixture()
     print("golden fixtures written to", HERE)

@@ -150,3 +150,19 @@ def test_resistance_matrix_matches_reference(golden):
     want = _projected(d["R"])
     assert np.abs(_projected(R) - want).max() <= 1e-9 * np.abs(want).max()
     assert np.abs(Y.sum(axis=1)).max() <= 1e-9 * np.abs(np.diag(Y)).max()
+
+
+def test_thermal_matches_reference(golden):
+    # solvers/thermal.py:200-300: steady with a Dirichlet sink and convective
+    # walls, theta-scheme transients (theta 1 and 1/2), direct solves
+    d = golden("thermal")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    conv = {"zhi": (2e4, 310.0), "xlo": (5e3, 295.0)}
+    T = O.thermal_steady(g, d["kappa"], d["q"], {"zlo": 300.0}, conv, method="direct")
+    assert np.abs(T - d["T_steady"]).max() <= 1e-9 * np.abs(d["T_steady"] - 300.0).max()
+    for theta in (1.0, 0.5):
+        Ts = O.thermal_transient(g, d["kappa"], d["rho_cp"], d["q"], 2e-5, 1e-6, 300.0,
+                                 {"zlo": 300.0}, conv, theta=theta, method="direct")
+        want = d[f"T_transient_theta{theta:g}"]
+        assert len(Ts) == want.shape[0]
+        assert np.abs(np.array(Ts) - want).max() <= 1e-9 * np.abs(want - 300.0).max()
