@@ -508,6 +508,169 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
   finish_pq<T, K, TmaTile<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
+// ---- K1 with the masses staged too ------------------------------------------------
+// Same arithmetic as k_stencil_tma, but each ring stage holds, besides the
+// p tile with its halo, the plane's three mass tiles loaded by TMA:
+//   ex: (z0.., y0..)        -> m(x), and m(x-1) from the previous stage;
+//   ey: (z0.., y0-1..)      -> m(y-1) and m(y);
+//   ez: (z0-ZP.., y0..)     -> m(z-1) and m(z) (ZP keeps the innermost
+//                              coordinate 16-byte aligned).
+// Out-of-range boxes read zero, which is exactly the missing edge at a wall,
+// so the inner loop has no global loads and no boundary branches.  Smaller
+// tiles (TY = 8) keep three CTAs per SM with two planes in flight each.
+template <typename T, int K>
+struct TmaTileM {
+  static constexpr int B = K * (int)sizeof(T);
+  static constexpr int MB = (int)sizeof(T);
+  static constexpr int TZ = 32;
+  static constexpr int TY = B <= 32 ? 8 : 4;
+  static constexpr int NS = 5;
+  static constexpr int ZP = 16 / MB;
+  static constexpr int HY = TY + 2, HZ = TZ + 2;
+  static constexpr int BOX = HY * HZ * B;
+  static constexpr int EXB = TZ * TY * MB;
+  static constexpr int EYB = TZ * (TY + 1) * MB;
+  static constexpr int EZB = (TZ + ZP) * TY * MB;
+  static constexpr int O_EX = (BOX + 127) / 128 * 128;
+  static constexpr int O_EY = O_EX + (EXB + 127) / 128 * 128;
+  static constexpr int O_EZ = O_EY + (EYB + 127) / 128 * 128;
+  static constexpr int SLOT = O_EZ + (EZB + 127) / 128 * 128;
+  static constexpr uint32_t TX = (uint32_t)(BOX + EXB + EYB + EZB);  // bytes per stage
+  static constexpr int THREADS = TZ * TY;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + NS * 8 + 128;
+  static constexpr bool OK = B >= 16;
+};
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::"
+      "bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(fs::smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(fs::smem_u32(bar))
+      : "memory");
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <= 32 ? 3 : 1))
+    k_stencil_tma_m(Dims d, const __grid_constant__ CUtensorMap tm_p,
+                    const __grid_constant__ CUtensorMap tm_ex,
+                    const __grid_constant__ CUtensorMap tm_ey,
+                    const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ q,
+                    double* __restrict__ partials, RhsState* st, Control* ctl) {
+  using C = TmaTileM<T, K>;
+  if (ctl->all_done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::NS * C::SLOT);
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const long long total = (long long)nbz * nby * d.nx;
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  long long u = (long long)blockIdx.x * per;
+  const long long u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  long long ticket = 0;
+  bool failed = false;
+  while (u < u_end && !failed) {
+    const long long col = u / d.nx;
+    const int xa = (int)(u % d.nx);
+    const int xb = (int)min((long long)d.nx, xa + (u_end - u));
+    const int bz = (int)(col % nbz), by = (int)(col / nbz);
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nplanes = (xb - xa) + 2;  // planes xa-1 .. xb
+    auto issue = [&](int j) {
+      const int s = (int)((ticket + j) % C::NS);
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 1 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_p, &bar[s], 0, z0 - 1, y0 - 1, x);
+      tma_load_3d(slot + C::O_EX, &tm_ex, &bar[s], z0, y0, x);
+      tma_load_3d(slot + C::O_EY, &tm_ey, &bar[s], z0, y0 - 1, x);
+      tma_load_3d(slot + C::O_EZ, &tm_ez, &bar[s], z0 - C::ZP, y0, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
+    for (int j = 0; j < nplanes; ++j) {
+      const long long tk = ticket + j;
+      const int s = (int)(tk % C::NS);
+      const bool ok = fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      if (j >= 2) {
+        if (inb) {
+          const int x = xa - 2 + j;
+          const long long n = ((long long)x * d.ny + y) * d.nz + z;
+          const unsigned char* sm = base + (int)((tk - 2) % C::NS) * C::SLOT;  // plane x-1
+          const unsigned char* sc = base + (int)((tk - 1) % C::NS) * C::SLOT;  // plane x
+          const unsigned char* sp = base + s * C::SLOT;                        // plane x+1
+          const T* pm = reinterpret_cast<const T*>(sm);
+          const T* pc = reinterpret_cast<const T*>(sc);
+          const T* pp = reinterpret_cast<const T*>(sp);
+          const T* exm = reinterpret_cast<const T*>(sm + C::O_EX);
+          const T* exc = reinterpret_cast<const T*>(sc + C::O_EX);
+          const T* eyc = reinterpret_cast<const T*>(sc + C::O_EY);
+          const T* ezc = reinterpret_cast<const T*>(sc + C::O_EZ);
+          const T mxm = exm[ty * C::TZ + tz], mxp = exc[ty * C::TZ + tz];
+          const T mym = eyc[ty * C::TZ + tz], myp = eyc[(ty + 1) * C::TZ + tz];
+          const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
+          const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
+          T c[K], v[K], qv[K];
+          ld_smem<T, K>(pc + cpos * K, c);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] = c[t];
+          ld_smem<T, K>(pm + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
+          ld_smem<T, K>(pp + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
+          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
+          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            qv[t] -= mzp * v[t];
+            acc[t] += (double)c[t] * (double)qv[t];
+          }
+          fs::stv<T, K>(q, n, qv);
+        }
+        __syncthreads();  // plane j-2 no longer read: its stage may refill
+        if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
+      }
+    }
+    ticket += nplanes;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      ctl->error = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+  finish_pq<T, K, TmaTileM<T, K>::THREADS>(acc, partials, st, ctl);
+}
+
 // ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
@@ -1054,6 +1217,8 @@ struct fs_pcg_plan {
   int g_init, g_apply, g_pnew, g_update, g_rel, g_fin, g_fold;
   int use_tma;
   CUtensorMap tm_p[2];
+  CUtensorMap tm_m[3];     // ex, ey, ez tiles of the mass-staging stencil
+  int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -1107,7 +1272,33 @@ struct Impl {
     P->g_init = fs_grid_blocks((const void*)k_init<T, K>, N);
     using C = TmaTile<T, K>;
     P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
-    if (C::OK && !plain_stencil()) {
+    {
+      const char* sel = getenv("FS_STENCIL");
+      const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
+      if (!C::OK || plain_stencil())
+        P->stencil_kind = 0;
+      else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0))
+        P->stencil_kind = 1;
+      else
+        P->stencil_kind = 2;
+    }
+    if (P->stencil_kind == 2) {
+      using CM = TmaTileM<T, K>;
+      cudaFuncSetAttribute(k_stencil_tma_m<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)CM::SMEM);
+      int per_sm = 0, dev = 0, sms = 148;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_tma_m<T, K>,
+                                                        CM::THREADS, CM::SMEM) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long cols = (long long)((P->d.nz + CM::TZ - 1) / CM::TZ) *
+                             ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx;
+      long long g = (long long)sms * per_sm;
+      if (g > cols) g = cols;
+      P->g_apply = (int)g;
+    } else if (P->stencil_kind == 1) {
       cudaFuncSetAttribute(k_stencil_tma<T, K>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)C::SMEM);
@@ -1134,8 +1325,9 @@ struct Impl {
   }
   static int maps(fs_pcg_plan* P) {
     using C = TmaTile<T, K>;
-    P->use_tma = (C::OK && !plain_stencil()) ? 1 : 0;
+    P->use_tma = P->stencil_kind != 0 ? 1 : 0;
     if constexpr (!C::OK) return FS_OK;
+    if (!P->use_tma) return FS_OK;
     auto encode = encode_fn();
     if (!encode) {
       fs_set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
@@ -1159,6 +1351,27 @@ struct Impl {
       if (rc != CUDA_SUCCESS) {
         fs_set_error_msg("cuTensorMapEncodeTiled rejected the stencil tensor map");
         return FS_CUDA_ERROR;
+      }
+    }
+    if (P->stencil_kind == 2) {
+      using CM = TmaTileM<T, K>;
+      const cuuint64_t MB = sizeof(T);
+      cuuint64_t mdims[3] = {(cuuint64_t)P->d.nz, (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
+      cuuint64_t mstr[2] = {MB * P->d.nz, MB * P->d.nz * P->d.ny};
+      cuuint32_t mes[3] = {1, 1, 1};
+      cuuint32_t boxes[3][3] = {{(cuuint32_t)CM::TZ, (cuuint32_t)CM::TY, 1},
+                                {(cuuint32_t)CM::TZ, (cuuint32_t)(CM::TY + 1), 1},
+                                {(cuuint32_t)(CM::TZ + CM::ZP), (cuuint32_t)CM::TY, 1}};
+      void* mb[3] = {P->ex, P->ey, P->ez};
+      for (int m = 0; m < 3; ++m) {
+        CUresult rc = encode(&P->tm_m[m], dt, 3, mb[m], mdims, mstr, boxes[m], mes,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (rc != CUDA_SUCCESS) {
+          fs_set_error_msg("cuTensorMapEncodeTiled rejected a mass tensor map");
+          return FS_CUDA_ERROR;
+        }
       }
     }
     return FS_OK;
@@ -1190,6 +1403,13 @@ struct Impl {
         break;
       case 1:
         if constexpr (TmaTile<T, K>::OK) {
+          if (P->stencil_kind == 2) {
+            using CM = TmaTileM<T, K>;
+            k_stencil_tma_m<T, K><<<P->g_apply, CM::THREADS, CM::SMEM, s>>>(
+                P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
+                P->partials, P->st, P->ctl);
+            break;
+          }
           if (!P->use_tma) {
             k_apply_pq<T, K><<<P->g_apply, fs::kBlock, 0, s>>>(
                 P->d, (const T*)P->ex, (const T*)P->ey, (const T*)P->ez,
