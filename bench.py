@@ -373,8 +373,6 @@ def learned_variant(timed, step_device, C_default, args):
     ms, outs = timed(lambda: step_device("mixed", "learned", net), nv, 1)
     Cl, _, info = outs[-1]
     ms0, outs0 = timed(lambda: step_device("mixed", "learned", net.zero()), 1, 0)
-    hnet = net.with_mode("hybrid")
-    msh, outsh = timed(lambda: step_device("mixed", "learned", hnet), 1, 1)
     scale = float(np.abs(np.diag(C_default)).max())
     err = None
     if FULLSIZE_JSON.exists() and tuple(int(v) for v in args.shape.split(",")) == SHAPE:
@@ -391,9 +389,7 @@ def learned_variant(timed, step_device, C_default, args):
                     f"output as the level-{LEVEL} correction",
             "network_zeroed": {"value": NBOX / (ms0 / 1000.0),
                                "iterations": outs0[-1][2]["iterations"]},
-            "hybrid_mode": {"value": NBOX / (msh / 1000.0),
-                            "iterations": outsh[-1][2]["iterations"],
-                            "learned_fallback": outsh[-1][2].get("learned_fallback")},
+
             "training": {"pairs": net.pairs, "geometries": len(train), "shape": [128, 128, 128],
                          "level": net.level, "epochs": EPOCHS, "batch": 8,
                          "data_seconds": net.data_time, "fit_seconds": net.train_time,

@@ -1337,7 +1337,10 @@ struct Impl {
     cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)P->d.nz,
                           (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
     cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
-    cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)C::HZ, (cuuint32_t)C::HY, 1};
+    // the p box of the kernel that will run: its tile has its own halo height
+    const int hz = P->stencil_kind == 2 ? TmaTileM<T, K>::HZ : C::HZ;
+    const int hy = P->stencil_kind == 2 ? TmaTileM<T, K>::HY : C::HY;
+    cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)hz, (cuuint32_t)hy, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;

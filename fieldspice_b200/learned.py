@@ -1,18 +1,19 @@
 """Learned coarse-level preconditioner: a BF16 3-D U-Net inside flexible CG.
 
 Where it sits.  The multigrid V-cycle of the CG plan smooths on the fine
-levels and, at one coarse level ``level``, asks the network for that level's
-correction instead of recursing further: z = post-smooth(P U(R pre-smooth(r))).
-The network costs ~128 kFLOP per node of its level per right-hand side; at
-level 2 of a 256x256x128 grid (64x64x32 nodes, 8 RHS) that is ~0.13 TFLOP
-per application on the tensor cores, where the same network on the fine
-grid would cost 64x more than the whole multigrid iteration it replaces.
-The network is nonlinear (ReLU), so the outer iteration is flexible CG;
-if FCG stalls the plan falls back to plain multigrid PCG, which is also the
-judge of its answer (same FP64 stopping rule, same charge integration).
+levels and, at one coarse level ``level`` (default 3), asks the network for
+that level's correction instead of recursing further ("replace" mode):
+z = post-smooth(P U(R pre-smooth(r))).  The network costs ~128 kFLOP per
+node of its level per right-hand side (17 GFLOP per application at level 3
+of a 256x256x128 grid, 8 RHS); on the fine grid the same network would cost
+more than the whole multigrid iteration it replaces.  A "hybrid" mode adds a
+V-cycle on the residual of the network's guess.  The network is nonlinear
+(ReLU), so the outer iteration is flexible CG; if FCG stalls the plan falls
+back to plain multigrid PCG, which is also the judge of its answer (same
+FP64 stopping rule, same charge integration).
 
 Training data.  Residual-to-error pairs generated by the path's own PCG on
-seeded geometries of the 256x256x128 family at 128^3: Jacobi-PCG iterates
+seeded geometries of the layered-box family at 128^3: Jacobi-PCG iterates
 x_k after k = 4 .. 512 iterations and the converged x*, so e = x* - x_k are
 the smooth errors Krylov iterations leave behind.  Each error is injected
 into the coarse level (node I of level l is fine node 2^l I; in that level's
