@@ -224,6 +224,204 @@ __global__ void __launch_bounds__(128)
   if (warp == 0) tc_dealloc(tbase, ncols);
 }
 
+// ---- persistent, warp-specialised variant ----------------------------------------
+// Same implicit GEMM as k_conv3d_tc, for layers whose weights and two window
+// stages fit in shared memory.  One CTA per SM loops over 128-row tiles
+// (tile = blockIdx.x + i * gridDim.x) with three roles:
+//   warp 4 (one thread): TMA producer, fills a 2-stage ring of 3-window tiles;
+//   warp 5 (one thread): MMA issuer, 27 x (C_in/16) MMAs per tile into one of
+//                        two TMEM accumulators, commits to "stage empty" and
+//                        "accumulator full";
+//   warps 0-3: epilogue, drain an accumulator (tcgen05.ld), store, release it.
+// So the loads of tile i+1, the MMAs of tile i and the epilogue of tile i-1
+// overlap.  Weights are loaded once per CTA.  Every wait is bounded; on a
+// timeout the thread records an error and stops its role, the others time
+// out in turn, and the CTA drains its own transfers before freeing TMEM.
+struct Conv2Cfg {
+  int W, BR;          // window rows (multiple of BR) and TMA box rows
+  size_t smem;
+};
+
+constexpr int kConv2Threads = 192;
+
+#ifdef FS_CONV_DEFINE_KERNELS
+__global__ void __launch_bounds__(kConv2Threads, 1)
+    k_conv3d_tc2(const __grid_constant__ CUtensorMap xmap, ConvArgs a, long long ntiles) {
+  extern __shared__ uint8_t conv2_smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)conv2_smem_raw + 1023) & ~(uintptr_t)1023);
+  const int nch = a.cin >> 3;
+  const uint32_t colb = (uint32_t)a.W * 16u;
+  const uint32_t stage_bytes = 3u * nch * colb;
+  uint8_t* Aring = smem;                          // 2 stages
+  uint8_t* Bw = Aring + 2 * (size_t)stage_bytes;  // 27 taps
+  const uint32_t wtap = (uint32_t)nch * a.cout * 16u;
+  uint64_t* bars = (uint64_t*)(Bw + (size_t)27 * wtap);
+  uint64_t* full = bars;          // [2] TMA -> MMA
+  uint64_t* empty = bars + 2;     // [2] MMA done reading a stage -> TMA
+  uint64_t* accfull = bars + 4;   // [2] MMA -> epilogue
+  uint64_t* accempty = bars + 6;  // [2] epilogue -> MMA (4 warp arrivals)
+  uint64_t* wbar = bars + 8;      // weights
+  uint32_t* tslot = (uint32_t*)(bars + 9);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t ncols = tmem_cols(2 * a.cout);
+  if (tid == 0) {
+    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    mbar_init(&accfull[0], 1);
+    mbar_init(&accfull[1], 1);
+    mbar_init(&accempty[0], 4);
+    mbar_init(&accempty[1], 4);
+    mbar_init(wbar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc_alloc(tslot, ncols);
+    tc_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const int nseg = a.W / a.BR;
+  const long long my_tiles =
+      blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  bool ok = true;
+  if (warp == 4) {
+    // ---- producer -----------------------------------------------------------------
+    if (lane == 0) {
+      mbar_arrive_expect_tx(wbar, 27u * wtap);
+      bulk_load(Bw, a.wpack, 27u * wtap, wbar);
+      long long issued = 0;
+      for (long long i = 0; i < my_tiles && ok; ++i) {
+        const int st = (int)(i & 1);
+        if (i >= 2) ok = mbar_wait_bounded(&empty[st], (uint32_t)(((i >> 1) - 1) & 1), kConvBudget);
+        if (!ok) break;
+        const long long m0 = (blockIdx.x + i * gridDim.x) * 128LL;
+        mbar_arrive_expect_tx(&full[st], stage_bytes);
+        uint8_t* A = Aring + (size_t)st * stage_bytes;
+        for (int w = 0; w < 3; ++w) {
+          const long long r0 = m0 + (long long)(w - 1) * a.g.S - a.g.Zp - 1;
+          for (int c = 0; c < nch; ++c)
+            for (int sg = 0; sg < nseg; ++sg)
+              tma_load_2d(A + (size_t)(w * nch + c) * colb + (size_t)sg * a.BR * 16, &xmap,
+                          &full[st], a.cin_off + 8 * c, (int)(r0 + (long long)sg * a.BR));
+        }
+        issued = i + 1;
+      }
+      // drain: the last stages' loads must land before the CTA exits
+      for (long long i = (issued > 2 ? issued - 2 : 0); i < issued; ++i)
+        (void)mbar_wait_bounded(&full[i & 1], (uint32_t)((i >> 1) & 1), kConvBudget);
+      (void)mbar_wait_bounded(wbar, 0, kConvBudget);
+      if (!ok && a.error) atomicExch(a.error, 1);
+    }
+  } else if (warp == 5) {
+    // ---- MMA issuer -----------------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(128, a.cout);
+      ok = mbar_wait_bounded(wbar, 0, kConvBudget);
+      long long committed = 0;
+      for (long long i = 0; i < my_tiles && ok; ++i) {
+        const int st = (int)(i & 1), ac = (int)(i & 1);
+        ok = mbar_wait_bounded(&full[st], (uint32_t)((i >> 1) & 1), kConvBudget);
+        if (ok && i >= 2)
+          ok = mbar_wait_bounded(&accempty[ac], (uint32_t)(((i >> 1) - 1) & 1), kConvBudget);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t abase = smem_u32(Aring + (size_t)st * stage_bytes), bbase = smem_u32(Bw);
+        for (int t = 0; t < 27; ++t) {
+          const int w = t / 9, dy = (t / 3) % 3, dz = t % 3;
+          const uint32_t rowoff = (uint32_t)(dy * a.g.Zp + dz) * 16u;
+          for (int s = 0; s < (a.cin >> 4); ++s) {
+            const uint64_t ad = umma_desc(abase + (uint32_t)(w * nch + 2 * s) * colb + rowoff, colb, 128);
+            const uint64_t bd = umma_desc(bbase + (uint32_t)t * wtap + (uint32_t)(2 * s * a.cout) * 16u,
+                                          (uint32_t)a.cout * 16u, 128);
+            tc_mma_bf16(tbase + (uint32_t)(ac * a.cout), ad, bd, idesc, (t > 0 || s > 0) ? 1u : 0u);
+          }
+        }
+        tc_commit(&empty[st]);
+        tc_commit(&accfull[ac]);
+        committed = i + 1;
+      }
+      // drain: the last MMAs must complete before TMEM is freed
+      if (committed > 0)
+        (void)mbar_wait_bounded(&accfull[(committed - 1) & 1], (uint32_t)(((committed - 1) >> 1) & 1),
+                                kConvBudget);
+      if (!ok && a.error) atomicExch(a.error, 1);
+    }
+  } else {
+    // ---- epilogue (warps 0-3, TMEM lanes 32 w .. 32 w + 31) ---------------------------
+    for (long long i = 0; i < my_tiles && ok; ++i) {
+      const int ac = (int)(i & 1);
+      ok = mbar_wait_bounded(&accfull[ac], (uint32_t)((i >> 1) & 1), kConvBudget);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const long long row = (blockIdx.x + i * gridDim.x) * 128LL + warp * 32 + lane;
+      bool interior = false;
+      if (row < a.g.R) {
+        const long long rr = row % a.g.V;
+        const int k = (int)(rr % a.g.Zp);
+        const int jj = (int)((rr / a.g.Zp) % a.g.Yp);
+        const int ii = (int)(rr / a.g.S);
+        interior = k >= 1 && k <= a.g.Z && jj >= 1 && jj <= a.g.Y && ii >= 1 && ii <= a.g.X;
+      }
+      for (int q = 0; q < (a.cout >> 4); ++q) {
+        float v[16];
+        tc_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ac * a.cout + q * 16), v);
+        if (row >= a.g.R) continue;
+        __nv_bfloat16* dst = a.out + row * a.out_stride + a.out_off + q * 16;
+        if (!interior) {
+          if (!a.accumulate) {
+            uint4 z = make_uint4(0, 0, 0, 0);
+            ((uint4*)dst)[0] = z;
+            ((uint4*)dst)[1] = z;
+          }
+          continue;
+        }
+        if (a.bias) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] += __ldg(a.bias + q * 16 + e);
+        }
+        if (a.relu) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] = fmaxf(v[e], 0.0f);
+        }
+        if (a.mask) {
+          const __nv_bfloat16* mp = a.mask + row * a.mask_stride + a.mask_off + q * 16;
+          uint4 mraw[2];
+          mraw[0] = ((const uint4*)mp)[0];
+          mraw[1] = ((const uint4*)mp)[1];
+          const __nv_bfloat16* mv = (const __nv_bfloat16*)mraw;
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            if (!(__bfloat162float(mv[e]) > 0.0f)) v[e] = 0.0f;
+        }
+        if (a.accumulate) {
+          uint4 oraw[2];
+          oraw[0] = ((const uint4*)dst)[0];
+          oraw[1] = ((const uint4*)dst)[1];
+          const __nv_bfloat16* ov = (const __nv_bfloat16*)oraw;
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] += __bfloat162float(ov[e]);
+        }
+        uint4 packed[2];
+        __nv_bfloat16* pv = (__nv_bfloat16*)packed;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) pv[e] = __float2bfloat16_rn(v[e]);
+        ((uint4*)dst)[0] = packed[0];
+        ((uint4*)dst)[1] = packed[1];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accempty[ac]);
+    }
+    if (!ok && lane == 0 && a.error) atomicExch(a.error, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc_dealloc(tbase, ncols);
+}
+#endif  // FS_CONV_DEFINE_KERNELS
+
 // Pack FP32 weights w[27][cout][cin] into the BF16 shared-memory image
 // [27][cin/8][cout][8]; flip != 0 packs the data-gradient operator instead:
 // taps reversed and the channel roles swapped (image [27][cout/8][cin][8]).

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "fieldspice_b200.h"
@@ -113,6 +114,63 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
   if (!conv_config(g, io.cin, io.cout, &c)) {
     fs_set_error_msg("conv3d: layer does not fit in shared memory");
     return FS_BAD_ARG;
+  }
+  // the persistent, warp-specialised kernel when its two window stages and
+  // all weights fit (FS_CONV=v1 forces the one-tile-per-CTA kernel)
+  {
+    const char* sel = getenv("FS_CONV");
+    const bool v1 = sel && strcmp(sel, "v1") == 0;
+    const int nch = io.cin / 8;
+    const long long need = 128LL + 2LL * g.Zp + 2;
+    const int nseg = (int)((need + 255) / 256);
+    const int BR = (int)(((need + nseg - 1) / nseg + 7) / 8 * 8);
+    const int W = nseg * BR;
+    const size_t smem2 = 1024 + 2 * (size_t)3 * nch * W * 16 + (size_t)27 * nch * io.cout * 16 + 128;
+    if (!v1 && smem2 <= 227u * 1024u && !io.accumulate) {
+      CUtensorMap map2;
+      int st2 = act_map(&map2, io.x, io.ctot_in, g.R, BR);
+      if (st2 != FS_OK) return st2;
+      ConvArgs a2;
+      a2.g = g;
+      a2.cin = io.cin;
+      a2.cin_off = io.cin_off;
+      a2.cout = io.cout;
+      a2.wpack = (const uint16_t*)io.wpack;
+      a2.bias = io.bias;
+      a2.out = (__nv_bfloat16*)io.out;
+      a2.out_stride = io.ctot_out;
+      a2.out_off = io.out_off;
+      a2.mask = (const __nv_bfloat16*)io.mask;
+      a2.mask_stride = io.ctot_mask;
+      a2.mask_off = io.mask_off;
+      a2.relu = io.relu;
+      a2.accumulate = 0;
+      a2.T = 1;
+      a2.W = W;
+      a2.BR = BR;
+      a2.phases = 1;
+      a2.error = io.error;
+      static bool attr2 = false;
+      if (!attr2) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             227 * 1024);
+        if (e != cudaSuccess) return fs_cuda_status("cudaFuncSetAttribute(conv2)", e);
+        attr2 = true;
+      }
+      const long long ntiles = (g.R + 127) / 128;
+      int per_sm = 1, dev = 0, sms = 148;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3d_tc2, kConv2Threads,
+                                                        smem2) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+      if (per_sm > 2) per_sm = 2;  // TMEM: two accumulators of <= 128 columns per CTA
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      long long grid = (long long)sms * per_sm;
+      if (grid > ntiles) grid = ntiles;
+      k_conv3d_tc2<<<(unsigned)grid, kConv2Threads, smem2, s>>>(map2, a2, ntiles);
+      FS_CHECK_LAUNCH("k_conv3d_tc2");
+      return FS_OK;
+    }
   }
   CUtensorMap map;
   int st = act_map(&map, io.x, io.ctot_in, g.R, c.BR);

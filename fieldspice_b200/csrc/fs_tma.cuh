@@ -97,3 +97,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src,
 }
 
 }  // namespace fs
+
+namespace fs {
+
+// Plain arrive (count 1) on an mbarrier of this CTA.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+}  // namespace fs

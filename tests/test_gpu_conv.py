@@ -13,6 +13,17 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["persistent", "v1"])
+def variant(request, monkeypatch):
+    """Both kernels: the persistent warp-specialised one (default where it
+    fits) and the one-tile-per-CTA kernel (FS_CONV=v1)."""
+    if request.param == "v1":
+        monkeypatch.setenv("FS_CONV", "v1")
+    else:
+        monkeypatch.delenv("FS_CONV", raising=False)
+    return request.param
+
+
 def _padded(x):
     """(B, X, Y, Z, C) -> zero-halo (B, X+2, Y+2, Z+2, C)."""
     import torch
@@ -73,8 +84,9 @@ def _close(got, want):
 
 @pytest.mark.parametrize("dims,cin,cout", [((2, 7, 9, 11), 16, 16), ((1, 12, 10, 9), 32, 48),
                                            ((3, 5, 6, 4), 64, 64), ((1, 6, 6, 30), 112, 48),
-                                           ((2, 4, 4, 70), 16, 32)])
-def test_conv_forward_matches_fp64(cuda, dims, cin, cout):
+                                           ((2, 4, 4, 70), 16, 32), ((4, 20, 18, 16), 16, 16),
+                                           ((8, 24, 24, 30), 16, 32)])
+def test_conv_forward_matches_fp64(cuda, variant, dims, cin, cout):
     import torch
     rng = np.random.default_rng(cin * 100 + cout)
     B, X, Y, Z = dims
@@ -108,7 +120,7 @@ def test_conv_channel_slices_mask_and_accumulate(cuda):
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 32), (112, 48)])
-def test_conv_data_gradient_matches_autograd(cuda, cin, cout):
+def test_conv_data_gradient_matches_autograd(cuda, variant, cin, cout):
     """The flipped pack turns the kernel into dL/dx of the forward conv."""
     import torch
     import torch.nn.functional as F
