@@ -60,6 +60,7 @@ struct ConvArgs {
   int W;                // staged window rows (a multiple of BR)
   int BR;               // rows per TMA box (<= 256, multiple of 8)
   int phases;           // 1: all taps resident; 3: one dx per phase
+  int nst;              // window ring stages of the persistent kernel (2..4)
   int* error;
 };
 
@@ -252,20 +253,21 @@ __global__ void __launch_bounds__(kConv2Threads, 1)
   const int nch = a.cin >> 3;
   const uint32_t colb = (uint32_t)a.W * 16u;
   const uint32_t stage_bytes = 3u * nch * colb;
-  uint8_t* Aring = smem;                          // 2 stages
-  uint8_t* Bw = Aring + 2 * (size_t)stage_bytes;  // 27 taps
+  const int nst = a.nst;
+  uint8_t* Aring = smem;                            // nst stages
+  uint8_t* Bw = Aring + (size_t)nst * stage_bytes;  // 27 taps
   const uint32_t wtap = (uint32_t)nch * a.cout * 16u;
   uint64_t* bars = (uint64_t*)(Bw + (size_t)27 * wtap);
-  uint64_t* full = bars;          // [2] TMA -> MMA
-  uint64_t* empty = bars + 2;     // [2] MMA done reading a stage -> TMA
-  uint64_t* accfull = bars + 4;   // [2] MMA -> epilogue
-  uint64_t* accempty = bars + 6;  // [2] epilogue -> MMA (4 warp arrivals)
-  uint64_t* wbar = bars + 8;      // weights
-  uint32_t* tslot = (uint32_t*)(bars + 9);
+  uint64_t* full = bars;           // [4] TMA -> MMA
+  uint64_t* empty = bars + 4;      // [4] MMA done reading a stage -> TMA
+  uint64_t* accfull = bars + 8;    // [2] MMA -> epilogue
+  uint64_t* accempty = bars + 10;  // [2] epilogue -> MMA (4 warp arrivals)
+  uint64_t* wbar = bars + 12;      // weights
+  uint32_t* tslot = (uint32_t*)(bars + 13);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t ncols = tmem_cols(2 * a.cout);
   if (tid == 0) {
-    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < 8; ++i) mbar_init(&bars[i], 1);
     mbar_init(&accfull[0], 1);
     mbar_init(&accfull[1], 1);
     mbar_init(&accempty[0], 4);
@@ -292,8 +294,9 @@ __global__ void __launch_bounds__(kConv2Threads, 1)
       bulk_load(Bw, a.wpack, 27u * wtap, wbar);
       long long issued = 0;
       for (long long i = 0; i < my_tiles && ok; ++i) {
-        const int st = (int)(i & 1);
-        if (i >= 2) ok = mbar_wait_bounded(&empty[st], (uint32_t)(((i >> 1) - 1) & 1), kConvBudget);
+        const int st = (int)(i % nst);
+        if (i >= nst)
+          ok = mbar_wait_bounded(&empty[st], (uint32_t)((i / nst - 1) & 1), kConvBudget);
         if (!ok) break;
         const long long m0 = (blockIdx.x + i * gridDim.x) * 128LL;
         mbar_arrive_expect_tx(&full[st], stage_bytes);
@@ -308,8 +311,8 @@ __global__ void __launch_bounds__(kConv2Threads, 1)
         issued = i + 1;
       }
       // drain: the last stages' loads must land before the CTA exits
-      for (long long i = (issued > 2 ? issued - 2 : 0); i < issued; ++i)
-        (void)mbar_wait_bounded(&full[i & 1], (uint32_t)((i >> 1) & 1), kConvBudget);
+      for (long long i = (issued > nst ? issued - nst : 0); i < issued; ++i)
+        (void)mbar_wait_bounded(&full[i % nst], (uint32_t)((i / nst) & 1), kConvBudget);
       (void)mbar_wait_bounded(wbar, 0, kConvBudget);
       if (!ok && a.error) atomicExch(a.error, 1);
     }
@@ -320,8 +323,8 @@ __global__ void __launch_bounds__(kConv2Threads, 1)
       ok = mbar_wait_bounded(wbar, 0, kConvBudget);
       long long committed = 0;
       for (long long i = 0; i < my_tiles && ok; ++i) {
-        const int st = (int)(i & 1), ac = (int)(i & 1);
-        ok = mbar_wait_bounded(&full[st], (uint32_t)((i >> 1) & 1), kConvBudget);
+        const int st = (int)(i % nst), ac = (int)(i & 1);
+        ok = mbar_wait_bounded(&full[st], (uint32_t)((i / nst) & 1), kConvBudget);
         if (ok && i >= 2)
           ok = mbar_wait_bounded(&accempty[ac], (uint32_t)(((i >> 1) - 1) & 1), kConvBudget);
         if (!ok) break;

@@ -125,8 +125,24 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
     const int nseg = (int)((need + 255) / 256);
     const int BR = (int)(((need + nseg - 1) / nseg + 7) / 8 * 8);
     const int W = nseg * BR;
-    const size_t smem2 = 1024 + 2 * (size_t)3 * nch * W * 16 + (size_t)27 * nch * io.cout * 16 + 128;
-    if (!v1 && smem2 <= 227u * 1024u && !io.accumulate) {
+    // deepest ring (up to 4 tile stages) that fits; prefer two CTAs per SM
+    int nst = 0;
+    size_t smem2 = 0;
+    for (int cand = 4; cand >= 2 && !nst; --cand) {
+      const size_t b = 1024 + (size_t)cand * 3 * nch * W * 16 + (size_t)27 * nch * io.cout * 16 + 160;
+      if (b <= 113u * 1024u) {
+        nst = cand;
+        smem2 = b;
+      }
+    }
+    for (int cand = 4; cand >= 2 && !nst; --cand) {
+      const size_t b = 1024 + (size_t)cand * 3 * nch * W * 16 + (size_t)27 * nch * io.cout * 16 + 160;
+      if (b <= 227u * 1024u) {
+        nst = cand;
+        smem2 = b;
+      }
+    }
+    if (!v1 && nst && !io.accumulate) {
       CUtensorMap map2;
       int st2 = act_map(&map2, io.x, io.ctot_in, g.R, BR);
       if (st2 != FS_OK) return st2;
@@ -149,6 +165,7 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
       a2.W = W;
       a2.BR = BR;
       a2.phases = 1;
+      a2.nst = nst;
       a2.error = io.error;
       static bool attr2 = false;
       if (!attr2) {
@@ -194,6 +211,7 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
   a.W = c.W;
   a.BR = c.BR;
   a.phases = c.phases;
+  a.nst = 0;
   a.error = io.error;
   static bool attr_set = false;
   if (!attr_set) {

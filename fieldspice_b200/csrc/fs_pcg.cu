@@ -84,6 +84,7 @@ struct Control {
   int any_ru;
   int error;    // a bounded wait expired (TMA stage never landed)
   int precond;  // 0: CG on A~ (Jacobi), 1: multigrid-preconditioned CG
+  int flexible; // 1: nonlinear preconditioner (flexible CG): restart at updates
   unsigned int tickets[kTickets];
   unsigned int pad[2];
 };
@@ -288,7 +289,8 @@ __global__ void __launch_bounds__(fs::kBlock)
       ctl->tol = tol;
       ctl->maxiter = maxiter;
       ctl->delta = delta;
-      ctl->precond = precond;
+      ctl->precond = precond > 0 ? 1 : 0;
+      ctl->flexible = precond > 1 ? 1 : 0;
       ctl->error = 0;
       refresh_done(st, ctl, K);
     }
@@ -1032,6 +1034,9 @@ __global__ void __launch_bounds__(fs::kBlock)
               s.beta = g / s.gamma_old;
             }
             s.rmax = rn;
+            // flexible CG keeps one previous direction; after the residual
+            // is replaced, restart from the preconditioned residual
+            if (ctl->flexible) s.fresh = 1;
           }
         }
       }
@@ -1389,7 +1394,7 @@ struct Impl {
     k_init<T, K><<<P->g_init, fs::kBlock, 0, s>>>(
         P->d, P->mx, P->my, P->mz, P->dg, P->label, P->s64, P->phi, P->f, warm,
         (T*)P->x, (T*)P->r, (T*)P->p[0], P->partials, P->st, P->ctl, tol, maxiter,
-        delta, P->precond);
+        delta, P->precond ? (P->learned >= 0 ? 2 : 1) : 0);
   }
   // Iteration with parity `par` reads p[par] and writes p[1 - par].
   // Iteration with parity `par` reads p[par] and writes p[1 - par].
