@@ -129,13 +129,14 @@ __device__ __forceinline__ void apply_eq(const Dims& d, const T* __restrict__ ex
 }
 
 // One Chebyshev step: d = cd*d + cr*(b - A~ x_in), x_out = x_in + d.
-// x_zero: x_in is identically zero (first pre-smoothing step).
+// x_zero: x_in is identically zero (first pre-smoothing step); store_d = 0
+// on the last step of a sequence, whose d nobody reads.
 template <typename T, int K>
 __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     k_mg_cheb(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
               const T* __restrict__ ez, const T* __restrict__ xin,
               T* __restrict__ xout, T* __restrict__ dv,
-              const T* __restrict__ b, T cd, T cr, int x_zero,
+              const T* __restrict__ b, T cd, T cr, int x_zero, int store_d,
               const int* __restrict__ done) {
   if (*done) return;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
     }
 #pragma unroll
     for (int t = 0; t < K; ++t) xo[t] += dd[t];
-    stv<T, K>(dv, n, dd);
+    if (store_d) stv<T, K>(dv, n, dd);
     stv<T, K>(xout, n, xo);
   }
 }

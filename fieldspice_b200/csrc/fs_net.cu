@@ -115,11 +115,13 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
     fs_set_error_msg("conv3d: layer does not fit in shared memory");
     return FS_BAD_ARG;
   }
-  // the persistent, warp-specialised kernel when its two window stages and
-  // all weights fit (FS_CONV=v1 forces the one-tile-per-CTA kernel)
+  // The one-tile-per-CTA kernel is the default: measured over a U-Net
+  // forward at 64x64x32x8 it takes 1.51 ms against 1.77 ms for the
+  // persistent, warp-specialised kernel, which FS_CONV=v2 selects where its
+  // window ring and all weights fit.
   {
     const char* sel = getenv("FS_CONV");
-    const bool v1 = sel && strcmp(sel, "v1") == 0;
+    const bool v1 = !(sel && strcmp(sel, "v2") == 0);
     const int nch = io.cin / 8;
     const long long need = 128LL + 2LL * g.Zp + 2;
     const int nseg = (int)((need + 255) / 256);

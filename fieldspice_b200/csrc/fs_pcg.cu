@@ -1556,7 +1556,7 @@ struct Impl {
         if (!dry)
           fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
               L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
-              (T)cd[k], (T)cr[k], k == 0 ? 1 : 0, done);
+              (T)cd[k], (T)cr[k], k == 0 ? 1 : 0, k < deg - 1 ? 1 : 0, done);
         cur = out;
         ++*nl;
       }
@@ -1587,7 +1587,7 @@ struct Impl {
       if (!dry)
         fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
-            (T)cd[k], (T)cr[k], 0, done);
+            (T)cd[k], (T)cr[k], 0, k < deg - 1 ? 1 : 0, done);
       cur = out;
       ++*nl;
     }

@@ -13,12 +13,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=["persistent", "v1"])
+@pytest.fixture(params=["v1", "persistent"])
 def variant(request, monkeypatch):
-    """Both kernels: the persistent warp-specialised one (default where it
-    fits) and the one-tile-per-CTA kernel (FS_CONV=v1)."""
-    if request.param == "v1":
-        monkeypatch.setenv("FS_CONV", "v1")
+    """Both kernels: the one-tile-per-CTA kernel (default) and the persistent
+    warp-specialised one (FS_CONV=v2, where it fits)."""
+    if request.param == "persistent":
+        monkeypatch.setenv("FS_CONV", "v2")
     else:
         monkeypatch.delenv("FS_CONV", raising=False)
     return request.param
