@@ -171,87 +171,6 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
   }
 }
 
-// The whole coarsest-level Chebyshev solve in one CTA: x from 0, `deg`
-// steps d = cd_k d + cr_k (b - A~ x), x += d, with x (and the masses) in
-// shared memory and each thread's d and b in registers.  Replaces `deg`
-// separate launches on a level of a few thousand nodes.  NPT: nodes per
-// thread (N <= NPT * blockDim.x).
-constexpr int kCoarseThreads = 1024;
-constexpr int kCoarseMaxDeg = 64;
-struct ChebCoeffs {
-  float cd[kCoarseMaxDeg], cr[kCoarseMaxDeg];
-};
-
-template <typename T, int K, int NPT>
-__global__ void __launch_bounds__(kCoarseThreads, 1)
-    k_mg_coarse_solve(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
-                      const T* __restrict__ ez, const T* __restrict__ b, T* __restrict__ xout,
-                      int deg, ChebCoeffs co, const int* __restrict__ done) {
-  if (*done) return;
-  extern __shared__ unsigned char cs_smem[];
-  T* xs = reinterpret_cast<T*>(cs_smem);        // N * K
-  T* mx = xs + (size_t)d.N * K;                 // N each
-  T* my = mx + d.N;
-  T* mz = my + d.N;
-  for (long long n = threadIdx.x; n < d.N; n += blockDim.x) {
-    mx[n] = ex[n];
-    my[n] = ey[n];
-    mz[n] = ez[n];
-#pragma unroll
-    for (int t = 0; t < K; ++t) xs[n * K + t] = (T)0;
-  }
-  T dl[NPT][K], bl[NPT][K];
-#pragma unroll
-  for (int j = 0; j < NPT; ++j) {
-    const long long n = threadIdx.x + (long long)j * blockDim.x;
-#pragma unroll
-    for (int t = 0; t < K; ++t) {
-      dl[j][t] = (T)0;
-      bl[j][t] = n < d.N ? b[n * K + t] : (T)0;
-    }
-  }
-  __syncthreads();
-  for (int k = 0; k < deg; ++k) {
-    const T cdk = (T)co.cd[k], crk = (T)co.cr[k];
-    T xn[NPT][K];
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
-      const long long n = threadIdx.x + (long long)j * blockDim.x;
-      if (n >= d.N) continue;
-      int i, jj, kk;
-      node_ijk(d, n, i, jj, kk);
-      T ax[K];
-#pragma unroll
-      for (int t = 0; t < K; ++t) ax[t] = xs[n * K + t];
-      auto nbr = [&](T m, long long nb) {
-#pragma unroll
-        for (int t = 0; t < K; ++t) ax[t] -= m * xs[nb * K + t];
-      };
-      if (i > 0) nbr(mx[n - d.sx], n - d.sx);
-      if (i < d.nx - 1) nbr(mx[n], n + d.sx);
-      if (jj > 0) nbr(my[n - d.sy], n - d.sy);
-      if (jj < d.ny - 1) nbr(my[n], n + d.sy);
-      if (kk > 0) nbr(mz[n - 1], n - 1);
-      if (kk < d.nz - 1) nbr(mz[n], n + 1);
-#pragma unroll
-      for (int t = 0; t < K; ++t) {
-        dl[j][t] = cdk * dl[j][t] + crk * (bl[j][t] - ax[t]);
-        xn[j][t] = xs[n * K + t] + dl[j][t];
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
-      const long long n = threadIdx.x + (long long)j * blockDim.x;
-      if (n >= d.N) continue;
-#pragma unroll
-      for (int t = 0; t < K; ++t) xs[n * K + t] = xn[j][t];
-    }
-    __syncthreads();
-  }
-  for (long long n = threadIdx.x; n < (long long)d.N * K; n += blockDim.x) xout[n] = xs[n];
-}
-
 // res = b - A~ x
 template <typename T, int K>
 __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())

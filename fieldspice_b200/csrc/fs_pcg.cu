@@ -1451,7 +1451,6 @@ struct Impl {
   }
   // ---- multigrid ----------------------------------------------------------
   static void mg_setup(fs_pcg_plan* P, cudaStream_t s) {
-    coarse_attr();
     MgLevel& L0 = P->lev[0];
     L0.em[0] = P->ex;
     L0.em[1] = P->ey;
@@ -1487,25 +1486,6 @@ struct Impl {
       fs::k_mg_scales<T><<<g, fs::kBlock, 0, s>>>(c.d.N, c.s64, (T*)c.s,
                                                   (T*)c.sd);
     }
-  }
-  static size_t coarse_smem(const Dims& d) {
-    return ((size_t)d.N * K + 3 * (size_t)d.N) * sizeof(T);
-  }
-  // One-CTA coarse solve: up to 4096 nodes (4 per thread), shared memory
-  // within 200 KB, registers for d and b of 4 nodes x K RHS.
-  static bool coarse_fits(const Dims& d, int deg) {
-    if (deg > fs::kCoarseMaxDeg || d.N > 4LL * fs::kCoarseThreads) return false;
-    if (d.N > 2LL * fs::kCoarseThreads && sizeof(T) * K > 32) return false;
-    if (d.N > 1LL * fs::kCoarseThreads && sizeof(T) * K > 64) return false;
-    return coarse_smem(d) <= 200u * 1024u;
-  }
-  static void coarse_attr() {
-    cudaFuncSetAttribute(fs::k_mg_coarse_solve<T, K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    cudaFuncSetAttribute(fs::k_mg_coarse_solve<T, K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    cudaFuncSetAttribute(fs::k_mg_coarse_solve<T, K, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
   }
   // Launch one V-cycle on level l for right-hand side b; returns the index
   // of the level's x buffer that holds the result, and counts launches.
@@ -1555,28 +1535,6 @@ struct Impl {
     const T *e0 = (const T*)L.em[0], *e1 = (const T*)L.em[1], *e2 = (const T*)L.em[2];
     const int g = fs_grid_blocks((const void*)fs::k_mg_cheb<T, K>, L.d.N);
     int cur = 0;
-    // The coarsest level's Chebyshev solve in one CTA when it fits there.
-    if (last && coarse_fits(L.d, deg)) {
-      if (!dry) {
-        fs::ChebCoeffs co;
-        for (int k = 0; k < deg; ++k) {
-          co.cd[k] = (float)cd[k];
-          co.cr[k] = (float)cr[k];
-        }
-        const size_t sm = coarse_smem(L.d);
-        if (L.d.N <= 1024)
-          fs::k_mg_coarse_solve<T, K, 1><<<1, fs::kCoarseThreads, sm, s>>>(
-              L.d, e0, e1, e2, b, (T*)L.x[0], deg, co, done);
-        else if (L.d.N <= 2048)
-          fs::k_mg_coarse_solve<T, K, 2><<<1, fs::kCoarseThreads, sm, s>>>(
-              L.d, e0, e1, e2, b, (T*)L.x[0], deg, co, done);
-        else
-          fs::k_mg_coarse_solve<T, K, 4><<<1, fs::kCoarseThreads, sm, s>>>(
-              L.d, e0, e1, e2, b, (T*)L.x[0], deg, co, done);
-      }
-      ++*nl;
-      return 0;
-    }
     // Degree-2 pre-smoothing carries its residual along (x in x[1], the
     // residual in dv); otherwise Chebyshev steps then a residual pass.
     const bool resform = !last && deg == 2;
