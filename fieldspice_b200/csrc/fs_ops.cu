@@ -4,6 +4,7 @@
 #include <stdio.h>
 
 #include "fs_common.cuh"
+#include "fs_tma.cuh"
 
 using fs::Dims;
 
@@ -383,3 +384,38 @@ int fs_group_apply_noalloc(const double* mAx, const double* mAy,
 }
 
 }  // extern "C"
+
+// ---- bounded-wait self test ---------------------------------------------------------
+// One thread waits on an mbarrier that nothing will ever complete, with a
+// clock budget; when the budget runs out it records FS_TIMEOUT and returns.
+// This exercises, on the device, the path every TMA/tcgen05 wait of the
+// library takes on a timeout, without a hang and without a fault.
+namespace {
+__global__ void k_selftest_wait(long long budget, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    fs::mbar_init(&bar, 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const bool ok = fs::mbar_wait_bounded(&bar, 0, budget);
+    *status = ok ? FS_OK : FS_TIMEOUT;
+  }
+}
+}  // namespace
+
+extern "C" int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* stream) {
+  if (budget_cycles < 1 || budget_cycles > 4000000000LL || !status_host) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int* d = nullptr;
+  FS_CHECK(cudaMallocAsync((void**)&d, sizeof(int), s));
+  FS_CHECK(cudaMemsetAsync(d, 0xff, sizeof(int), s));
+  k_selftest_wait<<<1, 32, 0, s>>>(budget_cycles, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(status_host, d, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(d, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fs_cuda_status("fs_selftest_wait_timeout", e);
+  return FS_OK;
+}

@@ -328,6 +328,14 @@ int fs_pcg_plan_set_unet(fs_pcg_plan* plan, int level, int mode, float* theta, v
 /* Re-pack the plan's network weights after theta changed.                  */
 int fs_pcg_plan_sync_unet(fs_pcg_plan* plan, void* stream);
 
+
+/* Failure-detection self test: one device thread waits, with a budget of
+ * budget_cycles SM clocks, on an mbarrier nothing completes -- the path
+ * every staged-load wait of the library takes on a timeout.  *status_host
+ * receives FS_TIMEOUT when the bounded wait gave up (and the context stays
+ * usable).                                                                   */
+int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

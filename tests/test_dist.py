@@ -91,3 +91,42 @@ def test_two_ranks_gather_the_whole_batch_in_order():
         assert len(got[r]) == len(want)
         for a, b in zip(got[r], want):
             assert np.array_equal(a, b)
+
+
+def _failing_worker(rank, world, port, q):
+    """Rank 1 fails before the gather; rank 0 must learn of it through the
+    process group's timeout, not hang."""
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        q.put((rank, "raised"))
+        raise SystemExit(3)   # leaves without joining the collective
+    t0 = time.perf_counter()
+    try:
+        capacitance_matrices(_problems(), local=_oracle_local)
+        q.put((rank, "no error"))
+    except Exception as e:  # the gather times out / the peer is gone
+        q.put((rank, f"error after {time.perf_counter() - t0:.1f} s: {type(e).__name__}"))
+
+
+def test_a_failing_rank_is_detected_by_the_others():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert got[1] == "raised"
+    assert got[0].startswith("error after"), got[0]
