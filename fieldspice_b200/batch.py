@@ -27,8 +27,8 @@ from . import _lib as L
 from .boundaries import dirichlet_nodes
 from .device import DeviceOperator, EliminatedSystem, MAX_RHS, h2d, pad_rhs, upload_groups
 from .solvers.base import GPUConfig, SolverConfig, resolve_preconditioner
-from .solvers.poisson import (PoissonSolver, as_cell_array, capacitance_report,
-                              check_terminals, prepare_bc, raise_on_status)
+from .solvers.poisson import (PoissonSolver, capacitance_report, check_terminals, prepare_bc,
+                              raise_on_status, shield_nodes, upload_cell_property)
 
 __all__ = ["capacitance_matrices", "shard_by_cost", "problem_cost"]
 
@@ -63,10 +63,10 @@ class _Extraction:
     def __init__(self, grid, eps_cell, terminals, bc, cfg, gcfg):
         import torch
         self.grid = grid
-        eps = as_cell_array(eps_cell, grid, "eps_cell")
-        if np.any(eps <= 0.0):
+        _, eps, eps_min, _ = upload_cell_property(eps_cell, grid, "eps_cell")
+        if eps_min <= 0.0:
             raise ValueError("eps_cell must be strictly positive [F/m]")
-        if float(eps.min()) >= 1e-6:
+        if eps_min >= 1e-6:
             raise ValueError("eps_cell looks like a RELATIVE permittivity; "
                              "pass the absolute value in F/m")
         self.terms = check_terminals(terminals, grid)
@@ -78,16 +78,16 @@ class _Extraction:
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
         term_nodes = [np.asarray(t.nodes, np.int64) for t in self.terms]
-        shield = np.setdiff1d(wall_idx, np.concatenate(term_nodes))
         term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
+        wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
+        shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
         label = torch.zeros(self.op.N, dtype=torch.uint8, device=dev)
         if wall_idx.size:
-            label[h2d(wall_idx.astype(np.int64), torch.int64, dev)] = L.LABEL_FIXED
+            label[wall_dev] = L.LABEL_FIXED
         for n in term_dev:
             label[n] = L.LABEL_FIXED
-        self.has_shield = shield.size > 0
-        groups = term_dev + ([h2d(shield.astype(np.int64), torch.int64, dev)]
-                             if self.has_shield else [])
+        self.has_shield = shield_dev.numel() > 0
+        groups = term_dev + ([shield_dev] if self.has_shield else [])
         self.groups = groups
         self.gdev = upload_groups(groups, dev)
         self.tol = float(cfg.tol)

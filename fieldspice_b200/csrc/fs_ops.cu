@@ -419,3 +419,72 @@ extern "C" int fs_selftest_wait_timeout(long long budget_cycles, int* status_hos
   if (e != cudaSuccess) return fs_cuda_status("fs_selftest_wait_timeout", e);
   return FS_OK;
 }
+
+// ---- input validation on the device ---------------------------------------------------
+// min, max and the count of non-finite values of an FP64 array, in one pass
+// (the reference's eager checks of a cell property, poisson.py:733-742,
+// 872-877, without a host pass over the array).  Per-block partials, the
+// last block folds them in a fixed order.
+namespace {
+__global__ void k_prop_stats(const double* __restrict__ p, long long n, double* __restrict__ part,
+                             unsigned int* ticket, double* __restrict__ out) {
+  double mn = INFINITY, mx = -INFINITY, bad = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = p[i];
+    if (!isfinite(v)) {
+      bad += 1.0;
+    } else {
+      mn = fmin(mn, v);
+      mx = fmax(mx, v);
+    }
+  }
+  __shared__ double smn[fs::kBlock], smx[fs::kBlock], sbd[fs::kBlock];
+  smn[threadIdx.x] = mn;
+  smx[threadIdx.x] = mx;
+  sbd[threadIdx.x] = bad;
+  __syncthreads();
+  for (int w = fs::kBlock / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      smn[threadIdx.x] = fmin(smn[threadIdx.x], smn[threadIdx.x + w]);
+      smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + w]);
+      sbd[threadIdx.x] += sbd[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = smn[0];
+    part[3 * blockIdx.x + 1] = smx[0];
+    part[3 * blockIdx.x + 2] = sbd[0];
+  }
+  if (fs::last_block(ticket) && threadIdx.x == 0) {
+    double a = INFINITY, b = -INFINITY, c = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) {
+      a = fmin(a, __ldcg(part + 3 * k));
+      b = fmax(b, __ldcg(part + 3 * k + 1));
+      c += __ldcg(part + 3 * k + 2);
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+  }
+}
+}  // namespace
+
+extern "C" int fs_prop_stats(const double* p, long long n, double* stats_host, void* stream) {
+  if (!p || n < 1 || !stats_host) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int g = 592;
+  double* buf = nullptr;
+  FS_CHECK(cudaMallocAsync((void**)&buf, sizeof(double) * (3 * g + 3) + 64, s));
+  unsigned int* ticket = (unsigned int*)(buf + 3 * g + 3);
+  FS_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+  k_prop_stats<<<g, fs::kBlock, 0, s>>>(p, n, buf, ticket, buf + 3 * g);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(stats_host, buf + 3 * g, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(buf, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fs_cuda_status("fs_prop_stats", e);
+  return FS_OK;
+}

@@ -23,7 +23,8 @@ from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d,
                       pad_rhs, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
 
-__all__ = ["PoissonSolver", "check_terminals", "as_cell_array", "raise_on_status"]
+__all__ = ["PoissonSolver", "check_terminals", "as_cell_array", "raise_on_status",
+           "upload_cell_property", "shield_nodes"]
 
 
 def as_cell_array(a, grid, name: str) -> np.ndarray:
@@ -37,6 +38,41 @@ def as_cell_array(a, grid, name: str) -> np.ndarray:
     if not np.all(np.isfinite(arr)):
         raise ValueError(f"{name} contains non-finite values")
     return arr
+
+
+def upload_cell_property(a, grid, name: str):
+    """The checks of ``as_cell_array`` with the pass over the values on the
+    device: shape on the host, then one upload and one device reduction for
+    non-finite entries, min and max.  Returns ``(host array, device tensor,
+    min, max)``."""
+    import ctypes
+
+    import torch
+    arr = np.asarray(a, dtype=float)
+    if arr.shape == ():
+        arr = np.full(grid.shape_cells, float(arr))
+    if arr.shape != tuple(grid.shape_cells):
+        raise ValueError(f"{name} must have shape {tuple(grid.shape_cells)}, "
+                         f"got {arr.shape}")
+    from ..device import device
+    dev = h2d(arr, torch.float64, device())
+    stats = (ctypes.c_double * 3)()
+    L.check("fs_prop_stats", L.lib().fs_prop_stats(L.ptr(dev), dev.numel(), stats,
+                                                   L.stream_ptr()))
+    if stats[2] > 0:
+        raise ValueError(f"{name} contains non-finite values")
+    return arr, dev, float(stats[0]), float(stats[1])
+
+
+def shield_nodes(wall_dev, term_dev, n_nodes: int):
+    """Wall nodes that belong to no terminal (sorted, on the device)."""
+    import torch
+    if wall_dev.numel() == 0:
+        return wall_dev
+    mark = torch.zeros(n_nodes, dtype=torch.bool, device=wall_dev.device)
+    for t in term_dev:
+        mark[t] = True
+    return wall_dev[~mark[wall_dev]]
 
 
 def as_node_vector(a, grid, name: str) -> np.ndarray:
@@ -139,17 +175,17 @@ class PoissonSolver:
         self.grid = grid
         self.cfg = config or SolverConfig()
         self.gpu = gpu or GPUConfig()
-        eps_cell = as_cell_array(eps_cell, grid, "eps_cell")
-        if np.any(eps_cell <= 0.0):
+        eps_cell, eps_dev, eps_min, _ = upload_cell_property(eps_cell, grid, "eps_cell")
+        if eps_min <= 0.0:
             raise ValueError("eps_cell must be strictly positive [F/m]")
-        if float(eps_cell.min()) >= 1e-6:
+        if eps_min >= 1e-6:
             raise ValueError(
                 f"eps_cell looks like a RELATIVE permittivity (min "
-                f"{eps_cell.min():.4g}); fieldspice is strict SI and wants the "
+                f"{eps_min:.4g}); fieldspice is strict SI and wants the "
                 "absolute value in F/m. Multiply by eps0.")
         self.eps_cell = eps_cell
         self.eps_mode = eps_mode
-        self.op = DeviceOperator(grid, eps_cell, mode=eps_mode)
+        self.op = DeviceOperator(grid, eps_dev, mode=eps_mode)
         self._L = None
         self.last_capacitance_report: dict[str, Any] = {}
         self.last_device_time = 0.0
@@ -212,10 +248,9 @@ class PoissonSolver:
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
         term_nodes = [np.asarray(t.nodes, np.int64) for t in terms]
-        shield = np.setdiff1d(wall_idx, np.concatenate(term_nodes))
         term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
         wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
-        shield_dev = h2d(shield.astype(np.int64), torch.int64, dev)
+        shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
         C, q_shield, info = extract_capacitance(
             self.op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,

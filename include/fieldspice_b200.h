@@ -336,6 +336,11 @@ int fs_pcg_plan_sync_unet(fs_pcg_plan* plan, void* stream);
  * usable).                                                                   */
 int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* stream);
 
+
+/* min, max and the number of non-finite entries of an FP64 device array
+ * (stats_host[3], host); the eager input checks of a cell property.        */
+int fs_prop_stats(const double* p, long long n, double* stats_host, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
