@@ -277,6 +277,28 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// Degree-2 post-smoothing in two passes.  With r0 = b - A~ x (a residual
+// pass), the two Chebyshev steps d1 = c0 r0, d2 = cd1 d1 + cr1 (r0 - A~ d1)
+// collapse to x2 = x + alpha r0 + beta A~ r0, alpha = c0 (1 + cd1) + cr1,
+// beta = -cr1 c0: 6 vector passes instead of 8.
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
+    k_mg_post2(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+               const T* __restrict__ ez, const T* __restrict__ x, const T* __restrict__ r0,
+               T* __restrict__ xout, T alpha, T beta, const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    T ar[K], rv[K], xv[K];
+    apply_eq<T, K>(d, ex, ey, ez, r0, n, ar);
+    ldv_ro<T, K>(r0, n, rv);
+    ldv_ro<T, K>(x, n, xv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) xv[t] += alpha * rv[t] + beta * ar[t];
+    stv<T, K>(xout, n, xv);
+  }
+}
+
 // Per-axis trilinear weights of fine index i onto coarse index I (0 if none).
 __device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
   const int dlt = i - 2 * I;

@@ -1582,14 +1582,28 @@ struct Impl {
     ++*nl;
     const bool tr = !dry && l == 0 && P->trace;
     if (tr) cudaEventRecordWithFlags(P->ev[6], s, cudaEventRecordExternal);
-    for (int k = 0; k < deg; ++k) {  // post-smoothing from the corrected x
+    if (deg == 2) {  // post-smoothing as residual pass + polynomial pass
       const int out = 1 - cur;
-      if (!dry)
-        fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
-            L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
-            (T)cd[k], (T)cr[k], 0, k < deg - 1 ? 1 : 0, done);
+      if (!dry) {
+        fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
+        const double alpha = cr[0] * (1.0 + cd[1]) + cr[1], beta = -cr[1] * cr[0];
+        fs::k_mg_post2<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[cur], (const T*)L.res, (T*)L.x[out], (T)alpha,
+            (T)beta, done);
+      }
       cur = out;
-      ++*nl;
+      *nl += 2;
+    } else {
+      for (int k = 0; k < deg; ++k) {  // post-smoothing from the corrected x
+        const int out = 1 - cur;
+        if (!dry)
+          fs::k_mg_cheb<T, K><<<g, fs::kBlock, 0, s>>>(
+              L.d, e0, e1, e2, (const T*)L.x[cur], (T*)L.x[out], (T*)L.dv, b,
+              (T)cd[k], (T)cr[k], 0, k < deg - 1 ? 1 : 0, done);
+        cur = out;
+        ++*nl;
+      }
     }
     if (tr) cudaEventRecordWithFlags(P->ev[7], s, cudaEventRecordExternal);
     return cur;
