@@ -22,7 +22,7 @@ from .grid import RectilinearGrid
 from .solvers.base import ConvergenceError, GPUConfig, Result, SolverConfig, Terminal
 from . import extraction, solvers  # noqa: E402
 from .solvers import eqs, poisson, thermal  # noqa: E402,F401
-from . import batch, learned  # noqa: E402,F401
+from . import batch, circuit, learned  # noqa: E402,F401
 
 __version__ = "0.1.0"
 

@@ -95,6 +95,8 @@ _SIGNATURES = {
     "fs_pcg_plan_sync_unet": (c_int, [c_void_p, c_void_p]),
     "fs_selftest_wait_timeout": (c_int, [c_longlong, POINTER(c_int), c_void_p]),
     "fs_prop_stats": (c_int, [c_void_p, c_longlong, POINTER(c_double), c_void_p]),
+    "fs_rhs_superpose": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double),
+                                 c_void_p, c_void_p, c_longlong, c_void_p]),
     "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
     "fs_pcg_plan_launches": (c_longlong, [c_void_p]),

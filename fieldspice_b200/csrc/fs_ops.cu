@@ -488,3 +488,40 @@ extern "C" int fs_prop_stats(const double* p, long long n, double* stats_host, v
   if (e != cudaSuccess) return fs_cuda_status("fs_prop_stats", e);
   return FS_OK;
 }
+
+namespace {
+struct SuperposeCoef {
+  double c[16];
+};
+
+// out[n] = base[n] + sum_c coef[c] * phi[n*k + c0 + c]: the back-substitution
+// of a field region as a superposition of its unit-excitation solutions.
+__global__ void __launch_bounds__(fs::kBlock)
+    k_rhs_superpose(const double* __restrict__ phi, int k, int c0, int ncols,
+                    SuperposeCoef coef, const double* __restrict__ base,
+                    double* __restrict__ out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = base ? base[i] : 0.0;
+    const double* row = phi + i * k + c0;
+    for (int c = 0; c < ncols; ++c) acc = fma(coef.c[c], row[c], acc);
+    out[i] = acc;
+  }
+}
+}  // namespace
+
+extern "C" int fs_rhs_superpose(const double* phi, int k, int c0, int ncols,
+                                const double* coef_host, const double* base,
+                                double* out, long long n, void* stream) {
+  if (!phi || !out || !coef_host || n < 0 || k < 1 || c0 < 0 || ncols < 0 ||
+      ncols > 16 || c0 + ncols > k)
+    return FS_BAD_ARG;
+  if (n == 0) return FS_OK;
+  SuperposeCoef cf{};
+  for (int c = 0; c < ncols; ++c) cf.c[c] = coef_host[c];
+  int g = fs_grid_blocks((const void*)k_rhs_superpose, n);
+  k_rhs_superpose<<<g, fs::kBlock, 0, (cudaStream_t)stream>>>(phi, k, c0, ncols, cf,
+                                                               base, out, n);
+  FS_CHECK_LAUNCH("k_rhs_superpose");
+  return FS_OK;
+}

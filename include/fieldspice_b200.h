@@ -341,6 +341,16 @@ int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* st
  * (stats_host[3], host); the eager input checks of a cell property.        */
 int fs_prop_stats(const double* p, long long n, double* stats_host, void* stream);
 
+/* ---- §8f: field region (fieldspice/circuit/coupling.py) ----------------------
+ * out[i] = base[i] + sum_{c<ncols} coef_host[c] * phi[i*k + c0 + c] for
+ * i < n (FP64; base may be NULL for 0; ncols <= 16, c0 + ncols <= k): the
+ * interior back-substitution of FieldRegion.accept_timestep
+ * (coupling.py:248-262) as a superposition of the cached unit-excitation
+ * solutions (columns of K_ii^-1 K_it) on the history solution.              */
+int fs_rhs_superpose(const double* phi, int k, int c0, int ncols,
+                     const double* coef_host, const double* base, double* out,
+                     long long n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -664,3 +664,92 @@ def eqs_transient(g: Grid, eps_cell, sigma_cell, fixed_groups, values_at,
 def laplacian_apply(g: Grid, mass_edge, x):
     """``L @ x`` with the assembled CSR (reference arithmetic)."""
     return nodal_laplacian(g, mass_edge) @ x
+
+
+# ---------------------------------------------------------------------------
+# Field region stamped into a netlist -- circuit/coupling.py:55-275
+# ---------------------------------------------------------------------------
+class FieldRegionCPU:
+    """Exact reduction of a meshed EQS region to its electrodes.
+
+    ``reduce(dt)`` follows coupling.py:140-181: ``K = L_eps/dt + L_sigma``
+    (``L_sigma`` at dc), split by the electrode map ``P`` and interior
+    selector ``S`` (:117-125); ``Y = K_tt - K_ti K_ii^-1 K_it``, measured
+    asymmetry, then symmetrised; an all-zero ``K`` gives ``Y = 0`` (:156-167).
+    ``history(dt)`` is ``f_eff = P f - K_ti K_ii^-1 S f`` with ``f = (L_eps/dt)
+    phi`` (:183-193); ``accept(v, dt)`` back-substitutes the interior
+    ``u = K_ii^-1 (f_i - K_it v)`` with the electrodes at ``v`` (:248-262).
+    ``terminals``: node-index arrays, one per electrode.
+    """
+
+    def __init__(self, g: Grid, eps_cell, sigma_cell, terminals, method="direct",
+                 tol=1e-12, mode="parallel"):
+        self.g = g
+        eps_cell = np.asarray(eps_cell, float)
+        sigma_cell = np.asarray(sigma_cell, float)
+        self.L_eps = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, eps_cell, mode)))
+        self.L_sig = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, sigma_cell, mode)))
+        elec = [np.asarray(t, np.intp).ravel() for t in terminals]
+        flat = np.concatenate(elec)
+        if np.unique(flat).size != flat.size:
+            raise ValueError("terminals overlap: a node belongs to two electrodes")
+        n = g.n_nodes
+        self.interior = np.setdiff1d(np.arange(n), flat)
+        rows = np.concatenate([np.full(e.size, k) for k, e in enumerate(elec)])
+        self.P = sp.csr_matrix((np.ones(flat.size), (rows, flat)), shape=(len(elec), n))
+        self.S = sp.csr_matrix((np.ones(self.interior.size),
+                                (np.arange(self.interior.size), self.interior)),
+                               shape=(self.interior.size, n))
+        self.elec = elec
+        self.method, self.tol = method, tol
+        self.cache: dict = {}
+        self.phi = np.zeros(n)
+        self.asymmetry = 0.0
+
+    def reduce(self, dt):
+        key = 0.0 if dt is None else float(dt)
+        if key in self.cache:
+            return self.cache[key]
+        K = (self.L_sig if dt is None else self.L_eps / dt + self.L_sig).tocsr()
+        P, S = self.P, self.S
+        K_tt = (P @ K @ P.T).toarray()
+        K_ti = (P @ K @ S.T).tocsr()
+        K_ii = (S @ K @ S.T).tocsr()
+        if K.nnz == 0 or float(abs(K).max()) == 0.0:
+            entry = {"Y": np.zeros_like(K_tt), "solver": None, "K_ti": K_ti}
+            self.asymmetry = 0.0
+            self.cache[key] = entry
+            return entry
+        if K_ii.shape[0] == 0:
+            Y, solver = K_tt, None
+        else:
+            solver = LinearSystemCPU(K_ii, method=self.method, tol=self.tol)
+            K_it = K_ti.T.tocsc()
+            W = np.column_stack([solver.solve(np.asarray(K_it[:, j].todense()).ravel())
+                                 for j in range(K_it.shape[1])])
+            Y = K_tt - K_ti @ W
+        self.asymmetry = float(np.abs(Y - Y.T).max() / max(np.abs(Y).max(), 1e-300))
+        entry = {"Y": 0.5 * (Y + Y.T), "solver": solver, "K_ti": K_ti}
+        self.cache[key] = entry
+        return entry
+
+    def history(self, dt):
+        if dt is None:
+            return np.zeros(len(self.elec))
+        entry = self.reduce(dt)
+        f = (self.L_eps / dt) @ self.phi
+        f_t = self.P @ f
+        if entry["solver"] is None:
+            return f_t
+        return f_t - entry["K_ti"] @ entry["solver"].solve(self.S @ f)
+
+    def accept(self, v, dt):
+        entry = self.reduce(dt)
+        v = np.asarray(v, float)
+        phi = np.zeros(self.g.n_nodes)
+        for k, e in enumerate(self.elec):
+            phi[e] = v[k]
+        if entry["solver"] is not None and dt is not None:
+            f_i = self.S @ ((self.L_eps / dt) @ self.phi)
+            phi[self.interior] = entry["solver"].solve(f_i - entry["K_ti"].T @ v)
+        self.phi = phi

@@ -172,6 +172,105 @@ def thermal_fixture():
     np.savez_compressed(HERE / "thermal.npz", **out)
 
 
+class _StampRecorder:
+    """Wraps a reference device; logs every stamp and accept with their inputs
+    and outputs (duck-typed: the MNA reads everything else through it)."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.log = []
+
+    def __getattr__(self, name):
+        return getattr(self.dev, name)
+
+    def _own(self, nmap, stamp):
+        idx = [nmap.get(n, -1) for n in self.dev.nodes]
+        return idx, stamp
+
+    def stamp_dc(self, G, I, x, nmap, t=None):
+        self.dev.stamp_dc(G, I, x, nmap, t)
+        self.log.append(("dc", None, self.dev.terminal_admittance(None).copy(), None, None))
+
+    def stamp_tran(self, G, I, x, x_prev, dt, nmap, t=None):
+        self.dev.stamp_tran(G, I, x, x_prev, dt, nmap, t)
+        entry = self.dev._reduce(dt)
+        f = self.dev._history(entry, dt)
+        self.log.append(("tran", dt, entry["Y"].copy(), np.array(f, float), None))
+
+    def accept_timestep(self, x, x_prev, dt, nmap):
+        v = np.array([0.0 if nmap.get(n, -1) < 0 else float(x[nmap[n]])
+                      for n in self.dev.nodes])
+        self.dev.accept_timestep(x, x_prev, dt, nmap)
+        self.log.append(("accept", dt, None, v, self.dev.phi.copy()))
+
+
+def field_region_geometry():
+    """Doped-silicon slab under oxide with two copper straps on it: a
+    substrate contact on the bottom plane and the two straps are the
+    electrodes (seeded graded x axis)."""
+    rng = np.random.default_rng(21)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 4e-6, 18)), np.linspace(0, 3e-6, 13),
+                        np.linspace(0, 1e-6, 9))
+    sig = np.full(g.shape_cells, 1e-4)          # leaky oxide
+    sig[:, :, :3] = 1e2                         # doped silicon
+    eps = np.full(g.shape_cells, 3.9 * eps0)
+    eps[:, :, :3] = 11.7 * eps0
+    sig[2:15, 2:5, 3:5] = 5.8e7                 # copper straps
+    sig[3:16, 8:11, 3:5] = 5.8e7
+    eps[2:15, 2:5, 3:5] = eps0
+    eps[3:16, 8:11, 3:5] = eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(0, 0, 0, 17, 12, 0), (2, 2, 3, 15, 5, 5), (3, 8, 3, 16, 11, 5)]
+    return g, eps, sig, boxes, nid
+
+
+def field_region_fixture():
+    """circuit/coupling.py:55-275: the reduced admittance of a three-electrode
+    region at dc and at two step sizes, then the region inside the reference's
+    own backward-Euler MNA transient (a stepped source through a resistor into
+    one strap, the other strap terminated): every stamp and accept the MNA
+    made is recorded with its inputs and outputs, so that another region
+    implementation can be replayed through the same call sequence."""
+    from fieldspice import sources as S
+    from fieldspice.circuit.coupling import FieldRegion
+    from fieldspice.circuit.mna import MNASolver, Netlist
+    g, eps, sig, boxes, nid = field_region_geometry()
+    terms = [Terminal(f"e{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(boxes)]
+    cfg = SolverConfig(tol=1e-12)
+    fr = FieldRegion("FR", g, eps, sig, terms, circuit_nodes=["0", "a", "b"], config=cfg)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "sigma": sig,
+           "boxes": np.asarray(boxes)}
+    out["Y_dc"] = fr.terminal_admittance(None).copy()
+    for dt in (1e-13, 2e-12):
+        out[f"Y_dt{dt:g}"] = fr.terminal_admittance(dt).copy()
+    rec = _StampRecorder(FieldRegion("FR", g, eps, sig, terms,
+                                     circuit_nodes=["0", "a", "b"], config=cfg))
+    net = Netlist()
+    net.add_vsource("V1", "in", "0", S.step(0.5e-12, 0.0, 1.0, trise=0.4e-12))
+    net.add_resistor("R1", "in", "a", 2e3)
+    net.add_resistor("R2", "b", "0", 5e3)
+    net.add_device(rec)
+    solver = MNASolver(net)
+    res = solver.transient(t_end=6e-12, dt=0.2e-12, method="be")
+    out["t"] = res.t
+    out["v_a"] = res.fields["x"][:, solver.index("a")]
+    out["v_b"] = res.fields["x"][:, solver.index("b")]
+    kinds = {"dc": 0, "tran": 1, "accept": 2}
+    out["ev_kind"] = np.array([kinds[e[0]] for e in rec.log])
+    out["ev_dt"] = np.array([0.0 if e[1] is None else e[1] for e in rec.log])
+    nE = len(terms)
+    out["ev_Y"] = np.array([e[2] if e[2] is not None else np.zeros((nE, nE))
+                            for e in rec.log])
+    out["ev_vec"] = np.array([e[3] if e[3] is not None else np.zeros(nE) for e in rec.log])
+    acc = [i for i, e in enumerate(rec.log) if e[0] == "accept"]
+    keep = acc[:: max(1, len(acc) // 4)] + acc[-1:]
+    out["phi_at"] = np.array(keep)
+    out["phi"] = np.array([rec.log[i][4] for i in keep])
+    out["asymmetry"] = fr.asymmetry
+    np.savez_compressed(HERE / "field_region.npz", **out)
+
+
 def rc_stack(n=60):
     d, Wd, H = 4e-6, 3e-6, 2e-6
     sigma1, er1, er2 = 1e3, 4.0, 2.0
@@ -256,13 +355,20 @@ def closed_forms():
     np.savez_compressed(HERE / "closed_forms.npz", **out)
 
 
+FIXTURES = {
+    "masses": masses_fixture,
+    "readme": readme_fixture,
+    "closed_forms": closed_forms,
+    "layered": lambda: (layered_fixture((32, 32, 16), 0, 1e-12),
+                        layered_fixture((48, 48, 24), 1, 1e-12)),
+    "eqs": eqs_fixture,
+    "resistance": resistance_fixture,
+    "thermal": thermal_fixture,
+    "field_region": field_region_fixture,
+}
+
 if __name__ == "__main__":
-    masses_fixture()
-    readme_fixture()
-    closed_forms()
-    layered_fixture((32, 32, 16), 0, 1e-12)
-    layered_fixture((48, 48, 24), 1, 1e-12)
-    eqs_fixture()
-    resistance_fixture()
-    thermal_fixture()
+    # with names on the command line only those fixtures are regenerated
+    for name in (sys.argv[1:] or list(FIXTURES)):
+        FIXTURES[name]()
     print("golden fixtures written to", HERE)

@@ -166,3 +166,35 @@ def test_thermal_matches_reference(golden):
         want = d[f"T_transient_theta{theta:g}"]
         assert len(Ts) == want.shape[0]
         assert np.abs(np.array(Ts) - want).max() <= 1e-9 * np.abs(want - 300.0).max()
+
+
+def field_region_terminals(d, g):
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    return [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+
+
+def test_field_region_matches_reference(golden):
+    """coupling.py: reduced admittances and the recorded MNA call sequence
+    (every history current and every accepted field) replayed through the
+    oracle's restatement."""
+    d = golden("field_region")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    fr = O.FieldRegionCPU(g, d["eps"], d["sigma"], field_region_terminals(d, g))
+    for key, dt in (("Y_dc", None), ("Y_dt1e-13", 1e-13), ("Y_dt2e-12", 2e-12)):
+        Y = fr.reduce(dt)["Y"]
+        assert np.abs(Y - d[key]).max() <= 1e-12 * np.abs(d[key]).max(), key
+    fr = O.FieldRegionCPU(g, d["eps"], d["sigma"], field_region_terminals(d, g))
+    phis = dict(zip(d["phi_at"].tolist(), d["phi"]))
+    for i, kind in enumerate(d["ev_kind"]):
+        dt = None if kind == 0 else float(d["ev_dt"][i])
+        if kind in (0, 1):
+            Y = fr.reduce(dt)["Y"]
+            assert np.abs(Y - d["ev_Y"][i]).max() <= 1e-12 * np.abs(Y).max()
+        if kind == 1:
+            f = fr.history(dt)
+            want = d["ev_vec"][i]
+            assert np.abs(f - want).max() <= 1e-10 * max(np.abs(want).max(), 1e-30)
+        if kind == 2:
+            fr.accept(d["ev_vec"][i], dt)
+            if i in phis:
+                assert np.abs(fr.phi - phis[i]).max() <= 1e-12
