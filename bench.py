@@ -282,6 +282,8 @@ def run_ours(args, rank, world, local_rank):
         variants["batch64"] = batch_variant(timed)
         variants["learned_fcg"] = learned_variant(timed, step_device, C, args)
         variants["eqs_transient"] = eqs_variant()
+        variants["field_region"] = field_region_variant()
+        variants["rlgc_2d"] = rlgc_variant()
 
     if rank != 0:
         return
@@ -444,6 +446,94 @@ def eqs_variant(shape=(192, 192, 96), steps=200):
             "current_err_vs_fp64_final": float(err[-1]),
             "per_step_err_quantiles": [float(np.quantile(err, q)) for q in (0.5, 0.9, 1.0)],
             "precision": "auto (mixed, FP64 continuation on stall)", "tol": TOL}
+
+
+def field_region_variant(shape=(128, 128, 64), steps=100, dt=1e-12):
+    """A meshed EQS region as a netlist element (circuit/coupling.py): copper
+    boxes in oxide over doped silicon, every box plus the bottom plane an
+    electrode.  Time of the Schur-complement reduction at dt = 1 ps (one
+    block solve of all unit excitations) and of the per-step device work
+    (history solve, stamp, back-substitution) with the electrode voltages of
+    a 10 ps ramp; Y and the history currents against the same region solved
+    in FP64 at relres 1e-12."""
+    import torch
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.circuit import FieldRegion
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    w = W.eqs_interconnect(shape, nbox=6, nports=2, seed=1)
+    g = w.grid()
+    nx, ny, nz = shape
+    nid = np.arange(nx * ny * nz).reshape(shape)
+    terms = [Terminal(f"box{i}", t) for i, t in enumerate(w.terminals)]
+    terms.append(Terminal("sub", nid[:, :, 0].ravel()))
+    names = [t.name for t in terms]
+    nmap = {n: i for i, n in enumerate(names[:-1])}      # "sub" is ground
+    ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
+
+    def run(precision, tol):
+        fr = FieldRegion("FR", g, w.eps_cell, w.sigma_cell, terms,
+                         circuit_nodes=names[:-1] + ["0"], config=SolverConfig(tol=tol),
+                         gpu=GPUConfig(precision=precision, preconditioner="mg"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Y = fr.terminal_admittance(dt).copy()
+        torch.cuda.synchronize()
+        t_red = time.perf_counter() - t0
+        nE = len(names) - 1
+        fs = []
+        t0 = time.perf_counter()
+        for k in range(1, steps + 1):
+            G = np.zeros((nE, nE))
+            I = np.zeros(nE)
+            fr.stamp_tran(G, I, None, None, dt, nmap)
+            fs.append(I.copy())
+            x = np.zeros(nE)
+            x[0] = ramp(k * dt)
+            fr.accept_timestep(x, None, dt, nmap)
+        torch.cuda.synchronize()
+        t_steps = time.perf_counter() - t0
+        fr.close()
+        return Y, np.array(fs), t_red, t_steps
+    Y, f, t_red, t_steps = run("auto", TOL)
+    Yf, ff, t_redf, t_stepsf = run("fp64", 1e-12)
+    return {"metric": f"field-region steps/s ({shape[0]}x{shape[1]}x{shape[2]}, "
+                      f"{len(terms)} electrodes, dt 1 ps)",
+            "value": steps / t_steps, "reduction_s": t_red, "steps": steps,
+            "fp64_reduction_s": t_redf, "fp64_value": steps / t_stepsf,
+            "Y_err_vs_fp64": float(np.abs(Y - Yf).max() / np.abs(Yf).max()),
+            "f_eff_err_vs_fp64": float(np.abs(f - ff).max() / max(np.abs(ff).max(), 1e-300)),
+            "nodes": int(np.prod(shape)), "tol": TOL}
+
+
+def rlgc_variant(nx=1201, ny=801):
+    """Per-unit-length RLGC of a coupled-microstrip cross-section
+    (extraction.rlgc_2d): three 2-D extractions (dielectric, vacuum,
+    conductivity) batched on one GPU with the semi-coarsened multigrid
+    (x and y halved, the two z planes kept); C and L against the same call in
+    FP64 at relres 1e-12."""
+    import torch
+    from fieldspice_b200 import extraction as EX
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    w = W.cross_section(nx, ny, nlines=3, seed=0)
+    g = w.grid()
+    terms = [Terminal(n, t) for n, t in zip(w.names, w.terminals)]
+
+    def run(precision, tol):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = EX.rlgc_2d(g, w.eps_cell, w.sigma_cell, terms, config=SolverConfig(tol=tol),
+                       gpu=GPUConfig(precision=precision, preconditioner="mg"))
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+    run("auto", TOL)                      # warm-up (plans, allocator)
+    r, t = run("auto", TOL)
+    rf, tf = run("fp64", 1e-12)
+    return {"metric": f"rlgc_2d calls/s ({nx}x{ny}x2 nodes, 4 conductors)",
+            "value": 1.0 / t, "seconds": t, "fp64_seconds": tf,
+            "C_err_vs_fp64": float(np.abs(r["C"] - rf["C"]).max() / np.abs(rf["C"]).max()),
+            "L_err_vs_fp64": float(np.abs(r["L"] - rf["L"]).max() / np.abs(rf["L"]).max()),
+            "Z0": [float(z) for z in r["Z0"]], "nodes": int(nx * ny * 2), "tol": TOL}
 
 
 def batch_variant(timed):

@@ -130,7 +130,7 @@ def _stats_list(arr, n):
             for s in arr[:n]]
 
 
-def _extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
+def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
     """Extract every problem on this GPU; returns the list of C matrices."""
     import torch
     out: list[Any] = [None] * len(problems)
@@ -206,7 +206,7 @@ def capacitance_matrices(problems: Sequence, config: SolverConfig | None = None,
     cfg = config or SolverConfig()
     gcfg = gpu or GPUConfig()
     problems = list(problems)
-    run = local or _extract_local
+    run = local or extract_local
     t0 = time.perf_counter()
     import torch.distributed as dist
     world, rank = 1, 0

@@ -2,7 +2,10 @@
 // system  A~ = S A S  (S = diag(A)^-1/2 on free nodes, 0 on fixed nodes).
 //
 // Levels.  Vertex-centred coarsening: coarse node I sits on fine node 2I, so
-// n_c = (n + 1) / 2 per axis.  The coarse operator is a rediscretisation of
+// n_c = (n + 1) / 2 per axis.  An axis too short to coarsen (the two node
+// planes of a 2-D cross-section, say) is kept as it is (n_c = n, coarse node I
+// on fine node I): semi-coarsening, recognised by every kernel below from
+// f.n == c.n on that axis.  The coarse operator is a rediscretisation of
 // the original Laplacian A: a coarse x-edge joins fine nodes 2I -> 2I+2, i.e.
 // two fine x-edges in series, and collects the 3 x 3 fine edge rows around
 // it with lateral weights (1/2, 1, 1/2) per direction, which reproduces the
@@ -29,6 +32,9 @@
 
 namespace fs {
 
+// Coarsening ratio of one axis: 2, or 1 where the axis is kept.
+__device__ __forceinline__ int ratio(int nf, int nc) { return nf == nc ? 1 : 2; }
+
 // ---- setup (FP64, original scale) ---------------------------------------------
 __device__ __forceinline__ double series2(double a, double b) {
   return (a > 0.0 && b > 0.0) ? 1.0 / (1.0 / a + 1.0 / b) : 0.0;
@@ -47,36 +53,44 @@ __global__ void k_mg_coarsen(Dims f, Dims c, const double* __restrict__ fmx,
        n += (long long)gridDim.x * blockDim.x) {
     int I, J, Kc;
     node_ijk(c, n, I, J, Kc);
-    const int i = 2 * I, j = 2 * J, k = 2 * Kc;
+    const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+    const int i = rx * I, j = ry * J, k = rz * Kc;
     const long long fn = ((long long)i * f.ny + j) * f.nz + k;
     clabel[n] = flabel[fn] == FS_LABEL_FREE ? FS_LABEL_FREE : FS_LABEL_FIXED;
-    // x-edge I -> I+1: fine x-edges i -> i+1 -> i+2 in series, lateral j, k
+    // lateral weight of offset a on an axis of ratio r: (1/2, 1, 1/2) when
+    // coarsened, the single fine row otherwise
+    auto lw = [&](int a, int r) { return r == 2 ? lat[a + 1] : 1.0; };
+    // x-edge I -> I+1: fine x-edges i -> i+1 -> i+2 in series (one fine edge
+    // on an uncoarsened axis), lateral j, k
     double sx = 0.0, sy = 0.0, sz = 0.0;
     if (I + 1 < c.nx) {
-      for (int a = -1; a <= 1; ++a)
-        for (int b = -1; b <= 1; ++b) {
+      for (int a = 1 - ry; a <= ry - 1; ++a)
+        for (int b = 1 - rz; b <= rz - 1; ++b) {
           const int jj = j + a, kk = k + b;
           if (jj < 0 || jj >= f.ny || kk < 0 || kk >= f.nz) continue;
           const long long m0 = ((long long)i * f.ny + jj) * f.nz + kk;
-          sx += lat[a + 1] * lat[b + 1] * series2(fmx[m0], fmx[m0 + f.sx]);
+          sx += lw(a, ry) * lw(b, rz) *
+                (rx == 2 ? series2(fmx[m0], fmx[m0 + f.sx]) : fmx[m0]);
         }
     }
     if (J + 1 < c.ny) {
-      for (int a = -1; a <= 1; ++a)
-        for (int b = -1; b <= 1; ++b) {
+      for (int a = 1 - rx; a <= rx - 1; ++a)
+        for (int b = 1 - rz; b <= rz - 1; ++b) {
           const int ii = i + a, kk = k + b;
           if (ii < 0 || ii >= f.nx || kk < 0 || kk >= f.nz) continue;
           const long long m0 = ((long long)ii * f.ny + j) * f.nz + kk;
-          sy += lat[a + 1] * lat[b + 1] * series2(fmy[m0], fmy[m0 + f.sy]);
+          sy += lw(a, rx) * lw(b, rz) *
+                (ry == 2 ? series2(fmy[m0], fmy[m0 + f.sy]) : fmy[m0]);
         }
     }
     if (Kc + 1 < c.nz) {
-      for (int a = -1; a <= 1; ++a)
-        for (int b = -1; b <= 1; ++b) {
+      for (int a = 1 - rx; a <= rx - 1; ++a)
+        for (int b = 1 - ry; b <= ry - 1; ++b) {
           const int ii = i + a, jj = j + b;
           if (ii < 0 || ii >= f.nx || jj < 0 || jj >= f.ny) continue;
           const long long m0 = ((long long)ii * f.ny + jj) * f.nz + k;
-          sz += lat[a + 1] * lat[b + 1] * series2(fmz[m0], fmz[m0 + 1]);
+          sz += lw(a, rx) * lw(b, ry) *
+                (rz == 2 ? series2(fmz[m0], fmz[m0 + 1]) : fmz[m0]);
         }
     }
     cmx[n] = sx;
@@ -299,8 +313,10 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
   }
 }
 
-// Per-axis trilinear weights of fine index i onto coarse index I (0 if none).
+// Per-axis trilinear weights of fine index i onto coarse index I (0 if none);
+// the identity on an uncoarsened axis.
 __device__ __forceinline__ float pw(int i, int I, int nf, int nc) {
+  if (nf == nc) return i == I ? 1.0f : 0.0f;
   const int dlt = i - 2 * I;
   if (dlt == 0) return 1.0f;
   if (dlt == 1) return (I + 1 < nc) ? 0.5f : 1.0f;  // last fine node: weight 1
@@ -316,17 +332,18 @@ __global__ void k_mg_coarsen_diag(Dims f, Dims c, const double* __restrict__ fd,
        n += (long long)gridDim.x * blockDim.x) {
     int I, J, Kc;
     node_ijk(c, n, I, J, Kc);
+    const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
     double acc = 0.0;
-    for (int a = -1; a <= 1; ++a) {
-      const int i = 2 * I + a;
+    for (int a = 1 - rx; a <= rx - 1; ++a) {
+      const int i = rx * I + a;
       if (i < 0 || i >= f.nx) continue;
       const double wa = pw(i, I, f.nx, c.nx);
-      for (int b = -1; b <= 1; ++b) {
-        const int j = 2 * J + b;
+      for (int b = 1 - ry; b <= ry - 1; ++b) {
+        const int j = ry * J + b;
         if (j < 0 || j >= f.ny) continue;
         const double wb = wa * pw(j, J, f.ny, c.ny);
-        for (int e = -1; e <= 1; ++e) {
-          const int k = 2 * Kc + e;
+        for (int e = 1 - rz; e <= rz - 1; ++e) {
+          const int k = rz * Kc + e;
           if (k < 0 || k >= f.nz) continue;
           const double w = wb * pw(k, Kc, f.nz, c.nz);
           if (w != 0.0) acc += w * fd[((long long)i * f.ny + j) * f.nz + k];
@@ -353,16 +370,17 @@ __global__ void __launch_bounds__(kBlock)
     if (scale != (T)0) {
       int I, J, Kc;
       node_ijk(c, n, I, J, Kc);
-      for (int a = -1; a <= 1; ++a) {
-        const int i = 2 * I + a;
+      const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+      for (int a = 1 - rx; a <= rx - 1; ++a) {
+        const int i = rx * I + a;
         if (i < 0 || i >= f.nx) continue;
         const float wa = pw(i, I, f.nx, c.nx);
-        for (int b = -1; b <= 1; ++b) {
-          const int j = 2 * J + b;
+        for (int b = 1 - ry; b <= ry - 1; ++b) {
+          const int j = ry * J + b;
           if (j < 0 || j >= f.ny) continue;
           const float wb = wa * pw(j, J, f.ny, c.ny);
-          for (int e = -1; e <= 1; ++e) {
-            const int k = 2 * Kc + e;
+          for (int e = 1 - rz; e <= rz - 1; ++e) {
+            const int k = rz * Kc + e;
             if (k < 0 || k >= f.nz) continue;
             const long long fn = ((long long)i * f.ny + j) * f.nz + k;
             const T w = (T)(wb * pw(k, Kc, f.nz, c.nz)) * __ldg(sdf + fn);
@@ -381,58 +399,9 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// x_f += sd(f) * sum_I P(f,I) s_c(I) x_c(I)   (fine-centric, in place)
-template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
-    k_mg_prolong(Dims f, Dims c, const T* __restrict__ xc,
-                 const T* __restrict__ sc, const T* __restrict__ sdf,
-                 T* __restrict__ xf, const int* __restrict__ done) {
-  if (*done) return;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < f.N;
-       n += (long long)gridDim.x * blockDim.x) {
-    const T scale = sdf[n];
-    if (scale == (T)0) continue;
-    int i, j, k;
-    node_ijk(f, n, i, j, k);
-    int ci[2], cj[2], ck[2];
-    float wi[2], wj[2], wk[2];
-    int ni, nj, nk;
-    auto axis = [](int x, int nc, int (&cx)[2], float (&wx)[2], int& cnt) {
-      if ((x & 1) == 0) {
-        cx[0] = x >> 1; wx[0] = 1.0f; cnt = 1;
-      } else if (((x + 1) >> 1) < nc) {
-        cx[0] = x >> 1; cx[1] = (x + 1) >> 1; wx[0] = wx[1] = 0.5f; cnt = 2;
-      } else {
-        cx[0] = x >> 1; wx[0] = 1.0f; cnt = 1;
-      }
-    };
-    axis(i, c.nx, ci, wi, ni);
-    axis(j, c.ny, cj, wj, nj);
-    axis(k, c.nz, ck, wk, nk);
-    T acc[K];
-#pragma unroll
-    for (int t = 0; t < K; ++t) acc[t] = (T)0;
-    for (int a = 0; a < ni; ++a)
-      for (int b = 0; b < nj; ++b)
-        for (int e = 0; e < nk; ++e) {
-          const long long cn = ((long long)ci[a] * c.ny + cj[b]) * c.nz + ck[e];
-          const T w = (T)(wi[a] * wj[b] * wk[e]) * __ldg(sc + cn);
-          if (w == (T)0) continue;
-          T v[K];
-          ldv_ro<T, K>(xc, cn, v);
-#pragma unroll
-          for (int t = 0; t < K; ++t) acc[t] += w * v[t];
-        }
-    T xv[K];
-    ldv<T, K>(xf, n, xv);
-#pragma unroll
-    for (int t = 0; t < K; ++t) xv[t] += scale * acc[t];
-    stv<T, K>(xf, n, xv);
-  }
-}
-
 // Prolongation, coarse-cell-centric: the thread of coarse node (I, J, Kc)
-// writes the fine nodes 2I+a, 2J+b, 2Kc+c (a, b, c in {0, 1}) that it owns,
+// writes the fine nodes 2I+a, 2J+b, 2Kc+c (a, b, c in {0, 1}; only offset 0,
+// fine node I, on an uncoarsened axis) that it owns,
 // interpolating from the up to 8 coarse corners it loads once:
 //   x_f += sd(f) * sum_I P(f, I) s_c(I) x_c(I).
 template <typename T, int K>
@@ -445,7 +414,10 @@ __global__ void __launch_bounds__(kBlock)
        n += (long long)gridDim.x * blockDim.x) {
     int I, J, Kc;
     node_ijk(c, n, I, J, Kc);
-    const bool hx = I + 1 < c.nx, hy = J + 1 < c.ny, hz = Kc + 1 < c.nz;
+    const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+    // an upper coarse partner exists (and is used) only on coarsened axes
+    const bool hx = rx == 2 && I + 1 < c.nx, hy = ry == 2 && J + 1 < c.ny,
+               hz = rz == 2 && Kc + 1 < c.nz;
     // corner values v[a][b][e] = s_c x_c at (I+a, J+b, Kc+e); absent -> 0
     T v[2][2][2][K];
 #pragma unroll
@@ -470,18 +442,18 @@ __global__ void __launch_bounds__(kBlock)
     // or, on a last fine node with no upper partner, weight 1 from below)
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
-      const int i = 2 * I + a;
-      if (i >= f.nx) continue;
+      const int i = rx * I + a;
+      if (a >= rx || i >= f.nx) continue;
       const T wa0 = a == 0 ? (T)1 : (hx ? (T)0.5 : (T)1), wa1 = a == 0 ? (T)0 : (hx ? (T)0.5 : (T)0);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const int j = 2 * J + b;
-        if (j >= f.ny) continue;
+        const int j = ry * J + b;
+        if (b >= ry || j >= f.ny) continue;
         const T wb0 = b == 0 ? (T)1 : (hy ? (T)0.5 : (T)1), wb1 = b == 0 ? (T)0 : (hy ? (T)0.5 : (T)0);
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int k = 2 * Kc + e;
-          if (k >= f.nz) continue;
+          const int k = rz * Kc + e;
+          if (e >= rz || k >= f.nz) continue;
           const T we0 = e == 0 ? (T)1 : (hz ? (T)0.5 : (T)1), we1 = e == 0 ? (T)0 : (hz ? (T)0.5 : (T)0);
           const long long fn = ((long long)i * f.ny + j) * f.nz + k;
           const T scale = __ldg(sdf + fn);

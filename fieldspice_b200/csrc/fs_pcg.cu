@@ -1103,13 +1103,19 @@ struct MgLevel {
       off_x[2], off_b, off_dv, off_res;
 };
 
+// Level sizes: every axis of at least 5 nodes is halved (n -> (n + 1) / 2),
+// shorter axes are kept (semi-coarsening, e.g. the two node planes of a 2-D
+// cross-section), until the level holds at most `coarsest` nodes or no axis
+// can be coarsened.
 int mg_dims(const Dims& fine, long long coarsest, Dims* out) {
   int nl = 0;
   Dims d = fine;
   out[nl++] = d;
-  while (nl < kMaxLevels && d.N > coarsest && d.nx >= 5 && d.ny >= 5 &&
-         d.nz >= 5) {
-    d = fs::make_dims((d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2);
+  auto half = [](int n) { return n >= 5 ? (n + 1) / 2 : n; };
+  while (nl < kMaxLevels && d.N > coarsest) {
+    const int nx = half(d.nx), ny = half(d.ny), nz = half(d.nz);
+    if (nx == d.nx && ny == d.ny && nz == d.nz) break;
+    d = fs::make_dims(nx, ny, nz);
     out[nl++] = d;
   }
   return nl;

@@ -1,7 +1,12 @@
 """Parasitic extraction front door (``fieldspice/extraction.py``).
 
 :func:`capacitance_matrix` keeps the reference signature
-(``extraction.py:41-56``) and routes to the GPU :class:`PoissonSolver`.
+(``extraction.py:41-56``) and routes to the GPU :class:`PoissonSolver`;
+:func:`resistance_matrix` is the same solve with conductivity masses;
+:func:`rlgc_2d` runs its three cross-section extractions (real dielectric,
+vacuum, conductivity) as one batch of GPU solves.  The transmission-line and
+network-parameter helpers below it are the reference's closed forms on small
+host matrices (``extraction.py:236-317``).
 """
 
 from __future__ import annotations
@@ -11,7 +16,9 @@ from typing import Sequence
 
 import numpy as np
 
-__all__ = ["capacitance_matrix", "resistance_matrix", "to_spice_matrix"]
+__all__ = ["capacitance_matrix", "resistance_matrix", "to_spice_matrix", "rlgc_2d",
+           "characteristic_impedance", "check_lc_identity", "s_parameters", "y_to_z",
+           "z_to_y", "elmore_delay", "skin_depth"]
 
 
 def capacitance_matrix(grid, eps_cell: np.ndarray, terminals: Sequence,
@@ -87,3 +94,158 @@ def to_spice_matrix(c_maxwell: np.ndarray) -> np.ndarray:
     out = -c.copy()
     np.fill_diagonal(out, c.sum(axis=1))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Transmission lines (extraction.py:105-264)
+# ---------------------------------------------------------------------------
+def rlgc_2d(grid, eps_cell: np.ndarray, sigma_cell: np.ndarray, terminals: Sequence,
+            mu_cell: np.ndarray | None = None, freq: float = 0.0, config=None,
+            reference: int | str = -1, *, gpu=None) -> dict[str, np.ndarray]:
+    """Per-unit-length R, L, G, C matrices of a 2-D cross-section (``grid.Nz
+    == 1``, unit thickness in the collapsed direction), referenced to the
+    return conductor ``reference`` (index or name; default the last), as
+    ``extraction.py:108-206``.
+
+    ``C`` (real permittivity), ``C_air`` (vacuum everywhere) and ``G``
+    (conductivity in place of permittivity, floored at 1e-30 S/m) are three
+    capacitance extractions on the same grid, solved as one batch on the GPU;
+    ``L = mu_r mu0 eps0 C_air^-1`` by the TEM identity; ``R`` is the
+    reference's DC (optionally skin-corrected) series-resistance estimate.
+    Returns ``{"R", "L", "G", "C", "C_air", "eps_eff", "Z0", "v_p",
+    "reference"}``, matrices ``(nt-1, nt-1)``.
+    """
+    from .batch import extract_local
+    from .solvers.base import GPUConfig, SolverConfig
+    from .units import eps0, mu0
+    if grid.Nz != 1:
+        raise ValueError("rlgc_2d needs a 2D cross-section (grid.Nz == 1)")
+    terminals = list(terminals)
+    nt = len(terminals)
+    if nt < 2:
+        raise ValueError(
+            "rlgc_2d needs at least two conductors: one signal and one return")
+    if isinstance(reference, str):
+        names = [t.name for t in terminals]
+        if reference not in names:
+            raise ValueError(f"reference {reference!r} is not among {names}")
+        ref_i = names.index(reference)
+    else:
+        ref_i = int(reference) % nt
+    keep = [i for i in range(nt) if i != ref_i]
+    eps_cell = np.asarray(eps_cell, dtype=float)
+    sigma_cell = np.asarray(sigma_cell, dtype=float)
+    lossy = bool(np.any(sigma_cell > 0))
+    problems = [(grid, eps_cell, terminals), (grid, np.full_like(eps_cell, eps0), terminals)]
+    if lossy:
+        problems.append((grid, np.maximum(sigma_cell, 1e-30), terminals))
+    mats = extract_local(problems, config or SolverConfig(), gpu or GPUConfig(),
+                         len(problems), None)
+
+    def _reduce(m: np.ndarray) -> np.ndarray:
+        return np.asarray(m)[np.ix_(keep, keep)]
+
+    C = _reduce(mats[0])
+    C_air = _reduce(mats[1])
+    mu_r = 1.0
+    if mu_cell is not None:
+        mu_r = float(np.mean(np.asarray(mu_cell, dtype=float)) / mu0)
+    L = mu_r * mu0 * eps0 * np.linalg.inv(C_air)
+    G = _reduce(mats[2]) if lossy else np.zeros_like(C)
+    R = _series_resistance(grid, sigma_cell, [terminals[i] for i in keep], freq)
+    eps_eff = np.diag(C) / np.diag(C_air)
+    v_p = 1.0 / np.sqrt(np.diag(L) * np.diag(C))
+    Z0 = np.sqrt(np.diag(L) / np.diag(C))
+    return {"R": R, "L": L, "G": G, "C": C, "C_air": C_air, "eps_eff": eps_eff,
+            "Z0": Z0, "v_p": v_p, "reference": terminals[ref_i].name}
+
+
+def _series_resistance(grid, sigma_cell, terminals, freq) -> np.ndarray:
+    """DC (or skin-corrected) series resistance per unit length [ohm/m]
+    (``extraction.py:209-233``): every conductor gets the estimate of the
+    whole conducting cross-section, as in the reference."""
+    nt = len(terminals)
+    R = np.zeros((nt, nt))
+    cellvol = grid.cell_volumes()
+    length = grid.zn[-1] - grid.zn[0]
+    mask = sigma_cell > 0
+    for i in range(nt):
+        area = float(cellvol[mask].sum() / max(length, 1e-300)) if mask.any() else 0.0
+        sig = float(np.mean(sigma_cell[mask])) if mask.any() else 0.0
+        if area <= 0 or sig <= 0:
+            R[i, i] = 0.0
+            continue
+        r_dc = 1.0 / (sig * area)
+        if freq > 0:
+            delta = skin_depth(sig, freq)
+            perim = 4.0 * np.sqrt(area)
+            a_hf = min(area, perim * delta)
+            r_dc = max(r_dc, 1.0 / (sig * max(a_hf, 1e-300)))
+        R[i, i] = r_dc
+    return R
+
+
+def characteristic_impedance(rlgc: dict, freq=0.0) -> np.ndarray:
+    """``Z0 = sqrt((R + jwL)/(G + jwC))`` [ohm]; lossless at ``freq=0``."""
+    R, L, G, C = (np.atleast_2d(rlgc[k]) for k in ("R", "L", "G", "C"))
+    w = 2.0 * np.pi * np.asarray(freq, dtype=float)
+    if np.all(w == 0):
+        return np.sqrt(np.diag(L) / np.diag(C))
+    num = np.diag(R) + 1j * w[..., None] * np.diag(L)
+    den = np.diag(G) + 1j * w[..., None] * np.diag(C)
+    return np.sqrt(num / den)
+
+
+def check_lc_identity(rlgc: dict, eps_r: float = 1.0, mu_r: float = 1.0) -> float:
+    """Max relative deviation of ``L C`` from ``mu eps I`` (TEM identity)."""
+    from .units import eps0, mu0
+    L = np.atleast_2d(rlgc["L"])
+    C = np.atleast_2d(rlgc["C"])
+    target = mu_r * mu0 * eps_r * eps0 * np.eye(L.shape[0])
+    scale = max(np.abs(target).max(), 1e-300)
+    return float(np.abs(L @ C - target).max() / scale)
+
+
+# ---------------------------------------------------------------------------
+# Network parameters (extraction.py:267-317)
+# ---------------------------------------------------------------------------
+def y_to_z(y: np.ndarray) -> np.ndarray:
+    """Admittance (or a stack of them) to impedance."""
+    return np.linalg.inv(np.asarray(y))
+
+
+def z_to_y(z: np.ndarray) -> np.ndarray:
+    return np.linalg.inv(np.asarray(z))
+
+
+def s_parameters(y: np.ndarray, z0=50.0) -> np.ndarray:
+    """``S = (I - Z0 Y)(I + Z0 Y)^-1`` for one ``(n, n)`` admittance or a
+    stack ``(nf, n, n)``, real reference impedance (scalar or per port)."""
+    y = np.asarray(y)
+    single = y.ndim == 2
+    Y = y[None, ...] if single else y
+    n = Y.shape[-1]
+    Z0 = np.eye(n) * z0 if np.isscalar(z0) else np.diag(np.asarray(z0, float))
+    eye = np.eye(n)
+    S = np.empty_like(Y, dtype=complex)
+    for k in range(Y.shape[0]):
+        A = Z0 @ Y[k]
+        S[k] = (eye - A) @ np.linalg.inv(eye + A)
+    return S[0] if single else S
+
+
+def elmore_delay(r: np.ndarray, c: np.ndarray) -> float:
+    """Elmore delay of an RC ladder, ``sum_i c_i sum_{j<=i} r_j`` [s]."""
+    r = np.asarray(r, dtype=float)
+    c = np.asarray(c, dtype=float)
+    if r.shape != c.shape:
+        raise ValueError("r and c must have the same shape")
+    return float(np.sum(c * np.cumsum(r)))
+
+
+def skin_depth(sigma: float, freq: float, mu_r: float = 1.0) -> float:
+    """``sqrt(2/(omega mu sigma))`` [m]; infinite at ``freq <= 0``."""
+    from .units import mu0
+    if freq <= 0:
+        return float("inf")
+    return float(np.sqrt(2.0 / (2.0 * np.pi * freq * mu_r * mu0 * sigma)))

@@ -126,6 +126,11 @@ class RectilinearGrid:
     @property
     def zc(self) -> np.ndarray: return 0.5 * (self.zn[:-1] + self.zn[1:])
 
+    def cell_volumes(self) -> np.ndarray:
+        """Primal cell volumes, shape ``shape_cells`` (grid.py:383-386)."""
+        return (self.hx[:, None, None] * self.hy[None, :, None]
+                * self.hz[None, None, :])
+
     def node_volumes(self) -> np.ndarray:
         """Dual box volumes, shape ``shape_nodes`` (grid.py:388-396)."""
         return (self.hxd[:, None, None] * self.hyd[None, :, None]

@@ -14,6 +14,9 @@ and the reference itself can be fed byte-identical inputs.
 * :func:`batch_geometries` -- 64 uneven geometries of the same family.
 * :func:`eqs_interconnect` -- copper boxes in oxide over doped silicon for
   the backward-Euler EQS transient.
+* :func:`cross_section` -- a 2-D transmission-line cross-section (collapsed
+  z, two node planes): coupled microstrips on a two-layer substrate over a
+  ground plane, air above, for ``rlgc_2d``.
 """
 
 from __future__ import annotations
@@ -26,7 +29,7 @@ import numpy as np
 from .units import eps0
 
 __all__ = ["Workload", "parallel_plate", "layered_boxes", "batch_geometries",
-           "eqs_interconnect", "ramp"]
+           "eqs_interconnect", "cross_section", "ramp"]
 
 SIO2 = 3.9
 
@@ -223,3 +226,47 @@ def eqs_interconnect(shape=(192, 192, 96), nbox=6, nports=2, seed=0,
     return Workload(f"eqs_{nx}x{ny}x{nz}_s{seed}", x, y, z, eps, terms,
                     [f"port{i}" for i in range(nports)], {"zlo": 0.0},
                     sigma_cell=sig, boxes=boxes, meta={"seed": seed, "si_cells": si})
+
+
+def cross_section(nx: int = 301, ny: int = 201, width: float = 60e-6,
+                  height: float = 40e-6, nlines: int = 2, seed: int = 0) -> Workload:
+    """Coupled microstrips: ``nlines`` traces (6 um wide, 1 um thick, seeded
+    gaps) on a 12 um substrate (eps_r 4.4, sigma 1e-3 S/m) under a 2 um
+    solder mask (eps_r 3.0), air above, a ground plane on the bottom node
+    row; uniform ``nx x ny`` nodes, z collapsed (two planes, 1 m apart).
+    Terminals: the traces, then the ground; each holds both z planes."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.0, width, nx)
+    y = np.linspace(0.0, height, ny)
+    z = np.array([0.0, 1.0])
+    xc = 0.5 * (x[:-1] + x[1:])
+    yc = 0.5 * (y[:-1] + y[1:])
+    X, Y = np.meshgrid(xc, yc, indexing="ij")
+    eps = np.full((nx - 1, ny - 1, 1), eps0)
+    sig = np.zeros((nx - 1, ny - 1, 1))
+    sub = Y < 0.3 * height
+    eps[sub] = 4.4 * eps0
+    sig[sub] = 1e-3
+    mask = (Y >= 0.3 * height) & (Y < 0.35 * height)
+    eps[mask] = 3.0 * eps0
+    nid = np.arange(nx * ny * 2).reshape(nx, ny, 2)
+
+    def box(x0, x1, y0, y1):
+        i = np.flatnonzero((x >= x0) & (x <= x1))
+        j = np.flatnonzero((y >= y0) & (y <= y1))
+        return nid[i[0]:i[-1] + 1, j[0]:j[-1] + 1, :].ravel()
+    wl, t = 0.1 * width, 0.025 * height
+    gaps = rng.uniform(0.5, 1.5, max(0, nlines - 1)) * wl
+    span = nlines * wl + gaps.sum()
+    x0 = 0.5 * (width - span)
+    terms, names = [], []
+    y0 = 0.3 * height
+    for k in range(nlines):
+        terms.append(box(x0, x0 + wl, y0, y0 + t))
+        names.append(f"line{k}")
+        x0 += wl + (gaps[k] if k < nlines - 1 else 0.0)
+    terms.append(box(0.0, width, 0.0, 0.0))
+    names.append("gnd")
+    w = Workload(f"cross_section_{nx}x{ny}", x, y, z, eps, terms, names,
+                 sigma_cell=sig)
+    return w

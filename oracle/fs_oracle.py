@@ -753,3 +753,29 @@ class FieldRegionCPU:
             f_i = self.S @ ((self.L_eps / dt) @ self.phi)
             phi[self.interior] = entry["solver"].solve(f_i - entry["K_ti"].T @ v)
         self.phi = phi
+
+
+# ---------------------------------------------------------------------------
+# Per-unit-length line parameters -- extraction.py:108-206
+# ---------------------------------------------------------------------------
+def rlgc_2d_matrices(g: Grid, eps_cell, sigma_cell, terminals, reference=-1,
+                     method="direct", tol=1e-12):
+    """``C``, ``C_air``, ``G`` and ``L`` of a 2-D cross-section referenced to
+    conductor ``reference`` (an index), as ``extraction.py:168-199``: three
+    capacitance extractions (real permittivity, vacuum, conductivity floored
+    at 1e-30) with every wall insulating, the reference row and column
+    removed, and ``L = mu0 eps0 C_air^-1``."""
+    nt = len(terminals)
+    ref_i = int(reference) % nt
+    keep = [i for i in range(nt) if i != ref_i]
+    eps_cell = np.asarray(eps_cell, float)
+    sigma_cell = np.asarray(sigma_cell, float)
+    mu0 = 4e-7 * math.pi * 1.0000000000552
+
+    def cap(prop):
+        C, _ = capacitance_matrix(g, prop, terminals, method=method, tol=tol)
+        return C[np.ix_(keep, keep)]
+    C = cap(eps_cell)
+    C_air = cap(np.full_like(eps_cell, EPS0))
+    G = cap(np.maximum(sigma_cell, 1e-30)) if np.any(sigma_cell > 0) else np.zeros_like(C)
+    return {"C": C, "C_air": C_air, "G": G, "L": mu0 * EPS0 * np.linalg.inv(C_air)}

@@ -271,6 +271,55 @@ def field_region_fixture():
     np.savez_compressed(HERE / "field_region.npz", **out)
 
 
+def rlgc_fixture():
+    """extraction.py:108-233: per-unit-length R, L, G, C of a coupled
+    microstrip cross-section (two copper lines on a lossy substrate over a
+    ground plane, air above; seeded graded x axis, collapsed z) at dc and at
+    1 GHz, with the reference conductor given by index and by name."""
+    from fieldspice.extraction import rlgc_2d
+    rng = np.random.default_rng(5)
+    x = np.unique(np.concatenate([np.linspace(0, 40e-6, 41),
+                                  rng.uniform(12e-6, 28e-6, 10)]))
+    y = np.linspace(0, 30e-6, 31)
+    g = RectilinearGrid(x, y, None)
+    xc = 0.5 * (x[:-1] + x[1:])
+    yc = 0.5 * (y[:-1] + y[1:])
+    X, Y = np.meshgrid(xc, yc, indexing="ij")
+    eps = np.full(g.shape_cells, eps0)
+    sig = np.zeros(g.shape_cells)
+    sub = Y < 10e-6
+    eps[sub] = 4.4 * eps0
+    sig[sub] = 1e-3
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    xn, yn = g.xn, g.yn
+
+    def box(x0, x1, y0, y1):
+        i = np.flatnonzero((xn >= x0) & (xn <= x1))
+        j = np.flatnonzero((yn >= y0) & (yn <= y1))
+        return nid[i[0]:i[-1] + 1, j[0]:j[-1] + 1, :].ravel()
+    # copper exactly on the cells between each line's electrode nodes: a
+    # copper cell touching a free node would carry the substrate current
+    # through a 5.8e7 S/m edge, a difference of nearly equal potentials that
+    # no solver resolves beyond ~1e-5 relative
+    for x0, x1 in ((12e-6, 17e-6), (22e-6, 27e-6)):
+        i = np.flatnonzero((xn >= x0) & (xn <= x1))
+        j = np.flatnonzero((yn >= 10e-6) & (yn <= 12e-6))
+        sig[i[0]:i[-1], j[0]:j[-1], :] = 5.8e7
+    terms = [Terminal("s1", box(12e-6, 17e-6, 10e-6, 12e-6)),
+             Terminal("s2", box(22e-6, 27e-6, 10e-6, 12e-6)),
+             Terminal("gnd", box(0, 40e-6, 0, 0))]
+    out = {"x": x, "y": y, "eps": eps, "sigma": sig}
+    for i, t in enumerate(terms):
+        out[f"term{i}"] = t.nodes
+    for tag, kw in (("dc", {}), ("ghz", {"freq": 1e9}), ("name", {"reference": "gnd"}),
+                    ("ref0", {"reference": 0})):
+        r = rlgc_2d(g, eps, sig, terms, **kw)
+        for k in ("R", "L", "G", "C", "C_air", "eps_eff", "Z0", "v_p"):
+            out[f"{tag}_{k}"] = np.asarray(r[k])
+        out[f"{tag}_reference"] = np.array(r["reference"])
+    np.savez_compressed(HERE / "rlgc.npz", **out)
+
+
 def rc_stack(n=60):
     d, Wd, H = 4e-6, 3e-6, 2e-6
     sigma1, er1, er2 = 1e3, 4.0, 2.0
@@ -365,6 +414,7 @@ FIXTURES = {
     "resistance": resistance_fixture,
     "thermal": thermal_fixture,
     "field_region": field_region_fixture,
+    "rlgc": rlgc_fixture,
 }
 
 if __name__ == "__main__":

@@ -198,3 +198,17 @@ def test_field_region_matches_reference(golden):
             fr.accept(d["ev_vec"][i], dt)
             if i in phis:
                 assert np.abs(fr.phi - phis[i]).max() <= 1e-12
+
+
+def test_rlgc_matrices_match_reference(golden):
+    """extraction.py:108-206 on a coupled-microstrip cross-section: the
+    oracle's three capacitance extractions reproduce the reference's C,
+    C_air, G and L with the ground and with the first line as the return."""
+    d = golden("rlgc")
+    g = O.Grid(d["x"], d["y"], np.array([0.0, 1.0]))
+    terms = [d["term0"], d["term1"], d["term2"]]
+    for tag, ref in (("dc", -1), ("ref0", 0)):
+        got = O.rlgc_2d_matrices(g, d["eps"], d["sigma"], terms, reference=ref)
+        for k in ("C", "C_air", "G", "L"):
+            want = d[f"{tag}_{k}"]
+            assert np.abs(got[k] - want).max() <= 1e-10 * np.abs(want).max(), (tag, k)
