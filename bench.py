@@ -284,6 +284,7 @@ def run_ours(args, rank, world, local_rank):
         variants["eqs_transient"] = eqs_variant()
         variants["field_region"] = field_region_variant()
         variants["rlgc_2d"] = rlgc_variant()
+        variants["ac_admittance"] = ac_variant()
 
     if rank != 0:
         return
@@ -460,7 +461,7 @@ def field_region_variant(shape=(128, 128, 64), steps=100, dt=1e-12):
     from fieldspice_b200 import workloads as W
     from fieldspice_b200.circuit import FieldRegion
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
-    w = W.eqs_interconnect(shape, nbox=6, nports=2, seed=1)
+    w = W.eqs_interconnect(shape, nbox=6, nports=6, seed=1)
     g = w.grid()
     nx, ny, nz = shape
     nid = np.arange(nx * ny * nz).reshape(shape)
@@ -534,6 +535,40 @@ def rlgc_variant(nx=1201, ny=801):
             "C_err_vs_fp64": float(np.abs(r["C"] - rf["C"]).max() / np.abs(rf["C"]).max()),
             "L_err_vs_fp64": float(np.abs(r["L"] - rf["L"]).max() / np.abs(rf["L"]).max()),
             "Z0": [float(z) for z in r["Z0"]], "nodes": int(nx * ny * 2), "tol": TOL}
+
+
+def ac_variant(shape=(128, 128, 64), freqs=(1e6, 1e9, 1e10)):
+    """Harmonic EQS (solvers/ac.py): the 7x7 complex admittance of copper
+    boxes in oxide over doped silicon (every box and the bottom plane a
+    terminal) at three frequencies, each one complex-symmetric block solve
+    (COCG with the multigrid V-cycle of |A| + |B|).  Accuracy: reciprocity
+    of Y (the reference's own check) and row sums (no terminal current is
+    lost: every wall insulating)."""
+    import torch
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.solvers.ac import ACSolver
+    from fieldspice_b200.solvers.base import Terminal
+    w = W.eqs_interconnect(shape, nbox=6, nports=6, seed=2)
+    g = w.grid()
+    nx, ny, nz = shape
+    nid = np.arange(nx * ny * nz).reshape(shape)
+    terms = [Terminal(f"box{i}", t) for i, t in enumerate(w.terminals)]
+    terms.append(Terminal("sub", nid[:, :, 0].ravel()))
+    ac = ACSolver(g, w.eps_cell, w.sigma_cell)
+    ac.admittance_matrix(terms, freqs[:1])            # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Y = ac.admittance_matrix(terms, freqs)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    asym = max(float(np.abs(y - y.T).max() / np.abs(y).max()) for y in Y)
+    rows = max(float(np.abs(y.sum(axis=1)).max() / np.abs(np.diag(y)).max()) for y in Y)
+    its = [[s["iterations"] for s in st] for st in ac.last_stats]
+    return {"metric": f"AC admittance matrices/s ({shape[0]}x{shape[1]}x{shape[2]}, "
+                      f"{len(terms)} terminals)",
+            "value": len(freqs) / t, "seconds": t, "freqs": list(freqs),
+            "iterations": its, "asymmetry_max": asym, "row_sum_rel_max": rows,
+            "nodes": int(np.prod(shape))}
 
 
 def batch_variant(timed):

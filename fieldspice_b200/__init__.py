@@ -21,7 +21,7 @@ from .boundaries import BoundarySpec, Dirichlet, Neumann, wall_nodes
 from .grid import RectilinearGrid
 from .solvers.base import ConvergenceError, GPUConfig, Result, SolverConfig, Terminal
 from . import extraction, solvers  # noqa: E402
-from .solvers import eqs, poisson, thermal  # noqa: E402,F401
+from .solvers import ac, eqs, poisson, thermal  # noqa: E402,F401
 from . import batch, circuit, learned  # noqa: E402,F401
 
 __version__ = "0.1.0"

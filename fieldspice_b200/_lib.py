@@ -97,6 +97,12 @@ _SIGNATURES = {
     "fs_prop_stats": (c_int, [c_void_p, c_longlong, POINTER(c_double), c_void_p]),
     "fs_rhs_superpose": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double),
                                  c_void_p, c_void_p, c_longlong, c_void_p]),
+    "fs_pcg_plan_precondition": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fs_pcg_plan_scale": (c_int, [c_void_p, POINTER(c_void_p), POINTER(c_void_p)]),
+    "fs_ac_workspace_bytes": (c_int, [c_int, c_int, c_int, c_int, c_int, POINTER(c_size_t)]),
+    "fs_ac_solve": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                            c_void_p, c_double, c_int, c_void_p, c_size_t,
+                            POINTER(FsRhsStats), c_void_p]),
     "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
     "fs_pcg_plan_launches": (c_longlong, [c_void_p]),

@@ -21,8 +21,8 @@ source: ``K phi' = f`` on the interior with the electrodes at 0 and
 back-substitution after an accepted step (``coupling.py:248-262``,
 ``u = K_ii^-1 (f_i - K_it v)``) is, by linearity, ``phi' + sum_b v_b phi_b``:
 the cached unit solutions make it one superposition kernel instead of a
-second solve.  The AC stamp (``K = L_sigma + j w L_eps``, a complex-symmetric
-solve) is not on the GPU path and raises ``NotImplementedError``.
+second solve.  The AC stamp (``K = L_sigma + j w L_eps``) is the same unit
+excitation with the complex-symmetric solve of ``solvers/ac.py``.
 """
 
 from __future__ import annotations
@@ -147,6 +147,7 @@ class FieldRegion:
         self._phi = torch.zeros(n, dtype=torch.float64, device=dev)
         self._version = 0
         self.asymmetry: float = 0.0
+        self.last_history_stats: dict | None = None   # the last history solve's
         self.t: float = 0.0
         self.limited: bool = False
 
@@ -250,6 +251,7 @@ class FieldRegion:
                 L.ptr(hs.f), nx, ny, nz, 1, L.stream_ptr()))
             tol = float(self.cfg.tol)
             _, st = hs.solve(tol, self.gpu.maxiter, warm=True)
+            self.last_history_stats = st[0]
             raise_on_status(st, tol, "gpu-cg")
             # sum_{n in T} (K phi' - (L_eps/dt) phi)_n = K_ti u - P f
             f = -entry.K.group_sums(hs.phi, self._elec, minus=m, w=self._phi,
@@ -287,9 +289,17 @@ class FieldRegion:
             _stamp_i(I, idx[a], f[a])
 
     def stamp_ac(self, Y_mat, J, x_op, omega: float, nmap: Mapping[str, int]) -> None:
-        raise NotImplementedError(
-            "FieldRegion.stamp_ac needs a complex-symmetric solve "
-            "(K = L_sigma + j w L_eps), which the GPU path does not implement")
+        """Frequency domain, ``K = L_sigma + j w L_eps`` with no history
+        (coupling.py:214-236): the complex Schur complement by unit excitation
+        of the electrodes, one complex-symmetric GPU solve per electrode block."""
+        from ..solvers.ac import complex_admittance
+        opB = self.op_eps.combine(float(omega), self.op_eps, 0.0)
+        Yeff, _ = complex_admittance(self.op_sig, opB, self._elec, float(self.cfg.tol),
+                                     self.gpu)
+        idx = self._indices(nmap)
+        for a in range(len(idx)):
+            for b in range(len(idx)):
+                _stamp_g(Y_mat, idx[a], idx[b], Yeff[a, b])
 
     def accept_timestep(self, x, x_prev, dt: float, nmap: Mapping[str, int]) -> None:
         """Back-substitute the field once the step is accepted (coupling.py:248-262)."""

@@ -1250,6 +1250,10 @@ struct fs_pcg_plan {
   fs_unet* net = nullptr;
   void *net_u = nullptr, *net_r = nullptr;  // level vectors of mode 1
   int net_status = FS_OK;
+  // fs_pcg_plan_precondition: the caller's level-0 right-hand side and the
+  // level buffer that holds the V-cycle's output
+  const void* ext_b = nullptr;
+  void* ext_z = nullptr;
 };
 
 namespace {
@@ -1636,6 +1640,12 @@ struct Impl {
                                                 P->st, P->ctl);
     return nl + 1;
   }
+  // One V-cycle on a caller's equilibrated right-hand side (P->ext_b).
+  static void vcycle_ext(fs_pcg_plan* P, cudaStream_t s) {
+    long long nl = 0;
+    const int zi = vcycle(P, 0, (const T*)P->ext_b, s, &nl);
+    P->ext_z = P->lev[0].x[zi];
+  }
   static void finalize(fs_pcg_plan* P, cudaStream_t s) {
     k_finalize<T, K><<<P->g_fin, fs::kBlock, 0, s>>>(P->d, P->label, P->s64,
                                                      P->phi, (T*)P->x, P->st,
@@ -1658,6 +1668,7 @@ bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
     if (op == 9) { Impl<T, KK>::mg_setup(P, s); Impl<T, KK>::locate_z(P); } \
     if (op == 10) P->launches_per_iter = Impl<T, KK>::precondition(P, s); \
     if (op == 11) Impl<T, KK>::locate_z(P);                        \
+    if (op == 12) Impl<T, KK>::vcycle_ext(P, s);                   \
     return true;
   switch (k) {
     FS_OP(1)
@@ -2123,6 +2134,35 @@ int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, cons
   }
 #undef FS_EQ
   FS_CHECK_LAUNCH("k_eq_apply");
+  return FS_OK;
+}
+
+int fs_pcg_plan_scale(const fs_pcg_plan* P, const double** s64, const uint8_t** label) {
+  if (!P || !s64 || !label) return FS_BAD_ARG;
+  *s64 = P->s64;
+  *label = P->label;
+  return FS_OK;
+}
+
+int fs_pcg_plan_precondition(fs_pcg_plan* P, const void* r, void* z, void* stream) {
+  if (!P || !r || !z) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = (size_t)P->d.N * P->nrhs *
+                       (P->precision == FS_PRECISION_MIXED ? sizeof(float) : sizeof(double));
+  if (!P->precond) {  // Jacobi: the identity on the equilibrated system
+    FS_CHECK(cudaMemcpyAsync(z, r, bytes, cudaMemcpyDeviceToDevice, s));
+    return FS_OK;
+  }
+  if (P->learned >= 0) {
+    fs_set_error_msg("fs_pcg_plan_precondition: the plan carries a learned level");
+    return FS_BAD_ARG;
+  }
+  // the V-cycle kernels skip their work once a solve of this plan finished
+  FS_CHECK(cudaMemsetAsync(&P->ctl->all_done, 0, sizeof(int), s));
+  P->ext_b = r;
+  if (!dispatch(P, 12, s)) return FS_BAD_ARG;
+  FS_CHECK(cudaGetLastError());
+  FS_CHECK(cudaMemcpyAsync(z, P->ext_z, bytes, cudaMemcpyDeviceToDevice, s));
   return FS_OK;
 }
 

@@ -11,6 +11,7 @@ the reference's (relative residual of the equilibrated free-node system).
 
 from __future__ import annotations
 
+import ctypes
 import time
 import warnings
 from typing import Any, Sequence
@@ -284,22 +285,22 @@ class PoissonSolver:
     # -- single potential solve -------------------------------------------------
     def solve(self, terminals: Sequence | None = None, bc=None, rho_node=None,
               *, t: float = 0.0) -> Result:
-        """Potential for voltage-driven terminals, Dirichlet walls and free
-        charge (``poisson.py:967-1063``).
+        """Potential for voltage-driven, floating and charge-driven terminals,
+        Dirichlet walls and free charge (``poisson.py:967-1063``).
 
-        Floating and charge-driven terminals and periodic walls need the
-        node-merging reduction (``poisson.py:698-719``), which the GPU path
-        does not implement; they raise ``NotImplementedError``.
+        The reference merges every floating or charge-driven electrode into one
+        unknown (``P^T L P``, ``poisson.py:665-719``).  Here the same solution
+        comes from superposition, with the electrodes held as Dirichlet
+        conductors: one block solve gives the potential with every such
+        electrode at 0 V and the unit potential of each, and the small system
+        ``C V = Q - q_0`` (``C`` their mutual capacitances, ``Q`` the
+        prescribed charges, 0 for a floating one) fixes their potentials.
+        Periodic walls (also a node merge) are not implemented.
         """
         import torch
         t0 = time.perf_counter()
         grid = self.grid
         terms = check_terminals(terminals, grid)
-        for tt in terms:
-            if tt.driven != "voltage":
-                raise NotImplementedError(
-                    f"terminal {tt.name!r} is {tt.driven}-driven; the GPU path "
-                    "supports voltage-driven terminals only")
         bc = prepare_bc(bc, grid)
         dev = self.op.dev
         N = self.op.N
@@ -309,6 +310,10 @@ class PoissonSolver:
             b_free += as_node_vector(rho_node, grid, "rho_node") * vnode
 
         fixed, vals = _dirichlet_sets(bc, terms, grid, t)
+        floats = [tt for tt in terms if tt.driven != "voltage"]
+        if floats:
+            return self._solve_floating(terms, floats, fixed, vals, b_free,
+                                        rho_node is not None, t, t0)
         label = torch.zeros(N, dtype=torch.uint8, device=dev)
         pinned = None
         if fixed.size == 0:
@@ -336,14 +341,84 @@ class PoissonSolver:
         tol = float(self.cfg.tol)
         _, stats = system.solve(tol, self.gpu.maxiter)
         raise_on_status(stats, tol, "gpu-cg")
-        phi_d = system.phi
-        phi = phi_d.cpu().numpy().copy()
-        qnode = self.op.apply(phi_d).cpu().numpy() - b_free
-        info = {"method": f"gpu-cg-jacobi-{self.gpu.precision}", "n": N,
+        info = {"method": f"gpu-cg-{system.preconditioner}-{self.gpu.precision}", "n": N,
                 "n_factorised": system.n_free, "iterations": stats[0]["iterations"],
                 "residual": stats[0]["relres"], "pinned": pinned,
                 "setup_time": system.setup_time,
                 "solve_time": time.perf_counter() - t0}
+        res = self._potential_result(system.phi, terms, b_free, info, fixed.size, t0)
+        system.close()
+        return res
+
+    def _solve_floating(self, terms, floats, fixed, vals, b_free, with_src: bool,
+                        t: float, t0: float) -> Result:
+        """Floating / charge-driven electrodes by superposition (see solve)."""
+        import torch
+        N = self.op.N
+        dev = self.op.dev
+        nf = len(floats)
+        if nf + 1 > MAX_RHS:
+            raise NotImplementedError(
+                f"{nf} floating or charge-driven electrodes: the GPU path solves at "
+                f"most {MAX_RHS - 1} in one block")
+        if fixed.size == 0:
+            raise NotImplementedError(
+                "floating electrodes without any Dirichlet node (a driven terminal or "
+                "a grounded wall): the potential has no reference on the GPU path")
+        fnodes = [np.asarray(tt.nodes, np.intp) for tt in floats]
+        if np.isin(np.concatenate(fnodes), fixed).any():
+            raise NotImplementedError(
+                "a floating or charge-driven electrode touches a Dirichlet node")
+        k = pad_rhs(nf + 1)
+        label = torch.zeros(N, dtype=torch.uint8, device=dev)
+        fixed_d = torch.as_tensor(fixed, device=dev)
+        label[fixed_d] = L.LABEL_FIXED
+        fnodes_d = [h2d(nd.astype(np.int64), torch.int64, dev) for nd in fnodes]
+        for nd in fnodes_d:
+            label[nd] = L.LABEL_FIXED
+        system = EliminatedSystem(self.op, label, nf + 1, precision=self.gpu.precision,
+                                  with_source=with_src,
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+        # column 0: the driven potentials (floating electrodes at 0 V) and the
+        # free charge; column 1 + f: electrode f at 1 V, everything else 0 V
+        phi_h = np.zeros((N, k))
+        phi_h[fixed, 0] = vals
+        for f, nd in enumerate(fnodes):
+            phi_h[nd, 1 + f] = 1.0
+        system.phi.copy_(h2d(phi_h.ravel(), torch.float64, dev))
+        if with_src:
+            f_h = np.zeros((N, k))
+            f_h[:, 0] = b_free
+            system.f.copy_(h2d(f_h.ravel(), torch.float64, dev))
+        tol = float(self.cfg.tol)
+        _, stats = system.solve(tol, self.gpu.maxiter)
+        raise_on_status(stats, tol, "gpu-cg")
+        Q = self.op.group_sums(system.phi, fnodes_d, nrhs=k)
+        q0 = Q[:, 0] - np.array([b_free[nd].sum() for nd in fnodes])
+        Cff = Q[:, 1:nf + 1]
+        target = np.array([float(tt.value_at(t)) if tt.driven == "current" else 0.0
+                           for tt in floats])
+        V = np.linalg.solve(Cff, target - q0)
+        phi_d = torch.empty(N, dtype=torch.float64, device=dev)
+        coef = (ctypes.c_double * (nf + 1))(1.0, *V)
+        L.check("fs_rhs_superpose", L.lib().fs_rhs_superpose(
+            L.ptr(system.phi), k, 0, nf + 1, coef, None, L.ptr(phi_d), N, L.stream_ptr()))
+        info = {"method": f"gpu-cg-{system.preconditioner}-{self.gpu.precision}", "n": N,
+                "n_factorised": system.n_free,
+                "iterations": max(s["iterations"] for s in stats),
+                "residual": max(s["relres"] for s in stats), "pinned": None,
+                "floating_potentials": V.tolist(), "setup_time": system.setup_time,
+                "solve_time": time.perf_counter() - t0}
+        res = self._potential_result(phi_d, terms, b_free, info, fixed.size, t0)
+        system.close()
+        return res
+
+    def _potential_result(self, phi_d, terms, b_free, info, n_fixed: int, t0: float) -> Result:
+        """``Result`` of a potential solve (poisson.py:1082-1097)."""
+        grid = self.grid
+        N = self.op.N
+        phi = phi_d.cpu().numpy().copy()
+        qnode = self.op.apply(phi_d).cpu().numpy() - b_free
         res = Result(grid=grid)
         res.fields["phi"] = phi.reshape((1,) + tuple(grid.shape_nodes))
         res.fields["e"] = (-grad_edges(grid, phi)).reshape(1, -1)
@@ -356,12 +431,11 @@ class PoissonSolver:
         res.scalars["total_charge"] = np.array([float(qnode.sum())])
         res.meta["linear"] = info
         res.meta["n_unknowns"] = N
-        res.meta["n_dirichlet"] = int(fixed.size)
+        res.meta["n_dirichlet"] = int(n_fixed)
         res.meta.setdefault("solver", self.name)
         res.meta.setdefault("assumptions", list(self.assumptions))
         res.meta.setdefault("wall_time", time.perf_counter() - t0)
         res.meta.setdefault("grid_cells", tuple(grid.shape_cells))
-        system.close()
         return res
 
     def _diagonal(self) -> np.ndarray:

@@ -351,6 +351,33 @@ int fs_rhs_superpose(const double* phi, int k, int c0, int ncols,
                      const double* coef_host, const double* base, double* out,
                      long long n, void* stream);
 
+/* ---- a plan's preconditioner on a caller's vectors ---------------------------
+ * z = M r for the plan's equilibrated system: one multigrid V-cycle (identity
+ * for a Jacobi plan) on N*nrhs values in the plan's precision.  The plan must
+ * not carry a learned level.  fs_pcg_plan_scale exposes the plan's FP64
+ * scaling s = diag^-1/2 (0 on non-free nodes) and its classified labels
+ * (FS_LABEL_*: free, fixed, solo, pinned).                                   */
+int fs_pcg_plan_precondition(fs_pcg_plan* plan, const void* r, void* z, void* stream);
+int fs_pcg_plan_scale(const fs_pcg_plan* plan, const double** s64, const uint8_t** label);
+
+/* ---- §8f-4: harmonic EQS, the complex-symmetric solve -------------------------
+ * Replaces the per-frequency sparse LU of fieldspice/solvers/ac.py:95-145
+ * (ACSolver.solve / admittance_matrix): K phi = 0 with K = A + jB, A and B
+ * node-padded edge masses (3N FP64 each, x | y | z like fs_build_masses'
+ * output: A = sigma - w eps'' masses, B = w eps' masses), phi fixed on the
+ * nodes labelled FIXED.  phi: N x K FP64, K = the power of two >= 2*ncplx,
+ * column c < K/2 the real and K/2 + c the imaginary part of right-hand side
+ * c (ncplx <= 8); Dirichlet values in, solution out.  COCG on the system
+ * equilibrated by diag(|A| + |B|)^-1/2, preconditioned by the multigrid
+ * V-cycle (precond = FS_PRECOND_MG) of |A| + |B| or by nothing
+ * (FS_PRECOND_JACOBI); stopping rule ||S r|| <= tol ||S b|| on the true FP64
+ * residual.  stats: ncplx entries.                                          */
+int fs_ac_workspace_bytes(int nx, int ny, int nz, int ncplx, int precond, size_t* bytes);
+int fs_ac_solve(int nx, int ny, int nz, int ncplx, int precond, const double* mA,
+                const double* mB, const uint8_t* label_in, double* phi, double tol,
+                int maxiter, void* workspace, size_t workspace_bytes, fs_rhs_stats* stats,
+                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -779,3 +779,85 @@ def rlgc_2d_matrices(g: Grid, eps_cell, sigma_cell, terminals, reference=-1,
     C_air = cap(np.full_like(eps_cell, EPS0))
     G = cap(np.maximum(sigma_cell, 1e-30)) if np.any(sigma_cell > 0) else np.zeros_like(C)
     return {"C": C, "C_air": C_air, "G": G, "L": mu0 * EPS0 * np.linalg.inv(C_air)}
+
+
+# ---------------------------------------------------------------------------
+# Harmonic EQS -- solvers/ac.py:34-181
+# ---------------------------------------------------------------------------
+def ac_system(g: Grid, eps_cell, sigma_cell, freq):
+    """``K = L_sigma + j w (L_eps' + j L_eps'')`` as complex CSR (ac.py:79-95)."""
+    eps = np.asarray(eps_cell)
+    L_sig = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, np.asarray(sigma_cell, float))))
+    L_eps = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, np.real(eps).astype(float))))
+    L_eps = L_eps.astype(complex)
+    if np.iscomplexobj(eps) and np.any(np.imag(eps) != 0.0):
+        L_eps = L_eps + 1j * nodal_laplacian(
+            g, edge_mass_vector(g, cell_to_edge(g, np.imag(eps).astype(float))))
+    w = 2.0 * np.pi * float(freq)
+    return sp.csr_matrix(L_sig.astype(complex) + 1j * w * L_eps)
+
+
+def ac_potential(K, n, fixed, values):
+    """Complex Dirichlet elimination and sparse LU (ac.py:166-181, :143)."""
+    idx = np.asarray(fixed, np.intp)
+    vals = np.asarray(values, complex)
+    x0 = np.zeros(n, complex)
+    x0[idx] = vals
+    b = -(K @ x0)
+    mask = np.ones(n, bool)
+    mask[idx] = False
+    Dm = sp.diags(mask.astype(float))
+    A = sp.csr_matrix(Dm @ K @ Dm + sp.diags((~mask).astype(float)))
+    b[idx] = vals
+    return spla.spsolve(A.tocsc(), b)
+
+
+def ac_admittance(g: Grid, eps_cell, sigma_cell, terminals, freqs):
+    """``Y[k, i, j]`` by unit excitation (ac.py:123-148)."""
+    terms = [np.asarray(t, np.intp) for t in terminals]
+    fixed = np.concatenate(terms)
+    nt = len(terms)
+    freqs = np.atleast_1d(np.asarray(freqs, float))
+    Y = np.zeros((freqs.size, nt, nt), complex)
+    for k, f in enumerate(freqs):
+        K = ac_system(g, eps_cell, sigma_cell, f)
+        for j in range(nt):
+            vals = np.concatenate([np.full(t.size, 1.0 if m == j else 0.0)
+                                   for m, t in enumerate(terms)])
+            cur = K @ ac_potential(K, g.n_nodes, fixed, vals)
+            for i, t in enumerate(terms):
+                Y[k, i, j] = cur[t].sum()
+    return Y
+
+
+def ac_schur(g: Grid, eps_cell, sigma_cell, terminals, omega):
+    """The field region's frequency-domain stamp ``Y_eff = K_tt - K_ti
+    K_ii^-1 K_it`` with ``K = L_sigma + j w L_eps`` (coupling.py:214-236),
+    by unit excitation (the same matrix)."""
+    return ac_admittance(g, eps_cell, sigma_cell, terminals, [omega / (2.0 * np.pi)])[0]
+
+
+# ---------------------------------------------------------------------------
+# Floating / charge-driven electrodes -- poisson.py:665-719, 1030-1063
+# ---------------------------------------------------------------------------
+def merged_potential(g: Grid, eps_cell, fixed, values, merge_groups, b_ext, mode="parallel"):
+    """``phi = P x`` with every node set in ``merge_groups`` merged into one
+    unknown (``P`` has one 1 per row), ``P^T L P x = P^T b`` with the Dirichlet
+    rows eliminated and a direct solve (poisson.py:665-719, 1041-1058).
+    ``b_ext``: node charges (free charge, a charge-driven electrode's charge
+    on its first node).  Fixed nodes must not belong to a merged group.
+    Returns ``(phi, L)``."""
+    n = g.n_nodes
+    Lm = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, np.asarray(eps_cell, float), mode)))
+    label = np.arange(n)
+    for grp in merge_groups:
+        grp = np.asarray(grp, np.intp)
+        label[grp] = grp[0]
+    uniq, red = np.unique(label, return_inverse=True)
+    P = sp.csr_matrix((np.ones(n), (np.arange(n), red)), shape=(n, uniq.size))
+    A = sp.csr_matrix(P.T @ Lm @ P)
+    b = P.T @ np.asarray(b_ext, float)
+    fixed_r = red[np.asarray(fixed, np.intp)]
+    A_bc, b_bc = apply_dirichlet(A, b, fixed_r, np.asarray(values, float))
+    x = spla.spsolve(A_bc.tocsc(), b_bc)
+    return P @ x, Lm

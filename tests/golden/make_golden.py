@@ -293,17 +293,19 @@ def rlgc_fixture():
     nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
     xn, yn = g.xn, g.yn
 
+    tol = 1e-12  # node coordinates carry round-off (linspace)
+
     def box(x0, x1, y0, y1):
-        i = np.flatnonzero((xn >= x0) & (xn <= x1))
-        j = np.flatnonzero((yn >= y0) & (yn <= y1))
+        i = np.flatnonzero((xn >= x0 - tol) & (xn <= x1 + tol))
+        j = np.flatnonzero((yn >= y0 - tol) & (yn <= y1 + tol))
         return nid[i[0]:i[-1] + 1, j[0]:j[-1] + 1, :].ravel()
     # copper exactly on the cells between each line's electrode nodes: a
     # copper cell touching a free node would carry the substrate current
     # through a 5.8e7 S/m edge, a difference of nearly equal potentials that
     # no solver resolves beyond ~1e-5 relative
     for x0, x1 in ((12e-6, 17e-6), (22e-6, 27e-6)):
-        i = np.flatnonzero((xn >= x0) & (xn <= x1))
-        j = np.flatnonzero((yn >= 10e-6) & (yn <= 12e-6))
+        i = np.flatnonzero((xn >= x0 - tol) & (xn <= x1 + tol))
+        j = np.flatnonzero((yn >= 10e-6 - tol) & (yn <= 12e-6 + tol))
         sig[i[0]:i[-1], j[0]:j[-1], :] = 5.8e7
     terms = [Terminal("s1", box(12e-6, 17e-6, 10e-6, 12e-6)),
              Terminal("s2", box(22e-6, 27e-6, 10e-6, 12e-6)),
@@ -318,6 +320,80 @@ def rlgc_fixture():
             out[f"{tag}_{k}"] = np.asarray(r[k])
         out[f"{tag}_reference"] = np.array(r["reference"])
     np.savez_compressed(HERE / "rlgc.npz", **out)
+
+
+def ac_fixture():
+    """solvers/ac.py:34-164: admittance matrices of a seeded three-terminal
+    structure (graded grid; a lossy dielectric eps' - j eps'' over doped
+    silicon, two copper pads) at four frequencies, the terminal currents of
+    ``solve`` with complex drive values, and the complex Schur complement of
+    the field region of ``field_region_fixture`` (``FieldRegion.stamp_ac``,
+    coupling.py:214-236) at 1 GHz."""
+    from fieldspice.circuit.coupling import FieldRegion
+    from fieldspice.solvers.ac import ACSolver
+    rng = np.random.default_rng(33)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 6e-6, 16)), np.sort(rng.uniform(0, 4e-6, 12)),
+                        np.linspace(0, 2e-6, 10))
+    eps = np.full(g.shape_cells, 3.9 * eps0, dtype=complex)
+    eps[:, :, 4:] = (4.2 - 0.08j) * eps0           # lossy dielectric (tan d ~ 0.02)
+    sig = np.zeros(g.shape_cells)
+    sig[:, :, :3] = 10.0                            # doped silicon
+    eps[:, :, :3] = 11.7 * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(2, 2, 6, 5, 5, 7), (9, 6, 6, 13, 9, 8), (0, 0, 0, 15, 11, 0)]
+    terms = [Terminal(f"t{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(boxes)]
+    # the pads are electrodes: no copper conductivity inside them, whose
+    # 5.8e7 S/m edges would carry the LU's round-off on the fixed rows
+    # (|phi - v| ~ 1e-16) into the terminal currents at the 1e-5 level
+    freqs = np.array([1e3, 1e6, 1e9, 1e11])
+    ac = ACSolver(g, eps, sig)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "sigma": sig,
+           "boxes": np.asarray(boxes), "freqs": freqs}
+    out["Y"] = ac.admittance_matrix(terms, freqs)
+    drive = [Terminal("t0", terms[0].nodes, voltage=1.0),
+             Terminal("t1", terms[1].nodes, voltage=0.5),
+             Terminal("t2", terms[2].nodes, voltage=0.0)]
+    r = ac.solve(drive, freqs[1:])
+    out["solve_i"] = np.array([r.terminals[t.name]["i"] for t in drive])
+    out["solve_v"] = np.array([r.terminals[t.name]["v"] for t in drive])
+    # the field region of field_region_fixture, small-signal at 1 GHz
+    g2, eps2, sig2, boxes2, nid2 = field_region_geometry()
+    t2 = [Terminal(f"e{i}", nid2[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+          for i, (a0, b0, c0, a1, b1, c1) in enumerate(boxes2)]
+    fr = FieldRegion("FR", g2, eps2, sig2, t2, circuit_nodes=["0", "a", "b"])
+    Ym = np.zeros((2, 2), dtype=complex)
+    fr.stamp_ac(Ym, np.zeros(2, dtype=complex), None, 2 * np.pi * 1e9, {"a": 0, "b": 1})
+    out["fr_stamp_ac"] = Ym
+    np.savez_compressed(HERE / "ac.npz", **out)
+
+
+def floating_fixture():
+    """poisson.py:967-1063 with the node-merging reduction (:665-719): a
+    grounded-bottom layered box with a driven electrode, a floating conductor
+    and a charge-driven conductor, plus free charge; potential, terminal
+    voltages and charges."""
+    rng = np.random.default_rng(41)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 3e-6, 14)), np.linspace(0, 2e-6, 11),
+                        np.linspace(0, 1.5e-6, 9))
+    eps = np.full(g.shape_cells, 3.9 * eps0)
+    eps[:, :, :3] = 7.0 * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(2, 2, 4, 4, 4, 5), (7, 3, 3, 9, 6, 5), (10, 6, 5, 12, 8, 6)]
+    nodes = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in boxes]
+    terms = [Terminal("drv", nodes[0], voltage=1.0), Terminal("flt", nodes[1]),
+             Terminal("chg", nodes[2], current=2e-17)]
+    rho = np.zeros(g.shape_nodes)
+    rho[5, 5, 6] = 1e3
+    bc = BoundarySpec(zlo=Dirichlet(0.0))
+    ps = PoissonSolver(g, eps, SolverConfig(linear_solver="direct", tol=1e-12))
+    r = ps.solve(terms, bc, rho_node=rho)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "boxes": np.asarray(boxes),
+           "rho": rho, "phi": r.fields["phi"][0].ravel()}
+    for t in terms:
+        out[f"v_{t.name}"] = r.terminals[t.name]["v"]
+        out[f"q_{t.name}"] = r.terminals[t.name]["q"]
+    np.savez_compressed(HERE / "floating.npz", **out)
 
 
 def rc_stack(n=60):
@@ -415,6 +491,8 @@ FIXTURES = {
     "thermal": thermal_fixture,
     "field_region": field_region_fixture,
     "rlgc": rlgc_fixture,
+    "ac": ac_fixture,
+    "floating": floating_fixture,
 }
 
 if __name__ == "__main__":

@@ -1,0 +1,133 @@
+"""GPU harmonic EQS solve (``solvers/ac.py``) against the reference (needs a B200).
+
+* Admittance matrices of a seeded three-terminal structure (graded grid,
+  lossy dielectric ``eps' - j eps''`` over doped silicon) at four
+  frequencies, a complex-driven ``solve`` and the field region's
+  frequency-domain stamp, recorded from the reference in
+  ``tests/golden/ac.npz`` (the reference factorises ``K`` with a sparse LU;
+  here conjugate-orthogonal CG with the multigrid V-cycle of ``|A| + |B|``).
+* The closed forms of the reference's tests (``tests/test_quasistatic.py``):
+  a lossy slab's admittance is ``G + j w C``, the admittance is reciprocal,
+  and its dc limit is the resistive solve.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+EPS0 = 8.8541878188e-12
+
+
+def _structure(d):
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import Terminal
+    g = RectilinearGrid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [Terminal(f"t{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(d["boxes"])]
+    return g, terms
+
+
+@pytest.mark.parametrize("preconditioner", ["mg", "jacobi"])
+def test_ac_admittance_matches_reference(cuda, golden, preconditioner):
+    from fieldspice_b200.solvers.ac import ACSolver
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
+    d = golden("ac")
+    g, terms = _structure(d)
+    ac = ACSolver(g, d["eps"], d["sigma"], SolverConfig(tol=1e-12),
+                  gpu=GPUConfig(preconditioner=preconditioner))
+    Y = ac.admittance_matrix(terms, d["freqs"])
+    for k in range(d["freqs"].size):
+        want = d["Y"][k]
+        assert np.abs(Y[k] - want).max() <= 1e-9 * np.abs(want).max(), k
+    if preconditioner == "mg":
+        # the multigrid-preconditioned COCG needs a few tens of iterations
+        its = [s["iterations"] for st in ac.last_stats for s in st]
+        assert max(its) <= 80, its
+
+
+def test_ac_solve_matches_reference(cuda, golden):
+    from fieldspice_b200.solvers.ac import ACSolver
+    from fieldspice_b200.solvers.base import SolverConfig, Terminal
+    d = golden("ac")
+    g, terms = _structure(d)
+    drive = [Terminal(t.name, t.nodes, voltage=v) for t, v in zip(terms, (1.0, 0.5, 0.0))]
+    r = ACSolver(g, d["eps"], d["sigma"], SolverConfig(tol=1e-12)).solve(drive, d["freqs"][1:])
+    for j, t in enumerate(drive):
+        want = d["solve_i"][j]
+        assert np.abs(r.i(t.name) - want).max() <= 1e-9 * np.abs(d["solve_i"]).max()
+        assert np.allclose(r.v(t.name), d["solve_v"][j], rtol=0, atol=1e-15)
+
+
+def test_field_region_stamp_ac_matches_reference(cuda, golden):
+    from fieldspice_b200.circuit import FieldRegion
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import SolverConfig, Terminal
+    f = golden("field_region")
+    g = RectilinearGrid(f["x"], f["y"], f["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [Terminal(f"e{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(f["boxes"])]
+    fr = FieldRegion("FR", g, f["eps"], f["sigma"], terms, circuit_nodes=["0", "a", "b"],
+                     config=SolverConfig(tol=1e-12))
+    Ym = np.zeros((2, 2), dtype=complex)
+    fr.stamp_ac(Ym, np.zeros(2, dtype=complex), None, 2 * np.pi * 1e9, {"a": 0, "b": 1})
+    want = golden("ac")["fr_stamp_ac"]
+    assert np.abs(Ym - want).max() <= 1e-9 * np.abs(want).max()
+
+
+def _lossy_slab():
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import Terminal
+    d, W, H, er, sigma = 2e-6, 5e-6, 4e-6, 3.9, 1e-2
+    g = RectilinearGrid(np.linspace(0, d, 16), np.linspace(0, W, 6), np.linspace(0, H, 5))
+    eps = np.full(g.shape_cells, er * EPS0)
+    sig = np.full(g.shape_cells, sigma)
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [Terminal("hi", nid[0].ravel()), Terminal("lo", nid[-1].ravel())]
+    return g, eps, sig, terms, er * EPS0 * W * H / d, sigma * W * H / d
+
+
+@pytest.mark.parametrize("freq", [1e3, 1e6, 1e9, 1e12])
+def test_ac_admittance_is_g_plus_jwc(cuda, freq):
+    from fieldspice_b200.solvers.ac import ACSolver
+    g, eps, sig, terms, C, G = _lossy_slab()
+    Y = ACSolver(g, eps, sig).admittance_matrix(terms, [freq])
+    assert Y[0, 0, 0] == pytest.approx(G + 2j * np.pi * freq * C, rel=1e-9)
+
+
+def test_ac_admittance_is_reciprocal(cuda):
+    from fieldspice_b200.solvers.ac import ACSolver
+    from fieldspice_b200.solvers.base import SolverConfig
+    g, eps, sig, terms, _, _ = _lossy_slab()
+    Y = ACSolver(g, eps, sig, SolverConfig(tol=1e-13)).admittance_matrix(terms, [1e9])
+    assert abs(Y[0, 0, 1] - Y[0, 1, 0]) < 1e-12 * abs(Y[0, 0, 0])
+
+
+def test_ac_dc_limit_matches_resistive_solve(cuda):
+    from fieldspice_b200.solvers.ac import ACSolver
+    g, eps, sig, terms, _, G = _lossy_slab()
+    Y = ACSolver(g, eps, sig).admittance_matrix(terms, [0.0])
+    assert Y[0, 0, 0].real == pytest.approx(G, rel=1e-9)
+    assert abs(Y[0, 0, 0].imag) < 1e-20
+
+
+def test_ac_dispersive_permittivity_callable(cuda, golden):
+    """A callable eps(freq) (the A3 escape hatch, ac.py:41-45) gives the same
+    matrix as the array at that frequency."""
+    from fieldspice_b200.solvers.ac import ACSolver
+    d = golden("ac")
+    g, terms = _structure(d)
+    eps = d["eps"]
+    Y1 = ACSolver(g, lambda f: eps, d["sigma"]).admittance_matrix(terms, d["freqs"][2:3])
+    assert np.abs(Y1[0] - d["Y"][2]).max() <= 1e-9 * np.abs(d["Y"][2]).max()
+
+
+def test_ac_rejects_bad_input(cuda):
+    from fieldspice_b200.solvers.ac import ACSolver
+    g, eps, sig, terms, _, _ = _lossy_slab()
+    with pytest.raises(ValueError, match="shape"):
+        ACSolver(g, eps[:-1], sig)
+    with pytest.raises(ValueError, match="non-negative"):
+        ACSolver(g, eps, -sig)

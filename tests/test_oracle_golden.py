@@ -212,3 +212,48 @@ def test_rlgc_matrices_match_reference(golden):
         for k in ("C", "C_air", "G", "L"):
             want = d[f"{tag}_{k}"]
             assert np.abs(got[k] - want).max() <= 1e-10 * np.abs(want).max(), (tag, k)
+
+
+def test_ac_matches_reference(golden):
+    """solvers/ac.py: admittance matrices of a lossy three-terminal structure
+    at four frequencies, the currents of a complex-driven solve, and the
+    field region's frequency-domain stamp (coupling.py:214-236)."""
+    d = golden("ac")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    Y = O.ac_admittance(g, d["eps"], d["sigma"], terms, d["freqs"])
+    for k in range(d["freqs"].size):
+        assert np.abs(Y[k] - d["Y"][k]).max() <= 1e-9 * np.abs(d["Y"][k]).max(), k
+    # a driven solve is Y times the drive vector
+    v = np.array([1.0, 0.5, 0.0])
+    for k in range(1, d["freqs"].size):
+        want = d["solve_i"][:, k - 1]
+        assert np.abs(Y[k] @ v - want).max() <= 1e-9 * np.abs(want).max()
+    f = golden("field_region")
+    g2 = O.Grid(f["x"], f["y"], f["z"])
+    t2 = field_region_terminals(f, g2)
+    Ys = O.ac_schur(g2, f["eps"], f["sigma"], t2, 2 * np.pi * 1e9)
+    want = d["fr_stamp_ac"]
+    assert np.abs(Ys[1:, 1:] - want).max() <= 1e-9 * np.abs(want).max()
+
+
+def test_floating_electrodes_match_reference(golden):
+    """poisson.py: a floating and a charge-driven conductor merged into single
+    unknowns next to a driven electrode, a grounded floor and free charge."""
+    d = golden("floating")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    nodes = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    wall = nid[:, :, 0].ravel()
+    fixed = np.concatenate([wall, nodes[0]])
+    vals = np.concatenate([np.zeros(wall.size), np.ones(nodes[0].size)])
+    b_free = d["rho"].ravel() * g.node_volumes().ravel()
+    b_ext = b_free.copy()
+    b_ext[nodes[2][0]] += 2e-17
+    phi, Lm = O.merged_potential(g, d["eps"], fixed, vals, [nodes[1], nodes[2]], b_ext)
+    assert np.abs(phi - d["phi"]).max() <= 1e-10
+    q = Lm @ phi - b_free
+    for name, nd in zip(("drv", "flt", "chg"), nodes):
+        assert abs(q[nd].sum() - d[f"q_{name}"][0]) <= 1e-9 * abs(d["q_drv"][0])
+        assert abs(phi[nd[0]] - d[f"v_{name}"][0]) <= 1e-10
