@@ -19,6 +19,24 @@ pytestmark = pytest.mark.gpu
 EPS0 = 8.8541878188e-12
 
 
+def _floor(d, terms, freq):
+    """Round-off floor of the charge integration per terminal row: the
+    terminal's node currents sum edge currents ``m_e (phi_n - phi_nbr)``; where
+    a highly conducting region sits on the electrode (silicon at 1 kHz is
+    1e7 times more conducting than the dielectric is capacitive) the
+    potential difference is a few ulps of ``phi`` and FP64 round-off in phi
+    (the LU's or the iteration's) reaches the current as ``eps * sum |m_e|``."""
+    from oracle import fs_oracle as O
+    g = O.Grid(d["x"], d["y"], d["z"])
+    K = O.ac_system(g, d["eps"], d["sigma"], freq)
+    rowsum = np.asarray(abs(K).sum(axis=1)).ravel()
+    return np.array([64 * 2.2e-16 * rowsum[t.nodes].sum() for t in terms])
+
+
+def _close(Y, want, floor):
+    return np.all(np.abs(Y - want) <= 1e-9 * np.abs(want).max() + floor[:, None])
+
+
 def _structure(d):
     from fieldspice_b200.grid import RectilinearGrid
     from fieldspice_b200.solvers.base import Terminal
@@ -38,9 +56,8 @@ def test_ac_admittance_matches_reference(cuda, golden, preconditioner):
     ac = ACSolver(g, d["eps"], d["sigma"], SolverConfig(tol=1e-12),
                   gpu=GPUConfig(preconditioner=preconditioner))
     Y = ac.admittance_matrix(terms, d["freqs"])
-    for k in range(d["freqs"].size):
-        want = d["Y"][k]
-        assert np.abs(Y[k] - want).max() <= 1e-9 * np.abs(want).max(), k
+    for k, f in enumerate(d["freqs"]):
+        assert _close(Y[k], d["Y"][k], _floor(d, terms, f)), k
     if preconditioner == "mg":
         # the multigrid-preconditioned COCG needs a few tens of iterations
         its = [s["iterations"] for st in ac.last_stats for s in st]
@@ -54,9 +71,12 @@ def test_ac_solve_matches_reference(cuda, golden):
     g, terms = _structure(d)
     drive = [Terminal(t.name, t.nodes, voltage=v) for t, v in zip(terms, (1.0, 0.5, 0.0))]
     r = ACSolver(g, d["eps"], d["sigma"], SolverConfig(tol=1e-12)).solve(drive, d["freqs"][1:])
+    for k, f in enumerate(d["freqs"][1:]):
+        fl = _floor(d, terms, f)
+        got = np.array([r.i(t.name)[k] for t in drive])
+        want = d["solve_i"][:, k]
+        assert np.all(np.abs(got - want) <= 1e-9 * np.abs(want).max() + fl), k
     for j, t in enumerate(drive):
-        want = d["solve_i"][j]
-        assert np.abs(r.i(t.name) - want).max() <= 1e-9 * np.abs(d["solve_i"]).max()
         assert np.allclose(r.v(t.name), d["solve_v"][j], rtol=0, atol=1e-15)
 
 
@@ -119,9 +139,11 @@ def test_ac_dispersive_permittivity_callable(cuda, golden):
     from fieldspice_b200.solvers.ac import ACSolver
     d = golden("ac")
     g, terms = _structure(d)
+    from fieldspice_b200.solvers.base import SolverConfig
     eps = d["eps"]
-    Y1 = ACSolver(g, lambda f: eps, d["sigma"]).admittance_matrix(terms, d["freqs"][2:3])
-    assert np.abs(Y1[0] - d["Y"][2]).max() <= 1e-9 * np.abs(d["Y"][2]).max()
+    Y1 = ACSolver(g, lambda f: eps, d["sigma"], SolverConfig(tol=1e-12)).admittance_matrix(
+        terms, d["freqs"][2:3])
+    assert _close(Y1[0], d["Y"][2], _floor(d, terms, d["freqs"][2]))
 
 
 def test_ac_rejects_bad_input(cuda):
