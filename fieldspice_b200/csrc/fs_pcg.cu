@@ -87,6 +87,7 @@ struct Control {
   int flexible; // 1: nonlinear preconditioner (flexible CG): restart at updates
   unsigned int tickets[kTickets];
   unsigned int pad[2];
+  unsigned long long label_counts[4];  // free, fixed, solo, pinned nodes (level 0)
 };
 
 __device__ void refresh_done(RhsState* st, Control* ctl, int nrhs) {
@@ -114,7 +115,11 @@ __global__ void k_classify(Dims d, const double* __restrict__ mx,
                            const double* __restrict__ dgn,
                            const uint8_t* __restrict__ label_in,
                            uint8_t* __restrict__ label,
-                           double* __restrict__ s64) {
+                           double* __restrict__ s64,
+                           unsigned long long* __restrict__ counts) {
+  __shared__ unsigned int cnt[4];
+  if (threadIdx.x < 4) cnt[threadIdx.x] = 0u;
+  __syncthreads();
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     uint8_t lab = label_in[n] == FS_LABEL_FREE ? FS_LABEL_FREE : FS_LABEL_FIXED;
@@ -145,6 +150,12 @@ __global__ void k_classify(Dims d, const double* __restrict__ mx,
     }
     label[n] = lab;
     s64[n] = s;
+    if (counts) atomicAdd(&cnt[lab], 1u);
+  }
+  if (counts) {  // per-block counts, one global add per label
+    __syncthreads();
+    if (threadIdx.x < 4 && cnt[threadIdx.x])
+      atomicAdd(&counts[threadIdx.x], (unsigned long long)cnt[threadIdx.x]);
   }
 }
 
@@ -1487,7 +1498,7 @@ struct Impl {
       g = fs_grid_blocks((const void*)k_classify, c.d.N);
       k_classify<<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
                                           P->dg ? c.d64 : nullptr, c.label_in, c.label,
-                                          c.s64);
+                                          c.s64, nullptr);
       g = fs_grid_blocks((const void*)k_eq_masses<T>, c.d.N);
       k_eq_masses<T><<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
                                               c.s64, (T*)c.em[0], (T*)c.em[1],
@@ -1886,7 +1897,7 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
     return fail("memset state", e);
   int g = fs_grid_blocks((const void*)k_classify, P->d.N);
   k_classify<<<g, fs::kBlock, 0, s>>>(P->d, mx, my, mz, P->dg, label_in, P->label,
-                                      P->s64);
+                                      P->s64, P->ctl->label_counts);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail("k_classify", e);
   dispatch(P, 1, s);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail("k_eq_masses", e);
@@ -2134,6 +2145,16 @@ int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, cons
   }
 #undef FS_EQ
   FS_CHECK_LAUNCH("k_eq_apply");
+  return FS_OK;
+}
+
+int fs_pcg_plan_label_counts(const fs_pcg_plan* P, long long* counts, void* stream) {
+  if (!P || !counts) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned long long h[4];
+  FS_CHECK(cudaMemcpyAsync(h, P->ctl->label_counts, sizeof(h), cudaMemcpyDeviceToHost, s));
+  FS_CHECK(cudaStreamSynchronize(s));
+  for (int t = 0; t < 4; ++t) counts[t] = (long long)h[t];
   return FS_OK;
 }
 

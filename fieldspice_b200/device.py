@@ -263,8 +263,10 @@ class EliminatedSystem:
         lab_ptr = lib.fs_pcg_plan_labels(self._plan)
         off = lab_ptr - self.workspace.data_ptr()
         self.labels = self.workspace[off:off + N]
-        counts = torch.bincount(self.labels.to(torch.int64), minlength=4).cpu().numpy()
-        self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts[:4])
+        counts = (ctypes.c_longlong * 4)()
+        L.check("fs_pcg_plan_label_counts",
+                lib.fs_pcg_plan_label_counts(self._plan, counts, L.stream_ptr()))
+        self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts)
         self._net_ws = None
         self.learned_level = None
         self.learned_fallback = False

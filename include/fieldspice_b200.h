@@ -359,6 +359,9 @@ int fs_rhs_superpose(const double* phi, int k, int c0, int ncols,
  * (FS_LABEL_*: free, fixed, solo, pinned).                                   */
 int fs_pcg_plan_precondition(fs_pcg_plan* plan, const void* r, void* z, void* stream);
 int fs_pcg_plan_scale(const fs_pcg_plan* plan, const double** s64, const uint8_t** label);
+/* counts[4] (host): the plan's free, fixed, solo and pinned node counts, as
+ * classified at creation (LinearSystem's split, poisson.py:282-362).       */
+int fs_pcg_plan_label_counts(const fs_pcg_plan* plan, long long* counts, void* stream);
 
 /* ---- §8f-4: harmonic EQS, the complex-symmetric solve -------------------------
  * Replaces the per-frequency sparse LU of fieldspice/solvers/ac.py:95-145

@@ -426,8 +426,16 @@ class LinearSystemCPU:
 # Capacitance extraction -- poisson.py:1100-1249
 # ---------------------------------------------------------------------------
 def capacitance_matrix(g: Grid, eps_cell, terminals, dirichlet_walls=None,
-                       method="cg", tol=1e-10, symmetrise=True, mode="parallel"):
+                       method="cg", tol=1e-10, symmetrise=True, mode="parallel",
+                       charge="csr"):
     """Maxwell C by unit excitation; returns (C, report).
+
+    ``charge="csr"`` integrates ``L @ phi`` with the assembled matrix, as the
+    reference (poisson.py:1219-1224); ``charge="edges"`` evaluates the same
+    ``G^T (m * G phi)`` edge by edge, which avoids the cancellation of the
+    CSR diagonal against its off-diagonals on electrodes that carry very
+    large masses (a copper conductor inside an electrode: ``d ~ 1e8`` and the
+    round-off of ``d - sum m`` reaches the charge at ~1e-8).
 
     ``terminals``: list of node-index arrays.  ``dirichlet_walls``: {wall:
     value} (values are ignored, every Dirichlet wall is a grounded shield).
@@ -455,7 +463,11 @@ def capacitance_matrix(g: Grid, eps_cell, terminals, dirichlet_walls=None,
         phis.append(phi)
         iters.append(ls.info["iterations"])
         relres.append(ls.info["relres"])
-        q = Lmat @ phi
+        if charge == "edges":
+            Gm = grad_node_edge(g)
+            q = Gm.T @ (m * (Gm @ phi))
+        else:
+            q = Lmat @ phi
         for i, ti in enumerate(terms):
             C[i, j] = float(q[ti].sum())
         if shield.size:
@@ -759,7 +771,7 @@ class FieldRegionCPU:
 # Per-unit-length line parameters -- extraction.py:108-206
 # ---------------------------------------------------------------------------
 def rlgc_2d_matrices(g: Grid, eps_cell, sigma_cell, terminals, reference=-1,
-                     method="direct", tol=1e-12):
+                     method="direct", tol=1e-12, charge="csr"):
     """``C``, ``C_air``, ``G`` and ``L`` of a 2-D cross-section referenced to
     conductor ``reference`` (an index), as ``extraction.py:168-199``: three
     capacitance extractions (real permittivity, vacuum, conductivity floored
@@ -773,7 +785,7 @@ def rlgc_2d_matrices(g: Grid, eps_cell, sigma_cell, terminals, reference=-1,
     mu0 = 4e-7 * math.pi * 1.0000000000552
 
     def cap(prop):
-        C, _ = capacitance_matrix(g, prop, terminals, method=method, tol=tol)
+        C, _ = capacitance_matrix(g, prop, terminals, method=method, tol=tol, charge=charge)
         return C[np.ix_(keep, keep)]
     C = cap(eps_cell)
     C_air = cap(np.full_like(eps_cell, EPS0))
