@@ -35,6 +35,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1217,6 +1218,38 @@ bool valid_nrhs(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16;
 
 }  // namespace
 
+// Page-locked host slots for a plan's completion flag and per-RHS stats,
+// pinned once per process and reused: creating and destroying a plan per
+// extraction then makes no cudaMallocHost / cudaFreeHost call (the latter
+// synchronises the whole device).  Slots are kept until the process exits.
+struct HostSlot {
+  int flag;
+  int pad[3];
+  RhsState st[fs::kMaxRhs];
+};
+
+namespace {
+std::mutex g_slot_mu;
+std::vector<HostSlot*> g_slot_free;
+
+cudaError_t host_slot_get(HostSlot** out) {
+  {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    if (!g_slot_free.empty()) {
+      *out = g_slot_free.back();
+      g_slot_free.pop_back();
+      return cudaSuccess;
+    }
+  }
+  return cudaMallocHost((void**)out, sizeof(HostSlot));
+}
+
+void host_slot_put(HostSlot* slot) {
+  std::lock_guard<std::mutex> lk(g_slot_mu);
+  g_slot_free.push_back(slot);
+}
+}  // namespace
+
 struct fs_pcg_plan {
   Dims d;
   int nrhs, precision, precond;
@@ -1244,8 +1277,9 @@ struct fs_pcg_plan {
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
-  int* h_flag;
-  RhsState* h_st;
+  HostSlot* slot = nullptr;  // page-locked flag and stats (h_flag, h_st point in)
+  int* h_flag = nullptr;
+  RhsState* h_st = nullptr;
   long long launches;
   // Event samples around the kernels of the first iteration of every graph
   // launch: live per-kernel durations for the roofline figures.
@@ -1912,11 +1946,9 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
     dispatch(P, 9, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail("multigrid setup", e);
   }
-  if ((e = cudaMallocHost((void**)&P->h_flag, sizeof(int))) != cudaSuccess)
-    return fail("cudaMallocHost", e);
-  if ((e = cudaMallocHost((void**)&P->h_st, sizeof(RhsState) * fs::kMaxRhs)) !=
-      cudaSuccess)
-    return fail("cudaMallocHost", e);
+  if ((e = host_slot_get(&P->slot)) != cudaSuccess) return fail("cudaMallocHost", e);
+  P->h_flag = &P->slot->flag;
+  P->h_st = P->slot->st;
 
   // Capture `chunk` CG iterations once; the graph is replayed until the
   // device reports that every RHS has finished.
@@ -2295,8 +2327,7 @@ int fs_pcg_plan_destroy(fs_pcg_plan* P) {
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->cap) cudaStreamDestroy(P->cap);
-  if (P->h_flag) cudaFreeHost(P->h_flag);
-  if (P->h_st) cudaFreeHost(P->h_st);
+  if (P->slot) host_slot_put(P->slot);
   delete P;
   return FS_OK;
 }

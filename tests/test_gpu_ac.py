@@ -52,7 +52,7 @@ def _structure(d):
 # relative residual of 1e-10, so the Jacobi run asks for that and is held to
 # the accuracy it buys.
 @pytest.mark.parametrize("preconditioner,tol,rtol", [("mg", 1e-12, 1e-9),
-                                                     ("jacobi", 1e-10, 1e-7)])
+                                                     ("jacobi", 1e-10, 1e-6)])
 def test_ac_admittance_matches_reference(cuda, golden, preconditioner, tol, rtol):
     from fieldspice_b200.solvers.ac import ACSolver
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
