@@ -354,6 +354,23 @@ __device__ __forceinline__ void ld_smem(const T* p, T (&v)[K]) {
   }
 }
 
+template <typename T, int K>
+__device__ __forceinline__ void st_smem(T* p, const T (&v)[K]) {
+  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c)
+      reinterpret_cast<float4*>(p)[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2],
+                                                    v[4 * c + 3]);
+  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+#pragma unroll
+    for (int c = 0; c < K / 2; ++c)
+      reinterpret_cast<double2*>(p)[c] = make_double2(v[2 * c], v[2 * c + 1]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < K; ++c) p[c] = v[c];
+  }
+}
+
 template <typename T, int K, int NT>
 __device__ void finish_pq(double (&acc)[K], double* partials, RhsState* st,
                           Control* ctl) {
@@ -683,6 +700,185 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
     __syncthreads();
   }
   finish_pq<T, K, TmaTileM<T, K>::THREADS>(acc, partials, st, ctl);
+}
+
+// ---- K1 variant: q written through shared memory by TMA stores -------------------
+// The same computation as k_stencil_tma_m (p and the three mass tiles staged by
+// TMA, one thread per node of a TZ x TY column marching along x), but each
+// plane's q tile goes to shared memory and leaves with one bulk tensor store
+// instead of two 16-byte global stores per thread.  Two q buffers alternate;
+// the store of a buffer must have finished reading it before the buffer is
+// written again two planes later (bulk_group read wait by the issuing thread,
+// then the CTA barrier).  Four p stages keep three CTAs per SM resident.
+template <typename T, int K>
+struct TmaTileS {
+  using M = TmaTileM<T, K>;
+  static constexpr int B = M::B, TZ = M::TZ, TY = M::TY, HY = M::HY, HZ = M::HZ, ZP = M::ZP;
+  static constexpr int NS = 4;
+  static constexpr int SLOT = M::SLOT, O_EX = M::O_EX, O_EY = M::O_EY, O_EZ = M::O_EZ;
+  static constexpr uint32_t TX = M::TX;
+  static constexpr int QB = TZ * TY * B;  // one q tile, [TY][TZ][K]
+  static constexpr int O_Q = NS * SLOT;
+  static constexpr int THREADS = M::THREADS;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + 2 * (size_t)QB + NS * 8 + 128;
+  static constexpr bool OK = M::OK;
+};
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int c0,
+                                             int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+          (uint64_t)map),
+      "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(fs::smem_u32(src))
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// at most one committed store group may still be reading shared memory
+__device__ __forceinline__ void bulk_wait_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <= 32 ? 3 : 1))
+    k_stencil_tma_s(Dims d, const __grid_constant__ CUtensorMap tm_p,
+                    const __grid_constant__ CUtensorMap tm_ex,
+                    const __grid_constant__ CUtensorMap tm_ey,
+                    const __grid_constant__ CUtensorMap tm_ez,
+                    const __grid_constant__ CUtensorMap tm_q,
+                    double* __restrict__ partials, RhsState* st, Control* ctl) {
+  using C = TmaTileS<T, K>;
+  if (ctl->all_done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::O_Q + 2 * C::QB);
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const long long total = (long long)nbz * nby * d.nx;
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  long long u = (long long)blockIdx.x * per;
+  const long long u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  long long ticket = 0, qc = 0;
+  bool failed = false;
+  while (u < u_end && !failed) {
+    const long long col = u / d.nx;
+    const int xa = (int)(u % d.nx);
+    const int xb = (int)min((long long)d.nx, xa + (u_end - u));
+    const int bz = (int)(col % nbz), by = (int)(col / nbz);
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nplanes = (xb - xa) + 2;  // planes xa-1 .. xb
+    auto issue = [&](int j) {
+      const int s = (int)((ticket + j) % C::NS);
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 1 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_p, &bar[s], 0, z0 - 1, y0 - 1, x);
+      tma_load_3d(slot + C::O_EX, &tm_ex, &bar[s], z0, y0, x);
+      tma_load_3d(slot + C::O_EY, &tm_ey, &bar[s], z0, y0 - 1, x);
+      tma_load_3d(slot + C::O_EZ, &tm_ez, &bar[s], z0 - C::ZP, y0, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
+    for (int j = 0; j < nplanes; ++j) {
+      const long long tk = ticket + j;
+      const int s = (int)(tk % C::NS);
+      // the q buffer written this plane was last stored two planes ago
+      if (tid == 0 && j >= 2) bulk_wait_read_1();
+      const bool ok = fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      if (j >= 2) {
+        const int x = xa - 2 + j;
+        T* qt = reinterpret_cast<T*>(base + C::O_Q + (int)(qc & 1) * C::QB);
+        if (inb) {
+          const unsigned char* sm = base + (int)((tk - 2) % C::NS) * C::SLOT;  // plane x-1
+          const unsigned char* sc = base + (int)((tk - 1) % C::NS) * C::SLOT;  // plane x
+          const unsigned char* sp = base + s * C::SLOT;                        // plane x+1
+          const T* pm = reinterpret_cast<const T*>(sm);
+          const T* pc = reinterpret_cast<const T*>(sc);
+          const T* pp = reinterpret_cast<const T*>(sp);
+          const T* exm = reinterpret_cast<const T*>(sm + C::O_EX);
+          const T* exc = reinterpret_cast<const T*>(sc + C::O_EX);
+          const T* eyc = reinterpret_cast<const T*>(sc + C::O_EY);
+          const T* ezc = reinterpret_cast<const T*>(sc + C::O_EZ);
+          const T mxm = exm[ty * C::TZ + tz], mxp = exc[ty * C::TZ + tz];
+          const T mym = eyc[ty * C::TZ + tz], myp = eyc[(ty + 1) * C::TZ + tz];
+          const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
+          const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
+          T c[K], v[K], qv[K];
+          ld_smem<T, K>(pc + cpos * K, c);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] = c[t];
+          ld_smem<T, K>(pm + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
+          ld_smem<T, K>(pp + cpos * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
+          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
+          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            qv[t] -= mzp * v[t];
+            acc[t] += (double)c[t] * (double)qv[t];
+          }
+          st_smem<T, K>(qt + (ty * C::TZ + tz) * K, qv);
+        }
+        fence_proxy_async_smem();  // q tile writes -> visible to the bulk store
+        __syncthreads();           // plane j-2 no longer read; q tile complete
+        if (tid == 0) {
+          tma_store_4d(&tm_q, qt, 0, z0, y0, x);  // out-of-range rows are clipped
+          bulk_commit();
+          if (j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
+        }
+        ++qc;
+      }
+    }
+    ticket += nplanes;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      ctl->error = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) bulk_wait_all();  // q written out before the CTA's shared memory goes
+  finish_pq<T, K, TmaTileS<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
 // ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
@@ -1273,7 +1469,9 @@ struct fs_pcg_plan {
   int use_tma;
   CUtensorMap tm_p[2];
   CUtensorMap tm_m[3];     // ex, ey, ez tiles of the mass-staging stencil
-  int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses
+  CUtensorMap tm_q;        // q tiles of the TMA-store stencil
+  int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses,
+                           // 3: as 2 with q written by TMA stores
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -1339,10 +1537,28 @@ struct Impl {
         P->stencil_kind = 0;
       else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0))
         P->stencil_kind = 1;
+      else if (sel && strcmp(sel, "tmas") == 0)
+        P->stencil_kind = 3;
       else
         P->stencil_kind = 2;
     }
-    if (P->stencil_kind == 2) {
+    if (P->stencil_kind == 3) {
+      using CS = TmaTileS<T, K>;
+      cudaFuncSetAttribute(k_stencil_tma_s<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)CS::SMEM);
+      int per_sm = 0, dev = 0, sms = 148;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_tma_s<T, K>,
+                                                        CS::THREADS, CS::SMEM) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long cols = (long long)((P->d.nz + CS::TZ - 1) / CS::TZ) *
+                             ((P->d.ny + CS::TY - 1) / CS::TY) * P->d.nx;
+      long long g = (long long)sms * per_sm;
+      if (g > cols) g = cols;
+      P->g_apply = (int)g;
+    } else if (P->stencil_kind == 2) {
       using CM = TmaTileM<T, K>;
       cudaFuncSetAttribute(k_stencil_tma_m<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)CM::SMEM);
@@ -1398,8 +1614,8 @@ struct Impl {
                           (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
     cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
     // the p box of the kernel that will run: its tile has its own halo height
-    const int hz = P->stencil_kind == 2 ? TmaTileM<T, K>::HZ : C::HZ;
-    const int hy = P->stencil_kind == 2 ? TmaTileM<T, K>::HY : C::HY;
+    const int hz = P->stencil_kind >= 2 ? TmaTileM<T, K>::HZ : C::HZ;
+    const int hy = P->stencil_kind >= 2 ? TmaTileM<T, K>::HY : C::HY;
     cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)hz, (cuuint32_t)hy, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
@@ -1416,7 +1632,19 @@ struct Impl {
         return FS_CUDA_ERROR;
       }
     }
-    if (P->stencil_kind == 2) {
+    if (P->stencil_kind == 3) {
+      using CS = TmaTileS<T, K>;
+      cuuint32_t qbox[4] = {(cuuint32_t)K, (cuuint32_t)CS::TZ, (cuuint32_t)CS::TY, 1};
+      CUresult rc = encode(&P->tm_q, dt, 4, P->q, dims, strides, qbox, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rc != CUDA_SUCCESS) {
+        fs_set_error_msg("cuTensorMapEncodeTiled rejected the q tensor map");
+        return FS_CUDA_ERROR;
+      }
+    }
+    if (P->stencil_kind >= 2) {
       using CM = TmaTileM<T, K>;
       const cuuint64_t MB = sizeof(T);
       cuuint64_t mdims[3] = {(cuuint64_t)P->d.nz, (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
@@ -1466,6 +1694,13 @@ struct Impl {
         break;
       case 1:
         if constexpr (TmaTile<T, K>::OK) {
+          if (P->stencil_kind == 3) {
+            using CS = TmaTileS<T, K>;
+            k_stencil_tma_s<T, K><<<P->g_apply, CS::THREADS, CS::SMEM, s>>>(
+                P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], P->tm_q,
+                P->partials, P->st, P->ctl);
+            break;
+          }
           if (P->stencil_kind == 2) {
             using CM = TmaTileM<T, K>;
             k_stencil_tma_m<T, K><<<P->g_apply, CM::THREADS, CM::SMEM, s>>>(

@@ -1,0 +1,52 @@
+"""Every CG stencil kernel gives the reference's capacitance (needs a B200).
+
+``FS_STENCIL`` selects the kernel of ``q = A~ p, p.q`` when a plan is built:
+``plain`` (cached loads), ``tma1`` (p staged by TMA), the default (p and the
+three mass tiles staged by TMA) and ``tmas`` (as the default, with q leaving
+through shared memory by TMA stores).  Each runs the 48x48x24 layered
+extraction recorded from the reference (8 right-hand sides) and, against the
+cached-load kernel, the extraction of the first four terminals (4 RHS).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(golden):
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import Terminal
+    d = golden("layered_48x48x24_s1")
+    g = RectilinearGrid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    terms = [Terminal(f"box{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(d["boxes"])]
+    return d, g, terms
+
+
+def _extract(g, eps, terms, precision):
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
+    from fieldspice_b200.solvers.poisson import PoissonSolver
+    ps = PoissonSolver(g, eps, SolverConfig(tol=1e-11),
+                       gpu=GPUConfig(precision=precision, preconditioner="mg"))
+    return ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)))
+
+
+@pytest.mark.parametrize("variant", ["plain", "tma1", "default", "tmas"])
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_stencil_variant_matches_reference(cuda, golden, monkeypatch, variant, precision):
+    d, g, terms = _problem(golden)
+    monkeypatch.setenv("FS_STENCIL", "plain")
+    C4_plain = _extract(g, d["eps_cell"], terms[:4], precision)
+    if variant == "default":
+        monkeypatch.delenv("FS_STENCIL", raising=False)
+    else:
+        monkeypatch.setenv("FS_STENCIL", variant)
+    ref = d["C"]
+    scale = np.abs(np.diag(ref)).max()
+    C = _extract(g, d["eps_cell"], terms, precision)
+    assert np.abs(C - ref).max() / scale <= 1e-9
+    C4 = _extract(g, d["eps_cell"], terms[:4], precision)
+    assert np.abs(C4 - C4_plain).max() / np.abs(np.diag(C4_plain)).max() <= 1e-9
