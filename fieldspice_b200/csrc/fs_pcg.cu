@@ -35,6 +35,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -1472,6 +1473,7 @@ struct fs_pcg_plan {
   CUtensorMap tm_q;        // q tiles of the TMA-store stencil
   int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses,
                            // 3: as 2 with q written by TMA stores
+  int autotune = 0;        // time kinds 2, 3, 0 at creation and keep the fastest
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -1523,25 +1525,39 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// Process-wide record of the fastest CG stencil kernel per (grid, RHS block,
+// precision), filled by the first plan of each shape (the stencil autotuner).
+struct StencilKey {
+  int nx, ny, nz, k, es;
+  bool operator<(const StencilKey& o) const {
+    if (nx != o.nx) return nx < o.nx;
+    if (ny != o.ny) return ny < o.ny;
+    if (nz != o.nz) return nz < o.nz;
+    if (k != o.k) return k < o.k;
+    return es < o.es;
+  }
+};
+std::mutex g_stencil_mu;
+std::map<StencilKey, int> g_stencil_choice;
+
+int stencil_choice_get(const Dims& d, int k, int es) {
+  std::lock_guard<std::mutex> lk(g_stencil_mu);
+  auto it = g_stencil_choice.find(StencilKey{d.nx, d.ny, d.nz, k, es});
+  return it == g_stencil_choice.end() ? -1 : it->second;
+}
+
+void stencil_choice_put(const Dims& d, int k, int es, int kind) {
+  std::lock_guard<std::mutex> lk(g_stencil_mu);
+  g_stencil_choice[StencilKey{d.nx, d.ny, d.nz, k, es}] = kind;
+}
+
 template <typename T, int K>
 struct Impl {
-  static void grids(fs_pcg_plan* P) {
+  // Launch grid of the selected CG stencil kernel (persistent TMA kernels:
+  // SMs x resident CTAs, capped by the number of (z, y) column tiles x planes).
+  static void apply_grid(fs_pcg_plan* P) {
     const long long N = P->d.N;
-    P->g_init = fs_grid_blocks((const void*)k_init<T, K>, N);
     using C = TmaTile<T, K>;
-    P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
-    {
-      const char* sel = getenv("FS_STENCIL");
-      const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
-      if (!C::OK || plain_stencil())
-        P->stencil_kind = 0;
-      else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0))
-        P->stencil_kind = 1;
-      else if (sel && strcmp(sel, "tmas") == 0)
-        P->stencil_kind = 3;
-      else
-        P->stencil_kind = 2;
-    }
     if (P->stencil_kind == 3) {
       using CS = TmaTileS<T, K>;
       cudaFuncSetAttribute(k_stencil_tma_s<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1593,6 +1609,75 @@ struct Impl {
     } else {
       P->g_apply = fs_grid_blocks((const void*)k_apply_pq<T, K>, N);
     }
+  }
+  // Time the TMA-staged (2), TMA-store (3) and cached-load (0) stencils on this
+  // plan's buffers (3 launches each after a warm-up, CUDA events on the
+  // creation stream) and keep the fastest.  The launches write q, the
+  // partials and the per-RHS state; the state and control block are saved
+  // and restored around them.
+  static int autotune(fs_pcg_plan* P, cudaStream_t s) {
+    if constexpr (!TmaTile<T, K>::OK) {
+      return FS_OK;
+    } else {
+      unsigned char* st0 = (unsigned char*)P->st;
+      const size_t sbytes = (size_t)((unsigned char*)(P->ctl + 1) - st0);
+      std::vector<unsigned char> saved(sbytes);
+      FS_CHECK(cudaMemcpyAsync(saved.data(), st0, sbytes, cudaMemcpyDeviceToHost, s));
+      FS_CHECK(cudaMemsetAsync(P->p[1], 0, (size_t)P->d.N * K * sizeof(T), s));
+      const int cands[3] = {2, 3, 0};
+      float best = 3.4e38f;
+      int bestk = 2;
+      for (int c : cands) {
+        P->stencil_kind = c;
+        P->use_tma = c != 0;
+        apply_grid(P);
+        kernel(P, 1, 0, s);
+        FS_CHECK(cudaEventRecord(P->ev[0], s));
+        for (int r = 0; r < 3; ++r) kernel(P, 1, 0, s);
+        FS_CHECK(cudaEventRecord(P->ev[1], s));
+        FS_CHECK(cudaGetLastError());
+        FS_CHECK(cudaEventSynchronize(P->ev[1]));
+        float ms = 0.f;
+        FS_CHECK(cudaEventElapsedTime(&ms, P->ev[0], P->ev[1]));
+        if (ms < best) {
+          best = ms;
+          bestk = c;
+        }
+      }
+      P->stencil_kind = bestk;
+      P->use_tma = bestk != 0;
+      apply_grid(P);
+      FS_CHECK(cudaMemcpyAsync(st0, saved.data(), sbytes, cudaMemcpyHostToDevice, s));
+      FS_CHECK(cudaStreamSynchronize(s));
+      stencil_choice_put(P->d, K, (int)sizeof(T), bestk);
+      return FS_OK;
+    }
+  }
+  static void grids(fs_pcg_plan* P) {
+    const long long N = P->d.N;
+    P->g_init = fs_grid_blocks((const void*)k_init<T, K>, N);
+    using C = TmaTile<T, K>;
+    P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
+    {
+      const char* sel = getenv("FS_STENCIL");
+      const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
+      P->autotune = 0;
+      if (!C::OK || plain_stencil()) {
+        P->stencil_kind = 0;
+      } else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0)) {
+        P->stencil_kind = 1;
+      } else if (sel && strcmp(sel, "tmas") == 0) {
+        P->stencil_kind = 3;
+      } else if (sel && strcmp(sel, "tma_m") == 0) {
+        P->stencil_kind = 2;
+      } else {
+        // chosen by timing the candidates on the first plan of this shape
+        const int cached = stencil_choice_get(P->d, K, (int)sizeof(T));
+        P->stencil_kind = cached >= 0 ? cached : 2;
+        P->autotune = cached < 0;
+      }
+    }
+    apply_grid(P);
     P->g_update = fs_grid_blocks((const void*)k_update<T, K>, N);
     P->g_rel = fs_grid_blocks((const void*)k_reliable<T, K>, N);
     P->g_fold = fs_grid_blocks((const void*)k_fold<T, K>, N);
@@ -1632,7 +1717,7 @@ struct Impl {
         return FS_CUDA_ERROR;
       }
     }
-    if (P->stencil_kind == 3) {
+    if (P->stencil_kind == 2 || P->stencil_kind == 3) {  // 2 may be tuned into 3
       using CS = TmaTileS<T, K>;
       cuuint32_t qbox[4] = {(cuuint32_t)K, (cuuint32_t)CS::TZ, (cuuint32_t)CS::TY, 1};
       CUresult rc = encode(&P->tm_q, dt, 4, P->q, dims, strides, qbox, es,
@@ -1949,6 +2034,7 @@ bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
     if (op == 10) P->launches_per_iter = Impl<T, KK>::precondition(P, s); \
     if (op == 11) Impl<T, KK>::locate_z(P);                        \
     if (op == 12) Impl<T, KK>::vcycle_ext(P, s);                   \
+    if (op == 13) P->net_status = Impl<T, KK>::autotune(P, s);      \
     return true;
   switch (k) {
     FS_OP(1)
@@ -2194,6 +2280,15 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
   for (int t = 0; t < 8; ++t)
     if ((e = cudaEventCreate(&P->ev[t])) != cudaSuccess)
       return fail("cudaEventCreate", e);
+  if (P->autotune) {
+    dispatch(P, 13, s);
+    const int at = P->net_status;
+    P->net_status = FS_OK;
+    if (at != FS_OK) {
+      fs_pcg_plan_destroy(P);
+      return at;
+    }
+  }
   const int cst = capture_graph(P);
   if (cst != FS_OK) {
     fs_pcg_plan_destroy(P);
@@ -2414,6 +2509,8 @@ int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, cons
   FS_CHECK_LAUNCH("k_eq_apply");
   return FS_OK;
 }
+
+int fs_pcg_plan_stencil_kind(const fs_pcg_plan* P) { return P ? P->stencil_kind : -1; }
 
 int fs_pcg_plan_label_counts(const fs_pcg_plan* P, long long* counts, void* stream) {
   if (!P || !counts) return FS_BAD_ARG;

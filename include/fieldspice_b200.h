@@ -362,6 +362,12 @@ int fs_pcg_plan_scale(const fs_pcg_plan* plan, const double** s64, const uint8_t
 /* counts[4] (host): the plan's free, fixed, solo and pinned node counts, as
  * classified at creation (LinearSystem's split, poisson.py:282-362).       */
 int fs_pcg_plan_label_counts(const fs_pcg_plan* plan, long long* counts, void* stream);
+/* The CG stencil kernel the plan runs: 0 cached loads, 1 TMA-staged p,
+ * 2 TMA-staged p and masses, 3 as 2 with TMA stores of q.  Unless the
+ * FS_STENCIL environment variable names one, the first plan of each (grid,
+ * RHS block, precision) times kinds 2, 3 and 0 on its own buffers at creation
+ * and later plans of that shape reuse the fastest.                          */
+int fs_pcg_plan_stencil_kind(const fs_pcg_plan* plan);
 
 /* ---- §8f-4: harmonic EQS, the complex-symmetric solve -------------------------
  * Replaces the per-frequency sparse LU of fieldspice/solvers/ac.py:95-145

@@ -50,3 +50,25 @@ def test_stencil_variant_matches_reference(cuda, golden, monkeypatch, variant, p
     assert np.abs(C - ref).max() / scale <= 1e-9
     C4 = _extract(g, d["eps_cell"], terms[:4], precision)
     assert np.abs(C4 - C4_plain).max() / np.abs(np.diag(C4_plain)).max() <= 1e-9
+
+
+def test_stencil_autotuner_picks_and_caches(cuda, golden, monkeypatch):
+    """Without FS_STENCIL the first plan of a shape times the stencil kernels
+    and keeps the fastest; the next plan of the same shape reuses it."""
+    import torch
+
+    from fieldspice_b200 import _lib as L
+    from fieldspice_b200.device import DeviceOperator, EliminatedSystem
+    monkeypatch.delenv("FS_STENCIL", raising=False)
+    d, g, terms = _problem(golden)
+    op = DeviceOperator(g, d["eps_cell"])
+    label = torch.zeros(op.N, dtype=torch.uint8, device=op.dev)
+    for t in terms:
+        label[torch.as_tensor(t.nodes, device=op.dev)] = L.LABEL_FIXED
+    kinds = []
+    for _ in range(2):
+        sys_ = EliminatedSystem(op, label, 8, precision="mixed", preconditioner="mg")
+        kinds.append(L.lib().fs_pcg_plan_stencil_kind(sys_.plan))
+        sys_.close()
+    assert kinds[0] in (0, 2, 3)
+    assert kinds[1] == kinds[0]
