@@ -61,6 +61,9 @@ _SIGNATURES = {
                                    POINTER(c_void_p), c_void_p]),
     "fs_pcg_plan_create_diag": (c_int, [c_int] * 6 + [c_void_p] * 8 + [c_size_t,
                                         POINTER(c_void_p), c_void_p]),
+    "fs_pcg_plan_create_ex": (c_int, [c_int] * 6 + [c_void_p] * 4 + [c_int] + [c_void_p] * 4
+                              + [c_size_t, POINTER(c_void_p), c_void_p]),
+    "fs_periodic_masses": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
                                   POINTER(FsRhsStats), c_void_p]),
     "fs_pcg_plans_solve": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p), c_int,

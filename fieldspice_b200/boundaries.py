@@ -15,8 +15,8 @@ from typing import Callable
 
 import numpy as np
 
-__all__ = ["WALLS", "Dirichlet", "Neumann", "BoundarySpec", "wall_nodes",
-           "dirichlet_nodes", "check_supported"]
+__all__ = ["WALLS", "Dirichlet", "Neumann", "Periodic", "BoundarySpec", "wall_nodes",
+           "dirichlet_nodes", "check_supported", "periodic_mask"]
 
 WALLS = ("xlo", "xhi", "ylo", "yhi", "zlo", "zhi")
 _AXIS = {"xlo": 0, "xhi": 0, "ylo": 1, "yhi": 1, "zlo": 2, "zhi": 2}
@@ -42,6 +42,23 @@ class Neumann:
 
     is_dirichlet_like = False
     is_natural = True
+
+    def prescribed_value(self, t: float = 0.0):
+        return None
+
+
+@dataclass(frozen=True)
+class Periodic:
+    """Wrap-around identification of the two walls normal to an axis
+    (``fieldspice/boundaries.py:462-523``); set it on both walls.  The
+    electrostatic path supports ``offset = 0`` and ``phase = 0`` only, as
+    the reference's ``PoissonSolver`` does (``poisson.py:942-955``)."""
+    offset: float = 0.0
+    phase: float = 0.0
+
+    is_dirichlet_like = False
+    is_natural = False
+    kind = "periodic"
 
     def prescribed_value(self, t: float = 0.0):
         return None
@@ -86,17 +103,43 @@ def wall_nodes(grid, wall: str) -> np.ndarray:
     return (plane * strides[axis] + a[:, None] + b[None, :]).ravel()
 
 
-def check_supported(spec) -> None:
+def periodic_mask(spec) -> int:
+    """Bit mask of the periodic axes (bit 0 x, 1 y, 2 z).  Periodic must be set
+    on both walls of an axis (``boundaries.py:1111-1125``)."""
+    mask = 0
+    for a, (lo, hi) in enumerate((("xlo", "xhi"), ("ylo", "yhi"), ("zlo", "zhi"))):
+        plo = type(_wall(spec, lo)).__name__.lower() == "periodic"
+        phi_ = type(_wall(spec, hi)).__name__.lower() == "periodic"
+        if plo != phi_:
+            raise ValueError(f"axis {'xyz'[a]}: Periodic must be set on both walls "
+                             f"({lo} and {hi})")
+        if plo:
+            mask |= 1 << a
+    return mask
+
+
+def check_supported(spec, allow_periodic: bool = False) -> None:
     """Reject walls the GPU path does not implement, with a clear error.
 
-    Periodic walls need the node-merging reduction of
-    ``fieldspice/solvers/poisson.py:698-719``, absorbing walls have no
-    quasi-static meaning, and a Neumann wall with non-zero flux needs the
+    Periodic walls (the node-merging reduction of
+    ``fieldspice/solvers/poisson.py:665-719``) are accepted where the caller
+    implements them (``allow_periodic``: the electrostatic solve and
+    capacitance extraction) with zero offset and phase; absorbing walls have
+    no quasi-static meaning, and a Neumann wall with non-zero flux needs the
     ``neumann_load`` right-hand side (``boundaries.py:1031-1085``).
     """
+    if allow_periodic:
+        periodic_mask(spec)  # both walls of a periodic axis
     for w in WALLS:
         bc = _wall(spec, w)
         kind = type(bc).__name__.lower()
+        if kind == "periodic" and allow_periodic:
+            for nm in ("offset", "phase"):
+                if float(getattr(bc, nm, 0.0)) != 0.0:
+                    raise ValueError(
+                        f"wall {w}: PoissonSolver supports periodic boundaries only "
+                        f"with {nm} = 0; impose the drop with a driven terminal instead")
+            continue
         if getattr(bc, "is_dirichlet_like", False):
             continue  # Dirichlet, or a PEC symmetry wall at its value
         if kind == "neumann":

@@ -19,9 +19,15 @@ struct Dims {
   long long N;   // nodes
   long long sx;  // stride of i (ny*nz)
   int sy;        // stride of j (nz)
+  // Periodic axes (bit 0 x, 1 y, 2 z): the last and first planes of such an
+  // axis are joined by a wrap edge whose mass sits on the last plane; wx, wy,
+  // wz are the index distances from the first to the last plane.
+  int per;
+  long long wx;
+  int wy, wz;
 };
 
-inline Dims make_dims(int nx, int ny, int nz) {
+inline Dims make_dims(int nx, int ny, int nz, int per = 0) {
   Dims d;
   d.nx = nx;
   d.ny = ny;
@@ -29,7 +35,34 @@ inline Dims make_dims(int nx, int ny, int nz) {
   d.sy = nz;
   d.sx = (long long)ny * nz;
   d.N = (long long)nx * d.sx;
+  d.per = per;
+  d.wx = (long long)(nx - 1) * d.sx;
+  d.wy = (ny - 1) * nz;
+  d.wz = nz - 1;
   return d;
+}
+
+// The six edges of node n = (i, j, k) as edge(present, mass, neighbour).  On
+// a periodic axis the first and last planes are neighbours through the wrap
+// edge, whose mass is stored on the last plane; otherwise the missing edges
+// of boundary nodes are reported as absent (and their neighbour not read).
+template <typename M, typename E>
+__device__ __forceinline__ void edge6(const Dims& d, const M* __restrict__ mx,
+                                      const M* __restrict__ my, const M* __restrict__ mz,
+                                      long long n, int i, int j, int k, E&& edge) {
+  const bool px = d.per & 1, py = (d.per >> 1) & 1, pz = (d.per >> 2) & 1;
+  if (i > 0) edge(true, mx[n - d.sx], n - d.sx);
+  else edge(px, px ? mx[n + d.wx] : (M)0, n + d.wx);
+  if (i < d.nx - 1) edge(true, mx[n], n + d.sx);
+  else edge(px, mx[n], n - d.wx);
+  if (j > 0) edge(true, my[n - d.sy], n - d.sy);
+  else edge(py, py ? my[n + d.wy] : (M)0, n + d.wy);
+  if (j < d.ny - 1) edge(true, my[n], n + d.sy);
+  else edge(py, my[n], n - d.wy);
+  if (k > 0) edge(true, mz[n - 1], n - 1);
+  else edge(pz, pz ? mz[n + d.wz] : (M)0, n + d.wz);
+  if (k < d.nz - 1) edge(true, mz[n], n + 1);
+  else edge(pz, mz[n], n - d.wz);
 }
 
 __device__ __forceinline__ void node_ijk(const Dims& d, long long n, int& i,

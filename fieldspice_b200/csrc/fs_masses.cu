@@ -197,9 +197,49 @@ int fs_grid_blocks(const void* kernel, long long work_items) {
   return (int)want;
 }
 
+// Masses of the reduced (wrap-around) grid: every reduced node sums the
+// masses of the full-grid nodes merged into it (the first plane of a periodic
+// axis absorbs the last), component by component.  On a periodic axis the
+// own-direction mass of the last reduced plane is the full grid's edge into
+// the dropped plane, i.e. the wrap edge.
+__global__ void k_periodic_masses(fs::Dims f, fs::Dims r, const double* __restrict__ mf,
+                                  double* __restrict__ mr) {
+  const bool px = r.per & 1, py = (r.per >> 1) & 1, pz = (r.per >> 2) & 1;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < r.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    fs::node_ijk(r, n, i, j, k);
+    const int ni = (px && i == 0) ? 2 : 1, nj = (py && j == 0) ? 2 : 1,
+              nk = (pz && k == 0) ? 2 : 1;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b)
+        for (int c = 0; c < nk; ++c) {
+          const int fi = a ? f.nx - 1 : i, fj = b ? f.ny - 1 : j, fk = c ? f.nz - 1 : k;
+          const long long fn = ((long long)fi * f.ny + fj) * f.nz + fk;
+          for (int m = 0; m < 3; ++m) acc[m] += mf[m * f.N + fn];
+        }
+    for (int m = 0; m < 3; ++m) mr[m * r.N + n] = acc[m];
+  }
+}
+
 extern "C" {
 
 const char* fs_version(void) { return "fieldspice_b200 0.1.0 sm_100a"; }
+
+int fs_periodic_masses(const double* m_full, int nx, int ny, int nz, int periodic,
+                       double* m_reduced, void* stream) {
+  if (!m_full || !m_reduced || periodic < 1 || periodic > 7) return FS_BAD_ARG;
+  const int rx = nx - (periodic & 1), ry = ny - ((periodic >> 1) & 1),
+            rz = nz - ((periodic >> 2) & 1);
+  if (rx < 2 || ry < 2 || rz < 2) return FS_BAD_ARG;
+  const fs::Dims f = fs::make_dims(nx, ny, nz);
+  const fs::Dims r = fs::make_dims(rx, ry, rz, periodic);
+  int g = fs_grid_blocks((const void*)k_periodic_masses, r.N);
+  k_periodic_masses<<<g, fs::kBlock, 0, (cudaStream_t)stream>>>(f, r, m_full, m_reduced);
+  FS_CHECK_LAUNCH("k_periodic_masses");
+  return FS_OK;
+}
 
 const char* fs_status_string(int status) {
   switch (status) {

@@ -137,12 +137,7 @@ __global__ void k_classify(Dims d, const double* __restrict__ mx,
         dg += m;
         if (label_in[nb] == FS_LABEL_FREE) sfree += m;
       };
-      edge(i > 0, i > 0 ? mx[n - d.sx] : 0.0, n - d.sx);
-      edge(i < d.nx - 1, mx[n], n + d.sx);
-      edge(j > 0, j > 0 ? my[n - d.sy] : 0.0, n - d.sy);
-      edge(j < d.ny - 1, my[n], n + d.sy);
-      edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
-      edge(k < d.nz - 1, mz[n], n + 1);
+      edge6(d, mx, my, mz, n, i, j, k, edge);
       if (dg == 0.0)
         lab = FS_LABEL_PINNED;  // coupled to nothing: pinned to 0
       else if (sfree == 0.0)
@@ -172,9 +167,12 @@ __global__ void k_eq_masses(Dims d, const double* __restrict__ mx,
     int i, j, k;
     fs::node_ijk(d, n, i, j, k);
     const double s = s64[n];
-    ex[n] = (T)(i < d.nx - 1 ? mx[n] * s * s64[n + d.sx] : 0.0);
-    ey[n] = (T)(j < d.ny - 1 ? my[n] * s * s64[n + d.sy] : 0.0);
-    ez[n] = (T)(k < d.nz - 1 ? mz[n] * s * s64[n + 1] : 0.0);
+    // the +x/+y/+z edge of the node; on a periodic axis the last plane's edge
+    // is the wrap edge to the first plane
+    const bool px = d.per & 1, py = (d.per >> 1) & 1, pz = (d.per >> 2) & 1;
+    ex[n] = (T)(i < d.nx - 1 ? mx[n] * s * s64[n + d.sx] : (px ? mx[n] * s * s64[n - d.wx] : 0.0));
+    ey[n] = (T)(j < d.ny - 1 ? my[n] * s * s64[n + d.sy] : (py ? my[n] * s * s64[n - d.wy] : 0.0));
+    ez[n] = (T)(k < d.nz - 1 ? mz[n] * s * s64[n + 1] : (pz ? mz[n] * s * s64[n - d.wz] : 0.0));
   }
 }
 
@@ -228,12 +226,7 @@ __global__ void __launch_bounds__(fs::kBlock)
         if (!nb_free) bres[t] += m * v;
       }
     };
-    edge(i > 0, i > 0 ? mx[n - d.sx] : 0.0, n - d.sx);
-    edge(i < d.nx - 1, mx[n], n + d.sx);
-    edge(j > 0, j > 0 ? my[n - d.sy] : 0.0, n - d.sy);
-    edge(j < d.ny - 1, my[n], n + d.sy);
-    edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
-    edge(k < d.nz - 1, mz[n], n + 1);
+    edge6(d, mx, my, mz, n, i, j, k, edge);
     if (dgn) {
       const double dd = dgn[n];
       dg += dd;
@@ -1032,12 +1025,18 @@ __global__ void __launch_bounds__(fs::kBlock, fs::mg_min_blocks<T, K>())
 #pragma unroll
       for (int t = 0; t < K; ++t) qv[t] -= m * pn[t];
     };
-    if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
-    if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
-    if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
-    if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
-    if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
-    if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+    if (d.per) {  // periodic plans (cached-load kernel only): wrap edges
+      fs::edge6(d, ex, ey, ez, n, i, j, k, [&](bool ok, T m, long long nb) {
+        if (ok) nbr(m, nb);
+      });
+    } else {
+      if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
+      if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
+      if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
+      if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
+      if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
+      if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+    }
     fs::stv<T, K>(q, n, qv);
 #pragma unroll
     for (int t = 0; t < K; ++t) acc[t] += (double)pc[t] * (double)qv[t];
@@ -1174,12 +1173,7 @@ __global__ void __launch_bounds__(fs::kBlock)
 #pragma unroll
       for (int t = 0; t < K; ++t) res[t] -= m * (c[t] - v[t]);
     };
-    edge(i > 0, i > 0 ? mx[n - d.sx] : 0.0, n - d.sx);
-    edge(i < d.nx - 1, mx[n], n + d.sx);
-    edge(j > 0, j > 0 ? my[n - d.sy] : 0.0, n - d.sy);
-    edge(j < d.ny - 1, my[n], n + d.sy);
-    edge(k > 0, k > 0 ? mz[n - 1] : 0.0, n - 1);
-    edge(k < d.nz - 1, mz[n], n + 1);
+    edge6(d, mx, my, mz, n, i, j, k, edge);
     if (dgn) {
       const double dd = dgn[n];
 #pragma unroll
@@ -1662,7 +1656,7 @@ struct Impl {
       const char* sel = getenv("FS_STENCIL");
       const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
       P->autotune = 0;
-      if (!C::OK || plain_stencil()) {
+      if (!C::OK || plain_stencil() || P->d.per) {  // only the cached-load kernel wraps
         P->stencil_kind = 0;
       } else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0)) {
         P->stencil_kind = 1;
@@ -2163,8 +2157,22 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
                             const uint8_t* label_in, double* phi,
                             const double* f, void* workspace, size_t workspace_bytes,
                             fs_pcg_plan** plan, void* stream) {
+  return fs_pcg_plan_create_ex(nx, ny, nz, nrhs, precision, precond, mx, my, mz, diag, 0,
+                               label_in, phi, f, workspace, workspace_bytes, plan, stream);
+}
+
+int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int precond,
+                          const double* mx, const double* my, const double* mz,
+                          const double* diag, int periodic, const uint8_t* label_in,
+                          double* phi, const double* f, void* workspace,
+                          size_t workspace_bytes, fs_pcg_plan** plan, void* stream) {
   if (!plan) return FS_BAD_ARG;
   *plan = nullptr;
+  if (periodic < 0 || periodic > 7) return FS_BAD_ARG;
+  if (periodic && precond != FS_PRECOND_JACOBI) {
+    fs_set_error_msg("periodic axes: the multigrid hierarchy does not wrap; use Jacobi PCG");
+    return FS_BAD_ARG;
+  }
   size_t need = 0;
   int st = fs_pcg_workspace_bytes(nx, ny, nz, nrhs, precision, precond, &need);
   if (st != FS_OK) return st;
@@ -2177,7 +2185,7 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
   fs_pcg_plan* P = new (std::nothrow) fs_pcg_plan();
   if (!P) return FS_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  P->d = fs::make_dims(nx, ny, nz);
+  P->d = fs::make_dims(nx, ny, nz, periodic);
   P->nrhs = nrhs;
   P->precision = precision;
   P->precond = precond == FS_PRECOND_MG ? 1 : 0;

@@ -75,12 +75,14 @@ class DeviceOperator:
     """
 
     def __init__(self, grid, prop_cell=None, *, mode: str = "parallel",
-                 masses=None):
+                 masses=None, shape=None, periodic: int = 0):
         import torch
         self.grid = grid
-        self.shape = tuple(int(s) for s in grid.shape_nodes)
+        self.shape = (tuple(int(s) for s in grid.shape_nodes) if shape is None
+                      else tuple(int(s) for s in shape))
         self.N = int(np.prod(self.shape))
         self.dev = device()
+        self.periodic = int(periodic)   # wrap-around axes (bit 0 x, 1 y, 2 z)
         lib = L.lib()
         if masses is not None:
             self.m = masses
@@ -113,6 +115,21 @@ class DeviceOperator:
     def mz(self):
         return self.m[2]
 
+    def reduced(self, periodic: int) -> "DeviceOperator":
+        """The operator of the wrap-around grid of periodic axes ``periodic``
+        (the last node plane of each merged into the first, as the reference's
+        node-merging reduction, ``poisson.py:665-719``); FP64 masses built on
+        the device (``fs_periodic_masses``)."""
+        import torch
+        nx, ny, nz = self.shape
+        shape = (nx - (periodic & 1), ny - ((periodic >> 1) & 1), nz - ((periodic >> 2) & 1))
+        if min(shape) < 2:
+            raise ValueError("a periodic axis needs at least 3 node planes")
+        m = torch.empty((3, int(np.prod(shape))), dtype=torch.float64, device=self.dev)
+        L.check("fs_periodic_masses", L.lib().fs_periodic_masses(
+            L.ptr(self.m), nx, ny, nz, int(periodic), L.ptr(m), L.stream_ptr()))
+        return DeviceOperator(self.grid, masses=m, shape=shape, periodic=periodic)
+
     def combine(self, a: float, other: "DeviceOperator", b: float) -> "DeviceOperator":
         """``a*self + b*other`` edge by edge (eqs.py:279-280)."""
         import torch
@@ -121,7 +138,7 @@ class DeviceOperator:
                                        float(b), L.ptr(out), self.m.numel(),
                                        L.stream_ptr())
         L.check("fs_combine_masses", st)
-        return DeviceOperator(self.grid, masses=out)
+        return DeviceOperator(self.grid, masses=out, shape=self.shape, periodic=self.periodic)
 
     def edge_vector(self) -> np.ndarray:
         """Masses in the reference's concatenated [x|y|z] edge order (host)."""
@@ -237,6 +254,11 @@ class EliminatedSystem:
                 raise ValueError("preconditioner='learned' needs a trained network")
             if precision == "fp64":
                 raise ValueError("the learned preconditioner runs in mixed precision")
+        if op.periodic and preconditioner != "jacobi":
+            # the multigrid hierarchy and the TMA stencils do not wrap
+            if preconditioner == "learned":
+                raise ValueError("the learned preconditioner does not support periodic axes")
+            preconditioner = "jacobi"
         self.preconditioner = preconditioner
         self.learned = learned
         # optional FP64 node-diagonal term of the operator (kept alive here)
@@ -290,11 +312,11 @@ class EliminatedSystem:
         if ws.data_ptr() % 256:
             raise RuntimeError("device allocation is not 256-byte aligned")
         plan = ctypes.c_void_p()
-        st = lib.fs_pcg_plan_create_diag(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
-                                         L.ptr(op.my), L.ptr(op.mz), L.ptr(self.diag),
-                                         L.ptr(self.label_in), L.ptr(self.phi), L.ptr(self.f),
-                                         L.ptr(ws), nb.value, ctypes.byref(plan),
-                                         L.stream_ptr())
+        st = lib.fs_pcg_plan_create_ex(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
+                                       L.ptr(op.my), L.ptr(op.mz), L.ptr(self.diag),
+                                       int(op.periodic), L.ptr(self.label_in),
+                                       L.ptr(self.phi), L.ptr(self.f), L.ptr(ws), nb.value,
+                                       ctypes.byref(plan), L.stream_ptr())
         L.check("fs_pcg_plan_create", st)
         return plan, ws
 

@@ -19,7 +19,7 @@ from typing import Any, Sequence
 import numpy as np
 
 from .. import _lib as L
-from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes
+from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes, periodic_mask
 from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d,
                       pad_rhs, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
@@ -128,15 +128,32 @@ def check_terminals(terminals, grid) -> tuple:
     return out
 
 
-def prepare_bc(bc, grid):
+def prepare_bc(bc, grid, allow_periodic: bool = False):
     """Default all-Neumann; reject walls the GPU path does not implement."""
     bc = BoundarySpec.all_neumann() if bc is None else bc
     if not hasattr(bc, "get") and not hasattr(bc, "xlo"):
         raise ValueError(f"bc must be a BoundarySpec, got {type(bc).__name__}")
     if hasattr(bc, "validate"):
         bc.validate(grid)
-    check_supported(bc)
+    check_supported(bc, allow_periodic=allow_periodic)
     return bc
+
+
+def wrap_map(shape, mask: int) -> np.ndarray:
+    """Full node -> node of the wrap-around grid whose periodic axes (``mask``)
+    lose their last plane to the first (``poisson.py:942-955`` pairs)."""
+    nx, ny, nz = (int(v) for v in shape)
+    rx, ry, rz = nx - (mask & 1), ny - ((mask >> 1) & 1), nz - ((mask >> 2) & 1)
+    i = np.arange(nx)
+    j = np.arange(ny)
+    k = np.arange(nz)
+    if mask & 1:
+        i[-1] = 0
+    if mask & 2:
+        j[-1] = 0
+    if mask & 4:
+        k[-1] = 0
+    return ((i[:, None, None] * ry + j[None, :, None]) * rz + k[None, None, :]).ravel()
 
 
 def raise_on_status(stats: list[dict], tol: float, method: str) -> None:
@@ -245,18 +262,30 @@ class PoissonSolver:
         terms = check_terminals(terminals, grid)
         if not terms:
             raise ValueError("capacitance extraction needs at least one terminal")
-        bc = prepare_bc(bc, grid)
+        bc = prepare_bc(bc, grid, allow_periodic=True)
+        mask = periodic_mask(bc)
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
         term_nodes = [np.asarray(t.nodes, np.int64) for t in terms]
         term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
         wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
         shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
+        op, charges = self.op, None
+        if mask:
+            # periodic walls: solve on the wrap-around grid (the reference's
+            # P^T L P node merge), integrate the charges on the full grid
+            wmap = wrap_map(self.op.shape, mask)
+            op = self.op.reduced(mask)
+            groups = term_dev + ([shield_dev] if shield_dev.numel() else [])
+            charges = (self.op, h2d(wmap, torch.int64, dev), groups)
+            term_dev = [h2d(np.unique(wmap[n]), torch.int64, dev) for n in term_nodes]
+            wall_dev = h2d(np.unique(wmap[wall_idx]).astype(np.int64), torch.int64, dev)
+            shield_dev = shield_nodes(wall_dev, term_dev, op.N)
         C, q_shield, info = extract_capacitance(
-            self.op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
+            op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,
             preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-            learned=self.gpu.learned)
+            learned=None if mask else self.gpu.learned, charges=charges)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         rep["terminals"] = tuple(t.name for t in terms)
@@ -301,7 +330,8 @@ class PoissonSolver:
         t0 = time.perf_counter()
         grid = self.grid
         terms = check_terminals(terminals, grid)
-        bc = prepare_bc(bc, grid)
+        bc = prepare_bc(bc, grid, allow_periodic=True)
+        mask = periodic_mask(bc)
         dev = self.op.dev
         N = self.op.N
         vnode = self.node_volumes
@@ -311,6 +341,13 @@ class PoissonSolver:
 
         fixed, vals = _dirichlet_sets(bc, terms, grid, t)
         floats = [tt for tt in terms if tt.driven != "voltage"]
+        if mask:
+            if floats:
+                raise NotImplementedError(
+                    "floating or charge-driven electrodes together with periodic walls "
+                    "are not supported on the GPU path")
+            return self._solve_periodic(terms, mask, fixed, vals, b_free,
+                                        rho_node is not None, t0)
         if floats:
             return self._solve_floating(terms, floats, fixed, vals, b_free,
                                         rho_node is not None, t, t0)
@@ -347,6 +384,54 @@ class PoissonSolver:
                 "setup_time": system.setup_time,
                 "solve_time": time.perf_counter() - t0}
         res = self._potential_result(system.phi, terms, b_free, info, fixed.size, t0)
+        system.close()
+        return res
+
+    def _solve_periodic(self, terms, mask: int, fixed, vals, b_free, with_src: bool,
+                        t0: float) -> Result:
+        """Periodic walls: the solve on the wrap-around grid (the reference's
+        node merge P^T L P x = P^T b, ``poisson.py:1041-1058``), expanded back
+        to the full grid, where the charges and energy are evaluated."""
+        import torch
+        dev = self.op.dev
+        wmap = wrap_map(self.op.shape, mask)
+        op = self.op.reduced(mask)
+        Nr = op.N
+        b_r = np.bincount(wmap, weights=b_free, minlength=Nr)
+        # merged Dirichlet nodes: the value of the last one in index order wins,
+        # as numpy's assignment in apply_dirichlet does
+        fr = wmap[fixed]
+        uniq, last = np.unique(fr[::-1], return_index=True)
+        fixed_r, vals_r = uniq, np.asarray(vals)[::-1][last]
+        pinned = None
+        if fixed_r.size == 0:
+            d = self._diagonal(op)
+            pinned = int(np.argmax(np.abs(d)))
+            fixed_r, vals_r = np.array([pinned]), np.zeros(1)
+            warnings.warn(
+                "singular all-Neumann system: no Dirichlet node was found, so "
+                f"node {pinned} is pinned to 0 to fix the gauge.  Only "
+                "potential DIFFERENCES in the result are meaningful; the "
+                "absolute level is arbitrary.", RuntimeWarning, stacklevel=3)
+        label = torch.zeros(Nr, dtype=torch.uint8, device=dev)
+        fixed_d = h2d(fixed_r.astype(np.int64), torch.int64, dev)
+        label[fixed_d] = L.LABEL_FIXED
+        system = EliminatedSystem(op, label, 1, precision=self.gpu.precision,
+                                  with_source=with_src, preconditioner="jacobi")
+        system.phi.zero_()
+        system.phi[fixed_d] = h2d(vals_r, torch.float64, dev)
+        if with_src:
+            system.f.copy_(h2d(b_r, torch.float64, dev))
+        tol = float(self.cfg.tol)
+        _, stats = system.solve(tol, self.gpu.maxiter)
+        raise_on_status(stats, tol, "gpu-cg")
+        phi_full = system.phi.index_select(0, h2d(wmap, torch.int64, dev))
+        info = {"method": f"gpu-cg-jacobi-{self.gpu.precision}", "n": Nr,
+                "n_factorised": system.n_free, "iterations": stats[0]["iterations"],
+                "residual": stats[0]["relres"], "pinned": pinned, "periodic": mask,
+                "setup_time": system.setup_time, "solve_time": time.perf_counter() - t0}
+        res = self._potential_result(phi_full, terms, b_free, info, fixed_r.size, t0)
+        res.meta["n_unknowns"] = Nr
         system.close()
         return res
 
@@ -438,26 +523,41 @@ class PoissonSolver:
         res.meta.setdefault("grid_cells", tuple(grid.shape_cells))
         return res
 
-    def _diagonal(self) -> np.ndarray:
-        nx, ny, nz = self.op.shape
-        m = self.op.m.cpu().numpy().reshape(3, nx, ny, nz)
+    def _diagonal(self, op=None) -> np.ndarray:
+        """Sum of the incident masses per node (with the wrap edges of a
+        periodic operator)."""
+        op = self.op if op is None else op
+        nx, ny, nz = op.shape
+        m = op.m.cpu().numpy().reshape(3, nx, ny, nz)
         d = m[0] + m[1] + m[2]
         d[1:] += m[0, :-1]
         d[:, 1:] += m[1, :, :-1]
         d[:, :, 1:] += m[2, :, :, :-1]
+        if op.periodic & 1:
+            d[0] += m[0, -1]
+        if op.periodic & 2:
+            d[:, 0] += m[1, :, -1]
+        if op.periodic & 4:
+            d[:, :, 0] += m[2, :, :, -1]
         return d.ravel()
 
 
 def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                         tol: float, precision: str = "auto",
                         maxiter: int | None = None, preconditioner: str = "jacobi",
-                        learned=None):
+                        learned=None, charges=None):
     """Device core of the extraction: inputs already in HBM.
 
     ``term_dev``: sorted unique int64 node tensors, one per terminal;
     ``wall_dev``: Dirichlet wall nodes (grounded); ``shield_dev``: wall nodes
     that belong to no terminal.  Returns ``(C, q_shield, info)`` with ``C``
     not yet symmetrised (``poisson.py:1196-1224``).
+
+    ``charges``: for a wrap-around (periodic) ``op``, ``(full_op, node_map,
+    groups)``: each solution is expanded to the full grid through
+    ``node_map`` (full node -> reduced node) and the charges integrated there
+    on the full-grid node sets ``groups`` (terminals, then the shield), as the
+    reference does (``poisson.py:1218-1223``).
     """
     import torch
     dev = op.dev
@@ -476,6 +576,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
     q_shield = np.zeros(nt)
     stats_all: list[dict] = []
     system = None
+    gdev_full = None
     launches = 0
     setup_time = 0.0
     nx, ny, nz = op.shape
@@ -501,7 +602,14 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         launches += system.launches + 1
         raise_on_status(stats, tol, "gpu-cg")
         stats_all.extend(stats)
-        Q = op.group_sums(system.phi, groups, nrhs=k, nodes_dev=gdev)
+        if charges is None:
+            Q = op.group_sums(system.phi, groups, nrhs=k, nodes_dev=gdev)
+        else:
+            full_op, node_map, full_groups = charges
+            if gdev_full is None:
+                gdev_full = upload_groups(full_groups, dev)
+            phi_full = system.phi.view(op.N, k).index_select(0, node_map).reshape(-1)
+            Q = full_op.group_sums(phi_full, full_groups, nrhs=k, nodes_dev=gdev_full)
         launches += 1
         for c, j in enumerate(cols):
             C[:, j] = Q[:nt, c]

@@ -94,6 +94,16 @@ int fs_build_masses(const double* prop_cell, const double* hx, const double* hy,
                     const double* hzd, int nx, int ny, int nz, int mode,
                     double* mx, double* my, double* mz, void* stream);
 
+/* Edge masses of the wrap-around grid of periodic axes `periodic` (bit 0 x,
+ * 1 y, 2 z; fieldspice/boundaries.py periodic_pairs and the node merge of
+ * poisson.py:665-719): m_full is the 3 x N output of fs_build_masses on the
+ * nx x ny x nz grid, m_reduced (3 x N', FP64) receives the masses of the grid
+ * with the last plane of every periodic axis merged into the first (each
+ * reduced node sums its merged nodes' masses; the last reduced plane's
+ * own-direction mass is the wrap edge).  Reduced axes need >= 2 nodes.       */
+int fs_periodic_masses(const double* m_full, int nx, int ny, int nz, int periodic,
+                       double* m_reduced, void* stream);
+
 /* out = a*m1 + b*m2 elementwise over n values (FP64).  Builds the EQS masses
  * M_eps/dt + theta*M_sigma (fieldspice/solvers/eqs.py:279-280).            */
 int fs_combine_masses(const double* m1, const double* m2, double a, double b,
@@ -153,6 +163,17 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
                             const uint8_t* label_in, double* phi,
                             const double* f, void* workspace, size_t workspace_bytes,
                             fs_pcg_plan** plan, void* stream);
+/* The same with periodic axes (bit 0 x, bit 1 y, bit 2 z): the grid is the
+ * reduced node set of fieldspice's wrap-around identification (the last node
+ * plane of a periodic axis merged into the first, poisson.py:665-719, 942-955),
+ * and the first and last planes of each periodic axis are joined by a wrap
+ * edge whose mass is stored on the last plane (mx at i = nx-1, and so on).
+ * Jacobi-preconditioned CG only (precond = FS_PRECOND_JACOBI).              */
+int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int precond,
+                          const double* mx, const double* my, const double* mz,
+                          const double* diag, int periodic, const uint8_t* label_in,
+                          double* phi, const double* f, void* workspace,
+                          size_t workspace_bytes, fs_pcg_plan** plan, void* stream);
 /* Solve in place into phi.  warm_start != 0 keeps the free-node values of
  * phi as the initial guess (the tolerance stays relative to ||b||, as in
  * SciPy); otherwise the guess is 0.  stats: host array of nrhs entries.

@@ -873,3 +873,72 @@ def merged_potential(g: Grid, eps_cell, fixed, values, merge_groups, b_ext, mode
     A_bc, b_bc = apply_dirichlet(A, b, fixed_r, np.asarray(values, float))
     x = spla.spsolve(A_bc.tocsc(), b_bc)
     return P @ x, Lm
+
+
+# ---------------------------------------------------------------------------
+# Periodic walls -- boundaries.py:226-260 (pairs), poisson.py:665-719 (merge),
+# 942-955, 1041-1058 (solve), 1196-1224 (capacitance)
+# ---------------------------------------------------------------------------
+def periodic_groups(g: Grid, axes):
+    """The (lo, hi) node pairs identified by the periodic ``axes`` ("x", "y",
+    "z"), one two-node group per pair."""
+    shape = g.shape_nodes
+    nid = np.arange(g.n_nodes).reshape(shape)
+    groups = []
+    for a in axes:
+        ax = "xyz".index(a)
+        lo = np.take(nid, 0, axis=ax).ravel()
+        hi = np.take(nid, shape[ax] - 1, axis=ax).ravel()
+        groups.extend(np.array([p, q]) for p, q in zip(lo, hi))
+    return groups
+
+
+def _merge_matrix(n, groups):
+    """``P`` (n x n_reduced, one 1 per row) merging connected node groups."""
+    a = [np.full(len(gp) - 1, gp[0]) for gp in groups if len(gp) > 1]
+    b = [np.asarray(gp[1:]) for gp in groups if len(gp) > 1]
+    if not a:
+        return sp.identity(n, format="csr"), np.arange(n)
+    from scipy.sparse.csgraph import connected_components
+    adj = sp.coo_matrix((np.ones(sum(x.size for x in a)), (np.concatenate(a), np.concatenate(b))),
+                        shape=(n, n))
+    _, label = connected_components(adj, directed=False)
+    P = sp.coo_matrix((np.ones(n), (np.arange(n), label)), shape=(n, label.max() + 1)).tocsr()
+    return P, label
+
+
+def periodic_capacitance(g: Grid, eps_cell, terminals, axes, dirichlet_walls=None):
+    """Maxwell C with periodic ``axes``: unit excitations solved on ``P^T L P``
+    (direct), charges ``L phi`` on the full grid (poisson.py:1196-1224);
+    unsymmetrised."""
+    Lm = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, np.asarray(eps_cell, float))))
+    P, red = _merge_matrix(g.n_nodes, periodic_groups(g, axes))
+    A_r = sp.csr_matrix(P.T @ Lm @ P)
+    wall_idx, _ = dirichlet_nodes(g, dirichlet_walls or {})
+    terms = [np.asarray(t, np.intp) for t in terminals]
+    fixed = np.unique(np.concatenate([wall_idx] + terms))
+    fixed_r = red[fixed]
+    A_bc, _ = apply_dirichlet(A_r, np.zeros(A_r.shape[0]), fixed_r, np.zeros(fixed_r.size))
+    lu = spla.splu(A_bc.tocsc())
+    C = np.zeros((len(terms), len(terms)))
+    for j, tj in enumerate(terms):
+        x0 = np.zeros(A_r.shape[0])
+        x0[red[tj]] = 1.0
+        b = -(A_r @ x0)
+        b[fixed_r] = x0[fixed_r]
+        q = Lm @ (P @ lu.solve(b))
+        for i, ti in enumerate(terms):
+            C[i, j] = q[ti].sum()
+    return C
+
+
+def periodic_potential(g: Grid, eps_cell, fixed, values, axes, b_free):
+    """Potential with periodic ``axes``, Dirichlet ``fixed``/``values`` and
+    node charges ``b_free`` (poisson.py:1041-1058, direct solve); returns
+    ``(phi, L)`` on the full grid."""
+    Lm = nodal_laplacian(g, edge_mass_vector(g, cell_to_edge(g, np.asarray(eps_cell, float))))
+    P, red = _merge_matrix(g.n_nodes, periodic_groups(g, axes))
+    A_r = sp.csr_matrix(P.T @ Lm @ P)
+    A_bc, b_bc = apply_dirichlet(A_r, P.T @ np.asarray(b_free, float), red[np.asarray(fixed)],
+                                 np.asarray(values, float))
+    return P @ spla.spsolve(A_bc.tocsc(), b_bc), Lm

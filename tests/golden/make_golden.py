@@ -396,6 +396,46 @@ def floating_fixture():
     np.savez_compressed(HERE / "floating.npz", **out)
 
 
+def periodic_fixture():
+    """poisson.py:942-955, 1041-1058, 1196-1224 with Periodic walls: a layered
+    unit cell periodic in x (and one periodic in x and y), grounded floor,
+    three box electrodes (one crossing the x wrap); the capacitance matrix and
+    a driven potential with free charge."""
+    from fieldspice.boundaries import Periodic
+    rng = np.random.default_rng(51)
+    g = RectilinearGrid(np.linspace(0, 3e-6, 17), np.sort(rng.uniform(0, 2e-6, 11)),
+                        np.linspace(0, 1e-6, 9))
+    eps = np.full(g.shape_cells, 3.9 * eps0)
+    eps[:, :, :3] = 7.0 * eps0
+    eps[:, 6:, 5:] = 2.5 * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(3, 2, 4, 6, 5, 5), (9, 5, 3, 12, 8, 5)]
+    terms = [Terminal(f"b{i}", nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel())
+             for i, (a0, b0, c0, a1, b1, c1) in enumerate(boxes)]
+    # a strip across the x wrap: both boundary planes belong to it
+    wrap = np.concatenate([nid[14:, 3:7, 6:8].ravel(), nid[:2, 3:7, 6:8].ravel()])
+    terms.append(Terminal("wrap", wrap))
+    cfg = SolverConfig(linear_solver="direct", tol=1e-12)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "boxes": np.asarray(boxes),
+           "wrap_nodes": wrap}
+    for tag, walls in (("x", ("x",)), ("xy", ("x", "y"))):
+        kw = {"zlo": Dirichlet(0.0)}
+        for a in walls:
+            kw[f"{a}lo"] = Periodic()
+            kw[f"{a}hi"] = Periodic()
+        bc = BoundarySpec(**kw)
+        ps = PoissonSolver(g, eps, cfg)
+        out[f"C_{tag}"] = ps.capacitance_matrix(terms, bc)
+        drive = [Terminal(t.name, t.nodes, voltage=v) for t, v in zip(terms, (1.0, -0.5, 0.25))]
+        rho = np.zeros(g.shape_nodes)
+        rho[7, 7, 6] = 2e3
+        r = ps.solve(drive, bc, rho_node=rho)
+        out[f"phi_{tag}"] = r.fields["phi"][0].ravel()
+        out[f"q_{tag}"] = np.array([r.terminals[t.name]["q"][0] for t in drive])
+        out["rho"] = rho
+    np.savez_compressed(HERE / "periodic.npz", **out)
+
+
 def rc_stack(n=60):
     d, Wd, H = 4e-6, 3e-6, 2e-6
     sigma1, er1, er2 = 1e3, 4.0, 2.0
@@ -493,6 +533,7 @@ FIXTURES = {
     "rlgc": rlgc_fixture,
     "ac": ac_fixture,
     "floating": floating_fixture,
+    "periodic": periodic_fixture,
 }
 
 if __name__ == "__main__":

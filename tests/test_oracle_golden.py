@@ -257,3 +257,29 @@ def test_floating_electrodes_match_reference(golden):
     for name, nd in zip(("drv", "flt", "chg"), nodes):
         assert abs(q[nd].sum() - d[f"q_{name}"][0]) <= 1e-9 * abs(d["q_drv"][0])
         assert abs(phi[nd[0]] - d[f"v_{name}"][0]) <= 1e-10
+
+
+def _periodic_terms(d, g):
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    t = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    return t + [d["wrap_nodes"]]
+
+
+@pytest.mark.parametrize("tag,axes", [("x", ("x",)), ("xy", ("x", "y"))])
+def test_periodic_walls_match_reference(golden, tag, axes):
+    """poisson.py with Periodic walls: capacitance (symmetrised) and a driven
+    potential with free charge, through the oracle's node merge."""
+    d = golden("periodic")
+    g = O.Grid(d["x"], d["y"], d["z"])
+    terms = _periodic_terms(d, g)
+    C = O.periodic_capacitance(g, d["eps"], terms, axes, {"zlo": 0.0})
+    C = 0.5 * (C + C.T)
+    assert np.abs(C - d[f"C_{tag}"]).max() <= 1e-10 * np.abs(np.diag(C)).max()
+    wall = np.arange(g.n_nodes).reshape(g.shape_nodes)[:, :, 0].ravel()
+    fixed = np.concatenate([wall] + terms)
+    vals = np.concatenate([np.zeros(wall.size)] + [np.full(t.size, v)
+                                                  for t, v in zip(terms, (1.0, -0.5, 0.25))])
+    fixed, vals = O.unique_last(fixed, vals)
+    b_free = d["rho"].ravel() * g.node_volumes().ravel()
+    phi, Lm = O.periodic_potential(g, d["eps"], fixed, vals, axes, b_free)
+    assert np.abs(phi - d[f"phi_{tag}"]).max() <= 1e-10
