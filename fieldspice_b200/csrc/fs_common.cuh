@@ -73,11 +73,110 @@ __device__ __forceinline__ void node_ijk(const Dims& d, long long n, int& i,
   j = (int)(t - (long long)i * d.ny);
 }
 
-// ---- RHS-interleaved vector loads/stores (128-bit where the width allows) --
+// ---- RHS-interleaved vector loads/stores -----------------------------------
+// 128-bit accesses by default.  `Wide` selects sm_100's 256-bit accesses
+// (ld/st.global.v8.f32, .v4.f64) for nodes of 8 FP32 or 4 FP64 values: one
+// instruction per 32-byte node, so a warp request covers whole sectors.
+// Measured on the 256x256x128 extraction, they speed up the streaming CG
+// kernels (p update 0.138 -> 0.120 ms, x/r update 0.285 -> 0.264 ms) but
+// slow the neighbour-gathering smoother and stencil kernels (the degree-2
+// post-smoother 0.193 -> 0.258 ms), so only the streaming kernels ask for
+// them.  The 256-bit form needs a 32-byte aligned node; nodes are n*32 bytes
+// apart, so only the base pointer is checked (a uniform branch) and a base
+// that is only 16-byte aligned takes 128-bit accesses.  Every pointer given
+// to these helpers is global memory.
+__device__ __forceinline__ bool aligned32(const void* p) {
+  return (reinterpret_cast<uintptr_t>(p) & 31) == 0;
+}
+
+template <bool NC>
+__device__ __forceinline__ void ld256(const float* p, float& a0, float& a1, float& a2, float& a3,
+                                      float& a4, float& a5, float& a6, float& a7) {
+  if constexpr (NC)  // read-only data: the compiler may schedule it freely
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a0), "=f"(a1), "=f"(a2), "=f"(a3), "=f"(a4), "=f"(a5), "=f"(a6),
+                   "=f"(a7)
+                 : "l"(p));
+  else
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a0), "=f"(a1), "=f"(a2), "=f"(a3), "=f"(a4), "=f"(a5), "=f"(a6),
+                   "=f"(a7)
+                 : "l"(p)
+                 : "memory");
+}
+
+template <bool NC>
+__device__ __forceinline__ void ld256(const double* p, double& a0, double& a1, double& a2,
+                                      double& a3) {
+  if constexpr (NC)
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(a0), "=d"(a1), "=d"(a2), "=d"(a3)
+                 : "l"(p));
+  else
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(a0), "=d"(a1), "=d"(a2), "=d"(a3)
+                 : "l"(p)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st256(float* p, float a0, float a1, float a2, float a3, float a4,
+                                      float a5, float a6, float a7) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a0),
+               "f"(a1), "f"(a2), "f"(a3), "f"(a4), "f"(a5), "f"(a6), "f"(a7)
+               : "memory");
+}
+
+__device__ __forceinline__ void st256(double* p, double a0, double a1, double a2, double a3) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a0), "d"(a1), "d"(a2),
+               "d"(a3)
+               : "memory");
+}
+
+// Whole 32-byte chunks of a node, one 256-bit access each (p 32-byte aligned).
+template <bool NC, typename T, int K>
+__device__ __forceinline__ void ld_chunks32(const T* p, T (&v)[K]) {
+  if constexpr (std::is_same<T, float>::value) {
+#pragma unroll
+    for (int c = 0; c < K / 8; ++c)
+      ld256<NC>(p + 8 * c, v[8 * c], v[8 * c + 1], v[8 * c + 2], v[8 * c + 3], v[8 * c + 4],
+                v[8 * c + 5], v[8 * c + 6], v[8 * c + 7]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c)
+      ld256<NC>(p + 4 * c, v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+  }
+}
+
 template <typename T, int K>
+__device__ __forceinline__ void st_chunks32(T* p, const T (&v)[K]) {
+  if constexpr (std::is_same<T, float>::value) {
+#pragma unroll
+    for (int c = 0; c < K / 8; ++c)
+      st256(p + 8 * c, v[8 * c], v[8 * c + 1], v[8 * c + 2], v[8 * c + 3], v[8 * c + 4],
+            v[8 * c + 5], v[8 * c + 6], v[8 * c + 7]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < K / 4; ++c) st256(p + 4 * c, v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+  }
+}
+
+// K values of T fill whole 32-byte chunks
+template <typename T, int K>
+constexpr bool node_is_32b() {
+  return (K * (int)sizeof(T)) % 32 == 0 &&
+         (std::is_same<T, float>::value || std::is_same<T, double>::value);
+}
+
+template <typename T, int K, bool Wide = false>
 __device__ __forceinline__ void ldv(const T* __restrict__ base, long long n,
                                     T (&v)[K]) {
   const T* p = base + n * K;
+  if constexpr (Wide && node_is_32b<T, K>()) {
+    if (aligned32(base)) {
+      ld_chunks32<false, T, K>(p, v);
+      return;
+    }
+  }
   if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
 #pragma unroll
     for (int c = 0; c < K / 4; ++c) {
@@ -105,10 +204,16 @@ __device__ __forceinline__ void ldv(const T* __restrict__ base, long long n,
 }
 
 // Read-only-path variant for arrays that no thread writes during the kernel.
-template <typename T, int K>
+template <typename T, int K, bool Wide = false>
 __device__ __forceinline__ void ldv_ro(const T* __restrict__ base, long long n,
                                        T (&v)[K]) {
   const T* p = base + n * K;
+  if constexpr (Wide && node_is_32b<T, K>()) {
+    if (aligned32(base)) {
+      ld_chunks32<true, T, K>(p, v);
+      return;
+    }
+  }
   if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
 #pragma unroll
     for (int c = 0; c < K / 4; ++c) {
@@ -135,10 +240,16 @@ __device__ __forceinline__ void ldv_ro(const T* __restrict__ base, long long n,
   }
 }
 
-template <typename T, int K>
+template <typename T, int K, bool Wide = false>
 __device__ __forceinline__ void stv(T* __restrict__ base, long long n,
                                     const T (&v)[K]) {
   T* p = base + n * K;
+  if constexpr (Wide && node_is_32b<T, K>()) {
+    if (aligned32(base)) {
+      st_chunks32<T, K>(p, v);
+      return;
+    }
+  }
   if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
 #pragma unroll
     for (int c = 0; c < K / 4; ++c)

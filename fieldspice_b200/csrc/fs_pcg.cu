@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     const uint8_t lab = label[n];
-    fs::stv<T, K>(x, n, zero);
-    fs::stv<T, K>(p, n, zero);
+    fs::stv<T, K, true>(x, n, zero);
+    fs::stv<T, K, true>(p, n, zero);
     if (lab == FS_LABEL_FIXED) {
-      fs::stv<T, K>(r, n, zero);
+      fs::stv<T, K, true>(r, n, zero);
       continue;
     }
     int i, j, k;
@@ -245,14 +245,14 @@ __global__ void __launch_bounds__(fs::kBlock)
         acc[K + t] += bs * bs;
         if (!warm) phi[n * K + t] = 0.0;
       }
-      fs::stv<T, K>(r, n, rv);
+      fs::stv<T, K, true>(r, n, rv);
     } else {
       // Solo: every coupled neighbour is fixed, so x = b / diag exactly
       // (poisson.py:559-564).  Pinned: coupled to nothing, x = 0 (:522).
 #pragma unroll
       for (int t = 0; t < K; ++t)
         phi[n * K + t] = (lab == FS_LABEL_SOLO) ? bres[t] / dg : 0.0;
-      fs::stv<T, K>(r, n, zero);
+      fs::stv<T, K, true>(r, n, zero);
     }
   }
   fs::block_partials<2 * K>(acc, partials);
@@ -328,18 +328,42 @@ struct TmaTile {
   static constexpr bool OK = B >= 16;                // TMA row >= 16 B
 };
 
+// A node's K values are NC 16-byte chunks.  A quarter-warp's 16-byte accesses
+// are served together; eight consecutive lanes that read chunk c of their
+// nodes, NC*16 bytes apart, span 8*NC*16 bytes and so meet each bank NC times
+// (with 32-byte nodes lanes 0 and 4 share banks).  Each lane therefore walks its node's chunks
+// in rotated order, (c + r) mod NC with r = (lane mod 8) * NC / 8, which puts
+// a quarter-warp's eight reads on all 32 banks.  The registers then hold the
+// chunks rotated: the per-node arithmetic does not care (the masses are the
+// same for every RHS), stores put each chunk back in its place, and the
+// per-RHS dot accumulators are un-rotated once at the end (`unrotate`).
 template <typename T, int K>
-__device__ __forceinline__ void ld_smem(const T* p, T (&v)[K]) {
-  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+struct NodeChunks {
+  static constexpr int B = K * (int)sizeof(T);
+  static constexpr bool VEC = B % 16 == 0;
+  static constexpr int NC = VEC ? B / 16 : 1;             // 1, 2, 4 or 8
+  static constexpr int W = VEC ? 16 / (int)sizeof(T) : K;  // values per chunk
+};
+
+template <typename T, int K>
+__device__ __forceinline__ int chunk_rot() {
+  constexpr int NC = NodeChunks<T, K>::NC;
+  return NC > 1 ? (((int)(threadIdx.x & 7) * NC / 8) & (NC - 1)) : 0;
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void ld_smem(const T* p, T (&v)[K], int r) {
+  using NCh = NodeChunks<T, K>;
+  if constexpr (NCh::VEC && std::is_same<T, float>::value) {
 #pragma unroll
-    for (int c = 0; c < K / 4; ++c) {
-      float4 t = reinterpret_cast<const float4*>(p)[c];
+    for (int c = 0; c < NCh::NC; ++c) {
+      const float4 t = reinterpret_cast<const float4*>(p)[(c + r) & (NCh::NC - 1)];
       v[4 * c] = t.x; v[4 * c + 1] = t.y; v[4 * c + 2] = t.z; v[4 * c + 3] = t.w;
     }
-  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+  } else if constexpr (NCh::VEC && std::is_same<T, double>::value) {
 #pragma unroll
-    for (int c = 0; c < K / 2; ++c) {
-      double2 t = reinterpret_cast<const double2*>(p)[c];
+    for (int c = 0; c < NCh::NC; ++c) {
+      const double2 t = reinterpret_cast<const double2*>(p)[(c + r) & (NCh::NC - 1)];
       v[2 * c] = t.x; v[2 * c + 1] = t.y;
     }
   } else {
@@ -348,20 +372,45 @@ __device__ __forceinline__ void ld_smem(const T* p, T (&v)[K]) {
   }
 }
 
+// Store a node's values held in rotated chunk order (shared or global memory).
 template <typename T, int K>
-__device__ __forceinline__ void st_smem(T* p, const T (&v)[K]) {
-  if constexpr (std::is_same<T, float>::value && K % 4 == 0) {
+__device__ __forceinline__ void st_rot(T* p, const T (&v)[K], int r) {
+  using NCh = NodeChunks<T, K>;
+  if constexpr (NCh::VEC && std::is_same<T, float>::value) {
 #pragma unroll
-    for (int c = 0; c < K / 4; ++c)
-      reinterpret_cast<float4*>(p)[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2],
-                                                    v[4 * c + 3]);
-  } else if constexpr (std::is_same<T, double>::value && K % 2 == 0) {
+    for (int c = 0; c < NCh::NC; ++c)
+      reinterpret_cast<float4*>(p)[(c + r) & (NCh::NC - 1)] =
+          make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+  } else if constexpr (NCh::VEC && std::is_same<T, double>::value) {
 #pragma unroll
-    for (int c = 0; c < K / 2; ++c)
-      reinterpret_cast<double2*>(p)[c] = make_double2(v[2 * c], v[2 * c + 1]);
+    for (int c = 0; c < NCh::NC; ++c)
+      reinterpret_cast<double2*>(p)[(c + r) & (NCh::NC - 1)] =
+          make_double2(v[2 * c], v[2 * c + 1]);
   } else {
 #pragma unroll
     for (int c = 0; c < K; ++c) p[c] = v[c];
+  }
+}
+
+// Per-node values or per-RHS accumulators held in rotated chunk order, back in
+// RHS order.
+template <typename T, int K, typename V>
+__device__ __forceinline__ void unrotate(V (&a)[K], int r) {
+  using NCh = NodeChunks<T, K>;
+  if constexpr (NCh::NC > 1) {
+    V o[K];
+#pragma unroll
+    for (int c = 0; c < NCh::NC; ++c) {
+#pragma unroll
+      for (int tc = 0; tc < NCh::NC; ++tc) {
+        if (((c + r) & (NCh::NC - 1)) == tc) {
+#pragma unroll
+          for (int e = 0; e < NCh::W; ++e) o[tc * NCh::W + e] = a[c * NCh::W + e];
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < K; ++t) a[t] = o[t];
   }
 }
 
@@ -432,8 +481,10 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
 #pragma unroll
   for (int t = 0; t < K; ++t) acc[t] = 0.0;
   const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  const int rot = chunk_rot<T, K>();
   long long ticket = 0;  // planes issued so far by this block (ring position)
   bool failed = false;
+  bool bad = false;
 
   while (u < u_end && !failed) {
     const long long col = u / d.nx;
@@ -469,14 +520,10 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
     for (int j = 0; j < nplanes; ++j) {
       const long long tk = ticket + j;
       const int s = (int)(tk % C::NS);
-      const bool ok = fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1),
-                                            kWaitBudget);
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
+      // One CTA barrier per plane: a wait that ran out is carried to it
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
       if (j >= 2) {
-        if (inb) {
+        if (inb && !bad) {
           const int x = xa - 2 + j;
           const long long n = ((long long)x * d.ny + y) * d.nz + z;
           const T* pm = ring + (int)((tk - 2) % C::NS) * BOXT;
@@ -485,33 +532,37 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
           const T mxm = nm0, mxp = nm1, mym = nm2, myp = nm3, mzm = nm4, mzp = nm5;
           if (x + 1 < xb) FS_LOAD_MASSES(x + 1);
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c);
+          ld_smem<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v);
+          ld_smem<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v);
+          ld_smem<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
             acc[t] += (double)c[t] * (double)qv[t];
           }
-          fs::stv<T, K>(q, n, qv);
+          st_rot<T, K>(q + n * K, qv, rot);
         }
-        __syncthreads();  // plane j-2 no longer read: its stage may refill
+        // plane j-2 no longer read: its stage may refill
+        if (__syncthreads_or(bad)) {
+          failed = true;
+          break;
+        }
         if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
       }
     }
@@ -530,6 +581,7 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
     __syncthreads();
   }
   (void)p;
+  unrotate<T, K>(acc, rot);
   finish_pq<T, K, TmaTile<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
@@ -590,10 +642,11 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
   const int tid = threadIdx.x;
   const int tz = tid % C::TZ, ty = tid / C::TZ;
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const long long total = (long long)nbz * nby * d.nx;
-  const long long per = (total + gridDim.x - 1) / gridDim.x;
-  long long u = (long long)blockIdx.x * per;
-  const long long u_end = min(u + per, total);
+  // column-planes in 32-bit: N / (TZ * TY) of them (the launch checks the bound)
+  const int total = nbz * nby * d.nx;
+  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
+  int u = (int)blockIdx.x * per;
+  const int u_end = min(u + per, total);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -603,19 +656,21 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
 #pragma unroll
   for (int t = 0; t < K; ++t) acc[t] = 0.0;
   const int cpos = (ty + 1) * C::HZ + (tz + 1);
-  long long ticket = 0;
+  const int rot = chunk_rot<T, K>();
+  int ticket = 0;
   bool failed = false;
+  bool bad = false;
   while (u < u_end && !failed) {
-    const long long col = u / d.nx;
-    const int xa = (int)(u % d.nx);
-    const int xb = (int)min((long long)d.nx, xa + (u_end - u));
-    const int bz = (int)(col % nbz), by = (int)(col / nbz);
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
     const int z0 = bz * C::TZ, y0 = by * C::TY;
     const int z = z0 + tz, y = y0 + ty;
     const bool inb = z < d.nz && y < d.ny;
     const int nplanes = (xb - xa) + 2;  // planes xa-1 .. xb
     auto issue = [&](int j) {
-      const int s = (int)((ticket + j) % C::NS);
+      const int s = (ticket + j) % C::NS;
       unsigned char* slot = base + s * C::SLOT;
       const int x = xa - 1 + j;
       fs::mbar_arrive_expect_tx(&bar[s], C::TX);
@@ -627,19 +682,16 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
     if (tid == 0)
       for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
     for (int j = 0; j < nplanes; ++j) {
-      const long long tk = ticket + j;
-      const int s = (int)(tk % C::NS);
-      const bool ok = fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      // One CTA barrier per plane: a wait that ran out is carried to it
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
       if (j >= 2) {
-        if (inb) {
+        if (inb && !bad) {
           const int x = xa - 2 + j;
           const long long n = ((long long)x * d.ny + y) * d.nz + z;
-          const unsigned char* sm = base + (int)((tk - 2) % C::NS) * C::SLOT;  // plane x-1
-          const unsigned char* sc = base + (int)((tk - 1) % C::NS) * C::SLOT;  // plane x
+          const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;  // plane x-1
+          const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;  // plane x
           const unsigned char* sp = base + s * C::SLOT;                        // plane x+1
           const T* pm = reinterpret_cast<const T*>(sm);
           const T* pc = reinterpret_cast<const T*>(sc);
@@ -653,33 +705,37 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
           const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
           const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c);
+          ld_smem<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v);
+          ld_smem<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v);
+          ld_smem<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
             acc[t] += (double)c[t] * (double)qv[t];
           }
-          fs::stv<T, K>(q, n, qv);
+          st_rot<T, K>(q + n * K, qv, rot);
         }
-        __syncthreads();  // plane j-2 no longer read: its stage may refill
+        // plane j-2 no longer read: its stage may refill
+        if (__syncthreads_or(bad)) {
+          failed = true;
+          break;
+        }
         if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
       }
     }
@@ -693,6 +749,7 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
     }
     __syncthreads();
   }
+  unrotate<T, K>(acc, rot);
   finish_pq<T, K, TmaTileM<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
@@ -773,6 +830,7 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
 #pragma unroll
   for (int t = 0; t < K; ++t) acc[t] = 0.0;
   const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  const int rot = chunk_rot<T, K>();
   long long ticket = 0, qc = 0;
   bool failed = false;
   while (u < u_end && !failed) {
@@ -825,31 +883,31 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
           const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
           const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c);
+          ld_smem<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v);
+          ld_smem<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v);
+          ld_smem<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v);
+          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v);
+          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v);
+          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
             acc[t] += (double)c[t] * (double)qv[t];
           }
-          st_smem<T, K>(qt + (ty * C::TZ + tz) * K, qv);
+          st_rot<T, K>(qt + (ty * C::TZ + tz) * K, qv, rot);
         }
         fence_proxy_async_smem();  // q tile writes -> visible to the bulk store
         __syncthreads();           // plane j-2 no longer read; q tile complete
@@ -872,6 +930,7 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
     __syncthreads();
   }
   if (tid == 0) bulk_wait_all();  // q written out before the CTA's shared memory goes
+  unrotate<T, K>(acc, rot);
   finish_pq<T, K, TmaTileS<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
@@ -887,8 +946,8 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     T rv[K], zv[K];
-    fs::ldv_ro<T, K>(r, n, rv);
-    fs::ldv_ro<T, K>(z, n, zv);
+    fs::ldv_ro<T, K, true>(r, n, rv);
+    fs::ldv_ro<T, K, true>(z, n, zv);
 #pragma unroll
     for (int t = 0; t < K; ++t) acc[t] += (double)rv[t] * (double)zv[t];
   }
@@ -940,9 +999,9 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     T rv[K], zv[K], qv[K];
-    fs::ldv_ro<T, K>(r, n, rv);
-    fs::ldv_ro<T, K>(z, n, zv);
-    fs::ldv_ro<T, K>(q, n, qv);
+    fs::ldv_ro<T, K, true>(r, n, rv);
+    fs::ldv_ro<T, K, true>(z, n, zv);
+    fs::ldv_ro<T, K, true>(q, n, qv);
 #pragma unroll
     for (int t = 0; t < K; ++t) {
       acc[t] += (double)rv[t] * (double)zv[t];
@@ -993,11 +1052,11 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     T rv[K], pv[K];
-    fs::ldv_ro<T, K>(r, n, rv);
-    fs::ldv_ro<T, K>(pold, n, pv);
+    fs::ldv_ro<T, K, true>(r, n, rv);
+    fs::ldv_ro<T, K, true>(pold, n, pv);
 #pragma unroll
     for (int t = 0; t < K; ++t) pv[t] = act[t] ? rv[t] + beta[t] * pv[t] : pv[t];
-    fs::stv<T, K>(pnew, n, pv);
+    fs::stv<T, K, true>(pnew, n, pv);
   }
 }
 
@@ -1060,18 +1119,18 @@ __global__ void __launch_bounds__(fs::kBlock)
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
        n += (long long)gridDim.x * blockDim.x) {
     T pv[K], qv[K], xv[K], rv[K];
-    fs::ldv_ro<T, K>(p, n, pv);
-    fs::ldv_ro<T, K>(q, n, qv);
-    fs::ldv<T, K>(x, n, xv);
-    fs::ldv<T, K>(r, n, rv);
+    fs::ldv_ro<T, K, true>(p, n, pv);
+    fs::ldv_ro<T, K, true>(q, n, qv);
+    fs::ldv<T, K, true>(x, n, xv);
+    fs::ldv<T, K, true>(r, n, rv);
 #pragma unroll
     for (int t = 0; t < K; ++t) {
       xv[t] += alpha[t] * pv[t];
       rv[t] -= alpha[t] * qv[t];
       acc[t] += (double)rv[t] * (double)rv[t];
     }
-    fs::stv<T, K>(x, n, xv);
-    fs::stv<T, K>(r, n, rv);
+    fs::stv<T, K, true>(x, n, xv);
+    fs::stv<T, K, true>(r, n, rv);
   }
   fs::block_partials<K>(acc, partials);
   if (fs::last_block(&ctl->tickets[kTicketUpdate])) {
@@ -1126,13 +1185,16 @@ __global__ void __launch_bounds__(fs::kBlock)
     const double s = s64[n];
     if (s == 0.0) continue;  // x~ is 0 off the free nodes
     T xv[K];
+    double ph[K];
     fs::ldv<T, K>(x, n, xv);
+    fs::ldv<double, K>(phi, n, ph);  // whole node: vector accesses
 #pragma unroll
     for (int t = 0; t < K; ++t)
       if (ru[t]) {
-        phi[n * K + t] += (double)xv[t] * s;
+        ph[t] += (double)xv[t] * s;
         xv[t] = (T)0;
       }
+    fs::stv<double, K>(phi, n, ph);
     fs::stv<T, K>(x, n, xv);
   }
 }
@@ -1263,13 +1325,16 @@ __global__ void k_finalize(Dims d, const uint8_t* __restrict__ label,
     if (label[n] != FS_LABEL_FREE) continue;
     const double s = s64[n];
     T xv[K];
+    double ph[K];
     fs::ldv<T, K>(x, n, xv);
+    fs::ldv<double, K>(phi, n, ph);  // whole node: vector accesses
 #pragma unroll
     for (int t = 0; t < K; ++t) {
-      phi[n * K + t] += (double)xv[t] * s;  // correction since the last fold
+      ph[t] += (double)xv[t] * s;  // correction since the last fold
       xv[t] = (T)0;
-      if (zero[t]) phi[n * K + t] = 0.0;
+      if (zero[t]) ph[t] = 0.0;
     }
+    fs::stv<double, K>(phi, n, ph);
     fs::stv<T, K>(x, n, xv);
   }
   if (fs::last_block(&ctl->tickets[kTicketFin])) {
@@ -1655,10 +1720,15 @@ struct Impl {
     {
       const char* sel = getenv("FS_STENCIL");
       const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
+      // k_stencil_tma_m counts its column-planes in 32 bits
+      using CM = TmaTileM<T, K>;
+      const bool fits32 = (long long)((P->d.nz + CM::TZ - 1) / CM::TZ) *
+                              ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx <
+                          (1LL << 30);
       P->autotune = 0;
       if (!C::OK || plain_stencil() || P->d.per) {  // only the cached-load kernel wraps
         P->stencil_kind = 0;
-      } else if (!mass_ok || (sel && strcmp(sel, "tma1") == 0)) {
+      } else if (!mass_ok || !fits32 || (sel && strcmp(sel, "tma1") == 0)) {
         P->stencil_kind = 1;
       } else if (sel && strcmp(sel, "tmas") == 0) {
         P->stencil_kind = 3;
