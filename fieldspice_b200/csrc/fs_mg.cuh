@@ -185,6 +185,121 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
   }
 }
 
+// ---- coarsest level: the whole Chebyshev solve in one launch -----------------
+// The coarsest level is small (a few thousand nodes), so its degree-32
+// Chebyshev solve is launch-bound as 32 grid-wide steps.  Here one block per
+// right-hand side runs every step: the level's iterate lives in shared memory
+// (its neighbours are other threads' nodes), b and the step direction d of a
+// thread's own nodes in registers, the equilibrated masses in shared memory.
+// Each step computes d = cd d + cr (b - A~ x), x += d for all nodes into
+// registers, then a barrier, the writes of x, another barrier; the arithmetic
+// and its order are k_mg_cheb's, so the result is the same.
+constexpr int kCoarseThreads = 1024;
+constexpr int kCoarseMaxDeg = 64;
+// nodes per thread (registers: b, d and the new x of each): levels up to 8192
+// nodes in FP32, 4096 in FP64
+template <typename T>
+constexpr int coarse_npt() {
+  return sizeof(T) == 4 ? 8 : 4;
+}
+
+template <typename T>
+struct CoarseCoef {
+  T cd[kCoarseMaxDeg], cr[kCoarseMaxDeg];
+};
+
+// Shared memory of k_mg_coarse for a level of n nodes (x and three mass arrays).
+template <typename T>
+constexpr size_t coarse_smem(long long n) {
+  return (size_t)n * sizeof(T) * 4;
+}
+
+constexpr size_t kCoarseSmemCap = 160 * 1024;
+
+// Whether a coarsest level of n nodes and a degree fit k_mg_coarse.
+template <typename T>
+constexpr bool coarse_fits(long long n, int deg) {
+  return n >= 1 && n <= (long long)kCoarseThreads * coarse_npt<T>() && deg >= 1 &&
+         deg <= kCoarseMaxDeg && coarse_smem<T>(n) <= kCoarseSmemCap;
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kCoarseThreads)
+    k_mg_coarse(Dims d, const T* __restrict__ ex, const T* __restrict__ ey,
+                const T* __restrict__ ez, const T* __restrict__ b, T* __restrict__ xout,
+                const CoarseCoef<T> coef, int deg, const int* __restrict__ done) {
+  if (*done) return;
+  extern __shared__ unsigned char smem_raw[];
+  const int N = (int)d.N;
+  T* xs = reinterpret_cast<T*>(smem_raw);
+  T* mx = xs + N;
+  T* my = mx + N;
+  T* mz = my + N;
+  const int col = blockIdx.x;  // right-hand side
+  for (int n = threadIdx.x; n < N; n += kCoarseThreads) {
+    mx[n] = ex[n];
+    my[n] = ey[n];
+    mz[n] = ez[n];
+  }
+  // own nodes n = threadIdx.x + e * kCoarseThreads: b, d and the valid-neighbour mask
+  constexpr int NPT = coarse_npt<T>();
+  T bv[NPT], dv[NPT], xn[NPT];
+  int nb[NPT];
+#pragma unroll
+  for (int e = 0; e < NPT; ++e) {
+    const int n = threadIdx.x + e * kCoarseThreads;
+    bv[e] = (T)0;
+    dv[e] = (T)0;
+    nb[e] = 0;
+    if (n < N) {
+      bv[e] = b[(long long)n * K + col];
+      int i, j, k;
+      node_ijk(d, n, i, j, k);
+      nb[e] = (i > 0) | ((i < d.nx - 1) << 1) | ((j > 0) << 2) | ((j < d.ny - 1) << 3) |
+              ((k > 0) << 4) | ((k < d.nz - 1) << 5);
+    }
+  }
+  const int sx = (int)d.sx, sy = (int)d.sy;
+  for (int step = 0; step < deg; ++step) {
+    const T cd = coef.cd[step], cr = coef.cr[step];
+#pragma unroll
+    for (int e = 0; e < NPT; ++e) {
+      const int n = threadIdx.x + e * kCoarseThreads;
+      if (n >= N) continue;
+      T r, xo;
+      if (step == 0) {  // x_in = 0
+        r = bv[e];
+        xo = (T)0;
+      } else {
+        const int m = nb[e];
+        T ax = xs[n];
+        if (m & 1) ax -= mx[n - sx] * xs[n - sx];
+        if (m & 2) ax -= mx[n] * xs[n + sx];
+        if (m & 4) ax -= my[n - sy] * xs[n - sy];
+        if (m & 8) ax -= my[n] * xs[n + sy];
+        if (m & 16) ax -= mz[n - 1] * xs[n - 1];
+        if (m & 32) ax -= mz[n] * xs[n + 1];
+        xo = xs[n];
+        r = bv[e] - ax;
+      }
+      dv[e] = cd != (T)0 ? cd * dv[e] + cr * r : cr * r;
+      xn[e] = xo + dv[e];
+    }
+    __syncthreads();  // every read of x (and, first time, of the masses) done
+#pragma unroll
+    for (int e = 0; e < NPT; ++e) {
+      const int n = threadIdx.x + e * kCoarseThreads;
+      if (n < N) xs[n] = xn[e];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int e = 0; e < NPT; ++e) {
+    const int n = threadIdx.x + e * kCoarseThreads;
+    if (n < N) xout[(long long)n * K + col] = xn[e];
+  }
+}
+
 // res = b - A~ x
 template <typename T, int K>
 __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())

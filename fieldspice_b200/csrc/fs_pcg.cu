@@ -1890,6 +1890,10 @@ struct Impl {
   }
   // ---- multigrid ----------------------------------------------------------
   static void mg_setup(fs_pcg_plan* P, cudaStream_t s) {
+    // the cap every coarsest level that fits k_mg_coarse stays under (the
+    // attribute is process-wide: plans of other sizes share it)
+    cudaFuncSetAttribute(fs::k_mg_coarse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fs::kCoarseSmemCap);
     MgLevel& L0 = P->lev[0];
     L0.em[0] = P->ex;
     L0.em[1] = P->ey;
@@ -1989,6 +1993,18 @@ struct Impl {
       cur = 1;
       rfine = (const T*)L.dv;
       *nl += 2;
+    } else if (last && fs::coarse_fits<T>(L.d.N, deg)) {
+      // the whole coarsest-level solve in one launch, one block per RHS
+      fs::CoarseCoef<T> coef;
+      for (int k = 0; k < deg; ++k) {
+        coef.cd[k] = (T)cd[k];
+        coef.cr[k] = (T)cr[k];
+      }
+      cur = (deg - 1) % 2;  // the buffer the step-by-step solve ends in
+      if (!dry)
+        fs::k_mg_coarse<T, K><<<K, fs::kCoarseThreads, fs::coarse_smem<T>(L.d.N), s>>>(
+            L.d, e0, e1, e2, b, (T*)L.x[cur], coef, deg, done);
+      ++*nl;
     } else {
       for (int k = 0; k < deg; ++k) {  // pre-smoothing (or coarse solve) from 0
         const int out = k == 0 ? 0 : 1 - cur;
