@@ -934,6 +934,245 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
   finish_pq<T, K, TmaTileS<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
+// ---- multigrid: degree-2 pre-smoothing from 0 in one pass over b ------------------
+// k_mg_pre0 then k_mg_pre1 compute, from b alone,
+//   x1 = c0 b,  r1 = b - c0 A~b,  d1 = cd x1 + cr r1,  x2 = x1 + d1,  r2 = r1 - A~d1,
+// writing x1 and r1 (2 vectors) and reading them back at every node and its six
+// neighbours.  Here one x-march does both stencils: per x-plane one thread issues
+// TMA loads (no multicast) of the b tile with a two-node halo in y and z and of the
+// three equilibrated mass tiles into an NS-deep ring; stage 1 forms d1 on the tile
+// plus a one-node halo (the thread of each interior node, and one more node for 84
+// of the threads on the halo ring) into a three-plane ring of d1 tiles; stage 2,
+// one plane behind, forms A~d1 at the interior from that ring and from the d1, r1,
+// x1 and masses of its own node kept in registers.  b is read once and only x2,
+// r2 are written: 3 vectors + the masses per node instead of 7 + twice the masses.
+// The arithmetic, and its order, is that of the two kernels.  Out-of-range boxes
+// read zero, which is the wall (missing edges) and a zero right-hand side.
+// One CTA barrier per plane: the d1 ring has three slots, so stage 1 of plane q+1
+// writes the slot that stage 2 of plane q-2 read before the previous barrier.
+template <typename T, int K>
+struct PreTile {
+  static constexpr int B = K * (int)sizeof(T);
+  static constexpr int MB = (int)sizeof(T);
+  static constexpr int TZ = 32, TY = 8;
+  static constexpr int NS = 4;                      // input planes in the ring
+  static constexpr int IZ = TZ + 4, IY = TY + 4;    // b tile: two-node halo
+  static constexpr int RZ = TZ + 2, RY = TY + 2;    // d1 tile: one-node halo
+  static constexpr int ZP = 16 / MB;                // mass boxes start at z0 - ZP
+  static constexpr int WZ = TZ + 2 * ZP;            // mass box width (16-byte rows)
+  static constexpr int WY = TY + 3;                 // mass box rows from y0 - 2
+  static constexpr int BOXB = IZ * IY * B;
+  static constexpr int MBOX = WZ * WY * MB;
+  static constexpr int O_M0 = (BOXB + 127) / 128 * 128;
+  static constexpr int MBOXP = (MBOX + 127) / 128 * 128;
+  static constexpr int SLOT = O_M0 + 3 * MBOXP;
+  static constexpr uint32_t TX = (uint32_t)(BOXB + 3 * MBOX);  // bytes per plane
+  static constexpr int UPL = RZ * RY * B;           // one d1 plane
+  static constexpr int UPLP = (UPL + 127) / 128 * 128;
+  static constexpr int O_U = NS * SLOT;
+  static constexpr int O_BAR = O_U + 3 * UPLP;
+  static constexpr int THREADS = TZ * TY;
+  static constexpr int NHALO = 2 * RZ + 2 * (RY - 2);
+  static constexpr size_t SMEM = (size_t)O_BAR + NS * 8 + 128;
+  // 16..32-byte nodes: TMA rows of at least 16 bytes, two CTAs per SM
+  static constexpr bool OK = B >= 16 && B <= 32 && NHALO <= THREADS;
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(PreTile<T, K>::THREADS, 2)
+    k_mg_pre_fused(Dims d, const __grid_constant__ CUtensorMap tm_b,
+                   const __grid_constant__ CUtensorMap tm_ex,
+                   const __grid_constant__ CUtensorMap tm_ey,
+                   const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ x2,
+                   T* __restrict__ r2, T c0, T cd, T cr, const int* __restrict__ done,
+                   int* __restrict__ err) {
+  using C = PreTile<T, K>;
+  if (*done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::O_BAR);
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int rot = chunk_rot<T, K>();
+  // the halo-ring node of this thread (tid < NHALO), in d1-tile coordinates
+  int hz = 0, hy = 0;
+  if (tid < 2 * C::RZ) {
+    hz = tid % C::RZ;
+    hy = tid < C::RZ ? 0 : C::RY - 1;
+  } else if (tid < C::NHALO) {
+    const int k2 = tid - 2 * C::RZ;
+    hy = 1 + k2 / 2;
+    hz = (k2 & 1) ? C::RZ - 1 : 0;
+  }
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  // column-planes in 32 bits (the launch checks the bound)
+  const int total = nbz * nby * d.nx;
+  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
+  int u = (int)blockIdx.x * per;
+  const int u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  int ticket = 0, uc = 0;
+  bool failed = false, bad = false;
+  while (u < u_end && !failed) {
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nin = (xb - xa) + 4;  // input planes xa-2 .. xb+1
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % C::NS;
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 2 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_b, &bar[s], 0, z0 - 2, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nin; ++j) issue(j);
+    // own interior node: d1 of planes q-2 (dA), q-1 (dB), q (dC); r1, x1 and the
+    // six masses of planes q-1 (B) and q (C)
+    T dA[K], dB[K], dC[K], r1B[K], r1C[K], x1B[K], x1C[K];
+    T mB[6], mC[6];
+    for (int j = 0; j < nin; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (j < 2) continue;
+      // ---- stage 1: d1 on plane q = xa - 3 + j (input planes q-1, q, q+1)
+      const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;
+      const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;
+      const unsigned char* sp = base + s * C::SLOT;
+      T* up = reinterpret_cast<T*>(base + C::O_U + (uc % 3) * C::UPLP);
+      if (!bad) {
+        const T* bm = reinterpret_cast<const T*>(sm);
+        const T* bc = reinterpret_cast<const T*>(sc);
+        const T* bp = reinterpret_cast<const T*>(sp);
+        const T* exm = reinterpret_cast<const T*>(sm + C::O_M0);
+        const T* exc = reinterpret_cast<const T*>(sc + C::O_M0);
+        const T* eyc = reinterpret_cast<const T*>(sc + C::O_M0 + C::MBOXP);
+        const T* ezc = reinterpret_cast<const T*>(sc + C::O_M0 + 2 * C::MBOXP);
+        // d1 at d1-tile node (rz, ry); the interior node also keeps r1, x1, masses
+        auto stage1 = [&](int rz, int ry, bool own) {
+          const int bi = (ry + 1) * C::IZ + (rz + 1);        // b tile
+          const int mi = (ry + 1) * C::WZ + (rz - 1 + C::ZP);  // mass tiles
+          const T mxm = exm[mi], mxp = exc[mi];
+          const T mym = eyc[mi - C::WZ], myp = eyc[mi];
+          const T mzm = ezc[mi - 1], mzp = ezc[mi];
+          T bv[K], ab[K], v[K];
+          ld_smem<T, K>(bc + bi * K, bv, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] = bv[t];
+          ld_smem<T, K>(bm + bi * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= mxm * v[t];
+          ld_smem<T, K>(bp + bi * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= mxp * v[t];
+          ld_smem<T, K>(bc + (bi - C::IZ) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= mym * v[t];
+          ld_smem<T, K>(bc + (bi + C::IZ) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= myp * v[t];
+          ld_smem<T, K>(bc + (bi - 1) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= mzm * v[t];
+          ld_smem<T, K>(bc + (bi + 1) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ab[t] -= mzp * v[t];
+          T dv[K];
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            const T xo = c0 * bv[t];          // k_mg_pre0
+            const T rv = bv[t] - c0 * ab[t];
+            dv[t] = cd * xo + cr * rv;        // k_mg_pre1
+            if (own) {
+              x1C[t] = xo;
+              r1C[t] = rv;
+              dC[t] = dv[t];
+            }
+          }
+          st_rot<T, K>(up + (ry * C::RZ + rz) * K, dv, rot);
+          if (own) {
+            mC[0] = mxm; mC[1] = mxp; mC[2] = mym; mC[3] = myp; mC[4] = mzm; mC[5] = mzp;
+          }
+        };
+        stage1(tz + 1, ty + 1, true);
+        if (tid < C::NHALO) stage1(hz, hy, false);
+      }
+      ++uc;
+      // d1 of plane q complete; input plane q-1 no longer read: its stage may refill
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0 && j - 2 + C::NS < nin) issue(j - 2 + C::NS);
+      // ---- stage 2: plane o = q - 1 = xa - 4 + j (d1 planes o-1, o, o+1)
+      if (j >= 4 && inb) {
+        const int x = xa - 4 + j;
+        const long long n = ((long long)x * d.ny + y) * d.nz + z;
+        const T* uo = reinterpret_cast<const T*>(base + C::O_U + ((uc - 2) % 3) * C::UPLP);
+        const int ui = (ty + 1) * C::RZ + (tz + 1);
+        T ad[K], v[K];
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+          ad[t] = dB[t];
+          ad[t] -= mB[0] * dA[t];
+        }
+#pragma unroll
+        for (int t = 0; t < K; ++t) ad[t] -= mB[1] * dC[t];
+        ld_smem<T, K>(uo + (ui - C::RZ) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ad[t] -= mB[2] * v[t];
+        ld_smem<T, K>(uo + (ui + C::RZ) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ad[t] -= mB[3] * v[t];
+        ld_smem<T, K>(uo + (ui - 1) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ad[t] -= mB[4] * v[t];
+        ld_smem<T, K>(uo + (ui + 1) * K, v, rot);
+        T xo[K], ro[K];
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+          ad[t] -= mB[5] * v[t];
+          xo[t] = x1B[t] + dB[t];
+          ro[t] = r1B[t] - ad[t];
+        }
+        st_rot<T, K>(x2 + n * K, xo, rot);
+        st_rot<T, K>(r2 + n * K, ro, rot);
+      }
+      // shift the own-node pipeline by one plane
+#pragma unroll
+      for (int t = 0; t < K; ++t) {
+        dA[t] = dB[t];
+        dB[t] = dC[t];
+        r1B[t] = r1C[t];
+        x1B[t] = x1C[t];
+      }
+#pragma unroll
+      for (int e = 0; e < 6; ++e) mB[e] = mC[e];
+    }
+    ticket += nin;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      *err = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+}
+
 // ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
@@ -1894,6 +2133,7 @@ struct Impl {
     // attribute is process-wide: plans of other sizes share it)
     cudaFuncSetAttribute(fs::k_mg_coarse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fs::kCoarseSmemCap);
+    pre_fused_setup();
     MgLevel& L0 = P->lev[0];
     L0.em[0] = P->ex;
     L0.em[1] = P->ey;
@@ -1967,6 +2207,84 @@ struct Impl {
     }
     return vcycle_plain(P, l, b, s, nl, dry);
   }
+  // Whether a level's degree-2 pre-smoothing runs as the fused single pass
+  // (k_mg_pre_fused); FS_MG_PRE=plain keeps the two-kernel form.
+  static bool pre_fused_ok(const MgLevel& L) {
+    using CP = PreTile<T, K>;
+    if constexpr (!CP::OK) {
+      return false;
+    } else {
+      const char* sel = getenv("FS_MG_PRE");
+      if (sel && strcmp(sel, "plain") == 0) return false;
+      if (((long long)L.d.nz * (long long)sizeof(T)) % 16 != 0) return false;  // mass rows
+      const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
+                             ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
+      return cols < (1LL << 30) && pre_per_sm() > 0;
+    }
+  }
+  // Resident k_mg_pre_fused blocks per SM (set with the shared-memory limit
+  // when a plan builds its hierarchy; 0 = the kernel cannot run).
+  static int& pre_per_sm() {
+    static int v = 0;
+    return v;
+  }
+  static void pre_fused_setup() {
+    using CP = PreTile<T, K>;
+    if constexpr (CP::OK) {
+      if (pre_per_sm() > 0) return;
+      if (cudaFuncSetAttribute(k_mg_pre_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)CP::SMEM) != cudaSuccess)
+        return;
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_pre_fused<T, K>,
+                                                        CP::THREADS, CP::SMEM) == cudaSuccess)
+        pre_per_sm() = per_sm;
+    }
+  }
+  // Encode the b and mass tensor maps of level L and launch k_mg_pre_fused
+  // (x2 into x[1], r2 into dv); false if a map cannot be made.
+  static bool launch_pre_fused(fs_pcg_plan* P, MgLevel& L, const T* b, T c0, T cd, T cr,
+                               cudaStream_t s) {
+    using CP = PreTile<T, K>;
+    if constexpr (!CP::OK) {
+      return false;
+    } else {
+      auto encode = encode_fn();
+      if (!encode) return false;
+      const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+      const cuuint64_t Bn = CP::B, MB = sizeof(T);
+      CUtensorMap tb, tm[3];
+      cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
+                            (cuuint64_t)L.d.nx};
+      cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
+      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)CP::IZ, (cuuint32_t)CP::IY, 1};
+      cuuint32_t es[4] = {1, 1, 1, 1};
+      if (encode(&tb, dt, 4, (void*)b, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+      cuuint64_t mdims[3] = {(cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
+      cuuint64_t mstr[2] = {MB * L.d.nz, MB * L.d.nz * L.d.ny};
+      cuuint32_t mbox[3] = {(cuuint32_t)CP::WZ, (cuuint32_t)CP::WY, 1};
+      for (int m = 0; m < 3; ++m)
+        if (encode(&tm[m], dt, 3, L.em[m], mdims, mstr, mbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+          return false;
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
+                             ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
+      long long g = (long long)sms * pre_per_sm();
+      if (g > cols) g = cols;
+      k_mg_pre_fused<T, K><<<(int)g, CP::THREADS, CP::SMEM, s>>>(
+          L.d, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
+          &P->ctl->error);
+      return true;
+    }
+  }
   static int vcycle_plain(fs_pcg_plan* P, int l, const T* b, cudaStream_t s,
                           long long* nl, bool dry = false) {
     MgLevel& L = P->lev[l];
@@ -1982,7 +2300,20 @@ struct Impl {
     // residual in dv); otherwise Chebyshev steps then a residual pass.
     const bool resform = !last && deg == 2;
     const T* rfine = (const T*)L.res;
-    if (resform) {
+    if (resform && pre_fused_ok(L)) {
+      // x2 -> x[1], r2 -> dv in one pass over b; the two-kernel form if the
+      // tensor maps cannot be made for these buffers
+      if (!dry && !launch_pre_fused(P, L, b, (T)cr[0], (T)cd[1], (T)cr[1], s)) {
+        fs::k_mg_pre0<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, b, (T*)L.x[0], (T*)L.res, (T)cr[0], done);
+        fs::k_mg_pre1<T, K><<<g, fs::kBlock, 0, s>>>(
+            L.d, e0, e1, e2, (const T*)L.x[0], (const T*)L.res, (T*)L.x[1],
+            (T*)L.dv, (T)cd[1], (T)cr[1], done);
+      }
+      cur = 1;
+      rfine = (const T*)L.dv;
+      *nl += 1;
+    } else if (resform) {
       if (!dry) {
         fs::k_mg_pre0<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, b, (T*)L.x[0], (T*)L.res, (T)cr[0], done);
