@@ -352,7 +352,7 @@ __device__ __forceinline__ int chunk_rot() {
 }
 
 template <typename T, int K>
-__device__ __forceinline__ void ld_smem(const T* p, T (&v)[K], int r) {
+__device__ __forceinline__ void ld_rot(const T* p, T (&v)[K], int r) {
   using NCh = NodeChunks<T, K>;
   if constexpr (NCh::VEC && std::is_same<T, float>::value) {
 #pragma unroll
@@ -372,7 +372,8 @@ __device__ __forceinline__ void ld_smem(const T* p, T (&v)[K], int r) {
   }
 }
 
-// Store a node's values held in rotated chunk order (shared or global memory).
+// Load (ld_rot) or store (st_rot) a node's values in rotated chunk order, from
+// or to shared or global memory (generic addressing).
 template <typename T, int K>
 __device__ __forceinline__ void st_rot(T* p, const T (&v)[K], int r) {
   using NCh = NodeChunks<T, K>;
@@ -532,25 +533,25 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
           const T mxm = nm0, mxp = nm1, mym = nm2, myp = nm3, mzm = nm4, mzp = nm5;
           if (x + 1 < xb) FS_LOAD_MASSES(x + 1);
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c, rot);
+          ld_rot<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v, rot);
+          ld_rot<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v, rot);
+          ld_rot<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
@@ -705,25 +706,25 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
           const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
           const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c, rot);
+          ld_rot<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v, rot);
+          ld_rot<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v, rot);
+          ld_rot<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
@@ -883,25 +884,25 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
           const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
           const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
           T c[K], v[K], qv[K];
-          ld_smem<T, K>(pc + cpos * K, c, rot);
+          ld_rot<T, K>(pc + cpos * K, c, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] = c[t];
-          ld_smem<T, K>(pm + cpos * K, v, rot);
+          ld_rot<T, K>(pm + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
-          ld_smem<T, K>(pp + cpos * K, v, rot);
+          ld_rot<T, K>(pp + cpos * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
-          ld_smem<T, K>(pc + (cpos - C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
-          ld_smem<T, K>(pc + (cpos + C::HZ) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + C::HZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
-          ld_smem<T, K>(pc + (cpos - 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
-          ld_smem<T, K>(pc + (cpos + 1) * K, v, rot);
+          ld_rot<T, K>(pc + (cpos + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) {
             qv[t] -= mzp * v[t];
@@ -951,7 +952,7 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
 // One CTA barrier per plane: the d1 ring has three slots, so stage 1 of plane q+1
 // writes the slot that stage 2 of plane q-2 read before the previous barrier.
 template <typename T, int K>
-struct PreTile {
+struct SmoothTile {
   static constexpr int B = K * (int)sizeof(T);
   static constexpr int MB = (int)sizeof(T);
   static constexpr int TZ = 32, TY = 8;
@@ -979,14 +980,14 @@ struct PreTile {
 };
 
 template <typename T, int K>
-__global__ void __launch_bounds__(PreTile<T, K>::THREADS, 2)
+__global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
     k_mg_pre_fused(Dims d, const __grid_constant__ CUtensorMap tm_b,
                    const __grid_constant__ CUtensorMap tm_ex,
                    const __grid_constant__ CUtensorMap tm_ey,
                    const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ x2,
                    T* __restrict__ r2, T c0, T cd, T cr, const int* __restrict__ done,
                    int* __restrict__ err) {
-  using C = PreTile<T, K>;
+  using C = SmoothTile<T, K>;
   if (*done) return;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -1068,25 +1069,25 @@ __global__ void __launch_bounds__(PreTile<T, K>::THREADS, 2)
           const T mym = eyc[mi - C::WZ], myp = eyc[mi];
           const T mzm = ezc[mi - 1], mzp = ezc[mi];
           T bv[K], ab[K], v[K];
-          ld_smem<T, K>(bc + bi * K, bv, rot);
+          ld_rot<T, K>(bc + bi * K, bv, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] = bv[t];
-          ld_smem<T, K>(bm + bi * K, v, rot);
+          ld_rot<T, K>(bm + bi * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= mxm * v[t];
-          ld_smem<T, K>(bp + bi * K, v, rot);
+          ld_rot<T, K>(bp + bi * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= mxp * v[t];
-          ld_smem<T, K>(bc + (bi - C::IZ) * K, v, rot);
+          ld_rot<T, K>(bc + (bi - C::IZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= mym * v[t];
-          ld_smem<T, K>(bc + (bi + C::IZ) * K, v, rot);
+          ld_rot<T, K>(bc + (bi + C::IZ) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= myp * v[t];
-          ld_smem<T, K>(bc + (bi - 1) * K, v, rot);
+          ld_rot<T, K>(bc + (bi - 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= mzm * v[t];
-          ld_smem<T, K>(bc + (bi + 1) * K, v, rot);
+          ld_rot<T, K>(bc + (bi + 1) * K, v, rot);
 #pragma unroll
           for (int t = 0; t < K; ++t) ab[t] -= mzp * v[t];
           T dv[K];
@@ -1130,16 +1131,16 @@ __global__ void __launch_bounds__(PreTile<T, K>::THREADS, 2)
         }
 #pragma unroll
         for (int t = 0; t < K; ++t) ad[t] -= mB[1] * dC[t];
-        ld_smem<T, K>(uo + (ui - C::RZ) * K, v, rot);
+        ld_rot<T, K>(uo + (ui - C::RZ) * K, v, rot);
 #pragma unroll
         for (int t = 0; t < K; ++t) ad[t] -= mB[2] * v[t];
-        ld_smem<T, K>(uo + (ui + C::RZ) * K, v, rot);
+        ld_rot<T, K>(uo + (ui + C::RZ) * K, v, rot);
 #pragma unroll
         for (int t = 0; t < K; ++t) ad[t] -= mB[3] * v[t];
-        ld_smem<T, K>(uo + (ui - 1) * K, v, rot);
+        ld_rot<T, K>(uo + (ui - 1) * K, v, rot);
 #pragma unroll
         for (int t = 0; t < K; ++t) ad[t] -= mB[4] * v[t];
-        ld_smem<T, K>(uo + (ui + 1) * K, v, rot);
+        ld_rot<T, K>(uo + (ui + 1) * K, v, rot);
         T xo[K], ro[K];
 #pragma unroll
         for (int t = 0; t < K; ++t) {
@@ -1157,6 +1158,211 @@ __global__ void __launch_bounds__(PreTile<T, K>::THREADS, 2)
         dB[t] = dC[t];
         r1B[t] = r1C[t];
         x1B[t] = x1C[t];
+      }
+#pragma unroll
+      for (int e = 0; e < 6; ++e) mB[e] = mC[e];
+    }
+    ticket += nin;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      *err = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+}
+
+// ---- multigrid: degree-2 post-smoothing in one pass ------------------------------
+// k_mg_residual then k_mg_post2 compute r0 = b - A~x (written, then read back at
+// every node and its six neighbours) and xout = x + alpha r0 + beta A~r0.  Here
+// one x-march does both, with the tiles of k_mg_pre_fused: x with a two-node
+// halo and the three mass tiles by TMA, r0 on the tile plus a one-node halo into
+// a three-plane ring (stage 1), A~r0 one plane behind at the interior (stage 2)
+// from that ring and from the r0, x and masses of the thread's own node kept in
+// registers.  b is only needed at the node itself: a plain load.  x and b are
+// read once and only xout is written: 3 vectors + the masses per node instead of
+// 6 + twice the masses.  The arithmetic, and its order, is that of the two
+// kernels.
+template <typename T, int K>
+__global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
+    k_mg_post_fused(Dims d, const __grid_constant__ CUtensorMap tm_x,
+                    const __grid_constant__ CUtensorMap tm_ex,
+                    const __grid_constant__ CUtensorMap tm_ey,
+                    const __grid_constant__ CUtensorMap tm_ez, const T* __restrict__ b,
+                    T* __restrict__ xout, T alpha, T beta, const int* __restrict__ done,
+                    int* __restrict__ err) {
+  using C = SmoothTile<T, K>;
+  if (*done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::O_BAR);
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int rot = chunk_rot<T, K>();
+  int hz = 0, hy = 0;  // the halo-ring node of this thread (tid < NHALO)
+  if (tid < 2 * C::RZ) {
+    hz = tid % C::RZ;
+    hy = tid < C::RZ ? 0 : C::RY - 1;
+  } else if (tid < C::NHALO) {
+    const int k2 = tid - 2 * C::RZ;
+    hy = 1 + k2 / 2;
+    hz = (k2 & 1) ? C::RZ - 1 : 0;
+  }
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const int total = nbz * nby * d.nx;
+  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
+  int u = (int)blockIdx.x * per;
+  const int u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  int ticket = 0, uc = 0;
+  bool failed = false, bad = false;
+  while (u < u_end && !failed) {
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nin = (xb - xa) + 4;  // input planes xa-2 .. xb+1
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % C::NS;
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 2 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_x, &bar[s], 0, z0 - 2, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nin; ++j) issue(j);
+    // own interior node: r0 of planes q-2 (rA), q-1 (rB), q (rC); x and the six
+    // masses of planes q-1 (B) and q (C)
+    T rA[K], rB[K], rC[K], xB[K], xC[K];
+    T mB[6], mC[6];
+    for (int j = 0; j < nin; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (j < 2) continue;
+      // ---- stage 1: r0 on plane q = xa - 3 + j (input planes q-1, q, q+1)
+      const int q = xa - 3 + j;
+      const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;
+      const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;
+      const unsigned char* sp = base + s * C::SLOT;
+      T* up = reinterpret_cast<T*>(base + C::O_U + (uc % 3) * C::UPLP);
+      if (!bad) {
+        const T* vm = reinterpret_cast<const T*>(sm);
+        const T* vc = reinterpret_cast<const T*>(sc);
+        const T* vp = reinterpret_cast<const T*>(sp);
+        const T* exm = reinterpret_cast<const T*>(sm + C::O_M0);
+        const T* exc = reinterpret_cast<const T*>(sc + C::O_M0);
+        const T* eyc = reinterpret_cast<const T*>(sc + C::O_M0 + C::MBOXP);
+        const T* ezc = reinterpret_cast<const T*>(sc + C::O_M0 + 2 * C::MBOXP);
+        auto stage1 = [&](int rz, int ry, bool own) {
+          const int bi = (ry + 1) * C::IZ + (rz + 1);
+          const int mi = (ry + 1) * C::WZ + (rz - 1 + C::ZP);
+          const T mxm = exm[mi], mxp = exc[mi];
+          const T mym = eyc[mi - C::WZ], myp = eyc[mi];
+          const T mzm = ezc[mi - 1], mzp = ezc[mi];
+          T xv[K], ax[K], v[K], bv[K];
+          // b at the node itself (0 off the grid, where x and the masses are 0 too)
+          const int gz = z0 - 1 + rz, gy = y0 - 1 + ry;
+          if (gz >= 0 && gz < d.nz && gy >= 0 && gy < d.ny && q >= 0 && q < d.nx) {
+            ld_rot<T, K>(b + (((long long)q * d.ny + gy) * d.nz + gz) * K, bv, rot);
+          } else {
+#pragma unroll
+            for (int t = 0; t < K; ++t) bv[t] = (T)0;
+          }
+          ld_rot<T, K>(vc + bi * K, xv, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] = xv[t];
+          ld_rot<T, K>(vm + bi * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] -= mxm * v[t];
+          ld_rot<T, K>(vp + bi * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] -= mxp * v[t];
+          ld_rot<T, K>(vc + (bi - C::IZ) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] -= mym * v[t];
+          ld_rot<T, K>(vc + (bi + C::IZ) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] -= myp * v[t];
+          ld_rot<T, K>(vc + (bi - 1) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) ax[t] -= mzm * v[t];
+          ld_rot<T, K>(vc + (bi + 1) * K, v, rot);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            ax[t] -= mzp * v[t];
+            bv[t] -= ax[t];  // r0, k_mg_residual
+          }
+          st_rot<T, K>(up + (ry * C::RZ + rz) * K, bv, rot);
+          if (own) {
+#pragma unroll
+            for (int t = 0; t < K; ++t) {
+              rC[t] = bv[t];
+              xC[t] = xv[t];
+            }
+            mC[0] = mxm; mC[1] = mxp; mC[2] = mym; mC[3] = myp; mC[4] = mzm; mC[5] = mzp;
+          }
+        };
+        stage1(tz + 1, ty + 1, true);
+        if (tid < C::NHALO) stage1(hz, hy, false);
+      }
+      ++uc;
+      // r0 of plane q complete; input plane q-1 no longer read: its stage may refill
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0 && j - 2 + C::NS < nin) issue(j - 2 + C::NS);
+      // ---- stage 2: plane o = q - 1 (r0 planes o-1, o, o+1), k_mg_post2
+      if (j >= 4 && inb) {
+        const int x = q - 1;
+        const long long n = ((long long)x * d.ny + y) * d.nz + z;
+        const T* uo = reinterpret_cast<const T*>(base + C::O_U + ((uc - 2) % 3) * C::UPLP);
+        const int ui = (ty + 1) * C::RZ + (tz + 1);
+        T ar[K], v[K];
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+          ar[t] = rB[t];
+          ar[t] -= mB[0] * rA[t];
+        }
+#pragma unroll
+        for (int t = 0; t < K; ++t) ar[t] -= mB[1] * rC[t];
+        ld_rot<T, K>(uo + (ui - C::RZ) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ar[t] -= mB[2] * v[t];
+        ld_rot<T, K>(uo + (ui + C::RZ) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ar[t] -= mB[3] * v[t];
+        ld_rot<T, K>(uo + (ui - 1) * K, v, rot);
+#pragma unroll
+        for (int t = 0; t < K; ++t) ar[t] -= mB[4] * v[t];
+        ld_rot<T, K>(uo + (ui + 1) * K, v, rot);
+        T xo[K];
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+          ar[t] -= mB[5] * v[t];
+          xo[t] = xB[t];
+          xo[t] += alpha * rB[t] + beta * ar[t];
+        }
+        st_rot<T, K>(xout + n * K, xo, rot);
+      }
+#pragma unroll
+      for (int t = 0; t < K; ++t) {
+        rA[t] = rB[t];
+        rB[t] = rC[t];
+        xB[t] = xC[t];
       }
 #pragma unroll
       for (int e = 0; e < 6; ++e) mB[e] = mC[e];
@@ -2207,19 +2413,22 @@ struct Impl {
     }
     return vcycle_plain(P, l, b, s, nl, dry);
   }
-  // Whether a level's degree-2 pre-smoothing runs as the fused single pass
-  // (k_mg_pre_fused); FS_MG_PRE=plain keeps the two-kernel form.
-  static bool pre_fused_ok(const MgLevel& L) {
-    using CP = PreTile<T, K>;
+  // Whether a level's degree-2 pre-smoothing (post = false) or post-smoothing
+  // (post = true) runs as a fused single pass (k_mg_pre_fused,
+  // k_mg_post_fused); FS_MG_PRE=plain / FS_MG_POST=plain keep the two-kernel
+  // forms.
+  static bool smooth_fused_ok(const MgLevel& L, bool post) {
+    using CP = SmoothTile<T, K>;
     if constexpr (!CP::OK) {
       return false;
     } else {
-      const char* sel = getenv("FS_MG_PRE");
+      const char* sel = getenv(post ? "FS_MG_POST" : "FS_MG_PRE");
       if (sel && strcmp(sel, "plain") == 0) return false;
+      if ((post ? post_per_sm() : pre_per_sm()) <= 0) return false;
       if (((long long)L.d.nz * (long long)sizeof(T)) % 16 != 0) return false;  // mass rows
       const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
                              ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
-      return cols < (1LL << 30) && pre_per_sm() > 0;
+      return cols < (1LL << 30);
     }
   }
   // Resident k_mg_pre_fused blocks per SM (set with the shared-memory limit
@@ -2228,59 +2437,98 @@ struct Impl {
     static int v = 0;
     return v;
   }
+  static int& post_per_sm() {
+    static int v = 0;
+    return v;
+  }
   static void pre_fused_setup() {
-    using CP = PreTile<T, K>;
+    using CP = SmoothTile<T, K>;
     if constexpr (CP::OK) {
-      if (pre_per_sm() > 0) return;
-      if (cudaFuncSetAttribute(k_mg_pre_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)CP::SMEM) != cudaSuccess)
-        return;
-      int per_sm = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_pre_fused<T, K>,
-                                                        CP::THREADS, CP::SMEM) == cudaSuccess)
-        pre_per_sm() = per_sm;
+      if (pre_per_sm() == 0 &&
+          cudaFuncSetAttribute(k_mg_pre_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)CP::SMEM) == cudaSuccess) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_pre_fused<T, K>,
+                                                          CP::THREADS, CP::SMEM) == cudaSuccess)
+          pre_per_sm() = per_sm;
+      }
+      if (post_per_sm() == 0 &&
+          cudaFuncSetAttribute(k_mg_post_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)CP::SMEM) == cudaSuccess) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_post_fused<T, K>,
+                                                          CP::THREADS, CP::SMEM) == cudaSuccess)
+          post_per_sm() = per_sm;
+      }
     }
   }
-  // Encode the b and mass tensor maps of level L and launch k_mg_pre_fused
-  // (x2 into x[1], r2 into dv); false if a map cannot be made.
-  static bool launch_pre_fused(fs_pcg_plan* P, MgLevel& L, const T* b, T c0, T cd, T cr,
-                               cudaStream_t s) {
-    using CP = PreTile<T, K>;
-    if constexpr (!CP::OK) {
+  // The tensor maps of a fused smoothing pass on level L: the K-interleaved
+  // vector `src` (two-node halo box) and the three equilibrated mass arrays.
+  static bool smooth_maps(const MgLevel& L, const T* src, CUtensorMap* tv, CUtensorMap* tm) {
+    using CP = SmoothTile<T, K>;
+    auto encode = encode_fn();
+    if (!encode) return false;
+    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t Bn = CP::B, MB = sizeof(T);
+    cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
+                          (cuuint64_t)L.d.nx};
+    cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
+    cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)CP::IZ, (cuuint32_t)CP::IY, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    if (encode(tv, dt, 4, (void*)src, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
-    } else {
-      auto encode = encode_fn();
-      if (!encode) return false;
-      const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-      const cuuint64_t Bn = CP::B, MB = sizeof(T);
-      CUtensorMap tb, tm[3];
-      cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
-                            (cuuint64_t)L.d.nx};
-      cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
-      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)CP::IZ, (cuuint32_t)CP::IY, 1};
-      cuuint32_t es[4] = {1, 1, 1, 1};
-      if (encode(&tb, dt, 4, (void*)b, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    cuuint64_t mdims[3] = {(cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
+    cuuint64_t mstr[2] = {MB * L.d.nz, MB * L.d.nz * L.d.ny};
+    cuuint32_t mbox[3] = {(cuuint32_t)CP::WZ, (cuuint32_t)CP::WY, 1};
+    for (int m = 0; m < 3; ++m)
+      if (encode(&tm[m], dt, 3, L.em[m], mdims, mstr, mbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
-      cuuint64_t mdims[3] = {(cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
-      cuuint64_t mstr[2] = {MB * L.d.nz, MB * L.d.nz * L.d.ny};
-      cuuint32_t mbox[3] = {(cuuint32_t)CP::WZ, (cuuint32_t)CP::WY, 1};
-      for (int m = 0; m < 3; ++m)
-        if (encode(&tm[m], dt, 3, L.em[m], mdims, mstr, mbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-          return false;
-      int dev = 0, sms = 148;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
-                             ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
-      long long g = (long long)sms * pre_per_sm();
-      if (g > cols) g = cols;
-      k_mg_pre_fused<T, K><<<(int)g, CP::THREADS, CP::SMEM, s>>>(
+    return true;
+  }
+  // Persistent grid of a fused smoothing pass on level L.
+  static int smooth_grid(const MgLevel& L, int per_sm) {
+    using CP = SmoothTile<T, K>;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
+                           ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
+    long long g = (long long)sms * per_sm;
+    if (g > cols) g = cols;
+    return (int)g;
+  }
+  // k_mg_pre_fused on level L (x2 into x[1], r2 into dv); false if a tensor
+  // map cannot be made for these buffers.
+  static bool launch_pre_fused(fs_pcg_plan* P, MgLevel& L, const T* b, T c0, T cd, T cr,
+                               cudaStream_t s) {
+    using CP = SmoothTile<T, K>;
+    if constexpr (!CP::OK) {
+      return false;
+    } else {
+      CUtensorMap tb, tm[3];
+      if (!smooth_maps(L, b, &tb, tm)) return false;
+      k_mg_pre_fused<T, K><<<smooth_grid(L, pre_per_sm()), CP::THREADS, CP::SMEM, s>>>(
           L.d, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
+          &P->ctl->error);
+      return true;
+    }
+  }
+  // k_mg_post_fused on level L (xout = x + alpha r0 + beta A~r0, r0 = b - A~x).
+  static bool launch_post_fused(fs_pcg_plan* P, MgLevel& L, const T* x, const T* b, T* xout,
+                                T alpha, T beta, cudaStream_t s) {
+    using CP = SmoothTile<T, K>;
+    if constexpr (!CP::OK) {
+      return false;
+    } else {
+      CUtensorMap tx, tm[3];
+      if (!smooth_maps(L, x, &tx, tm)) return false;
+      k_mg_post_fused<T, K><<<smooth_grid(L, post_per_sm()), CP::THREADS, CP::SMEM, s>>>(
+          L.d, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
           &P->ctl->error);
       return true;
     }
@@ -2300,7 +2548,7 @@ struct Impl {
     // residual in dv); otherwise Chebyshev steps then a residual pass.
     const bool resform = !last && deg == 2;
     const T* rfine = (const T*)L.res;
-    if (resform && pre_fused_ok(L)) {
+    if (resform && smooth_fused_ok(L, false)) {
       // x2 -> x[1], r2 -> dv in one pass over b; the two-kernel form if the
       // tensor maps cannot be made for these buffers
       if (!dry && !launch_pre_fused(P, L, b, (T)cr[0], (T)cd[1], (T)cr[1], s)) {
@@ -2370,16 +2618,18 @@ struct Impl {
     if (tr) cudaEventRecordWithFlags(P->ev[6], s, cudaEventRecordExternal);
     if (deg == 2) {  // post-smoothing as residual pass + polynomial pass
       const int out = 1 - cur;
-      if (!dry) {
+      const double alpha = cr[0] * (1.0 + cd[1]) + cr[1], beta = -cr[1] * cr[0];
+      const bool fused = smooth_fused_ok(L, true);
+      if (!dry && !(fused && launch_post_fused(P, L, (const T*)L.x[cur], b, (T*)L.x[out],
+                                               (T)alpha, (T)beta, s))) {
         fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
-        const double alpha = cr[0] * (1.0 + cd[1]) + cr[1], beta = -cr[1] * cr[0];
         fs::k_mg_post2<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, (const T*)L.x[cur], (const T*)L.res, (T*)L.x[out], (T)alpha,
             (T)beta, done);
       }
       cur = out;
-      *nl += 2;
+      *nl += fused ? 1 : 2;
     } else {
       for (int k = 0; k < deg; ++k) {  // post-smoothing from the corrected x
         const int out = 1 - cur;

@@ -1,10 +1,12 @@
-"""The fused multigrid pre-smoothing pass equals the two-kernel form (needs a B200).
+"""The fused multigrid smoothing passes equal the two-kernel forms (needs a B200).
 
 The degree-2 pre-smoothing of a V-cycle level (``k_mg_pre0`` then
 ``k_mg_pre1``: x1 = c0 b, r1 = b - c0 A~b, d1 = cd x1 + cr r1, x2 = x1 + d1,
-r2 = r1 - A~d1) runs as one TMA-staged x-march over b (``k_mg_pre_fused``)
-wherever the level's rows allow it; ``FS_MG_PRE=plain`` keeps the two
-kernels.  The arithmetic and its order are the same, so one V-cycle applied
+r2 = r1 - A~d1) runs as one TMA-staged x-march over b (``k_mg_pre_fused``),
+and the post-smoothing (``k_mg_residual`` then ``k_mg_post2``: r0 = b - A~x,
+x + alpha r0 + beta A~r0) as one over x (``k_mg_post_fused``), wherever the
+level's rows allow it; ``FS_MG_PRE=plain`` and ``FS_MG_POST=plain`` keep the
+two-kernel forms.  The arithmetic and its order are the same, so one V-cycle applied
 through ``fs_pcg_plan_precondition`` to the same vector agrees to round-off
 (the compilers of the two kernels may contract different products into
 FMAs).  The grid is ragged on purpose: y and z end inside a tile, x is odd,
@@ -50,16 +52,18 @@ def _vcycle(sys_, r):
     return z
 
 
+@pytest.mark.parametrize("which", ["FS_MG_PRE", "FS_MG_POST"])
 @pytest.mark.parametrize("precision,nrhs", [("mixed", 8), ("mixed", 4), ("fp64", 4)])
-def test_fused_presmoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs):
+def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, which):
     import torch
     sys_ = _system(precision, nrhs)
     dt = torch.float32 if precision == "mixed" else torch.float64
     gen = torch.Generator(device="cuda").manual_seed(11)
     r = torch.randn(sys_.op.N * sys_.k, dtype=dt, device="cuda", generator=gen)
     monkeypatch.delenv("FS_MG_PRE", raising=False)
+    monkeypatch.delenv("FS_MG_POST", raising=False)
     z_fused = _vcycle(sys_, r)
-    monkeypatch.setenv("FS_MG_PRE", "plain")
+    monkeypatch.setenv(which, "plain")
     z_plain = _vcycle(sys_, r)
     scale = z_plain.abs().max().item()
     tol = 1e-5 if precision == "mixed" else 1e-12
@@ -68,9 +72,10 @@ def test_fused_presmoothing_equals_two_kernels(cuda, monkeypatch, precision, nrh
     sys_.close()
 
 
-def test_fused_presmoothing_extraction_iterations(cuda, golden, monkeypatch):
+def test_fused_smoothing_extraction_iterations(cuda, golden, monkeypatch):
     """The 48x48x24 layered extraction recorded from the reference: the same C
-    and the same iteration counts with the fused pass and with the two kernels."""
+    and the same iteration counts with the fused passes and with the two-kernel
+    forms."""
     from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
     from fieldspice_b200.grid import RectilinearGrid
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
@@ -88,8 +93,10 @@ def test_fused_presmoothing_extraction_iterations(cuda, golden, monkeypatch):
         return C, list(ps.last_capacitance_report["linear"]["iterations"])
 
     monkeypatch.delenv("FS_MG_PRE", raising=False)
+    monkeypatch.delenv("FS_MG_POST", raising=False)
     C_f, it_f = run()
     monkeypatch.setenv("FS_MG_PRE", "plain")
+    monkeypatch.setenv("FS_MG_POST", "plain")
     C_p, it_p = run()
     scale = np.abs(np.diag(d["C"])).max()
     assert np.abs(C_f - d["C"]).max() / scale <= 1e-9
