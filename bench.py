@@ -239,6 +239,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"single": True, "shape": shape, "iterations": info["iterations"],
+                              "reliable_updates": info.get("reliable_updates"),
                               "kernel_ms": info["kernel_ms"],
                               "gpu_launches": info["gpu_launches"]}), flush=True)
         return
@@ -350,6 +351,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "iterations": info["iterations"],
+        "reliable_updates": info.get("reliable_updates"),
         "plan_setup_ms": 1e3 * info.get("setup_time", 0.0),
         "relres_fp64_max": info["residual"],
         "asymmetry_rel": rep["asymmetry_rel"],

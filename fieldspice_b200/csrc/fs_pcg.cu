@@ -68,12 +68,13 @@ struct RhsState {
   int nru;
   int nstall;        // reliable updates since the true residual last halved
   int fresh;         // preconditioned: next r.z starts the recurrence (beta 0)
-  int pad1;
+  int cand;          // iteration at which a deferred convergence check was asked
   double best;       // best true residual norm so far
 };
 
 constexpr int kStallUpdates = 6;
 constexpr int kRefreshEvery = 64;
+constexpr int kConvWait = 3;  // iterations a deferred convergence check may wait
 
 enum { kTicketApply = 0, kTicketUpdate, kTicketRel, kTicketInit,
        kTicketFin, kTicketRz, kTickets };
@@ -97,12 +98,21 @@ __device__ void refresh_done(RhsState* st, Control* ctl, int nrhs) {
   // reliable update streams every RHS column anyway (the vectors are
   // interleaved), so when one RHS asks for it every active RHS takes it:
   // the RHS stay in step and the update passes happen once, not once per
-  // RHS at scattered iterations.
-  int done = 1, ru = 0;
+  // RHS at scattered iterations.  A mixed-precision RHS whose recursive
+  // residual reached the tolerance (ru = 3) keeps iterating with the others
+  // (free: the block streams every column anyway) until every active RHS has
+  // got there, another RHS asks, or it has waited kConvWait iterations; then
+  // one FP64 check serves them all instead of one per convergence iteration.
+  int done = 1, ask = 0, cand_all = 1, any = 0, waited = 0;
   for (int t = 0; t < nrhs; ++t) {
     done &= !st[t].active;
-    ru |= st[t].ru;
+    if (!st[t].active) continue;
+    any = 1;
+    ask |= st[t].ru == 1;
+    cand_all &= st[t].ru == 3;
+    waited |= st[t].ru == 3 && st[t].iters - st[t].cand >= kConvWait;
   }
+  const int ru = ask || (any && cand_all) || waited;
   if (ru)
     for (int t = 0; t < nrhs; ++t)
       if (st[t].active && !st[t].ru) st[t].ru = 2;  // 2: taken along, not asked
@@ -1599,11 +1609,21 @@ __global__ void __launch_bounds__(fs::kBlock)
           const double rn = sqrt(g);
           // Reliable update: to verify convergence, at the cap, and in mixed
           // mode after a 1/delta drop or every kRefreshEvery iterations (so
-          // a stagnating low-precision recurrence is noticed).
-          if (rn < ctl->tol * s.bnorm || s.iters >= ctl->maxiter ||
+          // a stagnating low-precision recurrence is noticed).  In mixed mode
+          // the convergence check may wait for the other RHS (ru = 3, see
+          // refresh_done); FP64 solves check at once, as the reference does.
+          if (s.iters >= ctl->maxiter ||
               (ctl->delta > 0.0 &&
-               (rn < ctl->delta * s.rmax || s.iters % kRefreshEvery == 0)))
+               (rn < ctl->delta * s.rmax || s.iters % kRefreshEvery == 0))) {
             s.ru = 1;
+          } else if (rn < ctl->tol * s.bnorm) {
+            if (ctl->delta <= 0.0) {
+              s.ru = 1;
+            } else if (s.ru == 0) {
+              s.ru = 3;
+              s.cand = s.iters;
+            }
+          }
         }
       }
     }
@@ -1707,7 +1727,7 @@ __global__ void __launch_bounds__(fs::kBlock)
       if (s.ru) {
         const double g = tot[threadIdx.x];
         const double rn = sqrt(g);
-        const bool own = s.ru == 1;
+        const bool own = s.ru == 1 || s.ru == 3;
         s.nru += 1;
         s.ru = 0;
         s.relres = rn / s.bnorm;
