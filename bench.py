@@ -151,9 +151,8 @@ def kernel_bytes(N: int, k: int, s: int) -> dict:
     return {"pupdate": 3 * N * k * s,                 # read r|z, p_old; write p
             "stencil": N * (2 * k * s + 3 * s),       # read p, 3 masses; write q
             "update": 6 * N * k * s,                  # read p, q, x, r; write x, r
-            # fine-level post-smoothing, per launch of its two passes:
-            # r0 = b - A~x (read x, b, masses; write r0) and
-            # x2 = x + a r0 + b A~r0 (read x, r0, masses; write x2)
+            # fine-level post-smoothing, one fused pass (k_mg_post_fused):
+            # read x, b and the masses; write x2 = x + a r0 + b A~r0
             "smoother": N * (3 * k * s + 3 * s)}
 
 
