@@ -138,12 +138,19 @@ __global__ void k_unit_excitation(long long N, int nrhs,
                                   const int16_t* __restrict__ group,
                                   const uint8_t* __restrict__ label,
                                   double* __restrict__ phi) {
+  // pairs of values as 16-byte stores where the width and the base allow it
+  const bool pairs = (nrhs & 1) == 0 && (reinterpret_cast<uintptr_t>(phi) & 15) == 0;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
        n += (long long)gridDim.x * blockDim.x) {
     const bool fixed = label[n] == FS_LABEL_FIXED;
-    const int g = group[n];
-    for (int r = 0; r < nrhs; ++r)
-      phi[n * nrhs + r] = (fixed && g == r) ? 1.0 : 0.0;
+    const int g = fixed ? group[n] : -1;
+    if (pairs) {
+      double2* p2 = reinterpret_cast<double2*>(phi + n * nrhs);
+      for (int r = 0; r < nrhs; r += 2)
+        p2[r / 2] = make_double2(g == r ? 1.0 : 0.0, g == r + 1 ? 1.0 : 0.0);
+    } else {
+      for (int r = 0; r < nrhs; ++r) phi[n * nrhs + r] = g == r ? 1.0 : 0.0;
+    }
   }
 }
 

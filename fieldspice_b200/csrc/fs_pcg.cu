@@ -217,23 +217,41 @@ __global__ void __launch_bounds__(fs::kBlock)
     }
     int i, j, k;
     fs::node_ijk(d, n, i, j, k);
+    // whole-node vector accesses to the FP64 solution and source (no thread
+    // reads a node that another thread of this kernel writes: free nodes are
+    // zeroed only when no neighbour reads them, solo and pinned nodes have
+    // no free neighbours that read them)
     double res[K], bres[K], c[K];
+    if (f) {
+      fs::ldv<double, K>(f, n, res);
+    } else {
 #pragma unroll
-    for (int t = 0; t < K; ++t) {
-      res[t] = f ? f[n * K + t] : 0.0;
-      bres[t] = res[t];
-      c[t] = (lab == FS_LABEL_FREE && warm) ? phi[n * K + t] : 0.0;
+      for (int t = 0; t < K; ++t) res[t] = 0.0;
     }
+    if (lab == FS_LABEL_FREE && warm) {
+      fs::ldv<double, K>(phi, n, c);
+    } else {
+#pragma unroll
+      for (int t = 0; t < K; ++t) c[t] = 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < K; ++t) bres[t] = res[t];
     double dg = 0.0;
     auto edge = [&](bool ok, double m, long long nb) {
       if (!ok || m == 0.0) return;
       dg += m;
       const bool nb_free = label[nb] == FS_LABEL_FREE;
+      double v[K];
+      if (nb_free && !warm) {
+#pragma unroll
+        for (int t = 0; t < K; ++t) v[t] = 0.0;
+      } else {
+        fs::ldv<double, K>(phi, nb, v);
+      }
 #pragma unroll
       for (int t = 0; t < K; ++t) {
-        double v = nb_free ? (warm ? phi[nb * K + t] : 0.0) : phi[nb * K + t];
-        res[t] -= m * (c[t] - v);
-        if (!nb_free) bres[t] += m * v;
+        res[t] -= m * (c[t] - v[t]);
+        if (!nb_free) bres[t] += m * v[t];
       }
     };
     edge6(d, mx, my, mz, n, i, j, k, edge);
@@ -253,15 +271,16 @@ __global__ void __launch_bounds__(fs::kBlock)
         rv[t] = (T)rs;
         acc[t] += rs * rs;
         acc[K + t] += bs * bs;
-        if (!warm) phi[n * K + t] = 0.0;
+        c[t] = 0.0;
       }
+      if (!warm) fs::stv<double, K>(phi, n, c);
       fs::stv<T, K, true>(r, n, rv);
     } else {
       // Solo: every coupled neighbour is fixed, so x = b / diag exactly
       // (poisson.py:559-564).  Pinned: coupled to nothing, x = 0 (:522).
 #pragma unroll
-      for (int t = 0; t < K; ++t)
-        phi[n * K + t] = (lab == FS_LABEL_SOLO) ? bres[t] / dg : 0.0;
+      for (int t = 0; t < K; ++t) c[t] = (lab == FS_LABEL_SOLO) ? bres[t] / dg : 0.0;
+      fs::stv<double, K>(phi, n, c);
       fs::stv<T, K, true>(r, n, zero);
     }
   }
