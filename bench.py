@@ -204,6 +204,8 @@ def run_ours(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
+    step_wall_ms = []  # host wall time of each timed step (the last timed() call)
+
     def timed(fn, steps, warmup):
         for _ in range(warmup):
             out = fn()
@@ -213,9 +215,12 @@ def run_ours(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         outs = []
+        step_wall_ms.clear()
         e0.record(stream)
         for _ in range(steps):
+            t0 = time.perf_counter()
             outs.append(fn())
+            step_wall_ms.append(1e3 * (time.perf_counter() - t0))
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -255,6 +260,10 @@ def run_ours(args, rank, world, local_rank):
 
     D.TRANSFERS.update(h2d=0, d2h=0)
     ms_e2e, outs_e2e = timed(lambda: step_e2e(args.precision), args.steps, 1)
+    # every public call ends with C on the host, so each step's host wall time
+    # is that call's end-to-end time: the median and the worst show whether a
+    # few steps (the host thread off-CPU) set the mean
+    e2e_steps = sorted(step_wall_ms)
     h2d = D.TRANSFERS["h2d"] / (args.steps + 1)
     d2h = D.TRANSFERS["d2h"] / (args.steps + 1)
     e2e_value = n_solves_step * args.steps / (ms_e2e / 1000.0)
@@ -332,7 +341,9 @@ def run_ours(args, rank, world, local_rank):
         },
         "e2e": {"value": e2e_value, "unit": "solves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": ms_e2e / args.steps},
+                "ms_per_step": ms_e2e / args.steps,
+                "step_ms_median": e2e_steps[len(e2e_steps) // 2] if e2e_steps else None,
+                "step_ms_max": e2e_steps[-1] if e2e_steps else None},
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": gbs.get(dom), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s",
