@@ -3060,7 +3060,9 @@ int solve_check(fs_pcg_plan* P) {
   if (ok && P->precond)
     ok = cudaEventElapsedTime(&ms[5], P->ev[6], P->ev[7]) == cudaSuccess;
   if (ok) {
-    ms[5] /= (float)P->mg.smooth_deg;  // per launch
+    // the fine-level post-smoothing: one pass at degree 2 (fused, or the
+    // residual + polynomial pair), else one Chebyshev step per launch
+    if (P->mg.smooth_deg != 2) ms[5] /= (float)P->mg.smooth_deg;
     for (int t = 0; t < 6; ++t) P->kernel_ms[t] += ms[t];
     P->kernel_samples += 1;
   } else {
