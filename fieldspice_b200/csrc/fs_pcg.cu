@@ -1408,6 +1408,287 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
   }
 }
 
+// ---- the fused smoothing passes with each node split over two threads ------------
+// For 32-byte nodes (8 FP32 or 4 FP64 RHS) k_mg_pre_fused and k_mg_post_fused
+// are latency-bound on the warps two 256-thread CTAs per SM give them.  Here
+// the same tiles and shared-memory layout (SmoothTile) run 512 threads: thread
+// 2v+h owns 16-byte chunk h of node v, so a quarter-warp reads 128 contiguous
+// bytes (no bank conflicts, no rotation) and a warp stores whole sectors.  To
+// stay within 64 registers, stage 2 reads the node's own b / x and masses
+// from the input ring (the plane's stage is released after a second barrier,
+// when stage 2 is done with it) instead of carrying them in registers.
+template <typename T, int K>
+struct SplitTile {
+  using C = SmoothTile<T, K>;
+  static constexpr int W = K / 2;                 // values in one 16-byte chunk
+  static constexpr int THREADS = 2 * C::TZ * C::TY;
+  static constexpr bool OK = C::OK && C::B == 32;
+};
+
+template <typename T, int W>
+__device__ __forceinline__ void ld16(const T* p, T (&v)[W]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    v[0] = t.x; v[1] = t.y;
+  }
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void st16(T* p, const T (&v)[W]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  }
+}
+
+// POST = false: k_mg_pre_fused's arithmetic (src = b; out1 = x2, out2 = r2).
+// POST = true:  k_mg_post_fused's (src = x, b by loads; out1 = xout).
+template <typename T, int K, bool POST>
+__global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
+    k_mg_smooth_split(Dims d, const __grid_constant__ CUtensorMap tm_s,
+                      const __grid_constant__ CUtensorMap tm_ex,
+                      const __grid_constant__ CUtensorMap tm_ey,
+                      const __grid_constant__ CUtensorMap tm_ez, const T* __restrict__ b,
+                      T* __restrict__ out1, T* __restrict__ out2, T c0, T cd, T cr,
+                      const int* __restrict__ done, int* __restrict__ err) {
+  using C = SmoothTile<T, K>;
+  constexpr int W = SplitTile<T, K>::W;
+  if (*done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::O_BAR);
+  const int tid = threadIdx.x;
+  const int hf = tid & 1, v = tid >> 1;  // chunk, node of the tile
+  const int tz = v % C::TZ, ty = v / C::TZ;
+  int hz = 0, hy = 0;  // the halo-ring node of this thread pair (v < NHALO)
+  if (v < 2 * C::RZ) {
+    hz = v % C::RZ;
+    hy = v < C::RZ ? 0 : C::RY - 1;
+  } else if (v < C::NHALO) {
+    const int k2 = v - 2 * C::RZ;
+    hy = 1 + k2 / 2;
+    hz = (k2 & 1) ? C::RZ - 1 : 0;
+  }
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const int total = nbz * nby * d.nx;
+  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
+  int u = (int)blockIdx.x * per;
+  const int u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  int ticket = 0, uc = 0;
+  bool failed = false, bad = false;
+  while (u < u_end && !failed) {
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nin = (xb - xa) + 4;  // input planes xa-2 .. xb+1
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % C::NS;
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 2 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_s, &bar[s], 0, z0 - 2, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
+      tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nin; ++j) issue(j);
+    // own node, this thread's chunk: the stage-1 value (d1, or r0) of planes
+    // q-2 (A), q-1 (B), q (C); r1 of planes q-1, q (pre); the -x mass of q-1, q
+    T fA[W], fB[W], fC[W], r1B[W], r1C[W];
+    T mxB = (T)0, mxC = (T)0;
+    for (int j = 0; j < nin; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      const int q = xa - 3 + j;
+      // post: b of this step's stage-1 nodes, loaded before the stage wait so
+      // the two latencies overlap (0 off the grid)
+      T bo[W], bh[W];
+      if constexpr (POST) {
+        auto load_b = [&](int rz, int ry, T(&f)[W]) {
+          const int gz = z0 - 1 + rz, gy = y0 - 1 + ry;
+          if (j >= 2 && gz >= 0 && gz < d.nz && gy >= 0 && gy < d.ny && q >= 0 && q < d.nx) {
+            ld16<T, W>(b + (((long long)q * d.ny + gy) * d.nz + gz) * K + hf * W, f);
+          } else {
+#pragma unroll
+            for (int t = 0; t < W; ++t) f[t] = (T)0;
+          }
+        };
+        load_b(tz + 1, ty + 1, bo);
+        if (v < C::NHALO) {
+          load_b(hz, hy, bh);
+        } else {
+#pragma unroll
+          for (int t = 0; t < W; ++t) bh[t] = (T)0;
+        }
+      }
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (j < 2) continue;
+      // ---- stage 1 on plane q (input planes q-1, q, q+1)
+      const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;
+      const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;
+      const unsigned char* sp = base + s * C::SLOT;
+      T* up = reinterpret_cast<T*>(base + C::O_U + (uc % 3) * C::UPLP);
+      if (!bad) {
+        const T* vm = reinterpret_cast<const T*>(sm) + hf * W;
+        const T* vc = reinterpret_cast<const T*>(sc) + hf * W;
+        const T* vp = reinterpret_cast<const T*>(sp) + hf * W;
+        const T* exm = reinterpret_cast<const T*>(sm + C::O_M0);
+        const T* exc = reinterpret_cast<const T*>(sc + C::O_M0);
+        const T* eyc = reinterpret_cast<const T*>(sc + C::O_M0 + C::MBOXP);
+        const T* ezc = reinterpret_cast<const T*>(sc + C::O_M0 + 2 * C::MBOXP);
+        auto stage1 = [&](int rz, int ry, bool own, const T(&bb)[W]) {
+          const int bi = (ry + 1) * C::IZ + (rz + 1);
+          const int mi = (ry + 1) * C::WZ + (rz - 1 + C::ZP);
+          const T mxm = exm[mi], mxp = exc[mi];
+          const T mym = eyc[mi - C::WZ], myp = eyc[mi];
+          const T mzm = ezc[mi - 1], mzp = ezc[mi];
+          T cv[W], a[W], w[W];
+          ld16<T, W>(vc + bi * K, cv);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] = cv[t];
+          ld16<T, W>(vm + bi * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= mxm * w[t];
+          ld16<T, W>(vp + bi * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= mxp * w[t];
+          ld16<T, W>(vc + (bi - C::IZ) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= mym * w[t];
+          ld16<T, W>(vc + (bi + C::IZ) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= myp * w[t];
+          ld16<T, W>(vc + (bi - 1) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= mzm * w[t];
+          ld16<T, W>(vc + (bi + 1) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) a[t] -= mzp * w[t];
+          T f[W];
+          if constexpr (POST) {
+            // r0 = b - A~x (k_mg_residual)
+#pragma unroll
+            for (int t = 0; t < W; ++t) f[t] = bb[t] - a[t];
+          } else {
+#pragma unroll
+            for (int t = 0; t < W; ++t) {
+              const T xo = c0 * cv[t];          // k_mg_pre0
+              const T rv = cv[t] - c0 * a[t];
+              f[t] = cd * xo + cr * rv;         // k_mg_pre1: d1
+              if (own) r1C[t] = rv;
+            }
+          }
+          st16<T, W>(up + (ry * C::RZ + rz) * K + hf * W, f);
+          if (own) {
+#pragma unroll
+            for (int t = 0; t < W; ++t) fC[t] = f[t];
+            mxC = mxm;
+          }
+        };
+        stage1(tz + 1, ty + 1, true, bo);
+        if (v < C::NHALO) stage1(hz, hy, false, bh);
+      }
+      ++uc;
+      // the plane-q values are complete
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      // ---- stage 2 on plane o = q - 1 (its input stage sm is still resident)
+      if (j >= 4 && inb) {
+        const int x = q - 1;
+        const long long n = ((long long)x * d.ny + y) * d.nz + z;
+        const T* uo = reinterpret_cast<const T*>(base + C::O_U + ((uc - 2) % 3) * C::UPLP) +
+                      hf * W;
+        const int ui = (ty + 1) * C::RZ + (tz + 1);
+        const int bi = (ty + 2) * C::IZ + (tz + 2);
+        const int mi = (ty + 2) * C::WZ + (tz + C::ZP);
+        const T* exo = reinterpret_cast<const T*>(sm + C::O_M0);
+        const T* eyo = reinterpret_cast<const T*>(sm + C::O_M0 + C::MBOXP);
+        const T* ezo = reinterpret_cast<const T*>(sm + C::O_M0 + 2 * C::MBOXP);
+        T a[K / 2], w[W], cv[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+          a[t] = fB[t];
+          a[t] -= mxB * fA[t];
+        }
+        const T mxp = exo[mi];
+#pragma unroll
+        for (int t = 0; t < W; ++t) a[t] -= mxp * fC[t];
+        ld16<T, W>(uo + (ui - C::RZ) * K, w);
+        const T mym = eyo[mi - C::WZ];
+#pragma unroll
+        for (int t = 0; t < W; ++t) a[t] -= mym * w[t];
+        ld16<T, W>(uo + (ui + C::RZ) * K, w);
+        const T myp = eyo[mi];
+#pragma unroll
+        for (int t = 0; t < W; ++t) a[t] -= myp * w[t];
+        ld16<T, W>(uo + (ui - 1) * K, w);
+        const T mzm = ezo[mi - 1];
+#pragma unroll
+        for (int t = 0; t < W; ++t) a[t] -= mzm * w[t];
+        ld16<T, W>(uo + (ui + 1) * K, w);
+        const T mzp = ezo[mi];
+        ld16<T, W>(reinterpret_cast<const T*>(sm) + bi * K + hf * W, cv);  // b or x at o
+        T o1[W];
+        if constexpr (POST) {
+#pragma unroll
+          for (int t = 0; t < W; ++t) {
+            a[t] -= mzp * w[t];
+            o1[t] = cv[t];
+            o1[t] += c0 * fB[t] + cd * a[t];  // k_mg_post2: x + alpha r0 + beta A~r0
+          }
+          st16<T, W>(out1 + n * K + hf * W, o1);
+        } else {
+          T o2[W];
+#pragma unroll
+          for (int t = 0; t < W; ++t) {
+            a[t] -= mzp * w[t];
+            o1[t] = c0 * cv[t];     // x1
+            o1[t] += fB[t];         // x2 = x1 + d1
+            o2[t] = r1B[t] - a[t];  // r2 = r1 - A~d1
+          }
+          st16<T, W>(out1 + n * K + hf * W, o1);
+          st16<T, W>(out2 + n * K + hf * W, o2);
+        }
+      }
+      // stage 2 done with plane q-1: its stage may refill
+      __syncthreads();
+      if (tid == 0 && j - 2 + C::NS < nin) issue(j - 2 + C::NS);
+#pragma unroll
+      for (int t = 0; t < W; ++t) {
+        fA[t] = fB[t];
+        fB[t] = fC[t];
+        if constexpr (!POST) r1B[t] = r1C[t];
+      }
+      mxB = mxC;
+    }
+    ticket += nin;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      *err = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+}
+
 // ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
@@ -2470,6 +2751,17 @@ struct Impl {
       return cols < (1LL << 30);
     }
   }
+  // The two-threads-per-node form of the fused passes (32-byte nodes);
+  // FS_MG_SPLIT=0 keeps one thread per node.
+  static bool split_ok(bool post) {
+    if constexpr (!SplitTile<T, K>::OK) {
+      return false;
+    } else {
+      const char* sel = getenv("FS_MG_SPLIT");
+      if (sel && strcmp(sel, "0") == 0) return false;
+      return split_per_sm(post) > 0;
+    }
+  }
   // Resident k_mg_pre_fused blocks per SM (set with the shared-memory limit
   // when a plan builds its hierarchy; 0 = the kernel cannot run).
   static int& pre_per_sm() {
@@ -2480,8 +2772,31 @@ struct Impl {
     static int v = 0;
     return v;
   }
+  // k_mg_smooth_split (32-byte nodes): resident blocks per SM, pre and post
+  static int& split_per_sm(bool post) {
+    static int v[2] = {0, 0};
+    return v[post ? 1 : 0];
+  }
+  template <bool POST>
+  static void split_setup() {
+    using CP = SmoothTile<T, K>;
+    using CS = SplitTile<T, K>;
+    if constexpr (CS::OK) {
+      if (split_per_sm(POST) > 0) return;
+      if (cudaFuncSetAttribute(k_mg_smooth_split<T, K, POST>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)CP::SMEM) != cudaSuccess)
+        return;
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_smooth_split<T, K, POST>,
+                                                        CS::THREADS, CP::SMEM) == cudaSuccess)
+        split_per_sm(POST) = per_sm;
+    }
+  }
   static void pre_fused_setup() {
     using CP = SmoothTile<T, K>;
+    split_setup<false>();
+    split_setup<true>();
     if constexpr (CP::OK) {
       if (pre_per_sm() == 0 &&
           cudaFuncSetAttribute(k_mg_pre_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2551,6 +2866,13 @@ struct Impl {
     } else {
       CUtensorMap tb, tm[3];
       if (!smooth_maps(L, b, &tb, tm)) return false;
+      if (split_ok(false)) {
+        k_mg_smooth_split<T, K, false>
+            <<<smooth_grid(L, split_per_sm(false)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+                L.d, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
+                &P->ctl->all_done, &P->ctl->error);
+        return true;
+      }
       k_mg_pre_fused<T, K><<<smooth_grid(L, pre_per_sm()), CP::THREADS, CP::SMEM, s>>>(
           L.d, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
           &P->ctl->error);
@@ -2566,6 +2888,13 @@ struct Impl {
     } else {
       CUtensorMap tx, tm[3];
       if (!smooth_maps(L, x, &tx, tm)) return false;
+      if (split_ok(true)) {
+        k_mg_smooth_split<T, K, true>
+            <<<smooth_grid(L, split_per_sm(true)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+                L.d, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
+                &P->ctl->all_done, &P->ctl->error);
+        return true;
+      }
       k_mg_post_fused<T, K><<<smooth_grid(L, post_per_sm()), CP::THREADS, CP::SMEM, s>>>(
           L.d, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
           &P->ctl->error);

@@ -5,8 +5,9 @@ The degree-2 pre-smoothing of a V-cycle level (``k_mg_pre0`` then
 r2 = r1 - A~d1) runs as one TMA-staged x-march over b (``k_mg_pre_fused``),
 and the post-smoothing (``k_mg_residual`` then ``k_mg_post2``: r0 = b - A~x,
 x + alpha r0 + beta A~r0) as one over x (``k_mg_post_fused``), wherever the
-level's rows allow it; ``FS_MG_PRE=plain`` and ``FS_MG_POST=plain`` keep the
-two-kernel forms.  The arithmetic and its order are the same, so one V-cycle applied
+level's rows allow it (for 32-byte nodes with each node split over two threads,
+``k_mg_smooth_split``; ``FS_MG_SPLIT=0`` keeps one thread per node);
+``FS_MG_PRE=plain`` and ``FS_MG_POST=plain`` keep the two-kernel forms.  The arithmetic and its order are the same, so one V-cycle applied
 through ``fs_pcg_plan_precondition`` to the same vector agrees to round-off
 (the compilers of the two kernels may contract different products into
 FMAs).  The grid is ragged on purpose: y and z end inside a tile, x is odd,
@@ -52,9 +53,12 @@ def _vcycle(sys_, r):
     return z
 
 
+@pytest.mark.parametrize("split", ["1", "0"])
 @pytest.mark.parametrize("which", ["FS_MG_PRE", "FS_MG_POST"])
 @pytest.mark.parametrize("precision,nrhs", [("mixed", 8), ("mixed", 4), ("fp64", 4)])
-def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, which):
+def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, which, split):
+    """split "1": 32-byte nodes (8 FP32 / 4 FP64 RHS) run the two-threads-per-node
+    pass (k_mg_smooth_split); "0" keeps one thread per node."""
     import torch
     sys_ = _system(precision, nrhs)
     dt = torch.float32 if precision == "mixed" else torch.float64
@@ -62,6 +66,7 @@ def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, 
     r = torch.randn(sys_.op.N * sys_.k, dtype=dt, device="cuda", generator=gen)
     monkeypatch.delenv("FS_MG_PRE", raising=False)
     monkeypatch.delenv("FS_MG_POST", raising=False)
+    monkeypatch.setenv("FS_MG_SPLIT", split)
     z_fused = _vcycle(sys_, r)
     monkeypatch.setenv(which, "plain")
     z_plain = _vcycle(sys_, r)
