@@ -1420,7 +1420,7 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
 template <typename T, int K>
 struct SplitTile {
   using C = SmoothTile<T, K>;
-  static constexpr int W = K / 2;                 // values in one 16-byte chunk
+  static constexpr int W = K >= 2 ? K / 2 : 1;    // values in one 16-byte chunk
   static constexpr int THREADS = 2 * C::TZ * C::TY;
   static constexpr bool OK = C::OK && C::B == 32;
 };
@@ -1687,6 +1687,145 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
     }
     __syncthreads();
   }
+}
+
+// ---- K1 with each node split over two threads (stencil kind 4) -------------------
+// k_stencil_tma_m's tiles, ring and single barrier per plane, for 32-byte
+// nodes: 512 threads, thread 2v+h owning 16-byte chunk h of node v (chunk reads
+// of a quarter-warp are 128 contiguous bytes, q stores cover whole sectors).
+// One of the candidates the stencil autotuner times.
+template <typename T, int K>
+struct TmaTileSplit {
+  using M = TmaTileM<T, K>;
+  static constexpr int W = K >= 2 ? K / 2 : 1;
+  static constexpr int THREADS = 2 * M::TZ * M::TY;
+  static constexpr bool OK = M::OK && M::B == 32;
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TmaTileSplit<T, K>::THREADS, 2)
+    k_stencil_split(Dims d, const __grid_constant__ CUtensorMap tm_p,
+                    const __grid_constant__ CUtensorMap tm_ex,
+                    const __grid_constant__ CUtensorMap tm_ey,
+                    const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ q,
+                    double* __restrict__ partials, RhsState* st, Control* ctl) {
+  using C = TmaTileM<T, K>;
+  constexpr int W = TmaTileSplit<T, K>::W;
+  if (ctl->all_done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::NS * C::SLOT);
+  const int tid = threadIdx.x;
+  const int hf = tid & 1, v = tid >> 1;
+  const int tz = v % C::TZ, ty = v / C::TZ;
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  const int total = nbz * nby * d.nx;
+  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
+  int u = (int)blockIdx.x * per;
+  const int u_end = min(u + per, total);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  double acc[W];
+#pragma unroll
+  for (int t = 0; t < W; ++t) acc[t] = 0.0;
+  const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  int ticket = 0;
+  bool failed = false, bad = false;
+  while (u < u_end && !failed) {
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nplanes = (xb - xa) + 2;  // planes xa-1 .. xb
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % C::NS;
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 1 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_p, &bar[s], 0, z0 - 1, y0 - 1, x);
+      tma_load_3d(slot + C::O_EX, &tm_ex, &bar[s], z0, y0, x);
+      tma_load_3d(slot + C::O_EY, &tm_ey, &bar[s], z0, y0 - 1, x);
+      tma_load_3d(slot + C::O_EZ, &tm_ez, &bar[s], z0 - C::ZP, y0, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
+    for (int j = 0; j < nplanes; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (j >= 2) {
+        if (inb && !bad) {
+          const int x = xa - 2 + j;
+          const long long n = ((long long)x * d.ny + y) * d.nz + z;
+          const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;  // plane x-1
+          const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;  // plane x
+          const unsigned char* sp = base + s * C::SLOT;                   // plane x+1
+          const T* pm = reinterpret_cast<const T*>(sm) + hf * W;
+          const T* pc = reinterpret_cast<const T*>(sc) + hf * W;
+          const T* pp = reinterpret_cast<const T*>(sp) + hf * W;
+          const T* exm = reinterpret_cast<const T*>(sm + C::O_EX);
+          const T* exc = reinterpret_cast<const T*>(sc + C::O_EX);
+          const T* eyc = reinterpret_cast<const T*>(sc + C::O_EY);
+          const T* ezc = reinterpret_cast<const T*>(sc + C::O_EZ);
+          const T mxm = exm[ty * C::TZ + tz], mxp = exc[ty * C::TZ + tz];
+          const T mym = eyc[ty * C::TZ + tz], myp = eyc[(ty + 1) * C::TZ + tz];
+          const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
+          const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
+          T c[W], w[W], qv[W];
+          ld16<T, W>(pc + cpos * K, c);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] = c[t];
+          ld16<T, W>(pm + cpos * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] -= mxm * w[t];
+          ld16<T, W>(pp + cpos * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] -= mxp * w[t];
+          ld16<T, W>(pc + (cpos - C::HZ) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] -= mym * w[t];
+          ld16<T, W>(pc + (cpos + C::HZ) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] -= myp * w[t];
+          ld16<T, W>(pc + (cpos - 1) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) qv[t] -= mzm * w[t];
+          ld16<T, W>(pc + (cpos + 1) * K, w);
+#pragma unroll
+          for (int t = 0; t < W; ++t) {
+            qv[t] -= mzp * w[t];
+            acc[t] += (double)c[t] * (double)qv[t];
+          }
+          st16<T, W>(q + n * K + hf * W, qv);
+        }
+        // plane j-2 no longer read: its stage may refill
+        if (__syncthreads_or(bad)) {
+          failed = true;
+          break;
+        }
+        if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
+      }
+    }
+    ticket += nplanes;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      ctl->error = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+  double full[K];  // this thread's chunk in RHS order, 0 for the other half
+#pragma unroll
+  for (int t = 0; t < K; ++t) full[t] = (t / W == hf) ? acc[t % W] : 0.0;
+  finish_pq<T, K, TmaTileSplit<T, K>::THREADS>(full, partials, st, ctl);
 }
 
 // ---- preconditioned CG: gamma = r~.z, beta = gamma / gamma_old ------------------
@@ -2398,6 +2537,25 @@ struct Impl {
       long long g = (long long)sms * per_sm;
       if (g > cols) g = cols;
       P->g_apply = (int)g;
+    } else if (P->stencil_kind == 4) {
+      if constexpr (TmaTileSplit<T, K>::OK) {
+        using CM = TmaTileM<T, K>;
+        using CSp = TmaTileSplit<T, K>;
+        cudaFuncSetAttribute(k_stencil_split<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)CM::SMEM);
+        int per_sm = 0, dev = 0, sms = 148;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_split<T, K>,
+                                                          CSp::THREADS, CM::SMEM) != cudaSuccess ||
+            per_sm < 1)
+          per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long long cols = (long long)((P->d.nz + CM::TZ - 1) / CM::TZ) *
+                               ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx;
+        long long g = (long long)sms * per_sm;
+        if (g > cols) g = cols;
+        P->g_apply = (int)g;
+      }
     } else if (P->stencil_kind == 2) {
       using CM = TmaTileM<T, K>;
       cudaFuncSetAttribute(k_stencil_tma_m<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2448,10 +2606,12 @@ struct Impl {
       std::vector<unsigned char> saved(sbytes);
       FS_CHECK(cudaMemcpyAsync(saved.data(), st0, sbytes, cudaMemcpyDeviceToHost, s));
       FS_CHECK(cudaMemsetAsync(P->p[1], 0, (size_t)P->d.N * K * sizeof(T), s));
-      const int cands[3] = {2, 3, 0};
+      // kind 4 (two threads per node) only for 32-byte nodes
+      const int cands[4] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1};
       float best = 3.4e38f;
       int bestk = 2;
       for (int c : cands) {
+        if (c < 0) continue;
         P->stencil_kind = c;
         P->use_tma = c != 0;
         apply_grid(P);
@@ -2499,6 +2659,8 @@ struct Impl {
         P->stencil_kind = 3;
       } else if (sel && strcmp(sel, "tma_m") == 0) {
         P->stencil_kind = 2;
+      } else if (sel && strcmp(sel, "tma_split") == 0) {
+        P->stencil_kind = TmaTileSplit<T, K>::OK ? 4 : 2;
       } else {
         // chosen by timing the candidates on the first plan of this shape
         const int cached = stencil_choice_get(P->d, K, (int)sizeof(T));
@@ -2621,6 +2783,15 @@ struct Impl {
                 P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
                 P->partials, P->st, P->ctl);
             break;
+          }
+          if constexpr (TmaTileSplit<T, K>::OK) {
+            if (P->stencil_kind == 4) {
+              using CM = TmaTileM<T, K>;
+              k_stencil_split<T, K><<<P->g_apply, TmaTileSplit<T, K>::THREADS, CM::SMEM, s>>>(
+                  P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
+                  P->partials, P->st, P->ctl);
+              break;
+            }
           }
           if (!P->use_tma) {
             k_apply_pq<T, K><<<P->g_apply, fs::kBlock, 0, s>>>(
@@ -2866,12 +3037,14 @@ struct Impl {
     } else {
       CUtensorMap tb, tm[3];
       if (!smooth_maps(L, b, &tb, tm)) return false;
-      if (split_ok(false)) {
-        k_mg_smooth_split<T, K, false>
-            <<<smooth_grid(L, split_per_sm(false)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
-                L.d, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
-                &P->ctl->all_done, &P->ctl->error);
-        return true;
+      if constexpr (SplitTile<T, K>::OK) {
+        if (split_ok(false)) {
+          k_mg_smooth_split<T, K, false>
+              <<<smooth_grid(L, split_per_sm(false)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+                  L.d, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
+                  &P->ctl->all_done, &P->ctl->error);
+          return true;
+        }
       }
       k_mg_pre_fused<T, K><<<smooth_grid(L, pre_per_sm()), CP::THREADS, CP::SMEM, s>>>(
           L.d, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
@@ -2888,12 +3061,14 @@ struct Impl {
     } else {
       CUtensorMap tx, tm[3];
       if (!smooth_maps(L, x, &tx, tm)) return false;
-      if (split_ok(true)) {
-        k_mg_smooth_split<T, K, true>
-            <<<smooth_grid(L, split_per_sm(true)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
-                L.d, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
-                &P->ctl->all_done, &P->ctl->error);
-        return true;
+      if constexpr (SplitTile<T, K>::OK) {
+        if (split_ok(true)) {
+          k_mg_smooth_split<T, K, true>
+              <<<smooth_grid(L, split_per_sm(true)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+                  L.d, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
+                  &P->ctl->all_done, &P->ctl->error);
+          return true;
+        }
       }
       k_mg_post_fused<T, K><<<smooth_grid(L, post_per_sm()), CP::THREADS, CP::SMEM, s>>>(
           L.d, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
