@@ -104,6 +104,7 @@ _SIGNATURES = {
     "fs_pcg_plan_scale": (c_int, [c_void_p, POINTER(c_void_p), POINTER(c_void_p)]),
     "fs_pcg_plan_label_counts": (c_int, [c_void_p, POINTER(c_longlong), c_void_p]),
     "fs_pcg_plan_stencil_kind": (c_int, [c_void_p]),
+    "fs_pcg_plan_stencil_times": (c_int, [c_void_p, POINTER(c_float)]),
     "fs_ac_workspace_bytes": (c_int, [c_int, c_int, c_int, c_int, c_int, POINTER(c_size_t)]),
     "fs_ac_solve": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                             c_void_p, c_double, c_int, c_void_p, c_size_t,

@@ -13,6 +13,14 @@ namespace fs {
 
 constexpr int kBlock = 256;  // threads per block for every grid-stride kernel
 constexpr int kMaxRhs = 16;
+// Per-device caches (kernel attributes, occupancy, SM counts) are indexed by
+// the current device ordinal; ordinals at or beyond this bound share slot 0.
+constexpr int kMaxDevices = 64;
+inline int current_device_slot() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
+  return d;
+}
 
 struct Dims {
   int nx, ny, nz;

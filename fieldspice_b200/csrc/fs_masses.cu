@@ -185,12 +185,14 @@ int fs_cuda_status(const char* where, cudaError_t err) {
 }
 
 int fs_grid_blocks(const void* kernel, long long work_items) {
-  static int sm_count = 0;
+  static int sm_counts[fs::kMaxDevices] = {};
+  int& sm_count = sm_counts[fs::current_device_slot()];
   if (sm_count == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (sm_count <= 0) sm_count = 148;
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    sm_count = n > 0 ? n : 148;
   }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, fs::kBlock,

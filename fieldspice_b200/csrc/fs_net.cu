@@ -169,12 +169,12 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
       a2.phases = 1;
       a2.nst = nst;
       a2.error = io.error;
-      static bool attr2 = false;
-      if (!attr2) {
+      static bool attr2[fs::kMaxDevices] = {};
+      if (!attr2[fs::current_device_slot()]) {
         cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              227 * 1024);
         if (e != cudaSuccess) return fs_cuda_status("cudaFuncSetAttribute(conv2)", e);
-        attr2 = true;
+        attr2[fs::current_device_slot()] = true;
       }
       const long long ntiles = (g.R + 127) / 128;
       int per_sm = 1, dev = 0, sms = 148;
@@ -215,12 +215,12 @@ int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
   a.phases = c.phases;
   a.nst = 0;
   a.error = io.error;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[fs::kMaxDevices] = {};
+  if (!attr_set[fs::current_device_slot()]) {
     cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          227 * 1024);
     if (e != cudaSuccess) return fs_cuda_status("cudaFuncSetAttribute(conv)", e);
-    attr_set = true;
+    attr_set[fs::current_device_slot()] = true;
   }
   const long long tiles = (g.R + 128LL * c.T - 1) / (128LL * c.T);
   if (tiles > 0x7fffffffLL) {

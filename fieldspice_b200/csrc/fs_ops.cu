@@ -193,7 +193,7 @@ static __device__ __align__(256) unsigned char
 // Host code may not pass `g_group_scratch` itself to a kernel: in host code
 // that name is a stand-in, not a device address.  The device address is
 // looked up once per device (with that device current) and cached.
-constexpr int kMaxDevices = 64;
+constexpr int kMaxDevices = fs::kMaxDevices;
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
 
@@ -345,6 +345,14 @@ int fs_group_apply_noalloc(const double* mAx, const double* mAy,
       ngroups < 1 || nx < 2 || ny < 2 || nz < 2 || nrhs < 1)
     return FS_BAD_ARG;
   if (mBx && (!mBy || !mBz || !w)) return FS_BAD_ARG;
+  // every argument is checked before the shared array is touched
+  if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8 && nrhs != 16) {
+    char msg[128];
+    snprintf(msg, sizeof(msg),
+             "fs_group_apply_noalloc: nrhs = %d; it must be 1, 2, 4, 8 or 16", nrhs);
+    fs_set_error_msg(msg);
+    return FS_BAD_ARG;
+  }
   if ((long long)ngroups * nrhs > kNoAllocMaxGroupRhs) {
     char msg[160];
     snprintf(msg, sizeof(msg),

@@ -2436,7 +2436,8 @@ struct fs_pcg_plan {
   CUtensorMap tm_q;        // q tiles of the TMA-store stencil
   int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses,
                            // 3: as 2 with q written by TMA stores
-  int autotune = 0;        // time kinds 2, 3, 0 at creation and keep the fastest
+  int autotune = 0;        // time kinds 2, 3, 0, 4 at creation and keep the fastest
+  float tune_ms[5] = {-1.f, -1.f, -1.f, -1.f, -1.f};  // ms per launch by kind (-1: untimed)
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -2592,11 +2593,15 @@ struct Impl {
       P->g_apply = fs_grid_blocks((const void*)k_apply_pq<T, K>, N);
     }
   }
-  // Time the TMA-staged (2), TMA-store (3) and cached-load (0) stencils on this
-  // plan's buffers (3 launches each after a warm-up, CUDA events on the
-  // creation stream) and keep the fastest.  The launches write q, the
-  // partials and the per-RHS state; the state and control block are saved
-  // and restored around them.
+  // Time the TMA-staged (2), TMA-store (3), cached-load (0) and split (4)
+  // stencils on this plan's buffers (a warm-up, then 3 launches each timed
+  // alone with CUDA events on the creation stream) and keep the fastest.
+  // Every CG kernel returns at once when the control block says all
+  // right-hand sides are done, which a stencil launch on this not yet
+  // initialised state sets (no RHS is active), so the flag is cleared before
+  // each launch, outside its event pair.  The launches write q, the partials
+  // and the per-RHS state; the state and control block are saved and
+  // restored around them.
   static int autotune(fs_pcg_plan* P, cudaStream_t s) {
     if constexpr (!TmaTile<T, K>::OK) {
       return FS_OK;
@@ -2610,19 +2615,28 @@ struct Impl {
       const int cands[4] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1};
       float best = 3.4e38f;
       int bestk = 2;
+      for (int c = 0; c < 5; ++c) P->tune_ms[c] = -1.f;
+      int* done = &P->ctl->all_done;
       for (int c : cands) {
         if (c < 0) continue;
         P->stencil_kind = c;
         P->use_tma = c != 0;
         apply_grid(P);
+        FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
         kernel(P, 1, 0, s);
-        FS_CHECK(cudaEventRecord(P->ev[0], s));
-        for (int r = 0; r < 3; ++r) kernel(P, 1, 0, s);
-        FS_CHECK(cudaEventRecord(P->ev[1], s));
-        FS_CHECK(cudaGetLastError());
-        FS_CHECK(cudaEventSynchronize(P->ev[1]));
         float ms = 0.f;
-        FS_CHECK(cudaEventElapsedTime(&ms, P->ev[0], P->ev[1]));
+        for (int r = 0; r < 3; ++r) {
+          FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
+          FS_CHECK(cudaEventRecord(P->ev[0], s));
+          kernel(P, 1, 0, s);
+          FS_CHECK(cudaEventRecord(P->ev[1], s));
+          FS_CHECK(cudaGetLastError());
+          FS_CHECK(cudaEventSynchronize(P->ev[1]));
+          float one = 0.f;
+          FS_CHECK(cudaEventElapsedTime(&one, P->ev[0], P->ev[1]));
+          ms += one;
+        }
+        P->tune_ms[c] = ms / 3.f;
         if (ms < best) {
           best = ms;
           bestk = c;
@@ -2934,19 +2948,20 @@ struct Impl {
     }
   }
   // Resident k_mg_pre_fused blocks per SM (set with the shared-memory limit
-  // when a plan builds its hierarchy; 0 = the kernel cannot run).
+  // when a plan builds its hierarchy; 0 = the kernel cannot run), per device:
+  // the shared-memory attribute is a per-device setting.
   static int& pre_per_sm() {
-    static int v = 0;
-    return v;
+    static int v[fs::kMaxDevices] = {};
+    return v[fs::current_device_slot()];
   }
   static int& post_per_sm() {
-    static int v = 0;
-    return v;
+    static int v[fs::kMaxDevices] = {};
+    return v[fs::current_device_slot()];
   }
   // k_mg_smooth_split (32-byte nodes): resident blocks per SM, pre and post
   static int& split_per_sm(bool post) {
-    static int v[2] = {0, 0};
-    return v[post ? 1 : 0];
+    static int v[fs::kMaxDevices][2] = {};
+    return v[fs::current_device_slot()][post ? 1 : 0];
   }
   template <bool POST>
   static void split_setup() {
@@ -3731,6 +3746,12 @@ int fs_eq_apply(const float* x, float* y, const float* ex, const float* ey, cons
 }
 
 int fs_pcg_plan_stencil_kind(const fs_pcg_plan* P) { return P ? P->stencil_kind : -1; }
+
+int fs_pcg_plan_stencil_times(const fs_pcg_plan* P, float* ms) {
+  if (!P || !ms) return FS_BAD_ARG;
+  for (int c = 0; c < 5; ++c) ms[c] = P->tune_ms[c];
+  return FS_OK;
+}
 
 int fs_pcg_plan_label_counts(const fs_pcg_plan* P, long long* counts, void* stream) {
   if (!P || !counts) return FS_BAD_ARG;

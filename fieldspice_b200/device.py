@@ -19,11 +19,21 @@ from . import _lib as L
 from .grid import grid_metric
 
 __all__ = ["DeviceOperator", "EliminatedSystem", "pad_rhs", "MAX_RHS",
-           "device", "h2d", "d2h", "TRANSFERS", "upload_groups"]
+           "device", "h2d", "d2h", "TRANSFERS", "PHASES", "mark", "upload_groups"]
 
 #: Bytes moved between host and device by the product path (host arrays
 #: uploaded, results read back); the benchmark reads it per step.
 TRANSFERS = {"h2d": 0, "d2h": 0}
+
+#: Host-side phase log of the public calls: ``None`` (off), or a list that
+#: receives ``(phase, wall seconds, process CPU seconds)`` at each phase end.
+PHASES: list | None = None
+
+
+def mark(phase: str) -> None:
+    """Record the end of ``phase`` in :data:`PHASES` when logging is on."""
+    if PHASES is not None:
+        PHASES.append((phase, time.perf_counter(), time.process_time()))
 
 
 def h2d(a, dtype, dev):

@@ -20,7 +20,7 @@ import numpy as np
 
 from .. import _lib as L
 from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes, periodic_mask
-from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d,
+from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d, mark,
                       pad_rhs, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
 
@@ -203,7 +203,9 @@ class PoissonSolver:
                 "absolute value in F/m. Multiply by eps0.")
         self.eps_cell = eps_cell
         self.eps_mode = eps_mode
+        mark("eps_upload_and_check")
         self.op = DeviceOperator(grid, eps_dev, mode=eps_mode)
+        mark("masses")
         self._L = None
         self.last_capacitance_report: dict[str, Any] = {}
         self.last_device_time = 0.0
@@ -266,10 +268,12 @@ class PoissonSolver:
         mask = periodic_mask(bc)
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
+        mark("terminal_checks")
         term_nodes = [np.asarray(t.nodes, np.int64) for t in terms]
         term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
         wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
         shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
+        mark("node_upload")
         op, charges = self.op, None
         if mask:
             # periodic walls: solve on the wrap-around grid (the reference's
@@ -288,6 +292,7 @@ class PoissonSolver:
             learned=None if mask else self.gpu.learned, charges=charges)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
+        mark("report")
         rep["terminals"] = tuple(t.name for t in terms)
         if symmetrise:
             C = 0.5 * (C + C.T)
@@ -587,9 +592,11 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         if system is None or system.k != k:
             if system is not None:
                 system.close()
+            mark("labels")
             system = EliminatedSystem(op, label, kb, precision=precision,
                                       preconditioner=preconditioner, learned=learned)
             setup_time += system.setup_time
+            mark("plan")
         system.nrhs = kb
         group.fill_(-1)
         for c, j in enumerate(cols):
@@ -599,6 +606,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                                              L.stream_ptr())
         L.check("fs_fill_unit_excitation", st)
         _, stats = system.solve(tol, maxiter)
+        mark("solve")
         launches += system.launches + 1
         raise_on_status(stats, tol, "gpu-cg")
         stats_all.extend(stats)
@@ -611,6 +619,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
             phi_full = system.phi.view(op.N, k).index_select(0, node_map).reshape(-1)
             Q = full_op.group_sums(phi_full, full_groups, nrhs=k, nodes_dev=gdev_full)
         launches += 1
+        mark("charge_and_readback")
         for c, j in enumerate(cols):
             C[:, j] = Q[:nt, c]
             if has_shield:
@@ -638,6 +647,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         "notes": (),
     }
     system.close()
+    mark("plan_release")
     return C, q_shield, info
 
 

@@ -240,7 +240,10 @@ int fs_group_apply(const double* mAx, const double* mAy, const double* mAz,
  * ngroups * nrhs must not exceed 2048 (larger sizes return FS_BAD_ARG with
  * the reason in fs_last_error()).  The first call on each device looks up
  * the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  Every call
+ * current; make that first call before any stream capture.  That address
+ * is kept for the life of the process, so a cudaDeviceReset between calls
+ * is not supported.  nrhs must be 1, 2, 4, 8 or 16; every argument is
+ * checked before the array is touched.  Every call
  * shares the one array and it keeps the previous call's contents: calls
  * that overlap on the GPU (two streams, two host threads) race on it and
  * must be serialised by the caller.  Never allocates or frees memory.     */
@@ -384,11 +387,16 @@ int fs_pcg_plan_scale(const fs_pcg_plan* plan, const double** s64, const uint8_t
  * classified at creation (LinearSystem's split, poisson.py:282-362).       */
 int fs_pcg_plan_label_counts(const fs_pcg_plan* plan, long long* counts, void* stream);
 /* The CG stencil kernel the plan runs: 0 cached loads, 1 TMA-staged p,
- * 2 TMA-staged p and masses, 3 as 2 with TMA stores of q.  Unless the
- * FS_STENCIL environment variable names one, the first plan of each (grid,
- * RHS block, precision) times kinds 2, 3 and 0 on its own buffers at creation
- * and later plans of that shape reuse the fastest.                          */
+ * 2 TMA-staged p and masses, 3 as 2 with TMA stores of q, 4 as 2 with each
+ * 32-byte node split over two threads.  Unless the FS_STENCIL environment
+ * variable names one, the first plan of each (grid, RHS block, precision)
+ * times kinds 2, 3, 0 (and 4 for 32-byte nodes) on its own buffers at
+ * creation and later plans of that shape reuse the fastest.                 */
 int fs_pcg_plan_stencil_kind(const fs_pcg_plan* plan);
+/* ms[5] (host): the mean time per launch of each stencil kind (index = kind)
+ * measured by this plan's autotuner; -1 for kinds it did not time (every
+ * entry is -1 when the plan reused an earlier choice or FS_STENCIL chose).  */
+int fs_pcg_plan_stencil_times(const fs_pcg_plan* plan, float* ms);
 
 /* ---- §8f-4: harmonic EQS, the complex-symmetric solve -------------------------
  * Replaces the per-frequency sparse LU of fieldspice/solvers/ac.py:95-145

@@ -24,7 +24,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = os.environ.get("FIELDSPICE_REF", "/root/reference")
+REF = os.environ.get("FIELDSPICE_REF")
+if not REF:
+    raise SystemExit("set FIELDSPICE_REF to the reference fieldspice source tree")
 sys.path.insert(0, REF)
 sys.path.insert(0, str(HERE.parents[1]))
 

@@ -73,3 +73,59 @@ def test_stencil_autotuner_picks_and_caches(cuda, golden, monkeypatch):
         sys_.close()
     assert kinds[0] in (0, 2, 3, 4)
     assert kinds[1] == kinds[0]
+
+
+def _uniform_system(shape, k, precision):
+    """A layered grid with its zlo plane fixed, as an eliminated system."""
+    import torch
+
+    from fieldspice_b200 import _lib as L
+    from fieldspice_b200.device import DeviceOperator, EliminatedSystem
+    from fieldspice_b200.grid import RectilinearGrid
+    g = RectilinearGrid(*[np.arange(n) * 10e-9 for n in shape])
+    eps = np.full(g.shape_cells, 3.9 * 8.854e-12)
+    eps[:, :, : shape[2] // 3] *= 2.0
+    op = DeviceOperator(g, eps)
+    label = torch.zeros(shape, dtype=torch.uint8, device=op.dev)
+    label[:, :, 0] = L.LABEL_FIXED
+    return EliminatedSystem(op, label.view(-1), k, precision=precision, preconditioner="mg")
+
+
+def test_stencil_autotuner_times_launches_that_work(cuda, monkeypatch):
+    """Each candidate the autotuner times must do the stencil's work: its mean
+    launch time is at least the algorithmic bytes over 10 TB/s (more than any
+    B200 HBM can move), far above the few microseconds of a launch that
+    returns at once.  200x184x96 nodes (269 MB per apply), 8 FP32 RHS, a
+    shape no other test uses, so this plan runs the autotuner."""
+    import ctypes
+
+    from fieldspice_b200 import _lib as L
+    monkeypatch.delenv("FS_STENCIL", raising=False)
+    shape = (200, 184, 96)
+    sys_ = _uniform_system(shape, 8, "mixed")
+    ms = (ctypes.c_float * 5)()
+    L.check("fs_pcg_plan_stencil_times", L.lib().fs_pcg_plan_stencil_times(sys_.plan, ms))
+    kind = L.lib().fs_pcg_plan_stencil_kind(sys_.plan)
+    sys_.close()
+    N = int(np.prod(shape))
+    floor_ms = N * (2 * 8 * 4 + 3 * 4) / 10e12 * 1e3
+    timed = {c: ms[c] for c in range(5) if ms[c] >= 0}
+    assert set(timed) == {0, 2, 3, 4}, list(ms)
+    for c, t in timed.items():
+        assert t >= floor_ms, (c, t, floor_ms)
+    assert timed[kind] == min(timed.values())
+
+
+@pytest.mark.parametrize("precision,k", [("mixed", 8), ("fp64", 4)])
+def test_tma_split_selected_for_32_byte_nodes(cuda, monkeypatch, precision, k):
+    """FS_STENCIL=tma_split runs the split kernel (kind 4) whenever a node is
+    32 bytes (8 FP32 or 4 FP64 values); other widths fall back to kind 2."""
+    from fieldspice_b200 import _lib as L
+    monkeypatch.setenv("FS_STENCIL", "tma_split")
+    sys_ = _uniform_system((48, 40, 32), k, precision)
+    assert L.lib().fs_pcg_plan_stencil_kind(sys_.plan) == 4
+    sys_.close()
+    other = 4 if k == 8 else 8
+    sys_ = _uniform_system((48, 40, 32), other, precision)
+    assert L.lib().fs_pcg_plan_stencil_kind(sys_.plan) == 2
+    sys_.close()
