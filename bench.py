@@ -161,6 +161,8 @@ def e2e_phase_report(calls, allocs):
         slow = max(out["phases"], key=lambda k: out["phases"][k][0])
         out["slowest_phase"] = slow
         out["allocs"] = allocs[i] if i < len(allocs) else None
+        out["summary"] = {"wall_ms": round(out["wall_ms"], 3), "cpu_ms": round(out["cpu_ms"], 3),
+                          "slowest_phase": slow, "slowest_phase_ms": out["phases"][slow]}
         return out
     if not calls:
         return {"worst": None, "median": None}
@@ -285,10 +287,10 @@ def run_ours(args, rank, world, local_rank):
                               "gpu_launches": info["gpu_launches"]}), flush=True)
         return
 
+    # clocks sampled over both timed regions (device-resident and end to end)
     sampler = ClockSampler(local_rank)
     sampler.start()
     ms_dev, outs = timed(lambda: step_device(args.precision), args.steps, args.warmup)
-    clocks = sampler.stop()
     C, qs, info = outs[-1]
     launches = sum(o[2]["gpu_launches"] for o in outs)
     k_rhs = NBOX
@@ -304,6 +306,7 @@ def run_ours(args, rank, world, local_rank):
     h2d = D.TRANSFERS["h2d"] / (args.steps + 1)
     d2h = D.TRANSFERS["d2h"] / (args.steps + 1)
     e2e_value = n_solves_step * args.steps / (ms_e2e / 1000.0)
+    clocks = sampler.stop()
     timed_calls = e2e_phases[-args.steps:]
     timed_allocs = alloc_stats[-args.steps:]
     e2e_detail = e2e_phase_report(timed_calls, timed_allocs)
@@ -384,7 +387,7 @@ def run_ours(args, rank, world, local_rank):
                 "ms_per_step": ms_e2e / args.steps,
                 "step_ms_median": e2e_steps[len(e2e_steps) // 2] if e2e_steps else None,
                 "step_ms_max": e2e_steps[-1] if e2e_steps else None,
-                "worst_call": e2e_detail["worst"], "median_call": e2e_detail["median"]},
+                "worst_call": e2e_detail["worst"]["summary"] if e2e_detail["worst"] else None},
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": gbs.get(dom), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s",
@@ -392,7 +395,6 @@ def run_ours(args, rank, world, local_rank):
             "traffic": (traffic * N if traffic else None),
             "algorithmic_bytes_per_launch": kb[dom],
             "ms_per_launch": times[dom], "samples": km["samples"],
-            "all_kernels_gbs": gbs, "all_kernels_ms": times,
             "precond_ms_per_iteration": km.get("precond_ms"),
         },
         "stencil_gbs": gbs.get("stencil"),
@@ -413,10 +415,12 @@ def run_ours(args, rank, world, local_rank):
     if line["learned_value"] and line["plain_pcg_value"]:
         line["learned_vs_plain_pcg"] = line["learned_value"] / line["plain_pcg_value"]
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(shape, info["iterations"], args.cpu_sample_iters)
-    # the variants in full on their own line first; the headline line last
-    if variants:
-        print(json.dumps({"variants": variants}), flush=True)
+        line["cpu_baseline"] = cpu_baseline(shape, info["iterations"],
+                                            max(2, args.cpu_sample_iters // NBOX))
+    # the variants and the e2e phase record in full on their own line first;
+    # the headline line last
+    print(json.dumps({"variants": variants, "e2e_calls": e2e_detail,
+                      "roofline_all_kernels": {"gbs": gbs, "ms": times}}), flush=True)
     print(json.dumps(line), flush=True)
 
 
@@ -460,6 +464,9 @@ def learned_variant(timed, step_device, C_default, args):
     ms, outs = timed(lambda: step_device("mixed", "learned", net), nv, 1)
     Cl, _, info = outs[-1]
     ms0, outs0 = timed(lambda: step_device("mixed", "learned", net.zero()), 1, 0)
+    # the same V-cycle with its own multigrid recursion below the network's
+    # level: plain multigrid PCG, the honest "method without the network"
+    ms_mg, outs_mg = timed(lambda: step_device("mixed", "mg"), nv, 1)
     scale = float(np.abs(np.diag(C_default)).max())
     err = None
     if FULLSIZE_JSON.exists() and tuple(int(v) for v in args.shape.split(",")) == SHAPE:
@@ -476,6 +483,10 @@ def learned_variant(timed, step_device, C_default, args):
                     f"output as the level-{LEVEL} correction",
             "network_zeroed": {"value": NBOX / (ms0 / 1000.0),
                                "iterations": outs0[-1][2]["iterations"]},
+            "multigrid_recursion": {"value": NBOX / (ms_mg / nv / 1000.0),
+                                    "iterations": outs_mg[-1][2]["iterations"],
+                                    "precond_ms": outs_mg[-1][2]["kernel_ms"]["precond_ms"]},
+            "vs_multigrid_recursion": (NBOX / (ms / nv / 1000.0)) / (NBOX / (ms_mg / nv / 1000.0)),
 
             "training": {"pairs": net.pairs, "geometries": len(train), "shape": [128, 128, 128],
                          "level": net.level, "epochs": EPOCHS, "batch": 8,
@@ -877,7 +888,7 @@ def run_reference(args, rank, world):
                           "unavailable": "reference package not installed in baseline/_ref"}),
               flush=True)
         return
-    sample = max(5, args.cpu_sample_iters // 4)
+    sample = max(2, args.cpu_sample_iters // 16)
     iters, src = _reference_iterations()
     calls = []
     for s_ in range(args.warmup + args.steps):

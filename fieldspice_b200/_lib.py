@@ -18,14 +18,14 @@ __all__ = ["lib", "FsRhsStats", "check", "FsError", "stream_ptr", "ptr",
            "FS_OK", "FS_NOT_CONVERGED", "FS_TIMEOUT", "FS_BAD_ARG", "FS_NAN",
            "FS_CUDA_ERROR", "FS_STALLED", "LABEL_FREE", "LABEL_FIXED", "LABEL_SOLO",
            "LABEL_PINNED", "DTYPE_F64", "DTYPE_F32", "PRECISION_FP64",
-           "PRECISION_MIXED", "PRECOND_JACOBI", "PRECOND_MG", "AVERAGE_PARALLEL", "AVERAGE_HARMONIC",
+           "PRECISION_MIXED", "PRECOND_JACOBI", "PRECOND_MG", "PRECOND_MG_AGG", "AVERAGE_PARALLEL", "AVERAGE_HARMONIC",
            "EXPORTED_SYMBOLS", "load_library"]
 
 FS_OK, FS_NOT_CONVERGED, FS_TIMEOUT, FS_BAD_ARG, FS_NAN, FS_CUDA_ERROR, FS_STALLED = range(7)
 LABEL_FREE, LABEL_FIXED, LABEL_SOLO, LABEL_PINNED = range(4)
 DTYPE_F64, DTYPE_F32 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-PRECOND_JACOBI, PRECOND_MG = 0, 1
+PRECOND_JACOBI, PRECOND_MG, PRECOND_MG_AGG = 0, 1, 2
 AVERAGE_PARALLEL, AVERAGE_HARMONIC = 0, 1
 
 
@@ -105,6 +105,10 @@ _SIGNATURES = {
     "fs_pcg_plan_label_counts": (c_int, [c_void_p, POINTER(c_longlong), c_void_p]),
     "fs_pcg_plan_stencil_kind": (c_int, [c_void_p]),
     "fs_pcg_plan_stencil_times": (c_int, [c_void_p, POINTER(c_float)]),
+    "fs_conv3d_wgrad_workspace_bytes": (c_int, [c_int, c_int, POINTER(c_size_t)]),
+    "fs_conv3d_wgrad_bf16": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
+                                     c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_size_t, c_void_p, c_void_p]),
     "fs_ac_workspace_bytes": (c_int, [c_int, c_int, c_int, c_int, c_int, POINTER(c_size_t)]),
     "fs_ac_solve": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                             c_void_p, c_double, c_int, c_void_p, c_size_t,

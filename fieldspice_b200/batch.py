@@ -93,7 +93,8 @@ class _Extraction:
         self.tol = float(cfg.tol)
         self.system = EliminatedSystem(
             self.op, label, nt, precision=gcfg.precision,
-            preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned)
+            preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned,
+            coarsening=gcfg.coarsening)
         self.maxiter = (self.system.default_maxiter() if gcfg.maxiter is None
                         else int(gcfg.maxiter))
         group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)

@@ -6,6 +6,9 @@ among Dirichlet-like walls the later wall in ``xlo, xhi, ylo, yhi, zlo, zhi``
 wins on a shared node.  Dirichlet, homogeneous Neumann and symmetry walls
 are supported on the GPU path; the reference's own ``BoundarySpec`` objects
 are accepted as long as every wall is one of those (:func:`check_supported`).
+A driven Neumann flux is the right-hand-side load of :func:`neumann_load`
+(``BoundarySpec.neumann_load``, ``:1031-1085``), which the reference applies
+in ``PoissonSolver.solve`` only (``poisson.py:957-964``).
 """
 
 from __future__ import annotations
@@ -16,7 +19,8 @@ from typing import Callable
 import numpy as np
 
 __all__ = ["WALLS", "Dirichlet", "Neumann", "Periodic", "BoundarySpec", "wall_nodes",
-           "dirichlet_nodes", "check_supported", "periodic_mask"]
+           "wall_dual_areas", "dirichlet_nodes", "neumann_load", "check_supported",
+           "periodic_mask"]
 
 WALLS = ("xlo", "xhi", "ylo", "yhi", "zlo", "zhi")
 _AXIS = {"xlo": 0, "xhi": 0, "ylo": 1, "yhi": 1, "zlo": 2, "zhi": 2}
@@ -37,11 +41,28 @@ class Dirichlet:
 
 @dataclass(frozen=True)
 class Neumann:
-    """Prescribed outward normal flux; the GPU path supports flux = 0."""
-    flux: float = 0.0
+    """Prescribed outward normal flux density (``boundaries.py:384-460``):
+    ``J.n`` [A/m^2] with a conductance operator, ``D.n`` [C/m^2] with a
+    capacitance one; a float, a 1-D array over the wall's nodes, or a
+    callable of t.  ``0`` is the natural (homogeneous) condition and needs
+    nothing; a driven flux enters ``PoissonSolver.solve``'s right-hand side
+    through :func:`neumann_load`."""
+    flux: float | Callable[[float], float] = 0.0
 
     is_dirichlet_like = False
-    is_natural = True
+
+    @property
+    def is_natural(self) -> bool:
+        return not callable(self.flux) and bool(np.all(np.asarray(self.flux, float) == 0.0))
+
+    def flux_at(self, t: float = 0.0) -> np.ndarray:
+        f = self.flux(float(t)) if callable(self.flux) else self.flux
+        arr = np.asarray(f, dtype=float)
+        if arr.ndim > 1:
+            raise ValueError(f"Neumann flux must be scalar or 1-D, got shape {arr.shape}")
+        if not np.all(np.isfinite(arr)):
+            raise ValueError(f"Neumann flux is not finite at t = {t} s")
+        return arr
 
     def prescribed_value(self, t: float = 0.0):
         return None
@@ -143,12 +164,7 @@ def check_supported(spec, allow_periodic: bool = False) -> None:
         if getattr(bc, "is_dirichlet_like", False):
             continue  # Dirichlet, or a PEC symmetry wall at its value
         if kind == "neumann":
-            flux = getattr(bc, "flux", 0.0)
-            if callable(flux) or np.any(np.asarray(flux, dtype=float) != 0.0):
-                raise NotImplementedError(
-                    f"wall {w}: driven Neumann flux is not supported on the GPU "
-                    "path; only homogeneous Neumann walls are")
-            continue
+            continue  # homogeneous, or a driven flux load (neumann_load)
         if getattr(bc, "is_natural", False) and kind != "periodic":
             continue  # PMC symmetry: the natural zero-flux condition
         raise NotImplementedError(
@@ -181,3 +197,41 @@ def dirichlet_nodes(spec, grid, t: float = 0.0):
     val_all = np.concatenate(val_parts)
     uniq, first_in_rev = np.unique(idx_all[::-1], return_index=True)
     return uniq.astype(np.intp, copy=False), val_all[::-1][first_in_rev]
+
+
+def wall_dual_areas(grid, wall: str) -> np.ndarray:
+    """Dual-face area of each wall node, in :func:`wall_nodes` order: the
+    product of the two in-plane dual widths (half widths at the edges)."""
+    if wall not in _AXIS:
+        raise ValueError(f"unknown wall {wall!r}; expected one of {WALLS}")
+    hd = [np.asarray(grid.hxd, float), np.asarray(grid.hyd, float),
+          np.asarray(grid.hzd, float)]
+    d0, d1 = [d for d in (0, 1, 2) if d != _AXIS[wall]]
+    return (hd[d0][:, None] * hd[d1][None, :]).ravel()
+
+
+def neumann_load(spec, grid, t: float = 0.0):
+    """Right-hand-side load of the driven Neumann walls, or ``None`` when
+    every Neumann wall is homogeneous (``boundaries.py:1031-1085``): the
+    outward flux density times each wall node's dual-face area, with a minus
+    sign (KCL: ``L phi = q - flux * A``); walls add on shared edge and corner
+    nodes, and Dirichlet wall nodes get no load."""
+    load = None
+    for w in WALLS:
+        bc = _wall(spec, w)
+        if type(bc).__name__.lower() != "neumann" or getattr(bc, "is_natural", True):
+            continue
+        idx = wall_nodes(grid, w)
+        try:
+            f = np.broadcast_to(bc.flux_at(t), idx.shape)
+        except ValueError as exc:
+            raise ValueError(f"wall {w}: Neumann flux of shape {np.shape(bc.flux_at(t))} "
+                             f"cannot be broadcast to the {idx.size} nodes on that "
+                             "wall") from exc
+        if load is None:
+            load = np.zeros(int(np.prod(grid.shape_nodes)))
+        load[idx] += -f * wall_dual_areas(grid, w)
+    if load is not None:
+        fixed, _ = dirichlet_nodes(spec, grid, t)
+        load[fixed] = 0.0
+    return load

@@ -210,7 +210,8 @@ class FieldRegion:
                 system = EliminatedSystem(K, self._label, len(cols),
                                           precision=self.gpu.precision,
                                           preconditioner=resolve_preconditioner(
-                                              self.cfg, self.gpu))
+                                              self.cfg, self.gpu),
+                                          coarsening=self.gpu.coarsening)
                 self._excite(system.phi, cols, k)
                 _, st = system.solve(tol, self.gpu.maxiter)
                 raise_on_status(st, tol, "gpu-cg")
@@ -242,7 +243,8 @@ class FieldRegion:
                 entry.history = EliminatedSystem(
                     entry.K, self._label, 1, precision=self.gpu.precision,
                     with_source=True,
-                    preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+                    preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+                    coarsening=self.gpu.coarsening)
             hs = entry.history
             nx, ny, nz = self.op_eps.shape
             m = entry.K_hist

@@ -450,4 +450,184 @@ __global__ void k_pack_weights(const float* __restrict__ w, int cin, int cout, i
 }
 #endif  // FS_CONV_DEFINE_KERNELS
 
+// ---- weight gradient on tensor cores ----------------------------------------------
+//   dW[t][co][ci] = sum_r dY[r][co] * X[r + off_t][ci]
+// is, per tap, a GEMM whose reduction index is the voxel row r: D[co][ci] +=
+// A B^T with A = dY (M = co, K = r) and B = the tap-shifted X (N = ci, K = r).
+// In the activation layout a row holds 8 channels per 16 bytes, so both
+// operands are MN-major (channels contiguous) and a one-row shift of the tap
+// window is +16 bytes of descriptor start address, as in the forward pass.
+// A CTA owns `rows_per` rows (a multiple of 128) and a group of taps with the
+// same dx (all 9 when 9 * cin columns fit in tensor memory, else the 3 taps of
+// one (dx, dy)); per 128-row subtile it stages dY (16 channel groups; groups
+// past cout stay zero, so M = 128 always) and the X window covering its taps
+// with 2-D TMA loads into a two-stage ring, one thread issues
+// ntap * 8 MMAs (M = 128, N = cin, K = 16) accumulating in tensor memory, and
+// at the end four warps drain D (lane = co) into the CTA's partial
+// pw[blockIdx.x][t][co][ci].  Waits are bounded: on a timeout the CTA records
+// an error, waits (bounded) for its own copies and MMAs, frees tensor memory
+// and returns.
+struct WgradArgs {
+  ConvGeom g;
+  int cin, cin_off, cout, cout_off;
+  int ntap;             // 9 (one dx) or 3 (one dx, dy) per blockIdx.y
+  long long rows_per;   // rows per blockIdx.x, a multiple of 128
+  int W, BR;            // X window rows (multiple of BR) and TMA box rows
+  float* pw;            // [gridDim.x][27][cout][cin]
+  int* error;
+};
+
+constexpr int kWgradThreads = 128;
+
+#ifdef FS_CONV_DEFINE_KERNELS
+__global__ void __launch_bounds__(kWgradThreads, 1)
+    k_conv_wgrad_tc(const __grid_constant__ CUtensorMap xmap,
+                    const __grid_constant__ CUtensorMap ymap, WgradArgs a) {
+  extern __shared__ uint8_t wg_smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)wg_smem_raw + 1023) & ~(uintptr_t)1023);
+  constexpr uint32_t kAgrp = 128u * 16u;           // one 8-channel group of 128 rows
+  const uint32_t abytes = 16u * kAgrp;             // dY stage: 16 groups (M = 128)
+  const int ncx = a.cin >> 3, ncy = a.cout >> 3;
+  const uint32_t colb = (uint32_t)a.W * 16u;       // one 8-channel group of the window
+  const uint32_t stage = abytes + (uint32_t)ncx * colb;
+  uint64_t* full = (uint64_t*)(smem + 2 * stage);  // [2] TMA -> MMA
+  uint64_t* done = full + 2;                       // [2] MMA -> stage free
+  uint32_t* tslot = (uint32_t*)(done + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long r_begin = (long long)blockIdx.x * a.rows_per;
+  const long long r_end = min(a.g.R, r_begin + a.rows_per);
+  const int nsub = r_end > r_begin ? (int)((r_end - r_begin + 127) / 128) : 0;
+  // taps of this CTA: t = dx*9 + dy*3 + dz; ntap = 9: dx = y; ntap = 3: (dx, dy)
+  const int t0 = blockIdx.y * a.ntap;
+  const int dx = t0 / 9;
+  const uint32_t ncols = tmem_cols(a.ntap * a.cin);
+  // zero the dY channel groups past cout in both stages (M is always 128)
+  for (uint32_t e = tid; e < (uint32_t)(16 - ncy) * kAgrp / 16u; e += blockDim.x) {
+    const uint32_t off = (uint32_t)ncy * kAgrp + e * 16u;
+    *(uint4*)(smem + off) = make_uint4(0, 0, 0, 0);
+    *(uint4*)(smem + stage + off) = make_uint4(0, 0, 0, 0);
+  }
+  fence_proxy_async_smem();
+  if (tid == 0) {
+    for (int i = 0; i < 4; ++i) mbar_init(&full[i], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc_alloc(tslot, ncols);
+    tc_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  bool ok = true;
+  int loaded = 0, mma_done = 0;  // subtiles whose loads / MMAs were issued (thread 0)
+  if (tid == 0) {
+    const uint32_t idesc = umma_idesc_bf16_mn(128, a.cin);
+    const int nseg = a.W / a.BR;
+    auto issue = [&](int i) {
+      uint8_t* st = smem + (size_t)(i & 1) * stage;
+      const long long m0 = r_begin + 128LL * i;
+      mbar_arrive_expect_tx(&full[i & 1], (uint32_t)ncy * kAgrp + (uint32_t)ncx * colb);
+      for (int c = 0; c < ncy; ++c)
+        tma_load_2d(st + (size_t)c * kAgrp, &ymap, &full[i & 1], a.cout_off + 8 * c, (int)m0);
+      const long long r0 = m0 + (long long)(dx - 1) * a.g.S - a.g.Zp - 1;
+      for (int c = 0; c < ncx; ++c)
+        for (int sg = 0; sg < nseg; ++sg)
+          tma_load_2d(st + abytes + (size_t)c * colb + (size_t)sg * a.BR * 16, &xmap,
+                      &full[i & 1], a.cin_off + 8 * c, (int)(r0 + (long long)sg * a.BR));
+      loaded = i + 1;
+    };
+    if (nsub > 0) issue(0);
+    for (int i = 0; i < nsub && ok; ++i) {
+      if (i + 1 < nsub) {
+        // the other stage is free once the MMAs of subtile i - 1 completed
+        if (i >= 1) ok = mbar_wait_bounded(&done[(i - 1) & 1], (uint32_t)(((i - 1) >> 1) & 1),
+                                           kConvBudget);
+        if (!ok) break;
+        issue(i + 1);
+      }
+      ok = mbar_wait_bounded(&full[i & 1], (uint32_t)((i >> 1) & 1), kConvBudget);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t sa = smem_u32(smem + (size_t)(i & 1) * stage);
+      const uint32_t sb = sa + abytes;
+      for (int tl = 0; tl < a.ntap; ++tl) {
+        const int t = t0 + tl;
+        const int dy = (t / 3) % 3, dz = t % 3;
+        const uint32_t woff = (uint32_t)(dy * a.g.Zp + dz) * 16u;
+        for (int kk = 0; kk < 8; ++kk) {  // 16 rows per MMA
+          const uint64_t ad = umma_desc(sa + (uint32_t)kk * 256u, 128u, kAgrp);
+          const uint64_t bd = umma_desc(sb + woff + (uint32_t)kk * 256u, 128u, colb);
+          tc_mma_bf16(tbase + (uint32_t)(tl * a.cin), ad, bd, idesc,
+                      (i > 0 || kk > 0) ? 1u : 0u);
+        }
+      }
+      tc_commit(&done[i & 1]);
+      mma_done = i + 1;
+    }
+    if (ok && nsub > 0)
+      ok = mbar_wait_bounded(&done[(nsub - 1) & 1], (uint32_t)(((nsub - 1) >> 1) & 1),
+                             kConvBudget);
+    if (!ok) {
+      // bounded wait for this CTA's own transfers and MMAs still in flight
+      if (loaded > 0)
+        (void)mbar_wait_bounded(&full[(loaded - 1) & 1], (uint32_t)(((loaded - 1) >> 1) & 1),
+                                kConvBudget);
+      if (mma_done > 0)
+        (void)mbar_wait_bounded(&done[(mma_done - 1) & 1],
+                                (uint32_t)(((mma_done - 1) >> 1) & 1), kConvBudget);
+      if (a.error) atomicExch(a.error, 1);
+    }
+  }
+  ok = __syncthreads_and(ok);
+  tc_fence_after();
+  if (ok) {
+    // lane = co; columns tl * cin + ci
+    const int co = warp * 32 + lane;
+    for (int tl = 0; tl < a.ntap; ++tl) {
+      for (int q = 0; q < (a.cin >> 4); ++q) {
+        float v[16];
+        if (nsub > 0) {
+          tc_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(tl * a.cin + q * 16), v);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] = 0.0f;
+        }
+        if (co >= a.cout) continue;
+        float* dst = a.pw + (((size_t)blockIdx.x * 27 + t0 + tl) * a.cout + co) * a.cin + q * 16;
+#pragma unroll
+        for (int e = 0; e < 16; e += 4) *(float4*)(dst + e) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc_dealloc(tbase, ncols);
+}
+
+// Bias gradient partials: pb[blockIdx.x][co] = sum of dY[r][co] over the rows
+// of group blockIdx.x (the same row groups as the weight gradient).
+__global__ void __launch_bounds__(256)
+    k_conv_bgrad(ConvGeom g, const __nv_bfloat16* __restrict__ dy, int ctot, int off, int cout,
+                 long long rows_per, float* __restrict__ pb) {
+  __shared__ float red[256];
+  const long long r_begin = (long long)blockIdx.x * rows_per;
+  const long long r_end = min(g.R, r_begin + rows_per);
+  const int per = 256 / cout;  // rows handled side by side (cout divides 256 or not: rest idle)
+  const int c = threadIdx.x % cout, lane_r = threadIdx.x / cout;
+  float acc = 0.0f;
+  if (lane_r < per)
+    for (long long r = r_begin + lane_r; r < r_end; r += per)
+      acc += __bfloat162float(dy[r * ctot + off + c]);
+  red[threadIdx.x] = lane_r < per ? acc : 0.0f;
+  __syncthreads();
+  if (threadIdx.x < cout) {
+    float s = 0.0f;
+    for (int k = 0; k < per; ++k) s += red[k * cout + threadIdx.x];
+    pb[(size_t)blockIdx.x * cout + threadIdx.x] = s;
+  }
+}
+#endif  // FS_CONV_DEFINE_KERNELS
+
 }  // namespace fs

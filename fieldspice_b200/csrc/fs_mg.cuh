@@ -590,4 +590,139 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// ---- aggregation hierarchy: Galerkin coarse operators --------------------------
+// The alternative hierarchy (FS_PRECOND_MG_AGG) for strongly discontinuous
+// coefficients (copper in oxide: edge masses 1e6 apart), where rediscretised
+// coarse operators and trilinear transfers smear a conductor over its
+// surroundings.  Coarse node I is the aggregate of the fine nodes
+// r*I .. r*I + r - 1 on each axis (r = 2 where the axis is coarsened, 1 where
+// it is kept; the last aggregate of an odd axis holds one node), so the level
+// sizes are those of the vertex-centred hierarchy.  P is 1 from an aggregate
+// to each of its FREE fine nodes and 0 on fixed ones; the coarse operator is
+// exactly P^T A P, which keeps the 7-point form:
+//   coarse edge mass I -> I+1 = the sum of the free-free fine edges crossing
+//     from aggregate I to aggregate I+1;
+//   coarse node term d_c(I) = sum over the aggregate's free nodes of their
+//     own term plus the masses of their edges to fixed nodes (the part of
+//     the diagonal the coarse edges do not carry); edges inside an aggregate
+//     cancel.
+// An aggregate with no free node is fixed.  A conductor region therefore
+// stays one strongly coupled block on every level, and its near-constant
+// modes (a floating copper box) have an exact coarse representation.
+
+__global__ void k_agg_coarsen(Dims f, Dims c, const double* __restrict__ fmx,
+                              const double* __restrict__ fmy,
+                              const double* __restrict__ fmz,
+                              const double* __restrict__ fdg,
+                              const uint8_t* __restrict__ flabel,
+                              double* __restrict__ cmx, double* __restrict__ cmy,
+                              double* __restrict__ cmz, double* __restrict__ cdg,
+                              uint8_t* __restrict__ clabel) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    int I, J, Kc;
+    node_ijk(c, n, I, J, Kc);
+    const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+    const int i0 = rx * I, j0 = ry * J, k0 = rz * Kc;
+    const int i1 = min(i0 + rx, f.nx) - 1, j1 = min(j0 + ry, f.ny) - 1,
+              k1 = min(k0 + rz, f.nz) - 1;
+    bool any_free = false;
+    double dg = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int i = i0; i <= i1; ++i)
+      for (int j = j0; j <= j1; ++j)
+        for (int k = k0; k <= k1; ++k) {
+          const long long fn = ((long long)i * f.ny + j) * f.nz + k;
+          if (flabel[fn] != FS_LABEL_FREE) continue;
+          any_free = true;
+          if (fdg) dg += fdg[fn];
+          // one fine edge of this free node: to a fixed node it stays on the
+          // diagonal; to a free node of the next aggregate up it is part of
+          // the coarse edge; inside the aggregate or towards the aggregate
+          // below (counted there) it adds nothing here
+          auto edge = [&](bool exists, double m, long long nb, bool up_cross, double& acc) {
+            if (!exists || m == 0.0) return;
+            if (flabel[nb] != FS_LABEL_FREE)
+              dg += m;
+            else if (up_cross)
+              acc += m;
+          };
+          double none = 0.0;
+          edge(i > 0, i > 0 ? fmx[fn - f.sx] : 0.0, fn - f.sx, false, none);
+          edge(i + 1 < f.nx, fmx[fn], fn + f.sx, i == i1, sx);
+          edge(j > 0, j > 0 ? fmy[fn - f.sy] : 0.0, fn - f.sy, false, none);
+          edge(j + 1 < f.ny, fmy[fn], fn + f.sy, j == j1, sy);
+          edge(k > 0, k > 0 ? fmz[fn - 1] : 0.0, fn - 1, false, none);
+          edge(k + 1 < f.nz, fmz[fn], fn + 1, k == k1, sz);
+        }
+    clabel[n] = any_free ? FS_LABEL_FREE : FS_LABEL_FIXED;
+    cdg[n] = any_free ? dg : 0.0;
+    cmx[n] = I + 1 < c.nx ? sx : 0.0;
+    cmy[n] = J + 1 < c.ny ? sy : 0.0;
+    cmz[n] = Kc + 1 < c.nz ? sz : 0.0;
+  }
+}
+
+// b_c(I) = s_c(I) * sum over the aggregate of sd_f(i) res(i)
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_agg_restrict(Dims f, Dims c, const T* __restrict__ res, const T* __restrict__ sdf,
+                   const T* __restrict__ sc, T* __restrict__ bc,
+                   const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const T scale = sc[n];
+    T acc[K];
+#pragma unroll
+    for (int t = 0; t < K; ++t) acc[t] = (T)0;
+    if (scale != (T)0) {
+      int I, J, Kc;
+      node_ijk(c, n, I, J, Kc);
+      const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+      const int i1 = min(rx * I + rx, f.nx), j1 = min(ry * J + ry, f.ny),
+                k1 = min(rz * Kc + rz, f.nz);
+      for (int i = rx * I; i < i1; ++i)
+        for (int j = ry * J; j < j1; ++j)
+          for (int k = rz * Kc; k < k1; ++k) {
+            const long long fn = ((long long)i * f.ny + j) * f.nz + k;
+            const T w = __ldg(sdf + fn);
+            if (w == (T)0) continue;
+            T v[K];
+            ldv_ro<T, K>(res, fn, v);
+#pragma unroll
+            for (int t = 0; t < K; ++t) acc[t] += w * v[t];
+          }
+#pragma unroll
+      for (int t = 0; t < K; ++t) acc[t] *= scale;
+    }
+    stv<T, K>(bc, n, acc);
+  }
+}
+
+// x_f(i) += sd_f(i) * s_c(I) * x_c(I), I the aggregate of fine node i (one
+// thread per fine node: coalesced fine accesses, coarse values from cache).
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_agg_prolong(Dims f, Dims c, const T* __restrict__ xc, const T* __restrict__ sc,
+                  const T* __restrict__ sdf, T* __restrict__ xf,
+                  const int* __restrict__ done) {
+  if (*done) return;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < f.N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const T sf = __ldg(sdf + n);
+    if (sf == (T)0) continue;
+    int i, j, k;
+    node_ijk(f, n, i, j, k);
+    const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
+    const long long cn = ((long long)(i / rx) * c.ny + j / ry) * c.nz + k / rz;
+    const T w = sf * __ldg(sc + cn);
+    T v[K], xv[K];
+    ldv_ro<T, K>(xc, cn, v);
+    ldv<T, K>(xf, n, xv);
+#pragma unroll
+    for (int t = 0; t < K; ++t) xv[t] += w * v[t];
+    stv<T, K>(xf, n, xv);
+  }
+}
+
 }  // namespace fs

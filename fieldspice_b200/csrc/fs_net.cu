@@ -96,6 +96,61 @@ int act_map(CUtensorMap* map, const void* base, int ctot, long long rows, int bo
   return FS_OK;
 }
 
+int wgrad_tc_launch(const ConvGeom& g, const void* x, int ctot_x, int xoff, int cin,
+                    const void* dy, int ctot_y, int yoff, int cout, int groups,
+                    long long rows_per, float* pw, float* pb, int* error, cudaStream_t s) {
+  if (cin < 16 || cin % 16 || cin > 160 || cout < 16 || cout % 16 || cout > 128 ||
+      xoff % 8 || yoff % 8 || ctot_x % 8 || ctot_y % 8 || xoff + cin > ctot_x ||
+      yoff + cout > ctot_y || !x || !dy || !pw || ((uintptr_t)x & 15) || ((uintptr_t)dy & 15) ||
+      groups < 1 || rows_per < 128 || rows_per % 128 || g.R <= 0 ||
+      (long long)groups * rows_per < g.R) {
+    fs_set_error_msg("conv3d wgrad: bad channel counts, offsets, alignment or row groups");
+    return FS_BAD_ARG;
+  }
+  WgradArgs a;
+  a.g = g;
+  a.cin = cin;
+  a.cin_off = xoff;
+  a.cout = cout;
+  a.cout_off = yoff;
+  a.ntap = 9 * cin <= 512 ? 9 : 3;  // tensor-memory columns ntap * cin <= 512
+  a.rows_per = rows_per;
+  const long long need = 128 + 2LL * g.Zp + 2;
+  const int nseg = (int)((need + 255) / 256);
+  a.BR = (int)(((need + nseg - 1) / nseg + 7) / 8 * 8);
+  a.W = nseg * a.BR;
+  a.pw = pw;
+  a.error = error;
+  const size_t stage = 16u * 128u * 16u + (size_t)(cin / 8) * a.W * 16u;
+  const size_t smem = 1024 + 2 * stage + 64;
+  if (smem > 227u * 1024u) {
+    fs_set_error_msg("conv3d wgrad: window does not fit in shared memory");
+    return FS_BAD_ARG;
+  }
+  CUtensorMap xmap, ymap;
+  int st = act_map(&xmap, x, ctot_x, g.R, a.BR);
+  if (st != FS_OK) return st;
+  st = act_map(&ymap, dy, ctot_y, g.R, 128);
+  if (st != FS_OK) return st;
+  static bool attr[fs::kMaxDevices] = {};
+  if (!attr[fs::current_device_slot()]) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad_tc,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e != cudaSuccess) return fs_cuda_status("cudaFuncSetAttribute(wgrad)", e);
+    attr[fs::current_device_slot()] = true;
+  }
+  dim3 grid((unsigned)groups, (unsigned)(27 / a.ntap));
+  k_conv_wgrad_tc<<<grid, kWgradThreads, smem, s>>>(xmap, ymap, a);
+  FS_CHECK_LAUNCH("k_conv_wgrad_tc");
+  if (pb) {
+    k_conv_bgrad<<<groups, 256, 0, s>>>(g, (const __nv_bfloat16*)dy, ctot_y, yoff, cout,
+                                        rows_per, pb);
+    FS_CHECK_LAUNCH("k_conv_bgrad");
+  }
+  return FS_OK;
+}
+
 int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s) {
   if (io.cin < 16 || io.cin % 16 || io.cout < 16 || io.cout % 16 || io.cout > 128 ||
       io.cin_off % 8 || io.ctot_in % 8 || io.out_off % 8 || io.ctot_out % 8 ||

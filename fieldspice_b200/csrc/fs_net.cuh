@@ -37,6 +37,12 @@ ConvGeom conv_geom(int batch, int X, int Y, int Z);
 bool conv_config(const ConvGeom& g, int cin, int cout, ConvCfg* c);
 int conv_launch(const ConvGeom& g, const ConvIO& io, cudaStream_t s);
 int pack_weights(const float* w, int cin, int cout, int flip, void* out, cudaStream_t s);
+// Weight-gradient partials of one convolution on tensor cores:
+// pw[G][27][cout][cin] (and pb[G][cout] when pb is not NULL) over G row
+// groups of rows_per rows (a multiple of 128) each.
+int wgrad_tc_launch(const ConvGeom& g, const void* x, int ctot_x, int xoff, int cin,
+                    const void* dy, int ctot_y, int yoff, int cout, int groups,
+                    long long rows_per, float* pw, float* pb, int* error, cudaStream_t s);
 
 }  // namespace fs
 

@@ -2346,7 +2346,7 @@ Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
   L.st = o; o = align_up(o + sizeof(RhsState) * fs::kMaxRhs);
   L.ctl = o; o = align_up(o + sizeof(Control));
   L.nlev = 0;
-  if (precond == FS_PRECOND_MG) {
+  if (precond == FS_PRECOND_MG || precond == FS_PRECOND_MG_AGG) {
     Dims dl[kMaxLevels];
     L.nlev = mg_dims(d, g_mg.coarsest_nodes, dl);
     for (int l = 0; l < L.nlev; ++l) {
@@ -2413,6 +2413,7 @@ void host_slot_put(HostSlot* slot) {
 struct fs_pcg_plan {
   Dims d;
   int nrhs, precision, precond;
+  int agg;                 // multigrid levels by aggregation (Galerkin coarse operators)
   int nlev;
   MgLevel lev[kMaxLevels];
   void* z;                 // preconditioned residual (level-0 V-cycle output)
@@ -2859,18 +2860,28 @@ struct Impl {
       const double* fm[3] = {l == 1 ? P->mx : f.m64[0], l == 1 ? P->my : f.m64[1],
                              l == 1 ? P->mz : f.m64[2]};
       const uint8_t* flab = l == 1 ? P->label : f.label;
-      g = fs_grid_blocks((const void*)fs::k_mg_coarsen, c.d.N);
-      fs::k_mg_coarsen<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fm[0], fm[1], fm[2],
-                                                flab, c.m64[0], c.m64[1],
-                                                c.m64[2], c.label_in);
-      if (P->dg) {
-        g = fs_grid_blocks((const void*)fs::k_mg_coarsen_diag, c.d.N);
-        fs::k_mg_coarsen_diag<<<g, fs::kBlock, 0, s>>>(f.d, c.d, l == 1 ? P->dg : f.d64,
-                                                       c.d64);
+      // the fine level's node term: the plan's (level 1) or the Galerkin
+      // remainder of the level above (aggregation)
+      const double* fdg = l == 1 ? P->dg : ((P->agg || P->dg) ? f.d64 : nullptr);
+      if (P->agg) {
+        g = fs_grid_blocks((const void*)fs::k_agg_coarsen, c.d.N);
+        fs::k_agg_coarsen<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fm[0], fm[1], fm[2], fdg, flab,
+                                                   c.m64[0], c.m64[1], c.m64[2], c.d64,
+                                                   c.label_in);
+      } else {
+        g = fs_grid_blocks((const void*)fs::k_mg_coarsen, c.d.N);
+        fs::k_mg_coarsen<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fm[0], fm[1], fm[2],
+                                                  flab, c.m64[0], c.m64[1],
+                                                  c.m64[2], c.label_in);
+        if (P->dg) {
+          g = fs_grid_blocks((const void*)fs::k_mg_coarsen_diag, c.d.N);
+          fs::k_mg_coarsen_diag<<<g, fs::kBlock, 0, s>>>(f.d, c.d, fdg, c.d64);
+        }
       }
+      const bool cdiag = P->agg || P->dg;
       g = fs_grid_blocks((const void*)k_classify, c.d.N);
       k_classify<<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
-                                          P->dg ? c.d64 : nullptr, c.label_in, c.label,
+                                          cdiag ? c.d64 : nullptr, c.label_in, c.label,
                                           c.s64, nullptr);
       g = fs_grid_blocks((const void*)k_eq_masses<T>, c.d.N);
       k_eq_masses<T><<<g, fs::kBlock, 0, s>>>(c.d, c.m64[0], c.m64[1], c.m64[2],
@@ -3160,16 +3171,26 @@ struct Impl {
       if (!resform)
         fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
-      fs::k_mg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
-          L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
+      if (P->agg)
+        fs::k_agg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
+            L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
+      else
+        fs::k_mg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
+            L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
     }
     *nl += resform ? 1 : 2;
     const int cc = vcycle(P, l + 1, (const T*)C.b, s, nl, dry);
     if (!dry) {
-      const int gp = fs_grid_blocks((const void*)fs::k_mg_prolong_cell<T, K>, C.d.N);
-      fs::k_mg_prolong_cell<T, K><<<gp, fs::kBlock, 0, s>>>(
-          L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd,
-          (T*)L.x[cur], done);
+      if (P->agg) {
+        const int gp = fs_grid_blocks((const void*)fs::k_agg_prolong<T, K>, L.d.N);
+        fs::k_agg_prolong<T, K><<<gp, fs::kBlock, 0, s>>>(
+            L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd, (T*)L.x[cur], done);
+      } else {
+        const int gp = fs_grid_blocks((const void*)fs::k_mg_prolong_cell<T, K>, C.d.N);
+        fs::k_mg_prolong_cell<T, K><<<gp, fs::kBlock, 0, s>>>(
+            L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd,
+            (T*)L.x[cur], done);
+      }
     }
     ++*nl;
     const bool tr = !dry && l == 0 && P->trace;
@@ -3362,7 +3383,8 @@ int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
   if (nx < 2 || ny < 2 || nz < 2 || !valid_nrhs(nrhs) || !bytes) return FS_BAD_ARG;
   if (precision != FS_PRECISION_FP64 && precision != FS_PRECISION_MIXED)
     return FS_BAD_ARG;
-  if (precond != FS_PRECOND_JACOBI && precond != FS_PRECOND_MG) return FS_BAD_ARG;
+  if (precond != FS_PRECOND_JACOBI && precond != FS_PRECOND_MG && precond != FS_PRECOND_MG_AGG)
+    return FS_BAD_ARG;
   *bytes = make_layout(fs::make_dims(nx, ny, nz), nrhs, precision, precond).total;
   return FS_OK;
 }
@@ -3413,7 +3435,8 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   P->d = fs::make_dims(nx, ny, nz, periodic);
   P->nrhs = nrhs;
   P->precision = precision;
-  P->precond = precond == FS_PRECOND_MG ? 1 : 0;
+  P->precond = (precond == FS_PRECOND_MG || precond == FS_PRECOND_MG_AGG) ? 1 : 0;
+  P->agg = precond == FS_PRECOND_MG_AGG ? 1 : 0;
   P->mg = g_mg;
   P->launches_per_iter = 0;
   P->mx = mx;

@@ -33,6 +33,21 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
          | ((uint32_t)(M >> 4) << 24);     // M / 16
 }
 
+// The same with both operands MN-major (the M or N index contiguous in 16-byte
+// groups of 8 elements, K the strided index): bits 15 and 16 of the
+// instruction descriptor.  With no swizzle a core matrix is then 8 K-rows of
+// 16 bytes; LBO = byte distance between 8-row K groups, SBO = byte distance
+// between 8-element M (or N) groups.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int M, int N) {
+  return umma_idesc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
+// Make this thread's generic-proxy shared-memory writes visible to the async
+// proxy (tensor-core operand reads, TMA) before a barrier.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void tc_alloc(uint32_t* dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                    (uint32_t)__cvta_generic_to_shared(dst_smem)),

@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <new>
@@ -236,24 +237,40 @@ void wgrad_launch(const fs::ConvGeom& g, const Vol& x, int xoff, const Vol& dy, 
                                                 rows_per, pw, pb);
 }
 
+// The weight gradient of training: on CUDA cores unless FS_WGRAD=tc selects
+// the tensor-core kernel.
+bool wgrad_on_cuda_cores() {
+  const char* sel = getenv("FS_WGRAD");
+  return !(sel && strcmp(sel, "tc") == 0);
+}
+
 // Weight and bias gradient of conv l into U->grad.
 int conv_wgrad(fs_unet* U, int l, const Vol& x, int xoff, const Vol& dy, int yoff,
                cudaStream_t s) {
   const fs::ConvGeom& g = U->g[x.lev];
-  long long rows_per = (g.R + kWgGroups - 1) / kWgGroups;
-  rows_per = (rows_per + fs::kWgRows - 1) / fs::kWgRows * fs::kWgRows;
-  const int CO = kCout[l] / 16, CI = kCin[l] / 16;
   float* pw = U->pw;
   float* pb = U->pb;
+  if (!wgrad_on_cuda_cores()) {
+    // tensor cores: row groups of whole 128-row subtiles
+    long long rows_per = (g.R + kWgGroups - 1) / kWgGroups;
+    rows_per = (rows_per + 127) / 128 * 128;
+    const int st = fs::wgrad_tc_launch(g, x.p, x.ctot, xoff, kCin[l], dy.p, dy.ctot, yoff,
+                                       kCout[l], kWgGroups, rows_per, pw, pb, U->err, s);
+    if (st != FS_OK) return st;
+  } else {
+    long long rows_per = (g.R + kWgGroups - 1) / kWgGroups;
+    rows_per = (rows_per + fs::kWgRows - 1) / fs::kWgRows * fs::kWgRows;
+    const int CO = kCout[l] / 16, CI = kCin[l] / 16;
 #define FS_WG(a, b) \
   if (CO == a && CI == b) wgrad_launch<a, b>(g, x, xoff, dy, yoff, rows_per, pw, pb, s); else
-  FS_WG(1, 1) FS_WG(2, 1) FS_WG(2, 2) FS_WG(3, 2) FS_WG(3, 3) FS_WG(4, 3) FS_WG(4, 4)
-  FS_WG(3, 7) FS_WG(2, 5) FS_WG(1, 3) {
-    fs_set_error_msg("unet: no weight-gradient kernel for this layer shape");
-    return FS_BAD_ARG;
-  }
+    FS_WG(1, 1) FS_WG(2, 1) FS_WG(2, 2) FS_WG(3, 2) FS_WG(3, 3) FS_WG(4, 3) FS_WG(4, 4)
+    FS_WG(3, 7) FS_WG(2, 5) FS_WG(1, 3) {
+      fs_set_error_msg("unet: no weight-gradient kernel for this layer shape");
+      return FS_BAD_ARG;
+    }
 #undef FS_WG
-  FS_CHECK_LAUNCH("k_conv_wgrad");
+    FS_CHECK_LAUNCH("k_conv_wgrad");
+  }
   const long long nw = 27LL * kCin[l] * kCout[l];
   fs::k_sum_groups<<<blocks_for(nw), 256, 0, s>>>(nw, kWgGroups, pw, U->grad + conv_woff(l));
   fs::k_sum_groups<<<1, 256, 0, s>>>(kCout[l], kWgGroups, pb, U->grad + conv_boff(l));
@@ -428,6 +445,37 @@ int unet_init(fs_unet* U, int X, int Y, int Z, int batch, int train, float* thet
 }
 
 extern "C" {
+
+int fs_conv3d_wgrad_workspace_bytes(int cin, int cout, size_t* bytes) {
+  if (cin < 16 || cout < 16 || !bytes) return FS_BAD_ARG;
+  *bytes = sizeof(float) * (size_t)kWgGroups * (27ull * cin * cout + cout) + 256;
+  return FS_OK;
+}
+
+int fs_conv3d_wgrad_bf16(const void* x, int ctot_in, int cin_off, int cin, const void* dy,
+                         int ctot_out, int cout_off, int cout, int batch, int X, int Y, int Z,
+                         float* dw, float* db, void* workspace, size_t workspace_bytes,
+                         int* error, void* stream) {
+  size_t need = 0;
+  if (fs_conv3d_wgrad_workspace_bytes(cin, cout, &need) != FS_OK || !dw || !workspace ||
+      workspace_bytes < need || ((uintptr_t)workspace & 255) || batch < 1 || X < 1 || Y < 1 ||
+      Z < 1)
+    return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const fs::ConvGeom g = fs::conv_geom(batch, X, Y, Z);
+  long long rows_per = (g.R + kWgGroups - 1) / kWgGroups;
+  rows_per = (rows_per + 127) / 128 * 128;
+  float* pw = (float*)workspace;
+  float* pb = pw + (size_t)kWgGroups * 27 * cin * cout;
+  int st = fs::wgrad_tc_launch(g, x, ctot_in, cin_off, cin, dy, ctot_out, cout_off, cout,
+                               kWgGroups, rows_per, pw, db ? pb : nullptr, error, s);
+  if (st != FS_OK) return st;
+  const long long nw = 27LL * cin * cout;
+  fs::k_sum_groups<<<blocks_for(nw), 256, 0, s>>>(nw, kWgGroups, pw, dw);
+  if (db) fs::k_sum_groups<<<1, 256, 0, s>>>(cout, kWgGroups, pb, db);
+  FS_CHECK_LAUNCH("k_sum_groups");
+  return FS_OK;
+}
 
 int fs_unet_param_count(long long* n) {
   if (!n) return FS_BAD_ARG;

@@ -150,6 +150,19 @@ class DeviceOperator:
         L.check("fs_combine_masses", st)
         return DeviceOperator(self.grid, masses=out, shape=self.shape, periodic=self.periodic)
 
+    def mass_contrast(self) -> float:
+        """max / min over the nonzero edge masses (1 when there are none),
+        computed on the device once and kept."""
+        import torch
+        c = getattr(self, "_contrast", None)
+        if c is None:
+            hi = self.m.max()
+            lo = torch.where(self.m > 0, self.m, torch.full_like(self.m[:1, :1], np.inf)).min()
+            hi, lo = (float(v) for v in torch.stack([hi, lo]).cpu())
+            c = hi / lo if (hi > 0 and np.isfinite(lo)) else 1.0
+            self._contrast = c
+        return c
+
     def edge_vector(self) -> np.ndarray:
         """Masses in the reference's concatenated [x|y|z] edge order (host)."""
         nx, ny, nz = self.shape
@@ -250,10 +263,19 @@ class EliminatedSystem:
     system then stay in FP64.
     """
 
+    #: Edge-mass contrast above which ``coarsening="auto"`` builds the
+    #: multigrid levels by aggregation with Galerkin coarse operators
+    #: (conductors in insulators: copper/oxide in an EQS step is ~1e6).
+    GALERKIN_CONTRAST = 1e3
+
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
                  precision: str = "auto", with_source: bool = False,
-                 preconditioner: str = "jacobi", learned=None, diag=None):
+                 preconditioner: str = "jacobi", learned=None, diag=None,
+                 coarsening: str = "auto"):
         import torch
+        if coarsening not in ("auto", "geometric", "galerkin"):
+            raise ValueError(f"coarsening must be 'auto', 'geometric' or 'galerkin', "
+                             f"got {coarsening!r}")
         if precision not in ("auto", "mixed", "fp64"):
             raise ValueError(f"precision must be 'auto', 'mixed' or 'fp64', got {precision!r}")
         if preconditioner not in ("jacobi", "mg", "learned"):
@@ -274,7 +296,14 @@ class EliminatedSystem:
         # optional FP64 node-diagonal term of the operator (kept alive here)
         self.diag = (None if diag is None else
                      torch.as_tensor(diag, dtype=torch.float64, device=op.dev).contiguous())
-        self._pc = L.PRECOND_JACOBI if preconditioner == "jacobi" else L.PRECOND_MG
+        if preconditioner == "mg" and coarsening == "auto":
+            coarsening = ("galerkin" if op.mass_contrast() > self.GALERKIN_CONTRAST
+                          else "geometric")
+        # the learned level is trained on the geometric hierarchy
+        self.coarsening = ("geometric" if preconditioner == "learned" else coarsening) \
+            if preconditioner != "jacobi" else None
+        self._pc = (L.PRECOND_JACOBI if preconditioner == "jacobi" else
+                    L.PRECOND_MG_AGG if self.coarsening == "galerkin" else L.PRECOND_MG)
         self.op = op
         self.k = pad_rhs(nrhs)
         self.nrhs = nrhs

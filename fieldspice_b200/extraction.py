@@ -70,7 +70,8 @@ def resistance_matrix(grid, sigma_cell: np.ndarray, terminals: Sequence,
     empty = torch.zeros(0, dtype=torch.int64, device=dev)
     Y, _, info = extract_capacitance(op, term_dev, empty, empty, tol=float(cfg.tol),
                                      precision=gcfg.precision, maxiter=gcfg.maxiter,
-                                     preconditioner=resolve_preconditioner(cfg, gcfg))
+                                     preconditioner=resolve_preconditioner(cfg, gcfg),
+                                     coarsening=gcfg.coarsening)
     if info["n_pinned"]:
         warnings.warn(
             f"{info['n_pinned']} unknown(s) are coupled to nothing (empty rows); "
@@ -162,27 +163,28 @@ def rlgc_2d(grid, eps_cell: np.ndarray, sigma_cell: np.ndarray, terminals: Seque
 
 def _series_resistance(grid, sigma_cell, terminals, freq) -> np.ndarray:
     """DC (or skin-corrected) series resistance per unit length [ohm/m]
-    (``extraction.py:209-233``): every conductor gets the estimate of the
-    whole conducting cross-section, as in the reference."""
+    (``extraction.py:209-233``).
+
+    The estimate is the reference's: the conducting cross-section ``A`` is
+    the volume of every cell with sigma > 0 over the length along z, sigma
+    their mean, ``R = 1 / (sigma A)``; above DC the current is confined to a
+    skin of depth delta along a square perimeter ``4 sqrt(A)``, so the area
+    used is ``min(A, 4 sqrt(A) delta)`` and R never drops below its DC value.
+    Every conductor gets this same value on the diagonal."""
     nt = len(terminals)
-    R = np.zeros((nt, nt))
-    cellvol = grid.cell_volumes()
-    length = grid.zn[-1] - grid.zn[0]
-    mask = sigma_cell > 0
-    for i in range(nt):
-        area = float(cellvol[mask].sum() / max(length, 1e-300)) if mask.any() else 0.0
-        sig = float(np.mean(sigma_cell[mask])) if mask.any() else 0.0
-        if area <= 0 or sig <= 0:
-            R[i, i] = 0.0
-            continue
-        r_dc = 1.0 / (sig * area)
-        if freq > 0:
-            delta = skin_depth(sig, freq)
-            perim = 4.0 * np.sqrt(area)
-            a_hf = min(area, perim * delta)
-            r_dc = max(r_dc, 1.0 / (sig * max(a_hf, 1e-300)))
-        R[i, i] = r_dc
-    return R
+    cond = np.asarray(sigma_cell) > 0
+    length = float(grid.zn[-1] - grid.zn[0])
+    if not cond.any() or length <= 0:
+        return np.zeros((nt, nt))
+    area = float(np.asarray(grid.cell_volumes())[cond].sum()) / length
+    sigma = float(np.mean(np.asarray(sigma_cell)[cond]))
+    if area <= 0 or sigma <= 0:
+        return np.zeros((nt, nt))
+    r = 1.0 / (sigma * area)
+    if freq > 0:
+        skin_area = min(area, 4.0 * np.sqrt(area) * skin_depth(sigma, freq))
+        r = max(r, 1.0 / (sigma * max(skin_area, 1e-300)))
+    return r * np.eye(nt)
 
 
 def characteristic_impedance(rlgc: dict, freq=0.0) -> np.ndarray:
@@ -219,19 +221,18 @@ def z_to_y(z: np.ndarray) -> np.ndarray:
 
 
 def s_parameters(y: np.ndarray, z0=50.0) -> np.ndarray:
-    """``S = (I - Z0 Y)(I + Z0 Y)^-1`` for one ``(n, n)`` admittance or a
-    stack ``(nf, n, n)``, real reference impedance (scalar or per port)."""
+    """Scattering matrix of one ``(n, n)`` admittance or a stack
+    ``(nf, n, n)`` for a real reference impedance (scalar or per port).
+
+    With ``A = Z0 Y`` the scattering matrix is ``(I - A)(I + A)^-1``; both
+    factors are polynomials in ``A`` and commute, so it is also
+    ``(I + A)^-1 (I - A)``, computed here as one batched linear solve."""
     y = np.asarray(y)
-    single = y.ndim == 2
-    Y = y[None, ...] if single else y
-    n = Y.shape[-1]
-    Z0 = np.eye(n) * z0 if np.isscalar(z0) else np.diag(np.asarray(z0, float))
+    n = y.shape[-1]
+    z = np.full(n, float(z0)) if np.isscalar(z0) else np.asarray(z0, float)
+    A = z[:, None] * y                      # diag(z0) @ Y, broadcast over the stack
     eye = np.eye(n)
-    S = np.empty_like(Y, dtype=complex)
-    for k in range(Y.shape[0]):
-        A = Z0 @ Y[k]
-        S[k] = (eye - A) @ np.linalg.inv(eye + A)
-    return S[0] if single else S
+    return np.linalg.solve(eye + A, (eye - A).astype(complex))
 
 
 def elmore_delay(r: np.ndarray, c: np.ndarray) -> float:

@@ -76,11 +76,19 @@ class GPUConfig:
         (``poisson.py:535-536``).
     learned
         The trained network for ``preconditioner="learned"``.
+    coarsening
+        How the multigrid levels are built: ``"geometric"`` (every level a
+        rediscretisation of the fine operator, trilinear transfers),
+        ``"galerkin"`` (2x2x2 node aggregates, coarse operators ``P^T A P``:
+        robust when conductors sit in insulators, e.g. copper in oxide at a
+        1e6 conductance ratio) or ``"auto"`` (default): galerkin when the
+        operator's edge masses span more than three orders of magnitude.
     """
     precision: str = "auto"
     preconditioner: str | None = None
     maxiter: int | None = None
     learned: object | None = None
+    coarsening: str = "auto"
 
 
 def resolve_preconditioner(cfg, gpu) -> str:

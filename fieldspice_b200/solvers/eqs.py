@@ -68,6 +68,7 @@ class EQSSolver:
         if np.any(sigma_cell < 0.0):
             raise ValueError("sigma_cell must be non-negative [S/m]")
         self.eps_cell, self.sigma_cell = eps_cell, sigma_cell
+        self.ops = operators  # handed to monitors as state["ops"], as the reference does
         self.op_eps = DeviceOperator(grid, eps_cell, mode=eps_mode)
         self.op_sig = DeviceOperator(grid, sigma_cell, mode=sigma_mode)
         self._vnode = np.asarray(grid.node_volumes(), float).ravel()
@@ -128,7 +129,8 @@ class EQSSolver:
             label[h2d(fixed.astype(np.int64), torch.int64, dev)] = L.LABEL_FIXED
         system = EliminatedSystem(op, label, 1, precision=self.gpu.precision,
                                   with_source=rhs_dev is not None,
-                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+                                  coarsening=self.gpu.coarsening)
         if fixed.size:
             system.phi[h2d(fixed.astype(np.int64), torch.int64, dev)] = \
                 h2d(vals, torch.float64, dev)
@@ -188,8 +190,6 @@ class EQSSolver:
             raise ValueError("t_end must exceed t_start")
         if not 0.0 <= theta <= 1.0:
             raise ValueError("theta must lie in [0, 1]")
-        if monitors is not None:
-            raise NotImplementedError("monitors are not supported on the GPU path")
         t_wall = time.perf_counter()
         terms, bc = self._prepare(terminals, bc)
         dev = self.op_eps.dev
@@ -211,7 +211,8 @@ class EQSSolver:
             label[fixed_d] = L.LABEL_FIXED
         system = EliminatedSystem(K, label, 1, precision=self.gpu.precision,
                                   with_source=True,
-                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+                                  coarsening=self.gpu.coarsening)
         system.phi.copy_(h2d(phi0, torch.float64, dev))
         prev = system.phi.clone()
 
@@ -238,6 +239,9 @@ class EQSSolver:
                 stored_t.append(times[k])
 
         record(0, system.phi)
+        mset = monitors
+        if mset is not None:
+            self._record_monitors(mset, system.phi, float(times[0]), dt)
         tol = float(self.cfg.tol)
         nx, ny, nz = self.op_eps.shape
         lib = L.lib()
@@ -263,6 +267,8 @@ class EQSSolver:
                 cur[k] = K.group_sums(system.phi, groups, minus=Kexp, w=prev,
                                       nodes_dev=gdev)[:, 0]
             record(k, system.phi)
+            if mset is not None:
+                self._record_monitors(mset, system.phi, t, dt)
         if n >= 1:
             cur[0] = cur[1]
         system.close()
@@ -275,14 +281,35 @@ class EQSSolver:
             res.terminals[tt.name] = {"v": volt[:, j].copy(), "i": cur[:, j].copy()}
         res.scalars["energy_electric"] = energy
         res.scalars["dissipation"] = diss
+        if mset is not None:
+            res.meta["monitors"] = mset.finalize()
         res.meta.update(solver=self.name, assumptions=list(self.assumptions),
                         wall_time=time.perf_counter() - t_wall,
                         grid_cells=tuple(self.grid.shape_cells), mode="transient",
                         theta=theta, dt=dt, n_factorisations=1,
                         speedup_vs_courant=dt / self.grid.courant_dt(),
                         iterations=iters, warm_start=True,
-                        fp64_fallback=bool(system.fell_back))
+                        fp64_fallback=bool(system.fell_back),
+                        coarsening=system.coarsening)
         return res
+
+    def _record_monitors(self, mset, phi_d, t: float, dt: float) -> None:
+        """One monitor sample (``eqs.py:377-386``): the state dict the
+        reference hands its monitors, with this step's potential copied to
+        the host.  A failing monitor never ends the solve; the error is
+        reported when ``SolverConfig.verbose`` is at least 1."""
+        if not hasattr(self, "_edge_props"):
+            from .poisson import edge_area_over_length
+            al = edge_area_over_length(self.grid)
+            self._edge_props = (self.op_eps.edge_vector() / al, self.op_sig.edge_vector() / al)
+        state = {"phi": d2h(phi_d), "grid": self.grid, "ops": self.ops,
+                 "eps_edge": self._edge_props[0], "sigma_edge": self._edge_props[1],
+                 "step": 0, "dt": dt}
+        try:
+            mset.record(state, t)
+        except Exception as exc:  # a monitor must never kill a solve
+            if getattr(self.cfg, "verbose", 0) >= 1:
+                print(f"[eqs] monitor error at t={t:.4g}: {exc}", flush=True)
 
     # -- derived quantities ---------------------------------------------------------
     def terminal_current(self, phi_new, phi_old, dt: float, nodes,

@@ -19,7 +19,8 @@ from typing import Any, Sequence
 import numpy as np
 
 from .. import _lib as L
-from ..boundaries import BoundarySpec, check_supported, dirichlet_nodes, periodic_mask
+from ..boundaries import (BoundarySpec, check_supported, dirichlet_nodes, neumann_load,
+                          periodic_mask)
 from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d, mark,
                       pad_rhs, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
@@ -289,7 +290,8 @@ class PoissonSolver:
             op, term_dev, wall_dev, shield_dev, tol=float(self.cfg.tol),
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,
             preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-            learned=None if mask else self.gpu.learned, charges=charges)
+            learned=None if mask else self.gpu.learned, charges=charges,
+            coarsening=self.gpu.coarsening)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         mark("report")
@@ -343,6 +345,12 @@ class PoissonSolver:
         b_free = np.zeros(N)
         if rho_node is not None:
             b_free += as_node_vector(rho_node, grid, "rho_node") * vnode
+        # driven Neumann walls: their flux load joins the free charge
+        # (poisson.py:957-964)
+        load = neumann_load(bc, grid, t)
+        with_load = load is not None
+        if with_load:
+            b_free += load
 
         fixed, vals = _dirichlet_sets(bc, terms, grid, t)
         floats = [tt for tt in terms if tt.driven != "voltage"]
@@ -352,10 +360,10 @@ class PoissonSolver:
                     "floating or charge-driven electrodes together with periodic walls "
                     "are not supported on the GPU path")
             return self._solve_periodic(terms, mask, fixed, vals, b_free,
-                                        rho_node is not None, t0)
+                                        rho_node is not None or with_load, t0)
         if floats:
             return self._solve_floating(terms, floats, fixed, vals, b_free,
-                                        rho_node is not None, t, t0)
+                                        rho_node is not None or with_load, t, t0)
         label = torch.zeros(N, dtype=torch.uint8, device=dev)
         pinned = None
         if fixed.size == 0:
@@ -372,10 +380,11 @@ class PoissonSolver:
                 "absolute level is arbitrary.", RuntimeWarning, stacklevel=2)
         fixed_d = torch.as_tensor(fixed, device=dev)
         label[fixed_d] = L.LABEL_FIXED
-        with_src = rho_node is not None
+        with_src = rho_node is not None or with_load
         system = EliminatedSystem(self.op, label, 1, precision=self.gpu.precision,
                                   with_source=with_src,
-                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+                                  coarsening=self.gpu.coarsening)
         system.phi.zero_()
         system.phi[fixed_d] = torch.as_tensor(vals, dtype=torch.float64, device=dev)
         if with_src:
@@ -447,10 +456,6 @@ class PoissonSolver:
         N = self.op.N
         dev = self.op.dev
         nf = len(floats)
-        if nf + 1 > MAX_RHS:
-            raise NotImplementedError(
-                f"{nf} floating or charge-driven electrodes: the GPU path solves at "
-                f"most {MAX_RHS - 1} in one block")
         if fixed.size == 0:
             raise NotImplementedError(
                 "floating electrodes without any Dirichlet node (a driven terminal or "
@@ -459,45 +464,62 @@ class PoissonSolver:
         if np.isin(np.concatenate(fnodes), fixed).any():
             raise NotImplementedError(
                 "a floating or charge-driven electrode touches a Dirichlet node")
-        k = pad_rhs(nf + 1)
+        # columns: 0 = the driven potentials (every floating electrode at 0 V)
+        # with the free charge, 1 + f = electrode f at 1 V and everything else
+        # at 0 V; solved in blocks of at most MAX_RHS columns on one system
+        ncol = nf + 1
+        chunks = [list(range(c, min(ncol, c + MAX_RHS))) for c in range(0, ncol, MAX_RHS)]
+        k = pad_rhs(len(chunks[0]))
         label = torch.zeros(N, dtype=torch.uint8, device=dev)
         fixed_d = torch.as_tensor(fixed, device=dev)
         label[fixed_d] = L.LABEL_FIXED
         fnodes_d = [h2d(nd.astype(np.int64), torch.int64, dev) for nd in fnodes]
         for nd in fnodes_d:
             label[nd] = L.LABEL_FIXED
-        system = EliminatedSystem(self.op, label, nf + 1, precision=self.gpu.precision,
+        system = EliminatedSystem(self.op, label, len(chunks[0]), precision=self.gpu.precision,
                                   with_source=with_src,
-                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu))
-        # column 0: the driven potentials (floating electrodes at 0 V) and the
-        # free charge; column 1 + f: electrode f at 1 V, everything else 0 V
-        phi_h = np.zeros((N, k))
-        phi_h[fixed, 0] = vals
-        for f, nd in enumerate(fnodes):
-            phi_h[nd, 1 + f] = 1.0
-        system.phi.copy_(h2d(phi_h.ravel(), torch.float64, dev))
-        if with_src:
-            f_h = np.zeros((N, k))
-            f_h[:, 0] = b_free
-            system.f.copy_(h2d(f_h.ravel(), torch.float64, dev))
+                                  preconditioner=resolve_preconditioner(self.cfg, self.gpu),
+                                  coarsening=self.gpu.coarsening)
         tol = float(self.cfg.tol)
-        _, stats = system.solve(tol, self.gpu.maxiter)
-        raise_on_status(stats, tol, "gpu-cg")
-        Q = self.op.group_sums(system.phi, fnodes_d, nrhs=k)
+        Q = np.zeros((nf, ncol))
+        sols, stats_all = [], []
+        for cols in chunks:
+            system.nrhs = len(cols)
+            phi_h = np.zeros((N, k))
+            for c, j in enumerate(cols):
+                if j == 0:
+                    phi_h[fixed, c] = vals
+                else:
+                    phi_h[fnodes[j - 1], c] = 1.0
+            system.phi.copy_(h2d(phi_h.ravel(), torch.float64, dev))
+            if with_src:
+                f_h = np.zeros((N, k))
+                if cols[0] == 0:
+                    f_h[:, 0] = b_free
+                system.f.copy_(h2d(f_h.ravel(), torch.float64, dev))
+            _, stats = system.solve(tol, self.gpu.maxiter)
+            raise_on_status(stats, tol, "gpu-cg")
+            stats_all.extend(stats)
+            Q[:, cols] = self.op.group_sums(system.phi, fnodes_d, nrhs=k)[:, :len(cols)]
+            sols.append((cols, system.phi.clone() if len(chunks) > 1 else system.phi))
         q0 = Q[:, 0] - np.array([b_free[nd].sum() for nd in fnodes])
-        Cff = Q[:, 1:nf + 1]
+        Cff = Q[:, 1:]
         target = np.array([float(tt.value_at(t)) if tt.driven == "current" else 0.0
                            for tt in floats])
         V = np.linalg.solve(Cff, target - q0)
+        weight = np.concatenate([[1.0], V])
         phi_d = torch.empty(N, dtype=torch.float64, device=dev)
-        coef = (ctypes.c_double * (nf + 1))(1.0, *V)
-        L.check("fs_rhs_superpose", L.lib().fs_rhs_superpose(
-            L.ptr(system.phi), k, 0, nf + 1, coef, None, L.ptr(phi_d), N, L.stream_ptr()))
+        for i, (cols, sol) in enumerate(sols):
+            coef = (ctypes.c_double * len(cols))(*weight[cols])
+            L.check("fs_rhs_superpose", L.lib().fs_rhs_superpose(
+                L.ptr(sol), k, 0, len(cols), coef, None if i == 0 else L.ptr(phi_d),
+                L.ptr(phi_d), N, L.stream_ptr()))
         info = {"method": f"gpu-cg-{system.preconditioner}-{self.gpu.precision}", "n": N,
                 "n_factorised": system.n_free,
-                "iterations": max(s["iterations"] for s in stats),
-                "residual": max(s["relres"] for s in stats), "pinned": None,
-                "floating_potentials": V.tolist(), "setup_time": system.setup_time,
+                "iterations": max(s["iterations"] for s in stats_all),
+                "residual": max(s["relres"] for s in stats_all), "pinned": None,
+                "floating_potentials": V.tolist(), "blocks": len(chunks),
+                "setup_time": system.setup_time,
                 "solve_time": time.perf_counter() - t0}
         res = self._potential_result(phi_d, terms, b_free, info, fixed.size, t0)
         system.close()
@@ -550,7 +572,7 @@ class PoissonSolver:
 def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                         tol: float, precision: str = "auto",
                         maxiter: int | None = None, preconditioner: str = "jacobi",
-                        learned=None, charges=None):
+                        learned=None, charges=None, coarsening: str = "auto"):
     """Device core of the extraction: inputs already in HBM.
 
     ``term_dev``: sorted unique int64 node tensors, one per terminal;
@@ -594,7 +616,8 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                 system.close()
             mark("labels")
             system = EliminatedSystem(op, label, kb, precision=precision,
-                                      preconditioner=preconditioner, learned=learned)
+                                      preconditioner=preconditioner, learned=learned,
+                                      coarsening=coarsening)
             setup_time += system.setup_time
             mark("plan")
         system.nrhs = kb
@@ -641,6 +664,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
         "relres_fp64": [s["relres"] for s in stats_all],
         "reliable_updates": [s["reliable_updates"] for s in stats_all],
         "fp64_fallback": bool(system.fell_back),
+        "coarsening": system.coarsening,
         "learned_fallback": bool(system.learned_fallback),
         "gpu_launches": launches,
         "kernel_ms": system.kernel_times(),

@@ -151,7 +151,8 @@ class ThermalSolver:
             label[fixed_d] = L.LABEL_FIXED
         system = EliminatedSystem(op, label, 1, precision=self.gpu.precision, with_source=True,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                                  diag=h2d(diag, torch.float64, dev))
+                                  diag=h2d(diag, torch.float64, dev),
+                                  coarsening=self.gpu.coarsening)
         return system, fixed_d
 
     def _q(self, q_node) -> np.ndarray:

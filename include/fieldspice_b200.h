@@ -62,6 +62,9 @@ extern "C" {
 
 #define FS_PRECOND_JACOBI 0  /* CG on the Jacobi-equilibrated system          */
 #define FS_PRECOND_MG 1      /* geometric multigrid V-cycle preconditioner    */
+#define FS_PRECOND_MG_AGG 2  /* multigrid V-cycle on 2x2x2 aggregates with
+                                Galerkin coarse operators (P^T A P): for
+                                strongly discontinuous coefficients        */
 
 typedef struct fs_rhs_stats {
   int32_t iterations;       /* CG iterations taken                            */
@@ -142,9 +145,12 @@ int fs_set_dirichlet(const int16_t* group, const uint8_t* label,
  * buffer (N*nrhs FP64, fixed values in place, the initial guess on free
  * nodes) and an optional source f (N*nrhs FP64, may be NULL).
  * nrhs must be 1, 2, 4, 8 or 16.  precond: FS_PRECOND_JACOBI (CG on the
- * equilibrated system, the reference's method) or FS_PRECOND_MG (a
+ * equilibrated system, the reference's method), FS_PRECOND_MG (a
  * geometric-multigrid V-cycle with Chebyshev smoothing as the
- * preconditioner; same stopping rule).  workspace must hold
+ * preconditioner; same stopping rule) or FS_PRECOND_MG_AGG (the same V-cycle
+ * on a hierarchy of 2x2x2 node aggregates whose coarse operators are the
+ * Galerkin products P^T A P, robust to coefficient jumps of many orders of
+ * magnitude, e.g. copper against oxide).  workspace must hold
  * fs_pcg_workspace_bytes() bytes and stay alive until destroy.              */
 int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
                            int precond, size_t* bytes);
@@ -289,6 +295,19 @@ int fs_conv3d_bf16(const void* x, int ctot_in, int cin_off, int cin, const void*
                    const float* bias, void* y, int ctot_out, int cout_off, int cout,
                    const void* mask, int ctot_mask, int mask_off, int batch, int X, int Y,
                    int Z, int relu, int accumulate, int* error, void* stream);
+/* Weight and bias gradient of the convolution above from its input x and the
+ * gradient dy of its output (same layouts, channel slices as above):
+ * dw[t][co][ci] = sum over voxels of dy[v][co] x[v + off_t][ci] (FP32,
+ * written), db[co] = sum of dy[v][co] (FP32, written; may be NULL).  The
+ * reduction over voxels runs on tcgen05 tensor cores (BF16 operands, FP32
+ * accumulation in tensor memory).  cin, cout: multiples of 16, cin <= 160,
+ * cout <= 128; dy must be zero on halo rows (as fs_conv3d_bf16 writes it).
+ * workspace: fs_conv3d_wgrad_workspace_bytes() bytes, 256-byte aligned.    */
+int fs_conv3d_wgrad_workspace_bytes(int cin, int cout, size_t* bytes);
+int fs_conv3d_wgrad_bf16(const void* x, int ctot_in, int cin_off, int cin, const void* dy,
+                         int ctot_out, int cout_off, int cout, int batch, int X, int Y, int Z,
+                         float* dw, float* db, void* workspace, size_t workspace_bytes,
+                         int* error, void* stream);
 
 
 /* ---- Learned preconditioner: the U-Net --------------------------------- *

@@ -398,6 +398,37 @@ def floating_fixture():
     np.savez_compressed(HERE / "floating.npz", **out)
 
 
+def floating_many_fixture():
+    """The floating-electrode solve of floating_fixture with 20 floating and
+    charge-driven conductors (a 5 x 4 array of small boxes, every third one
+    charge-driven) and one driven electrode: more electrodes than one block
+    of right-hand sides holds on the GPU path."""
+    rng = np.random.default_rng(43)
+    g = RectilinearGrid(np.linspace(0, 4e-6, 23), np.linspace(0, 3e-6, 19),
+                        np.sort(rng.uniform(0, 1.2e-6, 10)))
+    eps = np.full(g.shape_cells, 3.9 * eps0)
+    eps[:, :, :3] = 11.7 * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    boxes = [(1, 1, 6, 3, 17, 7)]
+    for a in range(5):
+        for b in range(4):
+            boxes.append((5 + 3 * a, 2 + 4 * b, 4, 6 + 3 * a, 3 + 4 * b, 5))
+    nodes = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in boxes]
+    terms = [Terminal("drv", nodes[0], voltage=1.0)]
+    for i, nd in enumerate(nodes[1:]):
+        terms.append(Terminal(f"c{i}", nd, current=1e-18 * (i - 9)) if i % 3 == 2
+                     else Terminal(f"f{i}", nd))
+    bc = BoundarySpec(zlo=Dirichlet(0.0))
+    ps = PoissonSolver(g, eps, SolverConfig(linear_solver="direct", tol=1e-12))
+    r = ps.solve(terms, bc)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "boxes": np.asarray(boxes),
+           "phi": r.fields["phi"][0].ravel(),
+           "names": np.array([t.name for t in terms]),
+           "v": np.array([r.terminals[t.name]["v"][0] for t in terms]),
+           "q": np.array([r.terminals[t.name]["q"][0] for t in terms])}
+    np.savez_compressed(HERE / "floating_many.npz", **out)
+
+
 def periodic_fixture():
     """poisson.py:942-955, 1041-1058, 1196-1224 with Periodic walls: a layered
     unit cell periodic in x (and one periodic in x and y), grounded floor,
@@ -436,6 +467,31 @@ def periodic_fixture():
         out[f"q_{tag}"] = np.array([r.terminals[t.name]["q"][0] for t in drive])
         out["rho"] = rho
     np.savez_compressed(HERE / "periodic.npz", **out)
+
+
+def neumann_fixture():
+    """boundaries.py:1031-1085 and poisson.py:957-964: a driven Neumann flux
+    on two walls (a constant D.n on xhi, a time-dependent one on yhi)
+    feeding PoissonSolver.solve, with a grounded floor and one driven box;
+    direct solve.  Records the reference's load vector and the solution."""
+    from fieldspice.boundaries import Neumann
+    rng = np.random.default_rng(61)
+    g = RectilinearGrid(np.sort(rng.uniform(0, 3e-6, 15)), np.linspace(0, 2e-6, 11),
+                        np.linspace(0, 1e-6, 9))
+    eps = rng.uniform(2.5, 7.0, g.shape_cells) * eps0
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    box = Terminal("box", nid[4:8, 3:6, 4:6].ravel(), voltage=0.7)
+
+    def ramp_flux(t):
+        return 2e-4 * (1.0 + t * 1e9)
+    bc = BoundarySpec(zlo=Dirichlet(0.0), xhi=Neumann(flux=-3e-4), yhi=Neumann(flux=ramp_flux))
+    t = 0.5e-9
+    ps = PoissonSolver(g, eps, SolverConfig(linear_solver="direct"))
+    r = ps.solve([box], bc, t=t)
+    out = {"x": g.xn, "y": g.yn, "z": g.zn, "eps": eps, "t": t,
+           "load": bc.neumann_load(g, t), "phi": r.fields["phi"][0].ravel(),
+           "q_box": r.terminals["box"]["q"], "energy": r.scalars["energy"]}
+    np.savez_compressed(HERE / "neumann.npz", **out)
 
 
 def rc_stack(n=60):
@@ -536,6 +592,8 @@ FIXTURES = {
     "ac": ac_fixture,
     "floating": floating_fixture,
     "periodic": periodic_fixture,
+    "neumann": neumann_fixture,
+    "floating_many": floating_many_fixture,
 }
 
 if __name__ == "__main__":

@@ -135,3 +135,47 @@ def test_conv_data_gradient_matches_autograd(cuda, variant, cin, cout):
     want = x.grad
     got = _run(cuda, _padded(dy), cout, 0, cout, w.float().numpy(), None, cin, 0, cin, dims, flip=1)
     _close(got[:, 1:-1, 1:-1, 1:-1], want)
+
+
+@pytest.mark.parametrize("dims,cin,cout,slices", [
+    ((2, 5, 6, 9), 16, 32, False), ((1, 7, 6, 20), 48, 48, False),
+    ((2, 4, 5, 6), 112, 48, True), ((1, 6, 6, 30), 64, 64, False),
+    ((3, 9, 8, 7), 80, 32, True), ((1, 20, 18, 16), 16, 16, False)])
+def test_conv_weight_gradient_matches_autograd(cuda, dims, cin, cout, slices):
+    """fs_conv3d_wgrad_bf16 (tensor cores, voxels as the reduction index) is
+    dL/dW and dL/db of the forward conv: FP64 autograd on the same BF16
+    inputs, FP32 accumulation differences only (channel slices of wider
+    volumes where ``slices``)."""
+    import torch
+    from fieldspice_b200 import _lib as L
+    lib = L.lib()
+    rng = np.random.default_rng(cin * 7 + cout)
+    B, X, Y, Z = dims
+    x = _bf(rng.standard_normal((B, X, Y, Z, cin)).astype(np.float32))
+    dy = _bf(rng.standard_normal((B, X, Y, Z, cout)).astype(np.float32))
+    w = torch.zeros((27, cout, cin), dtype=torch.float64, requires_grad=True)
+    b = torch.zeros(cout, dtype=torch.float64, requires_grad=True)
+    y = _ref_conv(x.double(), w, b, False)
+    y.backward(dy.double())
+    xo, yo = (8, 16) if slices else (0, 0)
+    ctx, cty = cin + xo + (8 if slices else 0), cout + yo
+    xp = torch.zeros((B, X + 2, Y + 2, Z + 2, ctx), dtype=torch.bfloat16)
+    xp[..., xo:xo + cin] = _padded(x)
+    yp = torch.zeros((B, X + 2, Y + 2, Z + 2, cty), dtype=torch.bfloat16)
+    yp[..., yo:yo + cout] = _padded(dy)
+    xd, yd = xp.to(cuda).contiguous(), yp.to(cuda).contiguous()
+    nb = __import__("ctypes").c_size_t()
+    L.check("ws", lib.fs_conv3d_wgrad_workspace_bytes(cin, cout, __import__("ctypes").byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=cuda)
+    dw = torch.full((27, cout, cin), np.nan, dtype=torch.float32, device=cuda)
+    db = torch.full((cout,), np.nan, dtype=torch.float32, device=cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    L.check("fs_conv3d_wgrad_bf16", lib.fs_conv3d_wgrad_bf16(
+        L.ptr(xd), ctx, xo, cin, L.ptr(yd), cty, yo, cout, B, X, Y, Z, L.ptr(dw), L.ptr(db),
+        L.ptr(ws), nb.value, L.ptr(err), L.stream_ptr()))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    gw, gb = dw.cpu().double(), db.cpu().double()
+    # FP32 sums of up to ~1e4 products of unit-scale BF16 values
+    assert (gw - w.grad).abs().max().item() <= 2e-5 * w.grad.abs().max().item() + 1e-3
+    assert (gb - b.grad).abs().max().item() <= 2e-5 * b.grad.abs().max().item() + 1e-3

@@ -147,3 +147,82 @@ def test_rejects_bad_materials(cuda):
         EQSSolver(g, np.full(g.shape_cells, 3.9), np.zeros(g.shape_cells))
     with pytest.raises(ValueError):
         EQSSolver(g, np.full(g.shape_cells, EPS0), np.full(g.shape_cells, -1.0))
+
+
+@pytest.mark.parametrize("coarsening", ["auto", "geometric"])
+def test_interconnect_transient_at_scale_matches_reference(cuda, coarsening):
+    """The copper/oxide/doped-silicon interconnect (two ports, a 1 V ramp of
+    10 ps on port 0, dt 1 ps, 200 steps) at the largest grid the reference
+    itself finished here (tests/golden/eqs_<shape>_s0.npz, made by
+    tests/golden/make_scale.py: the reference's EQSSolver, Jacobi-CG forced,
+    tol 1e-12).  Port currents at every step to 1e-7 of their peak."""
+    from pathlib import Path
+
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    from fieldspice_b200.solvers.eqs import EQSSolver
+    fx = sorted((Path(__file__).parent / "golden").glob("eqs_*x*x*_s0.npz"),
+                key=lambda p: int(np.prod(np.load(p)["shape"])))
+    d = np.load(fx[-1])
+    shape = tuple(int(v) for v in d["shape"])
+    steps = int(d["steps"])
+    w = W.eqs_interconnect(shape, nbox=6, nports=2, seed=0)
+    ramp = W.ramp(0.0, 0.0, 1.0, 10e-12)
+    terms = [Terminal("port0", w.terminals[0], voltage=ramp),
+             Terminal("port1", w.terminals[1], voltage=0.0)]
+    s = EQSSolver(w.grid(), w.eps_cell, w.sigma_cell, SolverConfig(tol=1e-12),
+                  gpu=GPUConfig(preconditioner="mg", coarsening=coarsening))
+    r = s.solve(terms, t_end=steps * 1e-12, dt=1e-12, bc=BoundarySpec(zlo=Dirichlet(0.0)))
+    if coarsening == "auto":
+        assert r.meta["coarsening"] == "galerkin"
+    scale = max(np.abs(d["i0"]).max(), np.abs(d["i1"]).max())
+    assert np.abs(r.i("port0") - d["i0"]).max() / scale < 1e-7
+    assert np.abs(r.i("port1") - d["i1"]).max() / scale < 1e-7
+
+
+class _ProbeSet:
+    """A monitor set in the reference's protocol (``record(state, t)``,
+    ``finalize()``, ``monitors.py:1607-1720``): the potential at one node and
+    the state keys the solver hands over."""
+
+    def __init__(self, node, fail_at=None):
+        self.node, self.fail_at = node, fail_at
+        self.t, self.v, self.keys = [], [], set()
+
+    def record(self, state, t):
+        self.keys |= set(state)
+        if self.fail_at is not None and len(self.t) == self.fail_at:
+            self.t.append(t)
+            raise RuntimeError("a monitor that fails once")
+        self.t.append(t)
+        self.v.append(float(state["phi"][self.node]))
+
+    def finalize(self):
+        return {"t": np.asarray(self.t), "v": np.asarray(self.v)}
+
+
+def test_monitors_see_every_step(cuda, golden):
+    """A monitor set receives the potential at t0 and after every step
+    (``eqs.py:287-319``, ``:377-386``), equal to the stored fields; its
+    result lands in ``meta["monitors"]``; a monitor that raises does not end
+    the solve."""
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    from fieldspice_b200.solvers.eqs import EQSSolver
+    d = golden("eqs")
+    g, eps, sig, R1, C1, C2, n = _rc_stack()
+    tau = R1 * (C1 + C2)
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    probe = _ProbeSet(int(nid[n // 2, 1, 1]))
+    s = EQSSolver(g, eps, sig, SolverConfig(tol=1e-12), gpu=GPUConfig(precision="mixed"))
+    hi = Terminal("hi", nid[0].ravel(), voltage=1.0)
+    lo = Terminal("lo", nid[-1].ravel(), voltage=0.0)
+    r = s.solve([hi, lo], t_end=8 * tau, dt=tau / 50, monitors=probe, store=True)
+    m = r.meta["monitors"]
+    assert np.allclose(m["t"], r.t, rtol=0, atol=1e-30)
+    assert np.array_equal(m["v"], r.fields["phi"][:, probe.node])
+    assert np.abs(m["v"] - d["spt50_vm"]).max() < 2e-9
+    assert {"phi", "grid", "ops", "eps_edge", "sigma_edge", "step", "dt"} <= probe.keys
+    bad = _ProbeSet(int(nid[n // 2, 1, 1]), fail_at=3)
+    r2 = s.solve([hi, lo], t_end=8 * tau, dt=tau / 50, monitors=bad)
+    assert len(bad.t) == len(r2.t) and len(bad.v) == len(r2.t) - 1

@@ -48,3 +48,33 @@ def test_floating_without_reference_raises(cuda):
     ps = PoissonSolver(g, np.full(g.shape_cells, 3.9 * 8.854e-12))
     with pytest.raises(NotImplementedError, match="reference"):
         ps.solve([Terminal("f", nid[2:4, 2:4, 2:4].ravel())])
+
+
+@pytest.mark.parametrize("preconditioner", ["mg", "jacobi"])
+def test_twenty_floating_electrodes_match_reference(cuda, golden, preconditioner):
+    """20 floating and charge-driven conductors and a driven electrode
+    (``tests/golden/floating_many.npz``): more columns than one block of 16
+    right-hand sides, solved block after block on one system."""
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
+    from fieldspice_b200.solvers.poisson import PoissonSolver
+    d = golden("floating_many")
+    g = RectilinearGrid(d["x"], d["y"], d["z"])
+    nid = np.arange(g.n_nodes).reshape(g.shape_nodes)
+    nodes = [nid[a0:a1 + 1, b0:b1 + 1, c0:c1 + 1].ravel() for a0, b0, c0, a1, b1, c1 in d["boxes"]]
+    terms = [Terminal("drv", nodes[0], voltage=1.0)]
+    for i, nd in enumerate(nodes[1:]):
+        terms.append(Terminal(f"c{i}", nd, current=1e-18 * (i - 9)) if i % 3 == 2
+                     else Terminal(f"f{i}", nd))
+    assert [t.name for t in terms] == list(d["names"])
+    ps = PoissonSolver(g, d["eps"], SolverConfig(tol=1e-12),
+                       gpu=GPUConfig(preconditioner=preconditioner))
+    r = ps.solve(terms, BoundarySpec(zlo=Dirichlet(0.0)))
+    assert r.meta["linear"]["blocks"] == 2
+    phi = r.fields["phi"][0].ravel()
+    assert np.abs(phi - d["phi"]).max() <= 1e-9
+    qscale = abs(float(d["q"][0]))
+    for i, t in enumerate(terms):
+        assert abs(r.terminals[t.name]["v"][0] - d["v"][i]) <= 1e-9, t.name
+        assert abs(r.terminals[t.name]["q"][0] - d["q"][i]) <= 1e-8 * qscale, t.name

@@ -6,10 +6,14 @@ layered-box family, then used as the coarse-level solver of the V-cycle
 inside flexible CG on a held-out geometry.  Checks:
 * the extraction converges to relres 1e-10 and its C matches an FP64
   multigrid extraction at relres 1e-12 to 1e-9 of max|diag C|;
-* what the trained network gains over the method without it: the same
-  flexible CG with the network's output set to zero (the V-cycle truncated at
-  the network's level, no coarse correction) needs several times more
-  iterations, and an untrained network does worse than the trained one.
+* what the trained network gains over the method without it, measured
+  against both ends: the same flexible CG with the network's output set to
+  zero (the V-cycle truncated at the network's level, no coarse correction)
+  and the same V-cycle with its own multigrid recursion below that level
+  (plain multigrid PCG, the stronger coarse solver).  The trained network
+  must recover most of the iterations the recursion saves over no coarse
+  correction at all, and do better than an untrained network; it does not
+  beat the recursion, which is exact up to smoothing on these levels.
 """
 
 import numpy as np
@@ -99,18 +103,26 @@ def test_hybrid_mode_converges_to_the_same_answer(cuda, trained):
 
 
 def test_trained_network_gains_over_the_method_without_it(cuda, trained):
-    """The V-cycle truncated at the network's level ('replace'): with the
-    trained network, with its output zeroed (no coarse correction) and with
-    an untrained network."""
+    """The V-cycle with the network as its level-2 correction ('replace'),
+    against the same V-cycle with that correction zeroed, with its own
+    multigrid recursion (plain multigrid PCG) and with an untrained network."""
     from fieldspice_b200.learned import LearnedPreconditioner
     from fieldspice_b200.solvers.base import GPUConfig
     w = _workloads([999])[0]
 
-    def iters(net):
-        _, rep = _extract(w, GPUConfig(preconditioner="learned", learned=net))
+    def iters(gpu):
+        _, rep = _extract(w, gpu)
         return max(rep["linear"]["iterations"])
+
+    def learned(net):
+        return iters(GPUConfig(preconditioner="learned", learned=net))
     rep_net = trained.with_mode("replace")
-    it_learned, it_zero = iters(rep_net), iters(rep_net.zero())
-    it_rand = iters(LearnedPreconditioner(level=2, seed=5, mode="replace"))
-    assert it_learned * 2 <= it_zero, (it_learned, it_zero)
+    it_learned, it_zero = learned(rep_net), learned(rep_net.zero())
+    it_rand = learned(LearnedPreconditioner(level=2, seed=5, mode="replace"))
+    it_mg = iters(GPUConfig(preconditioner="mg", coarsening="geometric"))
+    recovered = (it_zero - it_learned) / max(it_zero - it_mg, 1)
+    print(f"iterations: learned {it_learned}, zeroed {it_zero}, untrained {it_rand}, "
+          f"multigrid recursion {it_mg}; recovered {recovered:.2f}")
+    assert it_mg <= it_learned < it_zero, (it_mg, it_learned, it_zero)
+    assert recovered >= 0.5, (it_learned, it_zero, it_mg)
     assert it_learned < it_rand, (it_learned, it_rand)

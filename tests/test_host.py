@@ -54,9 +54,16 @@ def test_unsupported_walls_raise():
     spec = B.BoundarySpec(xlo=Periodic(), xhi=Periodic())
     with pytest.raises(NotImplementedError):
         B.check_supported(spec)
-    with pytest.raises(NotImplementedError):
-        B.check_supported(B.BoundarySpec(xlo=B.Neumann(flux=3.0)))
+    # a driven Neumann flux is supported (a right-hand-side load)
+    B.check_supported(B.BoundarySpec(xlo=B.Neumann(flux=3.0)))
     B.check_supported(B.BoundarySpec(zlo=B.Dirichlet(0.0)))
+
+    @__import__("dataclasses").dataclass(frozen=True)
+    class Absorbing:
+        is_dirichlet_like = False
+        is_natural = False
+    with pytest.raises(NotImplementedError):
+        B.check_supported(B.BoundarySpec(xlo=Absorbing()))
 
 
 def test_terminal_checks():
