@@ -33,6 +33,12 @@ struct Dims {
   int per;
   long long wx;
   int wy, wz;
+  // x-marching kernels: 0 = every CTA takes an even contiguous share of the
+  // column-planes (column after column); > 0 = CTA b takes x-planes
+  // [c * xc, (c + 1) * xc) of column (b mod ncols), c = b / ncols, so CTAs
+  // running at the same time march neighbouring columns over the same
+  // x-planes and re-read each other's halo rows from L2, not DRAM.
+  int xc;
 };
 
 inline Dims make_dims(int nx, int ny, int nz, int per = 0) {
@@ -47,7 +53,43 @@ inline Dims make_dims(int nx, int ny, int nz, int per = 0) {
   d.wx = (long long)(nx - 1) * d.sx;
   d.wy = (ny - 1) * nz;
   d.wz = nz - 1;
+  d.xc = 0;
   return d;
+}
+
+// The column-planes (u = column * nx + x) of this CTA in an x-marching
+// kernel over ncols (z, y) tile columns; see Dims::xc.
+template <typename I>
+__device__ __forceinline__ void march_range(const Dims& d, I ncols, I& u, I& u_end) {
+  const I total = ncols * (I)d.nx;
+  if (d.xc > 0) {
+    const I col = (I)blockIdx.x % ncols, chunk = (I)blockIdx.x / ncols;
+    const I xa = min((I)d.nx, chunk * (I)d.xc), xb = min((I)d.nx, xa + (I)d.xc);
+    u = col * (I)d.nx + xa;
+    u_end = col * (I)d.nx + xb;
+  } else {
+    const I per = (total + (I)gridDim.x - 1) / (I)gridDim.x;
+    u = (I)blockIdx.x * per;
+    u_end = min(u + per, total);
+  }
+}
+
+// Grid of an x-marching kernel with `resident` CTAs resident at once: the
+// lockstep assignment (d->xc > 0, chunks of at least 16 planes) when a
+// level's vectors are larger than `l2_bytes` (halo re-reads would go to DRAM),
+// else an even contiguous split (d->xc = 0) over at most `resident` CTAs.
+inline long long march_grid(Dims* d, long long ncols, long long resident,
+                            long long vector_bytes, long long l2_bytes) {
+  d->xc = 0;
+  const long long cols = ncols * d->nx;
+  if (vector_bytes > l2_bytes && ncols <= resident) {
+    long long chunks = resident / ncols;
+    if (chunks > d->nx / 16) chunks = d->nx / 16 > 0 ? d->nx / 16 : 1;
+    const int xc = (int)((d->nx + chunks - 1) / chunks);
+    d->xc = xc;
+    return ncols * ((d->nx + xc - 1) / xc);
+  }
+  return resident < cols ? resident : cols;
 }
 
 // The six edges of node n = (i, j, k) as edge(present, mass, neighbour).  On

@@ -496,10 +496,8 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
   const int tid = threadIdx.x;
   const int tz = tid % C::TZ, ty = tid / C::TZ;
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const long long total = (long long)nbz * nby * d.nx;   // column-planes
-  const long long per = (total + gridDim.x - 1) / gridDim.x;
-  long long u = (long long)blockIdx.x * per;
-  const long long u_end = min(u + per, total);
+  long long u = 0, u_end = 0;  // column-planes
+  fs::march_range<long long>(d, (long long)nbz * nby, u, u_end);
 
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
@@ -673,10 +671,8 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
   const int tz = tid % C::TZ, ty = tid / C::TZ;
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
   // column-planes in 32-bit: N / (TZ * TY) of them (the launch checks the bound)
-  const int total = nbz * nby * d.nx;
-  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
-  int u = (int)blockIdx.x * per;
-  const int u_end = min(u + per, total);
+  int u = 0, u_end = 0;
+  fs::march_range<int>(d, nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -783,6 +779,183 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
   finish_pq<T, K, TmaTileM<T, K>::THREADS>(acc, partials, st, ctl);
 }
 
+// ---- K1 with the direction update fused in ----------------------------------------
+// The CG direction p = z + beta p_old (k_pnew) formed inside the stencil: each
+// ring stage holds the z tile and the p_old tile (both with the one-node halo)
+// next to the plane's three mass tiles, every stencil point forms its p value
+// from the two, and the thread of a node writes its p (the new direction, for
+// the update kernel and the next iteration) and q = A~p, with p.q reduced as
+// in k_stencil_tma_m.  Every right-hand side takes p = z + beta p_old (one
+// FMA, k_pnew's arithmetic for an active one); an inactive one's direction is
+// never read again (its step length is 0 and a solve restarts from k_init),
+// so it needs no exception.  Per node: z and p_old read, p and q written
+// (4 vectors) instead of the 5 of k_pnew followed by the stencil.
+// a * b + c with one rounding (k_pnew's contracted r + beta * p_old)
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+
+template <typename T, int K>
+struct TmaTilePZ {
+  using M = TmaTileM<T, K>;
+  static constexpr int B = M::B, MB = M::MB, TZ = M::TZ, TY = M::TY, HY = M::HY,
+                       HZ = M::HZ, ZP = M::ZP;
+  static constexpr int NS = 4;
+  static constexpr int BOX = M::BOX;
+  static constexpr int EXB = M::EXB, EYB = M::EYB, EZB = M::EZB;
+  static constexpr int O_P = (BOX + 127) / 128 * 128;          // p_old tile
+  static constexpr int O_EX = O_P + (BOX + 127) / 128 * 128;
+  static constexpr int O_EY = O_EX + (EXB + 127) / 128 * 128;
+  static constexpr int O_EZ = O_EY + (EYB + 127) / 128 * 128;
+  static constexpr int SLOT = O_EZ + (EZB + 127) / 128 * 128;
+  static constexpr uint32_t TX = (uint32_t)(2 * BOX + EXB + EYB + EZB);
+  static constexpr int THREADS = TZ * TY;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + NS * 8 + K * sizeof(T) + 256;
+  static constexpr bool OK = M::OK;
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TmaTilePZ<T, K>::THREADS, 2)
+    k_stencil_pz(Dims d, const __grid_constant__ CUtensorMap tm_z,
+                 const __grid_constant__ CUtensorMap tm_pold,
+                 const __grid_constant__ CUtensorMap tm_ex,
+                 const __grid_constant__ CUtensorMap tm_ey,
+                 const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ pnew,
+                 T* __restrict__ q, double* __restrict__ partials, RhsState* st,
+                 Control* ctl) {
+  using C = TmaTilePZ<T, K>;
+  if (ctl->all_done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + C::NS * C::SLOT);
+  T* beta_s = reinterpret_cast<T*>(bar + C::NS);  // per RHS: p = z + beta p_old
+  const int tid = threadIdx.x;
+  const int tz = tid % C::TZ, ty = tid / C::TZ;
+  const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
+  int u = 0, u_end = 0;  // column-planes
+  fs::march_range<int>(d, nbz * nby, u, u_end);
+  if (tid == 0) {
+    for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  if (tid < K) beta_s[tid] = (T)st[tid].beta;
+  __syncthreads();
+  const int rot = chunk_rot<T, K>();
+  // the two coefficients in this thread's rotated chunk order
+  T cp[K];
+  {
+    // ld_rot's register order: slot (c, e) holds RHS ((c + rot) mod NC) * W + e
+    using NCh = NodeChunks<T, K>;
+#pragma unroll
+    for (int c = 0; c < NCh::NC; ++c)
+#pragma unroll
+      for (int e = 0; e < NCh::W; ++e)
+        cp[c * NCh::W + e] = beta_s[((c + rot) & (NCh::NC - 1)) * NCh::W + e];
+  }
+  double acc[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) acc[t] = 0.0;
+  const int cpos = (ty + 1) * C::HZ + (tz + 1);
+  int ticket = 0;
+  bool failed = false;
+  bool bad = false;
+  while (u < u_end && !failed) {
+    const int col = u / d.nx;
+    const int xa = u - col * d.nx;
+    const int xb = min(d.nx, xa + (u_end - u));
+    const int by = col / nbz, bz = col - by * nbz;
+    const int z0 = bz * C::TZ, y0 = by * C::TY;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inb = z < d.nz && y < d.ny;
+    const int nplanes = (xb - xa) + 2;  // planes xa-1 .. xb
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % C::NS;
+      unsigned char* slot = base + s * C::SLOT;
+      const int x = xa - 1 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], C::TX);
+      fs::tma_load_4d(slot, &tm_z, &bar[s], 0, z0 - 1, y0 - 1, x);
+      fs::tma_load_4d(slot + C::O_P, &tm_pold, &bar[s], 0, z0 - 1, y0 - 1, x);
+      tma_load_3d(slot + C::O_EX, &tm_ex, &bar[s], z0, y0, x);
+      tma_load_3d(slot + C::O_EY, &tm_ey, &bar[s], z0, y0 - 1, x);
+      tma_load_3d(slot + C::O_EZ, &tm_ez, &bar[s], z0 - C::ZP, y0, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < C::NS && j < nplanes; ++j) issue(j);
+    for (int j = 0; j < nplanes; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % C::NS;
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / C::NS) & 1), kWaitBudget);
+      if (j >= 2) {
+        if (inb && !bad) {
+          const int x = xa - 2 + j;
+          const long long n = ((long long)x * d.ny + y) * d.nz + z;
+          const unsigned char* sm = base + ((tk - 2) % C::NS) * C::SLOT;  // plane x-1
+          const unsigned char* sc = base + ((tk - 1) % C::NS) * C::SLOT;  // plane x
+          const unsigned char* sp = base + s * C::SLOT;                   // plane x+1
+          const T* exm = reinterpret_cast<const T*>(sm + C::O_EX);
+          const T* exc = reinterpret_cast<const T*>(sc + C::O_EX);
+          const T* eyc = reinterpret_cast<const T*>(sc + C::O_EY);
+          const T* ezc = reinterpret_cast<const T*>(sc + C::O_EZ);
+          const T mxm = exm[ty * C::TZ + tz], mxp = exc[ty * C::TZ + tz];
+          const T mym = eyc[ty * C::TZ + tz], myp = eyc[(ty + 1) * C::TZ + tz];
+          const T mzm = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP - 1];
+          const T mzp = ezc[ty * (C::TZ + C::ZP) + tz + C::ZP];
+          // p at tile node i of a plane: z + beta * p_old
+          auto pval = [&](const unsigned char* pl, int i, T (&v)[K]) {
+            T zv[K];
+            ld_rot<T, K>(reinterpret_cast<const T*>(pl) + i * K, zv, rot);
+            ld_rot<T, K>(reinterpret_cast<const T*>(pl + C::O_P) + i * K, v, rot);
+#pragma unroll
+            for (int t = 0; t < K; ++t) v[t] = fma_t(cp[t], v[t], zv[t]);
+          };
+          T c[K], v[K], qv[K];
+          pval(sc, cpos, c);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] = c[t];
+          pval(sm, cpos, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxm * v[t];
+          pval(sp, cpos, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mxp * v[t];
+          pval(sc, cpos - C::HZ, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mym * v[t];
+          pval(sc, cpos + C::HZ, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= myp * v[t];
+          pval(sc, cpos - 1, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) qv[t] -= mzm * v[t];
+          pval(sc, cpos + 1, v);
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            qv[t] -= mzp * v[t];
+            acc[t] += (double)c[t] * (double)qv[t];
+          }
+          st_rot<T, K>(pnew + n * K, c, rot);
+          st_rot<T, K>(q + n * K, qv, rot);
+        }
+        if (__syncthreads_or(bad)) {
+          failed = true;
+          break;
+        }
+        if (tid == 0 && j - 2 + C::NS < nplanes) issue(j - 2 + C::NS);
+      }
+    }
+    ticket += nplanes;
+    u += (xb - xa);
+  }
+  if (failed) {
+    if (tid == 0) {
+      ctl->error = 1;
+      for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
+  }
+  unrotate<T, K>(acc, rot);
+  finish_pq<T, K, TmaTilePZ<T, K>::THREADS>(acc, partials, st, ctl);
+}
+
 // ---- K1 variant: q written through shared memory by TMA stores -------------------
 // The same computation as k_stencil_tma_m (p and the three mass tiles staged by
 // TMA, one thread per node of a TZ x TY column marching along x), but each
@@ -847,10 +1020,8 @@ __global__ void __launch_bounds__(TmaTileS<T, K>::THREADS, (TmaTileS<T, K>::B <=
   const int tid = threadIdx.x;
   const int tz = tid % C::TZ, ty = tid / C::TZ;
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const long long total = (long long)nbz * nby * d.nx;
-  const long long per = (total + gridDim.x - 1) / gridDim.x;
-  long long u = (long long)blockIdx.x * per;
-  const long long u_end = min(u + per, total);
+  long long u = 0, u_end = 0;  // column-planes
+  fs::march_range<long long>(d, (long long)nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -1035,11 +1206,9 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
     hz = (k2 & 1) ? C::RZ - 1 : 0;
   }
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  // column-planes in 32 bits (the launch checks the bound)
-  const int total = nbz * nby * d.nx;
-  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
-  int u = (int)blockIdx.x * per;
-  const int u_end = min(u + per, total);
+  // column-planes in 32-bit: N / (TZ * TY) of them (the launch checks the bound)
+  int u = 0, u_end = 0;
+  fs::march_range<int>(d, nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -1240,10 +1409,8 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
     hz = (k2 & 1) ? C::RZ - 1 : 0;
   }
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const int total = nbz * nby * d.nx;
-  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
-  int u = (int)blockIdx.x * per;
-  const int u_end = min(u + per, total);
+  int u = 0, u_end = 0;  // column-planes
+  fs::march_range<int>(d, nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -1474,10 +1641,8 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
     hz = (k2 & 1) ? C::RZ - 1 : 0;
   }
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const int total = nbz * nby * d.nx;
-  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
-  int u = (int)blockIdx.x * per;
-  const int u_end = min(u + per, total);
+  int u = 0, u_end = 0;  // column-planes
+  fs::march_range<int>(d, nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -1719,10 +1884,8 @@ __global__ void __launch_bounds__(TmaTileSplit<T, K>::THREADS, 2)
   const int hf = tid & 1, v = tid >> 1;
   const int tz = v % C::TZ, ty = v / C::TZ;
   const int nbz = (d.nz + C::TZ - 1) / C::TZ, nby = (d.ny + C::TY - 1) / C::TY;
-  const int total = nbz * nby * d.nx;
-  const int per = (total + (int)gridDim.x - 1) / (int)gridDim.x;
-  int u = (int)blockIdx.x * per;
-  const int u_end = min(u + per, total);
+  int u = 0, u_end = 0;  // column-planes
+  fs::march_range<int>(d, nbz * nby, u, u_end);
   if (tid == 0) {
     for (int s = 0; s < C::NS; ++s) fs::mbar_init(&bar[s], 1);
     fs::fence_mbar_init();
@@ -2412,6 +2575,7 @@ void host_slot_put(HostSlot* slot) {
 
 struct fs_pcg_plan {
   Dims d;
+  Dims dm;                 // d with the x-marching assignment of the CG stencil
   int nrhs, precision, precond;
   int agg;                 // multigrid levels by aggregation (Galerkin coarse operators)
   int nlev;
@@ -2435,10 +2599,12 @@ struct fs_pcg_plan {
   CUtensorMap tm_p[2];
   CUtensorMap tm_m[3];     // ex, ey, ez tiles of the mass-staging stencil
   CUtensorMap tm_q;        // q tiles of the TMA-store stencil
+  CUtensorMap tm_z;        // z (r without a preconditioner) tiles of the fused stencil
+  int zmap_ok = 0;         // tm_z encoded (kind 5 available)
   int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses,
                            // 3: as 2 with q written by TMA stores
-  int autotune = 0;        // time kinds 2, 3, 0, 4 at creation and keep the fastest
-  float tune_ms[5] = {-1.f, -1.f, -1.f, -1.f, -1.f};  // ms per launch by kind (-1: untimed)
+  int autotune = 0;        // time kinds 2, 3, 0, 4, 5 at creation and keep the fastest
+  float tune_ms[6] = {-1.f, -1.f, -1.f, -1.f, -1.f, -1.f};  // ms per launch by kind (-1: untimed)
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -2470,6 +2636,24 @@ namespace {
 
 // The TMA-staged stencil is the default; FS_STENCIL=plain selects the
 // cached-load kernel (the same arithmetic) for comparison.
+// Vectors larger than this march in lockstep (Dims::xc): their halo rows
+// would not stay in the 126 MB L2 between neighbouring columns otherwise.
+constexpr long long kMarchL2Bytes = 64LL << 20;
+
+// Marching assignment of the CG stencils (lockstep unless FS_MARCH=contig)
+// and of the fused smoothing passes (contiguous unless FS_MARCH=lockstep):
+// measured at 256x256x128, 8 FP32 RHS, lockstep takes the fused stencil
+// from 0.272 to 0.251 ms but the smoothing passes from 0.296 to 0.311 ms
+// (two CTAs per SM leave 40 of 296 slots idle in lockstep).
+bool march_lockstep() {
+  const char* sel = getenv("FS_MARCH");
+  return !(sel && strcmp(sel, "contig") == 0);
+}
+bool march_lockstep_smoothing() {
+  const char* sel = getenv("FS_MARCH");
+  return sel && strcmp(sel, "lockstep") == 0;
+}
+
 bool plain_stencil() {
   const char* sel = getenv("FS_STENCIL");
   return sel && strcmp(sel, "plain") == 0;
@@ -2490,30 +2674,42 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Process-wide record of the fastest CG stencil kernel per (grid, RHS block,
-// precision), filled by the first plan of each shape (the stencil autotuner).
+// Process-wide cache of the fastest CG stencil kernel per shape class, filled
+// by the first plan of each class (the stencil autotuner): RHS block,
+// precision, node count to a power of two, and whether the z extent fills
+// whole 32-node tiles.  Plans whose vectors are smaller than
+// kTuneMinBytes are not tuned (the kernels differ by launch latency there)
+// and run the mass-staging stencil.
+constexpr long long kTuneMinBytes = 32LL << 20;
+
 struct StencilKey {
-  int nx, ny, nz, k, es;
+  int k, es, log2n, zfull;
   bool operator<(const StencilKey& o) const {
-    if (nx != o.nx) return nx < o.nx;
-    if (ny != o.ny) return ny < o.ny;
-    if (nz != o.nz) return nz < o.nz;
     if (k != o.k) return k < o.k;
-    return es < o.es;
+    if (es != o.es) return es < o.es;
+    if (log2n != o.log2n) return log2n < o.log2n;
+    return zfull < o.zfull;
   }
 };
 std::mutex g_stencil_mu;
 std::map<StencilKey, int> g_stencil_choice;
 
+StencilKey stencil_class(const Dims& d, int k, int es) {
+  int l = 0;
+  while ((1LL << (l + 1)) <= d.N) ++l;
+  return StencilKey{k, es, l, d.nz % 32 == 0 ? 1 : 0};
+}
+
 int stencil_choice_get(const Dims& d, int k, int es) {
+  if (d.N * k * es < kTuneMinBytes) return 2;
   std::lock_guard<std::mutex> lk(g_stencil_mu);
-  auto it = g_stencil_choice.find(StencilKey{d.nx, d.ny, d.nz, k, es});
+  auto it = g_stencil_choice.find(stencil_class(d, k, es));
   return it == g_stencil_choice.end() ? -1 : it->second;
 }
 
 void stencil_choice_put(const Dims& d, int k, int es, int kind) {
   std::lock_guard<std::mutex> lk(g_stencil_mu);
-  g_stencil_choice[StencilKey{d.nx, d.ny, d.nz, k, es}] = kind;
+  g_stencil_choice[stencil_class(d, k, es)] = kind;
 }
 
 template <typename T, int K>
@@ -2522,74 +2718,42 @@ struct Impl {
   // SMs x resident CTAs, capped by the number of (z, y) column tiles x planes).
   static void apply_grid(fs_pcg_plan* P) {
     const long long N = P->d.N;
-    using C = TmaTile<T, K>;
-    if (P->stencil_kind == 3) {
-      using CS = TmaTileS<T, K>;
-      cudaFuncSetAttribute(k_stencil_tma_s<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)CS::SMEM);
+    // persistent x-marching kernels: resident CTAs per SM x SMs, the lockstep
+    // column assignment (Dims::xc) when the vectors do not fit in L2
+    auto marching = [&](const void* kern, int threads, size_t smem, int tz, int ty) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       int per_sm = 0, dev = 0, sms = 148;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_tma_s<T, K>,
-                                                        CS::THREADS, CS::SMEM) != cudaSuccess ||
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) !=
+              cudaSuccess ||
           per_sm < 1)
         per_sm = 1;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const long long cols = (long long)((P->d.nz + CS::TZ - 1) / CS::TZ) *
-                             ((P->d.ny + CS::TY - 1) / CS::TY) * P->d.nx;
-      long long g = (long long)sms * per_sm;
-      if (g > cols) g = cols;
-      P->g_apply = (int)g;
+      const long long ncols = (long long)((P->d.nz + tz - 1) / tz) * ((P->d.ny + ty - 1) / ty);
+      P->dm = P->d;
+      P->g_apply = (int)fs::march_grid(&P->dm, ncols, (long long)sms * per_sm,
+                                       march_lockstep() ? N * K * (long long)sizeof(T) : 0,
+                                       kMarchL2Bytes);
+    };
+    P->dm = P->d;
+    if (P->stencil_kind == 3) {
+      using CS = TmaTileS<T, K>;
+      marching((const void*)k_stencil_tma_s<T, K>, CS::THREADS, CS::SMEM, CS::TZ, CS::TY);
+    } else if (P->stencil_kind == 5) {
+      using CZ = TmaTilePZ<T, K>;
+      marching((const void*)k_stencil_pz<T, K>, CZ::THREADS, CZ::SMEM, CZ::TZ, CZ::TY);
     } else if (P->stencil_kind == 4) {
       if constexpr (TmaTileSplit<T, K>::OK) {
         using CM = TmaTileM<T, K>;
-        using CSp = TmaTileSplit<T, K>;
-        cudaFuncSetAttribute(k_stencil_split<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)CM::SMEM);
-        int per_sm = 0, dev = 0, sms = 148;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_split<T, K>,
-                                                          CSp::THREADS, CM::SMEM) != cudaSuccess ||
-            per_sm < 1)
-          per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const long long cols = (long long)((P->d.nz + CM::TZ - 1) / CM::TZ) *
-                               ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx;
-        long long g = (long long)sms * per_sm;
-        if (g > cols) g = cols;
-        P->g_apply = (int)g;
+        marching((const void*)k_stencil_split<T, K>, TmaTileSplit<T, K>::THREADS, CM::SMEM,
+                 CM::TZ, CM::TY);
       }
     } else if (P->stencil_kind == 2) {
       using CM = TmaTileM<T, K>;
-      cudaFuncSetAttribute(k_stencil_tma_m<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)CM::SMEM);
-      int per_sm = 0, dev = 0, sms = 148;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_tma_m<T, K>,
-                                                        CM::THREADS, CM::SMEM) != cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const long long cols = (long long)((P->d.nz + CM::TZ - 1) / CM::TZ) *
-                             ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx;
-      long long g = (long long)sms * per_sm;
-      if (g > cols) g = cols;
-      P->g_apply = (int)g;
+      marching((const void*)k_stencil_tma_m<T, K>, CM::THREADS, CM::SMEM, CM::TZ, CM::TY);
     } else if (P->stencil_kind == 1) {
-      cudaFuncSetAttribute(k_stencil_tma<T, K>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)C::SMEM);
-      int per_sm = 0, dev = 0, sms = 148;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-              &per_sm, k_stencil_tma<T, K>, C::THREADS, C::SMEM) != cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const long long cols = (long long)((P->d.nz + C::TZ - 1) / C::TZ) *
-                             ((P->d.ny + C::TY - 1) / C::TY) * P->d.nx;
-      long long g = (long long)sms * per_sm;
-      if (g > cols) g = cols;
-      P->g_apply = (int)g;
+      using C = TmaTile<T, K>;
+      marching((const void*)k_stencil_tma<T, K>, C::THREADS, C::SMEM, C::TZ, C::TY);
     } else {
       P->g_apply = fs_grid_blocks((const void*)k_apply_pq<T, K>, N);
     }
@@ -2612,11 +2776,14 @@ struct Impl {
       std::vector<unsigned char> saved(sbytes);
       FS_CHECK(cudaMemcpyAsync(saved.data(), st0, sbytes, cudaMemcpyDeviceToHost, s));
       FS_CHECK(cudaMemsetAsync(P->p[1], 0, (size_t)P->d.N * K * sizeof(T), s));
-      // kind 4 (two threads per node) only for 32-byte nodes
-      const int cands[4] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1};
+      // kind 4 (two threads per node) only for 32-byte nodes; kind 5 (the
+      // direction update fused in) once its z tensor map exists.  Every
+      // candidate is timed with the direction update it needs: k_pnew and
+      // the stencil, or the fused kernel alone.
+      const int cands[5] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1, P->zmap_ok ? 5 : -1};
       float best = 3.4e38f;
       int bestk = 2;
-      for (int c = 0; c < 5; ++c) P->tune_ms[c] = -1.f;
+      for (int c = 0; c < 6; ++c) P->tune_ms[c] = -1.f;
       int* done = &P->ctl->all_done;
       for (int c : cands) {
         if (c < 0) continue;
@@ -2624,11 +2791,14 @@ struct Impl {
         P->use_tma = c != 0;
         apply_grid(P);
         FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
+        kernel(P, 0, 0, s);
+        FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
         kernel(P, 1, 0, s);
         float ms = 0.f;
         for (int r = 0; r < 3; ++r) {
           FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
           FS_CHECK(cudaEventRecord(P->ev[0], s));
+          kernel(P, 0, 0, s);
           kernel(P, 1, 0, s);
           FS_CHECK(cudaEventRecord(P->ev[1], s));
           FS_CHECK(cudaGetLastError());
@@ -2674,6 +2844,8 @@ struct Impl {
         P->stencil_kind = 3;
       } else if (sel && strcmp(sel, "tma_m") == 0) {
         P->stencil_kind = 2;
+      } else if (sel && strcmp(sel, "pz") == 0) {
+        P->stencil_kind = 5;  // falls back to 2 if the z tensor map cannot be made
       } else if (sel && strcmp(sel, "tma_split") == 0) {
         P->stencil_kind = TmaTileSplit<T, K>::OK ? 4 : 2;
       } else {
@@ -2689,6 +2861,46 @@ struct Impl {
     P->g_fold = fs_grid_blocks((const void*)k_fold<T, K>, N);
     P->g_fin = fs_grid_blocks((const void*)k_finalize<T, K>, N);
     P->g_rz = fs_grid_blocks((const void*)k_rz<T, K>, N);
+  }
+  // The z (or r) tensor map of the fused direction-update stencil (kind 5),
+  // once the multigrid output buffer is known; without it kind 5 is not
+  // offered (a plan that asked for it runs kind 2).
+  static int zmap(fs_pcg_plan* P) {
+    P->zmap_ok = 0;
+    if constexpr (!TmaTileM<T, K>::OK) {
+      return FS_OK;
+    } else {
+      const void* zb = P->precond ? P->z : P->r;
+      if (P->stencil_kind < 2 || !zb || P->d.per) {
+        if (P->stencil_kind == 5) {
+          P->stencil_kind = 2;
+          apply_grid(P);
+        }
+        return FS_OK;
+      }
+      auto encode = encode_fn();
+      if (!encode) return FS_OK;
+      const cuuint64_t B = TmaTileM<T, K>::B;
+      cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)P->d.nz, (cuuint64_t)P->d.ny,
+                            (cuuint64_t)P->d.nx};
+      cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
+      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)TmaTileM<T, K>::HZ,
+                           (cuuint32_t)TmaTileM<T, K>::HY, 1};
+      cuuint32_t es[4] = {1, 1, 1, 1};
+      const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+      CUresult rc = encode(&P->tm_z, dt, 4, const_cast<void*>(zb), dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rc == CUDA_SUCCESS) {
+        P->zmap_ok = 1;
+      } else if (P->stencil_kind == 5) {
+        P->stencil_kind = 2;
+      }
+      apply_grid(P);
+      return FS_OK;
+    }
   }
   static int maps(fs_pcg_plan* P) {
     using C = TmaTile<T, K>;
@@ -2779,23 +2991,31 @@ struct Impl {
   static void kernel(fs_pcg_plan* P, int which, int par, cudaStream_t s) {
     switch (which) {
       case 0:
+        if (P->stencil_kind == 5) break;  // the fused stencil forms p itself
         k_pnew<T, K><<<P->g_pnew, fs::kBlock, 0, s>>>(
             P->d, (const T*)(P->precond ? P->z : P->r), (const T*)P->p[par],
             (T*)P->p[1 - par], P->st, P->ctl);
         break;
       case 1:
         if constexpr (TmaTile<T, K>::OK) {
+          if (P->stencil_kind == 5) {
+            using CZ = TmaTilePZ<T, K>;
+            k_stencil_pz<T, K><<<P->g_apply, CZ::THREADS, CZ::SMEM, s>>>(
+                P->dm, P->tm_z, P->tm_p[par], P->tm_m[0], P->tm_m[1], P->tm_m[2],
+                (T*)P->p[1 - par], (T*)P->q, P->partials, P->st, P->ctl);
+            break;
+          }
           if (P->stencil_kind == 3) {
             using CS = TmaTileS<T, K>;
             k_stencil_tma_s<T, K><<<P->g_apply, CS::THREADS, CS::SMEM, s>>>(
-                P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], P->tm_q,
+                P->dm, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], P->tm_q,
                 P->partials, P->st, P->ctl);
             break;
           }
           if (P->stencil_kind == 2) {
             using CM = TmaTileM<T, K>;
             k_stencil_tma_m<T, K><<<P->g_apply, CM::THREADS, CM::SMEM, s>>>(
-                P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
+                P->dm, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
                 P->partials, P->st, P->ctl);
             break;
           }
@@ -2803,7 +3023,7 @@ struct Impl {
             if (P->stencil_kind == 4) {
               using CM = TmaTileM<T, K>;
               k_stencil_split<T, K><<<P->g_apply, TmaTileSplit<T, K>::THREADS, CM::SMEM, s>>>(
-                  P->d, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
+                  P->dm, P->tm_p[1 - par], P->tm_m[0], P->tm_m[1], P->tm_m[2], (T*)P->q,
                   P->partials, P->st, P->ctl);
               break;
             }
@@ -2816,7 +3036,7 @@ struct Impl {
           }
           using C = TmaTile<T, K>;
           k_stencil_tma<T, K><<<P->g_apply, C::THREADS, C::SMEM, s>>>(
-              P->d, P->tm_p[1 - par], (const T*)P->ex, (const T*)P->ey,
+              P->dm, P->tm_p[1 - par], (const T*)P->ex, (const T*)P->ey,
               (const T*)P->ez, (const T*)P->p[1 - par], (T*)P->q, P->partials,
               P->st, P->ctl);
         } else {
@@ -3042,16 +3262,19 @@ struct Impl {
     return true;
   }
   // Persistent grid of a fused smoothing pass on level L.
-  static int smooth_grid(const MgLevel& L, int per_sm) {
+  // Grid of a fused smoothing pass on level L with per_sm resident CTAs per
+  // SM; *dl receives the level's dims with the marching assignment.
+  static int smooth_grid(const MgLevel& L, int per_sm, Dims* dl) {
     using CP = SmoothTile<T, K>;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
-                           ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
-    long long g = (long long)sms * per_sm;
-    if (g > cols) g = cols;
-    return (int)g;
+    const long long ncols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
+                            ((L.d.ny + CP::TY - 1) / CP::TY);
+    *dl = L.d;
+    return (int)fs::march_grid(dl, ncols, (long long)sms * per_sm,
+                               march_lockstep_smoothing() ? L.d.N * K * (long long)sizeof(T) : 0,
+                               kMarchL2Bytes);
   }
   // k_mg_pre_fused on level L (x2 into x[1], r2 into dv); false if a tensor
   // map cannot be made for these buffers.
@@ -3065,15 +3288,18 @@ struct Impl {
       if (!smooth_maps(L, b, &tb, tm)) return false;
       if constexpr (SplitTile<T, K>::OK) {
         if (split_ok(false)) {
-          k_mg_smooth_split<T, K, false>
-              <<<smooth_grid(L, split_per_sm(false)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
-                  L.d, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
-                  &P->ctl->all_done, &P->ctl->error);
+          Dims dl;
+          const int g = smooth_grid(L, split_per_sm(false), &dl);
+          k_mg_smooth_split<T, K, false><<<g, SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+              dl, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
+              &P->ctl->all_done, &P->ctl->error);
           return true;
         }
       }
-      k_mg_pre_fused<T, K><<<smooth_grid(L, pre_per_sm()), CP::THREADS, CP::SMEM, s>>>(
-          L.d, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
+      Dims dl;
+      const int g = smooth_grid(L, pre_per_sm(), &dl);
+      k_mg_pre_fused<T, K><<<g, CP::THREADS, CP::SMEM, s>>>(
+          dl, tb, tm[0], tm[1], tm[2], (T*)L.x[1], (T*)L.dv, c0, cd, cr, &P->ctl->all_done,
           &P->ctl->error);
       return true;
     }
@@ -3089,15 +3315,18 @@ struct Impl {
       if (!smooth_maps(L, x, &tx, tm)) return false;
       if constexpr (SplitTile<T, K>::OK) {
         if (split_ok(true)) {
-          k_mg_smooth_split<T, K, true>
-              <<<smooth_grid(L, split_per_sm(true)), SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
-                  L.d, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
-                  &P->ctl->all_done, &P->ctl->error);
+          Dims dl;
+          const int g = smooth_grid(L, split_per_sm(true), &dl);
+          k_mg_smooth_split<T, K, true><<<g, SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
+              dl, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
+              &P->ctl->all_done, &P->ctl->error);
           return true;
         }
       }
-      k_mg_post_fused<T, K><<<smooth_grid(L, post_per_sm()), CP::THREADS, CP::SMEM, s>>>(
-          L.d, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
+      Dims dl;
+      const int g = smooth_grid(L, post_per_sm(), &dl);
+      k_mg_post_fused<T, K><<<g, CP::THREADS, CP::SMEM, s>>>(
+          dl, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
           &P->ctl->error);
       return true;
     }
@@ -3275,6 +3504,7 @@ bool dispatch_k(int k, fs_pcg_plan* P, int op, cudaStream_t s, int warm = 0,
     if (op == 11) Impl<T, KK>::locate_z(P);                        \
     if (op == 12) Impl<T, KK>::vcycle_ext(P, s);                   \
     if (op == 13) P->net_status = Impl<T, KK>::autotune(P, s);      \
+    if (op == 14) P->net_status = Impl<T, KK>::zmap(P);             \
     return true;
   switch (k) {
     FS_OP(1)
@@ -3523,6 +3753,8 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
     dispatch(P, 9, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail("multigrid setup", e);
   }
+  dispatch(P, 14, s);  // the fused stencil's z map, now that z is known
+  P->net_status = FS_OK;
   if ((e = host_slot_get(&P->slot)) != cudaSuccess) return fail("cudaMallocHost", e);
   P->h_flag = &P->slot->flag;
   P->h_st = P->slot->st;
@@ -3772,7 +4004,7 @@ int fs_pcg_plan_stencil_kind(const fs_pcg_plan* P) { return P ? P->stencil_kind 
 
 int fs_pcg_plan_stencil_times(const fs_pcg_plan* P, float* ms) {
   if (!P || !ms) return FS_BAD_ARG;
-  for (int c = 0; c < 5; ++c) ms[c] = P->tune_ms[c];
+  for (int c = 0; c < 6; ++c) ms[c] = P->tune_ms[c];
   return FS_OK;
 }
 

@@ -183,28 +183,31 @@ class DeviceOperator:
         L.check("fs_apply_laplacian", st)
         return out
 
-    def quadform(self, u, nrhs: int = 1) -> np.ndarray:
-        """``u^T L u`` per RHS (FP64)."""
+    def quadform(self, u, nrhs: int = 1, out=None):
+        """``u^T L u`` per RHS (FP64): a host array, or written into the
+        device tensor ``out`` (nrhs FP64 values) without a host copy."""
         import torch
         lib = L.lib()
         nb = ctypes.c_size_t()
         L.check("fs_quadform_workspace_bytes",
                 lib.fs_quadform_workspace_bytes(nrhs, ctypes.byref(nb)))
         ws = torch.empty(nb.value, dtype=torch.uint8, device=self.dev)
-        out = torch.empty(nrhs, dtype=torch.float64, device=self.dev)
+        dst = torch.empty(nrhs, dtype=torch.float64, device=self.dev) if out is None else out
         nx, ny, nz = self.shape
         st = lib.fs_quadform(L.ptr(self.mx), L.ptr(self.my), L.ptr(self.mz),
-                             L.ptr(u), nx, ny, nz, nrhs, L.ptr(out), L.ptr(ws),
+                             L.ptr(u), nx, ny, nz, nrhs, L.ptr(dst), L.ptr(ws),
                              nb.value, L.stream_ptr())
         L.check("fs_quadform", st)
-        return d2h(out)
+        return d2h(dst) if out is None else out
 
     def group_sums(self, u, groups, nrhs: int = 1, minus=None, w=None,
-                   nodes_dev=None) -> np.ndarray:
+                   nodes_dev=None, out=None):
         """``sum_{n in group} (L u - L_minus w)_n`` per group and RHS (FP64).
 
         ``groups`` is a list of node-index arrays; ``nodes_dev`` may carry the
-        already-uploaded ``(nodes, offsets)`` pair to skip the copy.
+        already-uploaded ``(nodes, offsets)`` pair to skip the copy.  Returns
+        a host ``(ngroups, nrhs)`` array, or writes the device tensor ``out``
+        (ngroups * nrhs FP64 values) without a host copy.
         """
         import torch
         lib = L.lib()
@@ -215,16 +218,17 @@ class DeviceOperator:
         L.check("fs_group_apply_workspace_bytes",
                 lib.fs_group_apply_workspace_bytes(ng, nrhs, ctypes.byref(nb)))
         ws = torch.empty(nb.value, dtype=torch.uint8, device=self.dev)
-        out = torch.empty(ng * nrhs, dtype=torch.float64, device=self.dev)
+        dst = (torch.empty(ng * nrhs, dtype=torch.float64, device=self.dev)
+               if out is None else out)
         nx, ny, nz = self.shape
         mb = (None, None, None) if minus is None else (minus.mx, minus.my, minus.mz)
         st = lib.fs_group_apply(L.ptr(self.mx), L.ptr(self.my), L.ptr(self.mz),
                                 L.ptr(u), *(L.ptr(t) for t in mb), L.ptr(w),
                                 L.ptr(nodes), L.ptr(offsets), ng, nx, ny, nz,
-                                nrhs, L.ptr(out), L.ptr(ws), nb.value,
+                                nrhs, L.ptr(dst), L.ptr(ws), nb.value,
                                 L.stream_ptr())
         L.check("fs_group_apply", st)
-        return d2h(out).reshape(ng, nrhs)
+        return d2h(dst).reshape(ng, nrhs) if out is None else out
 
 
 def upload_groups(groups, dev):

@@ -35,6 +35,16 @@ from .poisson import check_terminals, raise_on_status
 __all__ = ["EQSSolver"]
 
 
+def _walls_time_dependent(bc) -> bool:
+    """Whether a Dirichlet wall of ``bc`` takes a callable value."""
+    from ..boundaries import WALLS
+    for w in WALLS:
+        wall = bc.get(w) if hasattr(bc, "get") else getattr(bc, w, None)
+        if getattr(wall, "is_dirichlet_like", False) and callable(getattr(wall, "value", None)):
+            return True
+    return False
+
+
 class EQSSolver:
     """Time-domain electroquasistatic solver (``eqs.py:42-103``).
 
@@ -93,6 +103,45 @@ class EQSSolver:
         values = np.concatenate(val)
         uniq, last = np.unique(fixed[::-1], return_index=True)
         return uniq, values[::-1][last]
+
+    def _dirichlet_values(self, terminals, bc, fixed, dev):
+        """Per-step Dirichlet values of the fixed set ``fixed`` (fixed for the
+        run; the later source wins on a shared node, eqs.py:108-129) as a
+        function of t returning a device tensor.  When every source is
+        uniform (a terminal's voltage, a wall of one value) only the source
+        values cross to the device each step and a gather spreads them."""
+        import torch
+        srcs = [("term", tt) for tt in terminals if tt.driven == "voltage"]
+        idx = [np.asarray(tt.nodes, np.intp) for _, tt in srcs]
+        bidx, bval0 = (dirichlet_nodes(bc, self.grid, 0.0) if bc is not None
+                       else (np.zeros(0, np.intp), np.zeros(0)))
+        if bidx.size:
+            idx.append(bidx)
+        if not idx:
+            return lambda t: torch.zeros(0, dtype=torch.float64, device=dev)
+        cat = np.concatenate(idx)
+        owner = np.concatenate([np.full(a.size, j) for j, a in enumerate(idx)])
+        uniq, last = np.unique(cat[::-1], return_index=True)
+        pick = cat.size - 1 - last
+        assert np.array_equal(uniq, fixed)
+        walls_uniform = bidx.size == 0 or bool(np.all(np.asarray(bval0) == bval0[0]))
+        if walls_uniform and not (bc is not None and _walls_time_dependent(bc)):
+            owner_d = h2d(owner[pick].astype(np.int64), torch.int64, dev)
+            wall_v = float(bval0[0]) if bidx.size else 0.0
+
+            def values(t):
+                v = [float(tt.value_at(t)) for _, tt in srcs]
+                if bidx.size:
+                    v.append(wall_v)
+                return h2d(np.asarray(v), torch.float64, dev)[owner_d]
+            return values
+
+        def values_general(t):
+            parts = [np.full(a.size, float(tt.value_at(t))) for a, (_, tt) in zip(idx, srcs)]
+            if bidx.size:
+                parts.append(np.asarray(dirichlet_nodes(bc, self.grid, t)[1], float))
+            return h2d(np.concatenate(parts)[pick], torch.float64, dev)
+        return values_general
 
     def _node_weights(self, nodes) -> np.ndarray:
         """Dual-volume weights of a terminal's nodes (eqs.py:131-154)."""
@@ -218,22 +267,28 @@ class EQSSolver:
 
         groups = [np.asarray(tt.nodes, np.int64) for tt in terms]
         gdev = upload_groups(groups, dev) if groups else None
-        wts = [h2d(self._node_weights(g), torch.float64, dev) for g in groups]
-        nodes_dev = [h2d(g, torch.int64, dev) for g in groups]
-
         nt = len(terms)
-        cur = np.zeros((n + 1, nt))
-        volt = np.zeros((n + 1, nt))
-        energy = np.zeros(n + 1)
-        diss = np.zeros(n + 1)
+        f64 = dict(dtype=torch.float64, device=dev)
+        # per-step records stay on the device and come back once at the end
+        cur_d = torch.zeros((n + 1, max(nt, 1)), **f64)
+        volt_d = torch.zeros((n + 1, max(nt, 1)), **f64)
+        en_d = torch.zeros(n + 1, **f64)
+        diss_d = torch.zeros(n + 1, **f64)
+        if nt:
+            # terminal voltage = dual-volume weighted mean: one segment sum
+            seg = h2d(np.concatenate([np.full(gr.size, j) for j, gr in enumerate(groups)]),
+                      torch.int64, dev)
+            wcat = h2d(np.concatenate([self._node_weights(gr) for gr in groups]),
+                       torch.float64, dev)
+            ncat = gdev[0]
         stored, stored_t = [], []
         iters = []
 
         def record(k, phi_d):
-            for j in range(nt):
-                volt[k, j] = float((phi_d[nodes_dev[j]] * wts[j]).sum())
-            energy[k] = 0.5 * float(self.op_eps.quadform(phi_d)[0])
-            diss[k] = float(self.op_sig.quadform(phi_d)[0])
+            if nt:
+                volt_d[k].index_add_(0, seg, phi_d[ncat] * wcat)
+            self.op_eps.quadform(phi_d, out=en_d[k:k + 1])
+            self.op_sig.quadform(phi_d, out=diss_d[k:k + 1])
             if store and (k == 0 or k % max(1, store_every) == 0):
                 stored.append(d2h(phi_d).copy())
                 stored_t.append(times[k])
@@ -245,13 +300,9 @@ class EQSSolver:
         tol = float(self.cfg.tol)
         nx, ny, nz = self.op_eps.shape
         lib = L.lib()
+        step_values = self._dirichlet_values(terms, bc, fixed, dev)
         for k in range(1, n + 1):
             t = float(times[k])
-            f_fix, vals = self._dirichlet(terms, bc, t)
-            if not np.array_equal(f_fix, fixed):
-                raise NotImplementedError(
-                    "the set of Dirichlet nodes changes during the run; the GPU "
-                    "path keeps one eliminated system per run")
             prev.copy_(system.phi)
             inj = self._inject_dev(terms, t, dev)
             st = lib.fs_apply_laplacian(L.ptr(Kexp.mx), L.ptr(Kexp.my), L.ptr(Kexp.mz),
@@ -259,18 +310,22 @@ class EQSSolver:
                                         nx, ny, nz, 1, L.stream_ptr())
             L.check("fs_apply_laplacian", st)
             if fixed.size:
-                system.phi[fixed_d] = h2d(vals, torch.float64, dev)
+                system.phi[fixed_d] = step_values(t)
             _, stats = system.solve(tol, self.gpu.maxiter, warm=True)
             raise_on_status(stats, tol, "gpu-cg")
             iters.append(stats[0]["iterations"])
             if nt:
-                cur[k] = K.group_sums(system.phi, groups, minus=Kexp, w=prev,
-                                      nodes_dev=gdev)[:, 0]
+                K.group_sums(system.phi, groups, minus=Kexp, w=prev, nodes_dev=gdev,
+                             out=cur_d[k])
             record(k, system.phi)
             if mset is not None:
                 self._record_monitors(mset, system.phi, t, dt)
         if n >= 1:
-            cur[0] = cur[1]
+            cur_d[0] = cur_d[1]
+        cur = d2h(cur_d)[:, :nt]
+        volt = d2h(volt_d)[:, :nt]
+        energy = 0.5 * d2h(en_d)
+        diss = d2h(diss_d)
         system.close()
 
         res = Result(grid=self.grid, t=times)

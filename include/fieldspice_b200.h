@@ -407,14 +407,18 @@ int fs_pcg_plan_scale(const fs_pcg_plan* plan, const double** s64, const uint8_t
 int fs_pcg_plan_label_counts(const fs_pcg_plan* plan, long long* counts, void* stream);
 /* The CG stencil kernel the plan runs: 0 cached loads, 1 TMA-staged p,
  * 2 TMA-staged p and masses, 3 as 2 with TMA stores of q, 4 as 2 with each
- * 32-byte node split over two threads.  Unless the FS_STENCIL environment
+ * 32-byte node split over two threads, 5 as 2 with the direction update
+ * p = z + beta p_old formed inside the stencil from staged z and p_old tiles
+ * (no separate p-update kernel).  Unless the FS_STENCIL environment
  * variable names one, the first plan of each (grid, RHS block, precision)
- * times kinds 2, 3, 0 (and 4 for 32-byte nodes) on its own buffers at
- * creation and later plans of that shape reuse the fastest.                 */
+ * times kinds 2, 3, 0, 5 (and 4 for 32-byte nodes), each with the direction
+ * update it needs, on its own buffers at creation and later plans of that
+ * shape reuse the fastest.                                                  */
 int fs_pcg_plan_stencil_kind(const fs_pcg_plan* plan);
-/* ms[5] (host): the mean time per launch of each stencil kind (index = kind)
- * measured by this plan's autotuner; -1 for kinds it did not time (every
- * entry is -1 when the plan reused an earlier choice or FS_STENCIL chose).  */
+/* ms[6] (host): the mean time per iteration of the direction update and the
+ * stencil for each kind (index = kind) measured by this plan's autotuner;
+ * -1 for kinds it did not time (every entry is -1 when the plan reused an
+ * earlier choice or FS_STENCIL chose).                                      */
 int fs_pcg_plan_stencil_times(const fs_pcg_plan* plan, float* ms);
 
 /* ---- §8f-4: harmonic EQS, the complex-symmetric solve -------------------------
