@@ -63,7 +63,7 @@ class _Extraction:
     def __init__(self, grid, eps_cell, terminals, bc, cfg, gcfg):
         import torch
         self.grid = grid
-        _, eps, eps_min, _ = upload_cell_property(eps_cell, grid, "eps_cell")
+        _, eps, eps_min, eps_max = upload_cell_property(eps_cell, grid, "eps_cell")
         if eps_min <= 0.0:
             raise ValueError("eps_cell must be strictly positive [F/m]")
         if eps_min >= 1e-6:
@@ -74,7 +74,7 @@ class _Extraction:
         if nt == 0:
             raise ValueError("capacitance extraction needs at least one terminal")
         bc = prepare_bc(bc, grid)
-        self.op = DeviceOperator(grid, eps)
+        self.op = DeviceOperator(grid, eps, prop_range=(eps_min, eps_max))
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
         term_nodes = [np.asarray(t.nodes, np.int64) for t in self.terms]
@@ -95,8 +95,8 @@ class _Extraction:
             self.op, label, nt, precision=gcfg.precision,
             preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned,
             coarsening=gcfg.coarsening)
-        self.maxiter = (self.system.default_maxiter() if gcfg.maxiter is None
-                        else int(gcfg.maxiter))
+        # 0: the reference's cap max(500, 10 sqrt(n_free)), per plan on the device
+        self.maxiter = 0 if gcfg.maxiter is None else int(gcfg.maxiter)
         group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)
         for c, n in enumerate(term_dev):
             group[n] = c

@@ -193,6 +193,8 @@ def dirichlet_nodes(spec, grid, t: float = 0.0):
         val_parts.append(vals)
     if not idx_parts:
         return np.empty(0, dtype=np.intp), np.empty(0, dtype=float)
+    if len(idx_parts) == 1:  # one wall: its nodes are ascending and unique already
+        return idx_parts[0], val_parts[0]
     idx_all = np.concatenate(idx_parts)
     val_all = np.concatenate(val_parts)
     uniq, first_in_rev = np.unique(idx_all[::-1], return_index=True)

@@ -134,6 +134,12 @@ __device__ __forceinline__ void apply_eq(const Dims& d, const T* __restrict__ ex
 #pragma unroll
     for (int t = 0; t < K; ++t) ax[t] -= m * v[t];
   };
+  if (d.per) {  // a periodic level (aggregation hierarchy): wrap edges
+    edge6(d, ex, ey, ez, n, i, j, k, [&](bool ok, T m, long long nb) {
+      if (ok) nbr(m, nb);
+    });
+    return;
+  }
   if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
   if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
   if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
@@ -374,12 +380,18 @@ __global__ void __launch_bounds__(kBlock, mg_min_blocks<T, K>())
 #pragma unroll
       for (int t = 0; t < K; ++t) ad[t] -= m * (cd * a[t] + cr * c[t]);
     };
-    if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
-    if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
-    if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
-    if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
-    if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
-    if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+    if (d.per) {  // periodic level: wrap edges
+      edge6(d, ex, ey, ez, n, i, j, k, [&](bool ok, T m, long long nb) {
+        if (ok) nbr(m, nb);
+      });
+    } else {
+      if (i > 0) nbr(__ldg(ex + n - d.sx), n - d.sx);
+      if (i < d.nx - 1) nbr(__ldg(ex + n), n + d.sx);
+      if (j > 0) nbr(__ldg(ey + n - d.sy), n - d.sy);
+      if (j < d.ny - 1) nbr(__ldg(ey + n), n + d.sy);
+      if (k > 0) nbr(__ldg(ez + n - 1), n - 1);
+      if (k < d.nz - 1) nbr(__ldg(ez + n), n + 1);
+    }
 #pragma unroll
     for (int t = 0; t < K; ++t) {
       xv[t] += dc[t];
@@ -646,19 +658,26 @@ __global__ void k_agg_coarsen(Dims f, Dims c, const double* __restrict__ fmx,
             else if (up_cross)
               acc += m;
           };
+          // on a periodic axis the last plane's +edge is the wrap edge to the
+          // first plane (its mass stored on the last plane): the last
+          // aggregate's crossing to aggregate 0, kept on the last coarse plane
           double none = 0.0;
-          edge(i > 0, i > 0 ? fmx[fn - f.sx] : 0.0, fn - f.sx, false, none);
-          edge(i + 1 < f.nx, fmx[fn], fn + f.sx, i == i1, sx);
-          edge(j > 0, j > 0 ? fmy[fn - f.sy] : 0.0, fn - f.sy, false, none);
-          edge(j + 1 < f.ny, fmy[fn], fn + f.sy, j == j1, sy);
-          edge(k > 0, k > 0 ? fmz[fn - 1] : 0.0, fn - 1, false, none);
-          edge(k + 1 < f.nz, fmz[fn], fn + 1, k == k1, sz);
+          const bool px = f.per & 1, py = (f.per >> 1) & 1, pz = (f.per >> 2) & 1;
+          edge(i > 0 || px, i > 0 ? fmx[fn - f.sx] : fmx[fn + f.wx],
+               i > 0 ? fn - f.sx : fn + f.wx, false, none);
+          edge(i + 1 < f.nx || px, fmx[fn], i + 1 < f.nx ? fn + f.sx : fn - f.wx, i == i1, sx);
+          edge(j > 0 || py, j > 0 ? fmy[fn - f.sy] : fmy[fn + f.wy],
+               j > 0 ? fn - f.sy : fn + f.wy, false, none);
+          edge(j + 1 < f.ny || py, fmy[fn], j + 1 < f.ny ? fn + f.sy : fn - f.wy, j == j1, sy);
+          edge(k > 0 || pz, k > 0 ? fmz[fn - 1] : fmz[fn + f.wz],
+               k > 0 ? fn - 1 : fn + f.wz, false, none);
+          edge(k + 1 < f.nz || pz, fmz[fn], k + 1 < f.nz ? fn + 1 : fn - f.wz, k == k1, sz);
         }
     clabel[n] = any_free ? FS_LABEL_FREE : FS_LABEL_FIXED;
     cdg[n] = any_free ? dg : 0.0;
-    cmx[n] = I + 1 < c.nx ? sx : 0.0;
-    cmy[n] = J + 1 < c.ny ? sy : 0.0;
-    cmz[n] = Kc + 1 < c.nz ? sz : 0.0;
+    cmx[n] = (I + 1 < c.nx || (c.per & 1)) ? sx : 0.0;
+    cmy[n] = (J + 1 < c.ny || (c.per & 2)) ? sy : 0.0;
+    cmz[n] = (Kc + 1 < c.nz || (c.per & 4)) ? sz : 0.0;
   }
 }
 

@@ -322,7 +322,10 @@ __global__ void __launch_bounds__(fs::kBlock)
     __syncthreads();
     if (threadIdx.x == 0) {
       ctl->tol = tol;
-      ctl->maxiter = maxiter;
+      // maxiter <= 0: the reference's cap max(500, 10 sqrt(n_free))
+      // (poisson.py:535-536) from this plan's own classification
+      ctl->maxiter = maxiter > 0 ? maxiter
+                                 : max(500, (int)(10.0 * sqrt((double)ctl->label_counts[0])));
       ctl->delta = delta;
       ctl->precond = precond > 0 ? 1 : 0;
       ctl->flexible = precond > 1 ? 1 : 0;
@@ -2450,7 +2453,7 @@ int mg_dims(const Dims& fine, long long coarsest, Dims* out) {
   while (nl < kMaxLevels && d.N > coarsest) {
     const int nx = half(d.nx), ny = half(d.ny), nz = half(d.nz);
     if (nx == d.nx && ny == d.ny && nz == d.nz) break;
-    d = fs::make_dims(nx, ny, nz);
+    d = fs::make_dims(nx, ny, nz, fine.per);  // a periodic axis stays periodic
     out[nl++] = d;
   }
   return nl;
@@ -3154,6 +3157,7 @@ struct Impl {
   // k_mg_post_fused); FS_MG_PRE=plain / FS_MG_POST=plain keep the two-kernel
   // forms.
   static bool smooth_fused_ok(const MgLevel& L, bool post) {
+    if (L.d.per) return false;  // the TMA tiles do not wrap
     using CP = SmoothTile<T, K>;
     if constexpr (!CP::OK) {
       return false;
@@ -3370,7 +3374,7 @@ struct Impl {
       cur = 1;
       rfine = (const T*)L.dv;
       *nl += 2;
-    } else if (last && fs::coarse_fits<T>(L.d.N, deg)) {
+    } else if (last && !L.d.per && fs::coarse_fits<T>(L.d.N, deg)) {
       // the whole coarsest-level solve in one launch, one block per RHS
       fs::CoarseCoef<T> coef;
       for (int k = 0; k < deg; ++k) {
@@ -3646,8 +3650,9 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   if (!plan) return FS_BAD_ARG;
   *plan = nullptr;
   if (periodic < 0 || periodic > 7) return FS_BAD_ARG;
-  if (periodic && precond != FS_PRECOND_JACOBI) {
-    fs_set_error_msg("periodic axes: the multigrid hierarchy does not wrap; use Jacobi PCG");
+  if (periodic && precond == FS_PRECOND_MG) {
+    fs_set_error_msg("periodic axes: the rediscretised multigrid hierarchy does not wrap; "
+                     "use FS_PRECOND_MG_AGG (aggregates wrap) or Jacobi PCG");
     return FS_BAD_ARG;
   }
   size_t need = 0;
@@ -3760,8 +3765,11 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   P->h_st = P->slot->st;
 
   // Capture `chunk` CG iterations once; the graph is replayed until the
-  // device reports that every RHS has finished.
-  P->chunk = 16;
+  // device reports that every RHS has finished.  Multigrid solves take ~20
+  // iterations to 1e-10, so 12 per graph wastes at most a few launches that
+  // return at once after convergence (16 wasted up to 10); Jacobi takes
+  // thousands, where longer graphs save host round trips.
+  P->chunk = P->precond ? 12 : 32;
   if ((e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking)) !=
       cudaSuccess)
     return fail("cudaStreamCreate", e);
@@ -3881,13 +3889,21 @@ int solve_finish(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats,
 
 extern "C" {
 
+// Host bound on the iterations of a solve: maxiter, or for the device-side
+// default (maxiter <= 0) its largest possible value, n_free <= N.
+static long long host_maxiter(const fs_pcg_plan* P, int maxiter) {
+  if (maxiter > 0) return maxiter;
+  const long long d = (long long)(10.0 * sqrt((double)P->d.N));
+  return d > 500 ? d : 500;
+}
+
 int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
                       fs_rhs_stats* stats, void* stream) {
-  if (!P || !(tol > 0.0) || maxiter < 1) return FS_BAD_ARG;
+  if (!P || !(tol > 0.0)) return FS_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   int st = solve_begin(P, warm_start, tol, maxiter, s);
   if (st != FS_OK) return st;
-  const long long max_chunks = (long long)maxiter / P->chunk + 4;
+  const long long max_chunks = host_maxiter(P, maxiter) / P->chunk + 4;
   int timed_out = 1;
   cudaError_t e;
   for (long long c = 0; c < max_chunks; ++c) {
@@ -3905,8 +3921,7 @@ int fs_pcg_plan_solve(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
 int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
                        void* const* streams, int warm_start, double tol,
                        int maxiter, fs_rhs_stats* const* stats, int* status) {
-  if (!plans || nplans < 1 || !streams || !status || !(tol > 0.0) || maxiter < 1)
-    return FS_BAD_ARG;
+  if (!plans || nplans < 1 || !streams || !status || !(tol > 0.0)) return FS_BAD_ARG;
   for (int i = 0; i < nplans; ++i)
     if (!plans[i]) return FS_BAD_ARG;
   std::vector<int> active(nplans, 1);
@@ -3935,7 +3950,7 @@ int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
       if ((e = cudaStreamSynchronize((cudaStream_t)streams[i])) != cudaSuccess)
         return fs_cuda_status("cudaStreamSynchronize", e);
       const int done = solve_check(P);
-      const bool out = chunks[i] >= (long long)maxiter / P->chunk + 4;
+      const bool out = chunks[i] >= host_maxiter(P, maxiter) / P->chunk + 4;
       if (done || out) {
         active[i] = 0;
         --left;

@@ -237,11 +237,11 @@ void wgrad_launch(const fs::ConvGeom& g, const Vol& x, int xoff, const Vol& dy, 
                                                 rows_per, pw, pb);
 }
 
-// The weight gradient of training: on CUDA cores unless FS_WGRAD=tc selects
-// the tensor-core kernel.
+// The weight gradient of training: on tensor cores unless FS_WGRAD=cuda
+// selects the CUDA-core kernel.
 bool wgrad_on_cuda_cores() {
   const char* sel = getenv("FS_WGRAD");
-  return !(sel && strcmp(sel, "tc") == 0);
+  return sel && strcmp(sel, "cuda") == 0;
 }
 
 // Weight and bias gradient of conv l into U->grad.

@@ -85,7 +85,7 @@ class DeviceOperator:
     """
 
     def __init__(self, grid, prop_cell=None, *, mode: str = "parallel",
-                 masses=None, shape=None, periodic: int = 0):
+                 masses=None, shape=None, periodic: int = 0, prop_range=None):
         import torch
         self.grid = grid
         self.shape = (tuple(int(s) for s in grid.shape_nodes) if shape is None
@@ -93,6 +93,7 @@ class DeviceOperator:
         self.N = int(np.prod(self.shape))
         self.dev = device()
         self.periodic = int(periodic)   # wrap-around axes (bit 0 x, 1 y, 2 z)
+        self.material_contrast = None   # cell-property max/min, when known
         lib = L.lib()
         if masses is not None:
             self.m = masses
@@ -111,6 +112,17 @@ class DeviceOperator:
                                  avg, L.ptr(self.m[0]), L.ptr(self.m[1]),
                                  L.ptr(self.m[2]), L.stream_ptr())
         L.check("fs_build_masses", st)
+        # the material contrast (largest over smallest positive cell value),
+        # which decides the multigrid hierarchy; geometry (grading, a
+        # collapsed axis) is handled by the rediscretised levels either way,
+        # and a zero-conductivity region is decoupled, not a contrast
+        if prop_range is None and isinstance(prop_cell, np.ndarray):
+            pos = prop_cell[prop_cell > 0]
+            if pos.size:
+                prop_range = (float(pos.min()), float(pos.max()))
+        if prop_range is not None:
+            lo, hi = (float(v) for v in prop_range)
+            self.material_contrast = hi / lo if lo > 0.0 else None
 
     # -- mass arrays ---------------------------------------------------------
     @property
@@ -267,9 +279,10 @@ class EliminatedSystem:
     system then stay in FP64.
     """
 
-    #: Edge-mass contrast above which ``coarsening="auto"`` builds the
-    #: multigrid levels by aggregation with Galerkin coarse operators
-    #: (conductors in insulators: copper/oxide in an EQS step is ~1e6).
+    #: Material contrast (the operator's cell property, max over min; the
+    #: edge-mass contrast when the property is not known) above which
+    #: ``coarsening="auto"`` builds the multigrid levels by aggregation with
+    #: Galerkin coarse operators (copper/oxide in an EQS step is ~1e6).
     GALERKIN_CONTRAST = 1e3
 
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
@@ -291,18 +304,19 @@ class EliminatedSystem:
             if precision == "fp64":
                 raise ValueError("the learned preconditioner runs in mixed precision")
         if op.periodic and preconditioner != "jacobi":
-            # the multigrid hierarchy and the TMA stencils do not wrap
+            # of the multigrid hierarchies only the aggregation one wraps
             if preconditioner == "learned":
                 raise ValueError("the learned preconditioner does not support periodic axes")
-            preconditioner = "jacobi"
+            coarsening = "galerkin"
         self.preconditioner = preconditioner
         self.learned = learned
         # optional FP64 node-diagonal term of the operator (kept alive here)
         self.diag = (None if diag is None else
                      torch.as_tensor(diag, dtype=torch.float64, device=op.dev).contiguous())
         if preconditioner == "mg" and coarsening == "auto":
-            coarsening = ("galerkin" if op.mass_contrast() > self.GALERKIN_CONTRAST
-                          else "geometric")
+            contrast = (op.material_contrast if op.material_contrast is not None
+                        else op.mass_contrast())
+            coarsening = "galerkin" if contrast > self.GALERKIN_CONTRAST else "geometric"
         # the learned level is trained on the geometric hierarchy
         self.coarsening = ("geometric" if preconditioner == "learned" else coarsening) \
             if preconditioner != "jacobi" else None
@@ -328,10 +342,7 @@ class EliminatedSystem:
         lab_ptr = lib.fs_pcg_plan_labels(self._plan)
         off = lab_ptr - self.workspace.data_ptr()
         self.labels = self.workspace[off:off + N]
-        counts = (ctypes.c_longlong * 4)()
-        L.check("fs_pcg_plan_label_counts",
-                lib.fs_pcg_plan_label_counts(self._plan, counts, L.stream_ptr()))
-        self.n_free, self.n_fixed, self.n_solo, self.n_pinned = (int(c) for c in counts)
+        self._counts = None      # free / fixed / solo / pinned, read when first asked
         self._net_ws = None
         self.learned_level = None
         self.learned_fallback = False
@@ -363,6 +374,30 @@ class EliminatedSystem:
         L.check("fs_pcg_plan_create", st)
         return plan, ws
 
+    def _label_counts(self):
+        if self._counts is None:
+            counts = (ctypes.c_longlong * 4)()
+            L.check("fs_pcg_plan_label_counts",
+                    L.lib().fs_pcg_plan_label_counts(self._plan, counts, L.stream_ptr()))
+            self._counts = tuple(int(c) for c in counts)
+        return self._counts
+
+    @property
+    def n_free(self) -> int:
+        return self._label_counts()[0]
+
+    @property
+    def n_fixed(self) -> int:
+        return self._label_counts()[1]
+
+    @property
+    def n_solo(self) -> int:
+        return self._label_counts()[2]
+
+    @property
+    def n_pinned(self) -> int:
+        return self._label_counts()[3]
+
     def default_maxiter(self) -> int:
         """The reference's cap ``max(500, 10*sqrt(n))`` (poisson.py:535-536)."""
         return max(500, int(10 * math.sqrt(max(self.n_free, 1))))
@@ -382,8 +417,9 @@ class EliminatedSystem:
                     for s in stats[:self.nrhs]]
 
     def solve(self, tol: float, maxiter: int | None = None, *, warm: bool = False):
-        """Solve in place into ``phi``; returns (status, per-RHS stats dicts)."""
-        mi = self.default_maxiter() if maxiter is None else int(maxiter)
+        """Solve in place into ``phi``; returns (status, per-RHS stats dicts).
+        ``maxiter=None``: the reference's cap, evaluated on the device."""
+        mi = 0 if maxiter is None else int(maxiter)
         self.launches = 0
         if self.fell_back:
             return self._run(self._fp64[0], tol, mi, warm)

@@ -35,6 +35,12 @@ from .poisson import check_terminals, raise_on_status
 __all__ = ["EQSSolver"]
 
 
+def _contrast(prop: np.ndarray):
+    """Largest over smallest positive cell value (None when none is)."""
+    pos = prop[prop > 0]
+    return float(pos.max() / pos.min()) if pos.size else None
+
+
 def _walls_time_dependent(bc) -> bool:
     """Whether a Dirichlet wall of ``bc`` takes a callable value."""
     from ..boundaries import WALLS
@@ -252,6 +258,7 @@ class EQSSolver:
         times = t_start + dt * np.arange(n + 1)
 
         K = self.op_eps.combine(1.0 / dt, self.op_sig, theta)
+        K.material_contrast = _contrast(self.eps_cell / dt + theta * self.sigma_cell)
         Kexp = self.op_eps.combine(1.0 / dt, self.op_sig, -(1.0 - theta))
         fixed, _ = self._dirichlet(terms, bc, times[0])
         label = torch.zeros(N, dtype=torch.uint8, device=dev)

@@ -194,7 +194,7 @@ class PoissonSolver:
         self.grid = grid
         self.cfg = config or SolverConfig()
         self.gpu = gpu or GPUConfig()
-        eps_cell, eps_dev, eps_min, _ = upload_cell_property(eps_cell, grid, "eps_cell")
+        eps_cell, eps_dev, eps_min, eps_max = upload_cell_property(eps_cell, grid, "eps_cell")
         if eps_min <= 0.0:
             raise ValueError("eps_cell must be strictly positive [F/m]")
         if eps_min >= 1e-6:
@@ -205,7 +205,7 @@ class PoissonSolver:
         self.eps_cell = eps_cell
         self.eps_mode = eps_mode
         mark("eps_upload_and_check")
-        self.op = DeviceOperator(grid, eps_dev, mode=eps_mode)
+        self.op = DeviceOperator(grid, eps_dev, mode=eps_mode, prop_range=(eps_min, eps_max))
         mark("masses")
         self._L = None
         self.last_capacitance_report: dict[str, Any] = {}

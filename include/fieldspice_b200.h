@@ -174,7 +174,8 @@ int fs_pcg_plan_create_diag(int nx, int ny, int nz, int nrhs, int precision,
  * plane of a periodic axis merged into the first, poisson.py:665-719, 942-955),
  * and the first and last planes of each periodic axis are joined by a wrap
  * edge whose mass is stored on the last plane (mx at i = nx-1, and so on).
- * Jacobi-preconditioned CG only (precond = FS_PRECOND_JACOBI).              */
+ * precond = FS_PRECOND_JACOBI or FS_PRECOND_MG_AGG (the node aggregates wrap
+ * with the grid); FS_PRECOND_MG is refused with FS_BAD_ARG.                 */
 int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int precond,
                           const double* mx, const double* my, const double* mz,
                           const double* diag, int periodic, const uint8_t* label_in,
@@ -182,7 +183,9 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
                           size_t workspace_bytes, fs_pcg_plan** plan, void* stream);
 /* Solve in place into phi.  warm_start != 0 keeps the free-node values of
  * phi as the initial guess (the tolerance stays relative to ||b||, as in
- * SciPy); otherwise the guess is 0.  stats: host array of nrhs entries.
+ * SciPy); otherwise the guess is 0.  maxiter <= 0 caps the iterations at the
+ * reference's max(500, 10 sqrt(n_free)) (poisson.py:535-536) from the plan's
+ * own classification, on the device.  stats: host array of nrhs entries.
  * Returns FS_OK when every RHS converged, FS_NOT_CONVERGED if one hit
  * maxiter, FS_STALLED if a mixed-precision RHS stopped making progress,
  * FS_NAN on breakdown, FS_TIMEOUT if a staged load never arrived.           */
