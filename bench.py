@@ -77,11 +77,25 @@ def measured_peaks():
 
 
 def committed_traffic():
-    """Per-node DRAM bytes of the CG kernels from the committed ncu summary."""
+    """Per-node DRAM bytes of each kernel (by name) from the committed ncu
+    summary: ``{"kernels": {name: {"bytes_per_node": ...}}}``."""
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
-        return json.loads(p.read_text())
+        return json.loads(p.read_text()).get("kernels", {})
     return {}
+
+
+def kernel_names(s: int, k: int, stencil_kind: int) -> dict:
+    """The kernel each timed role runs as (template names as ncu lists them)."""
+    t = "float" if s == 4 else "double"
+    stencil = {5: "k_stencil_pz", 4: "k_stencil_split", 3: "k_stencil_tma_s",
+               2: "k_stencil_tma_m", 1: "k_stencil_tma"}.get(stencil_kind, "k_apply_pq")
+    split = k * s == 32  # 32-byte nodes: the two-threads-per-node smoothing pass
+    return {"stencil": f"{stencil}<{t}, {k}>",
+            "pupdate": f"k_pnew<{t}, {k}>",
+            "update": f"k_update<{t}, {k}>",
+            "smoother": (f"k_mg_smooth_split<{t}, {k}, 1>" if split
+                         else f"k_mg_post_fused<{t}, {k}>")}
 
 
 # ---------------------------------------------------------------------------
@@ -182,12 +196,14 @@ def e2e_phase_report(calls, allocs):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def kernel_bytes(N: int, k: int, s: int) -> dict:
+def kernel_bytes(N: int, k: int, s: int, stencil_kind: int = 2) -> dict:
     """Algorithmic bytes per launch of the CG kernels (each array once)."""
     return {"pupdate": 3 * N * k * s,                 # read r|z, p_old; write p
-            "stencil": N * (2 * k * s + 3 * s),       # read p, 3 masses; write q
+            # read p, 3 masses; write q -- with the direction update inside
+            # (kind 5) read z and p_old, write p and q
+            "stencil": N * ((4 if stencil_kind == 5 else 2) * k * s + 3 * s),
             "update": 6 * N * k * s,                  # read p, q, x, r; write x, r
-            # fine-level post-smoothing, one fused pass (k_mg_post_fused):
+            # fine-level post-smoothing, one fused pass (k_mg_smooth_split):
             # read x, b and the masses; write x2 = x + a r0 + b A~r0
             "smoother": N * (3 * k * s + 3 * s)}
 
@@ -350,8 +366,9 @@ def run_ours(args, rank, world, local_rank):
         return
     N = int(np.prod(shape))
     s = 8 if (args.precision == "fp64" or info.get("fp64_fallback")) else 4
-    kb = kernel_bytes(N, 8, s)
     km = info["kernel_ms"]
+    kb = kernel_bytes(N, 8, s, km.get("stencil_kind", 2))
+    names = kernel_names(s, 8, km.get("stencil_kind", 2))
     times = {"pupdate": km["pupdate_ms"], "stencil": km["stencil_ms"],
              "update": km["update_ms"]}
     if args.preconditioner == "mg":
@@ -359,7 +376,7 @@ def run_ours(args, rank, world, local_rank):
     dom = max(times, key=times.get)
     peak, peak_kind = measured_peaks()
     gbs = {k: kb[k] / (times[k] * 1e-3) / 1e9 for k in times if times[k] > 0}
-    traffic = committed_traffic().get(f"{dom}_{args.precision}_bytes_per_node")
+    traffic = committed_traffic().get(names[dom], {}).get("bytes_per_node")
     rep = capacitance_report(C, qs, info)
     # parity against the committed full-size oracle result (same seed-0 input)
     err_vs_oracle = None
@@ -397,7 +414,8 @@ def run_ours(args, rank, world, local_rank):
                 "step_ms_max": e2e_steps[-1] if e2e_steps else None,
                 "worst_call": e2e_detail["worst"]["summary"] if e2e_detail["worst"] else None},
         "roofline": {
-            "bound": "hbm", "kernel": dom, "achieved": gbs.get(dom), "peak": peak,
+            "bound": "hbm", "kernel": names[dom], "role": dom, "achieved": gbs.get(dom),
+            "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s",
             "frac": (gbs.get(dom) or 0.0) / peak,
             "traffic": (traffic * N if traffic else None),

@@ -322,11 +322,14 @@ __device__ __forceinline__ void stv(T* __restrict__ base, long long n,
 // (warp shuffle tree, then warps in index order) and writes one partial per
 // value.  The last block to finish (atomic ticket) sums the partials over
 // blocks, again in a fixed order, so results do not depend on scheduling.
-template <int M, int NT = kBlock>
-__device__ __forceinline__ void block_partials(double (&acc)[M],
-                                               double* __restrict__ partials) {
+// scratch: NT / 32 * M doubles of shared memory (a kernel whose dynamic
+// shared memory is free by then passes part of it: no static array that would
+// lower its occupancy).
+template <int M, int NT>
+__device__ __forceinline__ void block_partials_to(double (&acc)[M],
+                                                  double* __restrict__ partials,
+                                                  double* scratch) {
   static_assert(NT % 32 == 0 && NT >= 32, "block size must be whole warps");
-  __shared__ double sm[NT / 32][M];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int m = 0; m < M; ++m) {
@@ -334,15 +337,22 @@ __device__ __forceinline__ void block_partials(double (&acc)[M],
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
       v += __shfl_down_sync(0xffffffffu, v, off);
-    if (lane == 0) sm[warp][m] = v;
+    if (lane == 0) scratch[warp * M + m] = v;
   }
   __syncthreads();
   if (threadIdx.x < M) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < NT / 32; ++w) s += sm[w][threadIdx.x];
+    for (int w = 0; w < NT / 32; ++w) s += scratch[w * M + threadIdx.x];
     partials[(size_t)blockIdx.x * M + threadIdx.x] = s;
   }
+}
+
+template <int M, int NT = kBlock>
+__device__ __forceinline__ void block_partials(double (&acc)[M],
+                                               double* __restrict__ partials) {
+  __shared__ double sm[NT / 32 * M];
+  block_partials_to<M, NT>(acc, partials, sm);
 }
 
 // Returns true in exactly one block: the last one to arrive.  That block
@@ -363,24 +373,31 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
 
 // Sum partials[b*M + m] over b in a fixed order; call from the last block
 // (NT threads).  Result is valid in out[m] for all threads after the call.
-template <int M, int NT = kBlock>
-__device__ __forceinline__ void grid_total(const double* partials, int nblocks,
-                                           double (&out)[M]) {
+// scratch: NT doubles of shared memory.
+template <int M, int NT>
+__device__ __forceinline__ void grid_total_to(const double* partials, int nblocks,
+                                              double (&out)[M], double* scratch) {
   static_assert((NT & (NT - 1)) == 0, "block size must be a power of two");
-  __shared__ double red[NT];
   for (int m = 0; m < M; ++m) {
     double s = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += NT)
       s += __ldcg(partials + (size_t)b * M + m);
-    red[threadIdx.x] = s;
+    scratch[threadIdx.x] = s;
     __syncthreads();
     for (int w = NT / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      if (threadIdx.x < w) scratch[threadIdx.x] += scratch[threadIdx.x + w];
       __syncthreads();
     }
-    out[m] = red[0];
+    out[m] = scratch[0];
     __syncthreads();
   }
+}
+
+template <int M, int NT = kBlock>
+__device__ __forceinline__ void grid_total(const double* partials, int nblocks,
+                                           double (&out)[M]) {
+  __shared__ double red[NT];
+  grid_total_to<M, NT>(partials, nblocks, out, red);
 }
 
 }  // namespace fs

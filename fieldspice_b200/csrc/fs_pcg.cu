@@ -1578,6 +1578,37 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
   }
 }
 
+// gamma = r~.z (tot, per RHS) into the CG state: beta = gamma / gamma_old.
+// Called by every thread of the last block of the r.z reduction.
+template <int K>
+__device__ void rz_apply(const double (&tot)[K], RhsState* st, Control* ctl) {
+  if (threadIdx.x < K) {
+    RhsState& s = st[threadIdx.x];
+    if (s.active) {
+      const double g = tot[threadIdx.x];
+      if (!(g > 0.0) || !isfinite(g)) {
+        // M is SPD: r.Mr = 0 means r = 0; r.Mr < 0 means the FP32
+        // preconditioner lost definiteness on a mode below its resolution
+        // (reported as a stall, so "auto" continues in FP64); NaN/Inf is a
+        // breakdown.
+        s.active = 0;
+        s.status = (g == 0.0) ? FS_OK : (isfinite(g) ? FS_STALLED : FS_NAN);
+      } else if (s.fresh) {
+        s.gamma = g;
+        s.gamma_old = g;
+        s.beta = 0.0;
+        s.fresh = 0;
+      } else {
+        s.gamma_old = s.gamma;
+        s.gamma = g;
+        s.beta = g / s.gamma_old;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) refresh_done(st, ctl, K);
+}
+
 // ---- the fused smoothing passes with each node split over two threads ------------
 // For 32-byte nodes (8 FP32 or 4 FP64 RHS) k_mg_pre_fused and k_mg_post_fused
 // are latency-bound on the warps two 256-thread CTAs per SM give them.  Here
@@ -1616,7 +1647,10 @@ __device__ __forceinline__ void st16(T* p, const T (&v)[W]) {
 }
 
 // POST = false: k_mg_pre_fused's arithmetic (src = b; out1 = x2, out2 = r2).
-// POST = true:  k_mg_post_fused's (src = x, b by loads; out1 = xout).
+// POST = true:  k_mg_post_fused's (src = x, b by loads; out1 = xout).  On the
+// finest level b is the CG residual r~ and xout is z = M r~: with rz_partials
+// set, the pass also forms gamma = r~.z (k_rz: per-block FP64 partials, the
+// last block updates beta), so no separate pass re-reads r~ and z.
 template <typename T, int K, bool POST>
 __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
     k_mg_smooth_split(Dims d, const __grid_constant__ CUtensorMap tm_s,
@@ -1624,7 +1658,8 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
                       const __grid_constant__ CUtensorMap tm_ey,
                       const __grid_constant__ CUtensorMap tm_ez, const T* __restrict__ b,
                       T* __restrict__ out1, T* __restrict__ out2, T c0, T cd, T cr,
-                      const int* __restrict__ done, int* __restrict__ err) {
+                      const int* __restrict__ done, int* __restrict__ err,
+                      double* __restrict__ rz_partials, RhsState* st, Control* ctl) {
   using C = SmoothTile<T, K>;
   constexpr int W = SplitTile<T, K>::W;
   if (*done) return;
@@ -1653,6 +1688,9 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
   __syncthreads();
   int ticket = 0, uc = 0;
   bool failed = false, bad = false;
+  double rzacc[W];
+#pragma unroll
+  for (int t = 0; t < W; ++t) rzacc[t] = 0.0;
   while (u < u_end && !failed) {
     const int col = u / d.nx;
     const int xa = u - col * d.nx;
@@ -1821,6 +1859,12 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
             o1[t] += c0 * fB[t] + cd * a[t];  // k_mg_post2: x + alpha r0 + beta A~r0
           }
           st16<T, W>(out1 + n * K + hf * W, o1);
+          if (rz_partials) {  // r~.z: b was read one plane ago (an L2 hit)
+            T bo2[W];
+            ld16<T, W>(b + n * K + hf * W, bo2);
+#pragma unroll
+            for (int t = 0; t < W; ++t) rzacc[t] += (double)bo2[t] * (double)o1[t];
+          }
         } else {
           T o2[W];
 #pragma unroll
@@ -1854,6 +1898,24 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
       for (int s = 0; s < C::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
     }
     __syncthreads();
+  }
+  if constexpr (POST) {
+    if (rz_partials) {
+      // the d1 ring (written by threads only, never by TMA) is free now
+      constexpr int NT = SplitTile<T, K>::THREADS;
+      static_assert(NT * 8 <= 3 * C::UPLP, "reduction scratch exceeds the d1 ring");
+      double* scr = reinterpret_cast<double*>(base + C::O_U);
+      __syncthreads();
+      double acc[K];
+#pragma unroll
+      for (int t = 0; t < K; ++t) acc[t] = (t / W == hf) ? rzacc[t % W] : 0.0;
+      fs::block_partials_to<K, NT>(acc, rz_partials, scr);
+      if (fs::last_block(&ctl->tickets[kTicketRz])) {
+        double tot[K];
+        fs::grid_total_to<K, NT>(rz_partials, gridDim.x, tot, scr);
+        rz_apply<K>(tot, st, ctl);
+      }
+    }
   }
 }
 
@@ -2015,31 +2077,7 @@ __global__ void __launch_bounds__(fs::kBlock)
   if (fs::last_block(&ctl->tickets[kTicketRz])) {
     double tot[K];
     fs::grid_total<K>(partials, gridDim.x, tot);
-    if (threadIdx.x < K) {
-      RhsState& s = st[threadIdx.x];
-      if (s.active) {
-        const double g = tot[threadIdx.x];
-        if (!(g > 0.0) || !isfinite(g)) {
-          // M is SPD: r.Mr = 0 means r = 0; r.Mr < 0 means the FP32
-          // preconditioner lost definiteness on a mode below its resolution
-          // (reported as a stall, so "auto" continues in FP64); NaN/Inf is a
-          // breakdown.
-          s.active = 0;
-          s.status = (g == 0.0) ? FS_OK : (isfinite(g) ? FS_STALLED : FS_NAN);
-        } else if (s.fresh) {
-          s.gamma = g;
-          s.gamma_old = g;
-          s.beta = 0.0;
-          s.fresh = 0;
-        } else {
-          s.gamma_old = s.gamma;
-          s.gamma = g;
-          s.beta = g / s.gamma_old;
-        }
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) refresh_done(st, ctl, K);
+    rz_apply<K>(tot, st, ctl);
   }
 }
 
@@ -2585,6 +2623,9 @@ struct fs_pcg_plan {
   MgLevel lev[kMaxLevels];
   void* z;                 // preconditioned residual (level-0 V-cycle output)
   int g_rz;
+  int rz_request;          // set while the CG preconditioner runs: the finest
+                           // post-smoothing may form r~.z itself
+  int rz_fused;            // the last V-cycle did (no k_rz launch needed)
   long long launches_per_iter;
   MgParams mg;
   const double *mx, *my, *mz;
@@ -3296,7 +3337,7 @@ struct Impl {
           const int g = smooth_grid(L, split_per_sm(false), &dl);
           k_mg_smooth_split<T, K, false><<<g, SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
               dl, tb, tm[0], tm[1], tm[2], b, (T*)L.x[1], (T*)L.dv, c0, cd, cr,
-              &P->ctl->all_done, &P->ctl->error);
+              &P->ctl->all_done, &P->ctl->error, nullptr, nullptr, nullptr);
           return true;
         }
       }
@@ -3308,23 +3349,37 @@ struct Impl {
       return true;
     }
   }
+  // Whether the finest post-smoothing runs as k_mg_smooth_split, which can
+  // form r~.z in the same pass.
+  static bool post_split(const MgLevel& L) {
+    if constexpr (SplitTile<T, K>::OK) {
+      return smooth_fused_ok(L, true) && split_ok(true);
+    } else {
+      return false;
+    }
+  }
   // k_mg_post_fused on level L (xout = x + alpha r0 + beta A~r0, r0 = b - A~x).
-  static bool launch_post_fused(fs_pcg_plan* P, MgLevel& L, const T* x, const T* b, T* xout,
-                                T alpha, T beta, cudaStream_t s) {
+  // Returns 0 if a tensor map cannot be made for these buffers (nothing
+  // launched), 1 when launched, 2 when launched with r~.z formed in the pass
+  // (rz requested and the two-threads-per-node form runs).
+  static int launch_post_fused(fs_pcg_plan* P, MgLevel& L, const T* x, const T* b, T* xout,
+                               T alpha, T beta, bool rz, cudaStream_t s) {
     using CP = SmoothTile<T, K>;
     if constexpr (!CP::OK) {
-      return false;
+      return 0;
     } else {
       CUtensorMap tx, tm[3];
-      if (!smooth_maps(L, x, &tx, tm)) return false;
+      if (!smooth_maps(L, x, &tx, tm)) return 0;
       if constexpr (SplitTile<T, K>::OK) {
         if (split_ok(true)) {
           Dims dl;
           const int g = smooth_grid(L, split_per_sm(true), &dl);
+          const bool with_rz = rz && g <= kMaxBlocks;  // partials hold kMaxBlocks rows
           k_mg_smooth_split<T, K, true><<<g, SplitTile<T, K>::THREADS, CP::SMEM, s>>>(
               dl, tx, tm[0], tm[1], tm[2], b, xout, nullptr, alpha, beta, (T)0,
-              &P->ctl->all_done, &P->ctl->error);
-          return true;
+              &P->ctl->all_done, &P->ctl->error, with_rz ? P->partials : nullptr, P->st,
+              P->ctl);
+          return with_rz ? 2 : 1;
         }
       }
       Dims dl;
@@ -3332,7 +3387,7 @@ struct Impl {
       k_mg_post_fused<T, K><<<g, CP::THREADS, CP::SMEM, s>>>(
           dl, tx, tm[0], tm[1], tm[2], b, xout, alpha, beta, &P->ctl->all_done,
           &P->ctl->error);
-      return true;
+      return 1;
     }
   }
   static int vcycle_plain(fs_pcg_plan* P, int l, const T* b, cudaStream_t s,
@@ -3432,8 +3487,13 @@ struct Impl {
       const int out = 1 - cur;
       const double alpha = cr[0] * (1.0 + cd[1]) + cr[1], beta = -cr[1] * cr[0];
       const bool fused = smooth_fused_ok(L, true);
-      if (!dry && !(fused && launch_post_fused(P, L, (const T*)L.x[cur], b, (T*)L.x[out],
-                                               (T)alpha, (T)beta, s))) {
+      const bool want_rz = l == 0 && P->rz_request;
+      int how = 0;
+      if (!dry && fused)
+        how = launch_post_fused(P, L, (const T*)L.x[cur], b, (T*)L.x[out], (T)alpha,
+                                (T)beta, want_rz, s);
+      if (want_rz) P->rz_fused = dry ? (post_split(L) ? 1 : 0) : (how == 2 ? 1 : 0);
+      if (!dry && how == 0) {
         fs::k_mg_residual<T, K><<<g, fs::kBlock, 0, s>>>(
             L.d, e0, e1, e2, (const T*)L.x[cur], b, (T*)L.res, done);
         fs::k_mg_post2<T, K><<<g, fs::kBlock, 0, s>>>(
@@ -3460,23 +3520,32 @@ struct Impl {
   // captures kernels that read z before the first V-cycle of an iteration.
   static void locate_z(fs_pcg_plan* P) {
     long long nl = 0;
+    P->rz_request = P->learned < 0 ? 1 : 0;
+    P->rz_fused = 0;
     const int zi = vcycle(P, 0, (const T*)P->r, nullptr, &nl, true);
+    P->rz_request = 0;
     P->z = P->lev[0].x[zi];
-    P->launches_per_iter = nl + 1;
+    P->launches_per_iter = nl + (P->rz_fused ? 0 : 1);
   }
+  // z = M r~ and gamma = r~.z: in the finest post-smoothing pass when it can
+  // form the product (plain multigrid), else by k_rz / k_rz_flex.  Returns
+  // the number of launches.
   static long long precondition(fs_pcg_plan* P, cudaStream_t s) {
     long long nl = 0;
+    P->rz_request = P->learned < 0 ? 1 : 0;
+    P->rz_fused = 0;
     const int zi = vcycle(P, 0, (const T*)P->r, s, &nl);
+    P->rz_request = 0;
     P->z = P->lev[0].x[zi];
     if (P->learned >= 0)
       k_rz_flex<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r, (const T*)P->z,
                                                      (const T*)P->q, P->partials, P->st,
                                                      P->ctl);
-    else
+    else if (!P->rz_fused)
       k_rz<T, K><<<P->g_rz, fs::kBlock, 0, s>>>(P->d, (const T*)P->r,
                                                 (const T*)P->z, P->partials,
                                                 P->st, P->ctl);
-    return nl + 1;
+    return nl + (P->rz_fused ? 0 : 1);
   }
   // One V-cycle on a caller's equilibrated right-hand side (P->ext_b).
   static void vcycle_ext(fs_pcg_plan* P, cudaStream_t s) {
@@ -3674,6 +3743,8 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   P->agg = precond == FS_PRECOND_MG_AGG ? 1 : 0;
   P->mg = g_mg;
   P->launches_per_iter = 0;
+  P->rz_request = 0;
+  P->rz_fused = 0;
   P->mx = mx;
   P->dg = diag;
   P->my = my;

@@ -469,16 +469,18 @@ class EliminatedSystem:
         """Per-kernel device time sampled during the last solve (ms per
         launch): p update, stencil (A~p, p.q), update (x, r, r.r), reliable
         update, the preconditioner (V-cycle + r.z) and one fine-level
-        multigrid smoothing step."""
+        multigrid smoothing step; ``stencil_kind`` is the CG stencil the plan
+        runs (5: the direction update formed inside the stencil)."""
         ms = (ctypes.c_double * 6)()
         ns = ctypes.c_longlong()
         L.check("fs_pcg_plan_kernel_times",
                 L.load_library().fs_pcg_plan_kernel_times(self._last_plan, ms,
                                                           ctypes.byref(ns)))
         n = max(ns.value, 1)
+        kind = L.load_library().fs_pcg_plan_stencil_kind(self._last_plan)
         return {"samples": ns.value, "pupdate_ms": ms[0] / n, "stencil_ms": ms[1] / n,
                 "update_ms": ms[2] / n, "reliable_ms": ms[3] / n,
-                "precond_ms": ms[4] / n, "smoother_ms": ms[5] / n}
+                "precond_ms": ms[4] / n, "smoother_ms": ms[5] / n, "stencil_kind": kind}
 
     def close(self) -> None:
         lib = L.load_library()
