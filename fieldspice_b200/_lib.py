@@ -35,6 +35,28 @@ class FsRhsStats(ctypes.Structure):
                 ("reliable_updates", c_int32), ("reserved", c_int32)]
 
 
+class FsMgParams(ctypes.Structure):
+    """``fs_mg_params``: multigrid and stencil options of one plan."""
+    _fields_ = [("smooth_deg", c_int32), ("smooth_lo", c_double),
+                ("coarse_deg", c_int32), ("coarse_lo", c_double),
+                ("coarsest_nodes", c_longlong), ("stencil_kind", c_int32)]
+
+
+def mg_params(opts: dict | None):
+    """An ``FsMgParams`` from the library defaults updated by ``opts`` (keys
+    as the struct fields), or None for the defaults."""
+    if not opts:
+        return None
+    unknown = set(opts) - {f for f, _ in FsMgParams._fields_}
+    if unknown:
+        raise ValueError(f"unknown multigrid option(s): {sorted(unknown)}")
+    p = FsMgParams()
+    load_library().fs_mg_params_default(ctypes.byref(p))
+    for k, v in opts.items():
+        setattr(p, k, v)
+    return p
+
+
 class FsError(RuntimeError):
     """A library call returned a status other than FS_OK."""
 
@@ -63,6 +85,12 @@ _SIGNATURES = {
                                         POINTER(c_void_p), c_void_p]),
     "fs_pcg_plan_create_ex": (c_int, [c_int] * 6 + [c_void_p] * 4 + [c_int] + [c_void_p] * 4
                               + [c_size_t, POINTER(c_void_p), c_void_p]),
+    "fs_mg_params_default": (None, [POINTER(FsMgParams)]),
+    "fs_pcg_workspace_bytes_opt": (c_int, [c_int] * 6 + [POINTER(FsMgParams),
+                                                         POINTER(c_size_t)]),
+    "fs_pcg_plan_create_opt": (c_int, [c_int] * 6 + [c_void_p] * 4 + [c_int,
+                               POINTER(FsMgParams)] + [c_void_p] * 4
+                               + [c_size_t, POINTER(c_void_p), c_void_p]),
     "fs_periodic_masses": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "fs_pcg_plan_solve": (c_int, [c_void_p, c_int, c_double, c_int,
                                   POINTER(FsRhsStats), c_void_p]),
@@ -113,7 +141,6 @@ _SIGNATURES = {
     "fs_ac_solve": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                             c_void_p, c_double, c_int, c_void_p, c_size_t,
                             POINTER(FsRhsStats), c_void_p]),
-    "fs_mg_set_params": (c_int, [c_int, c_double, c_int, c_double, c_longlong]),
     "fs_pcg_plan_labels": (c_void_p, [c_void_p]),
     "fs_pcg_plan_launches": (c_longlong, [c_void_p]),
     "fs_pcg_plan_kernel_times": (c_int, [c_void_p, POINTER(c_double),

@@ -94,7 +94,7 @@ class _Extraction:
         self.system = EliminatedSystem(
             self.op, label, nt, precision=gcfg.precision,
             preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned,
-            coarsening=gcfg.coarsening)
+            coarsening=gcfg.coarsening, mg_params=gcfg.mg_params)
         # 0: the reference's cap max(500, 10 sqrt(n_free)), per plan on the device
         self.maxiter = 0 if gcfg.maxiter is None else int(gcfg.maxiter)
         group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)

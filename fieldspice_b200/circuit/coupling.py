@@ -211,7 +211,8 @@ class FieldRegion:
                                           precision=self.gpu.precision,
                                           preconditioner=resolve_preconditioner(
                                               self.cfg, self.gpu),
-                                          coarsening=self.gpu.coarsening)
+                                          coarsening=self.gpu.coarsening,
+                                          mg_params=self.gpu.mg_params)
                 self._excite(system.phi, cols, k)
                 _, st = system.solve(tol, self.gpu.maxiter)
                 raise_on_status(st, tol, "gpu-cg")
@@ -244,7 +245,8 @@ class FieldRegion:
                     entry.K, self._label, 1, precision=self.gpu.precision,
                     with_source=True,
                     preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                    coarsening=self.gpu.coarsening)
+                    coarsening=self.gpu.coarsening,
+                    mg_params=self.gpu.mg_params)
             hs = entry.history
             nx, ny, nz = self.op_eps.shape
             m = entry.K_hist

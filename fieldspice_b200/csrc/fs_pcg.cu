@@ -2454,18 +2454,39 @@ size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // ---- multigrid hierarchy ---------------------------------------------------------
 constexpr int kMaxLevels = 12;
-// Multigrid parameters (process-wide; a plan copies them when created).
-// Defaults from a sweep on the 256x256x128 8-terminal extraction: degree-2
-// smoothing on [0.3, 2] and a degree-32 Chebyshev solve on a coarsest level
-// of at most 4096 nodes gave the shortest extraction (20-21 iterations).
+// Multigrid and stencil options of one plan (fs_mg_params, copied at
+// creation; nothing process-wide).  Defaults from a sweep on the
+// 256x256x128 8-terminal extraction: degree-2 smoothing on [0.3, 2] and a
+// degree-32 Chebyshev solve on a coarsest level of at most 4096 nodes gave
+// the shortest extraction (20-21 iterations).
 struct MgParams {
   int smooth_deg = 2;          // Chebyshev degree, pre and post
   double smooth_lo = 0.3;      // smoothing interval [lo, 2] of A~
   int coarse_deg = 32;         // coarsest-level Chebyshev degree
   double coarse_lo = 0.03;
   long long coarsest_nodes = 4096;
+  int stencil_kind = -1;       // CG stencil 0..5; -1: FS_STENCIL, else autotuned
 };
-MgParams g_mg;
+
+// Options from the caller's struct (NULL: defaults); false if out of range.
+bool mg_params_from(const fs_mg_params* o, MgParams* out) {
+  MgParams m;
+  if (o) {
+    if (o->smooth_deg < 1 || o->smooth_deg > 16 || o->coarse_deg < 1 || o->coarse_deg > 64 ||
+        !(o->smooth_lo > 0.0 && o->smooth_lo < 2.0) ||
+        !(o->coarse_lo > 0.0 && o->coarse_lo < 2.0) || o->coarsest_nodes < 8 ||
+        o->stencil_kind < -1 || o->stencil_kind > 5)
+      return false;
+    m.smooth_deg = o->smooth_deg;
+    m.smooth_lo = o->smooth_lo;
+    m.coarse_deg = o->coarse_deg;
+    m.coarse_lo = o->coarse_lo;
+    m.coarsest_nodes = o->coarsest_nodes;
+    m.stencil_kind = o->stencil_kind;
+  }
+  *out = m;
+  return true;
+}
 
 struct MgLevel {
   Dims d;
@@ -2530,7 +2551,8 @@ long long max_blocks(const Dims& d) {
   return f > kMaxBlocks ? f : kMaxBlocks;
 }
 
-Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
+Layout make_layout(const Dims& d, int nrhs, int precision, int precond,
+                   long long coarsest_nodes) {
   const size_t tb = precision == FS_PRECISION_MIXED ? 4 : 8;
   const size_t N = (size_t)d.N;
   Layout L;
@@ -2552,7 +2574,7 @@ Layout make_layout(const Dims& d, int nrhs, int precision, int precond) {
   L.nlev = 0;
   if (precond == FS_PRECOND_MG || precond == FS_PRECOND_MG_AGG) {
     Dims dl[kMaxLevels];
-    L.nlev = mg_dims(d, g_mg.coarsest_nodes, dl);
+    L.nlev = mg_dims(d, coarsest_nodes, dl);
     for (int l = 0; l < L.nlev; ++l) {
       MgLevel& m = L.lev[l];
       m = MgLevel{};
@@ -2698,9 +2720,16 @@ bool march_lockstep_smoothing() {
   return sel && strcmp(sel, "lockstep") == 0;
 }
 
-bool plain_stencil() {
+// The CG stencil asked for: the plan's option, else FS_STENCIL (plain, tma1,
+// tma_m, tmas, tma_split, pz), else -1 (autotuned).
+int stencil_request(int opt) {
+  if (opt >= 0) return opt;
   const char* sel = getenv("FS_STENCIL");
-  return sel && strcmp(sel, "plain") == 0;
+  if (!sel) return -1;
+  static const char* names[6] = {"plain", "tma1", "tma_m", "tmas", "tma_split", "pz"};
+  for (int k = 0; k < 6; ++k)
+    if (strcmp(sel, names[k]) == 0) return k;
+  return -1;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -2872,7 +2901,7 @@ struct Impl {
     using C = TmaTile<T, K>;
     P->g_pnew = fs_grid_blocks((const void*)k_pnew<T, K>, N);
     {
-      const char* sel = getenv("FS_STENCIL");
+      const int want = stencil_request(P->mg.stencil_kind);
       const bool mass_ok = ((long long)P->d.nz * (long long)sizeof(T)) % 16 == 0;
       // k_stencil_tma_m counts its column-planes in 32 bits
       using CM = TmaTileM<T, K>;
@@ -2880,17 +2909,17 @@ struct Impl {
                               ((P->d.ny + CM::TY - 1) / CM::TY) * P->d.nx <
                           (1LL << 30);
       P->autotune = 0;
-      if (!C::OK || plain_stencil() || P->d.per) {  // only the cached-load kernel wraps
+      if (!C::OK || want == 0 || P->d.per) {  // only the cached-load kernel wraps
         P->stencil_kind = 0;
-      } else if (!mass_ok || !fits32 || (sel && strcmp(sel, "tma1") == 0)) {
+      } else if (!mass_ok || !fits32 || want == 1) {
         P->stencil_kind = 1;
-      } else if (sel && strcmp(sel, "tmas") == 0) {
+      } else if (want == 3) {
         P->stencil_kind = 3;
-      } else if (sel && strcmp(sel, "tma_m") == 0) {
+      } else if (want == 2) {
         P->stencil_kind = 2;
-      } else if (sel && strcmp(sel, "pz") == 0) {
+      } else if (want == 5) {
         P->stencil_kind = 5;  // falls back to 2 if the z tensor map cannot be made
-      } else if (sel && strcmp(sel, "tma_split") == 0) {
+      } else if (want == 4) {
         P->stencil_kind = TmaTileSplit<T, K>::OK ? 4 : 2;
       } else {
         // chosen by timing the candidates on the first plan of this shape
@@ -3667,29 +3696,34 @@ int capture_graph(fs_pcg_plan* P) {
 
 extern "C" {
 
-int fs_mg_set_params(int smooth_deg, double smooth_lo, int coarse_deg,
-                     double coarse_lo, long long coarsest_nodes) {
-  if (smooth_deg < 1 || smooth_deg > 16 || coarse_deg < 1 || coarse_deg > 64 ||
-      !(smooth_lo > 0.0 && smooth_lo < 2.0) || !(coarse_lo > 0.0 && coarse_lo < 2.0) ||
-      coarsest_nodes < 8)
-    return FS_BAD_ARG;
-  g_mg.smooth_deg = smooth_deg;
-  g_mg.smooth_lo = smooth_lo;
-  g_mg.coarse_deg = coarse_deg;
-  g_mg.coarse_lo = coarse_lo;
-  g_mg.coarsest_nodes = coarsest_nodes;
-  return FS_OK;
+void fs_mg_params_default(fs_mg_params* p) {
+  if (!p) return;
+  const MgParams m;
+  p->smooth_deg = m.smooth_deg;
+  p->smooth_lo = m.smooth_lo;
+  p->coarse_deg = m.coarse_deg;
+  p->coarse_lo = m.coarse_lo;
+  p->coarsest_nodes = m.coarsest_nodes;
+  p->stencil_kind = m.stencil_kind;
 }
 
-int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
-                           int precond, size_t* bytes) {
+int fs_pcg_workspace_bytes_opt(int nx, int ny, int nz, int nrhs, int precision,
+                               int precond, const fs_mg_params* opt, size_t* bytes) {
   if (nx < 2 || ny < 2 || nz < 2 || !valid_nrhs(nrhs) || !bytes) return FS_BAD_ARG;
   if (precision != FS_PRECISION_FP64 && precision != FS_PRECISION_MIXED)
     return FS_BAD_ARG;
   if (precond != FS_PRECOND_JACOBI && precond != FS_PRECOND_MG && precond != FS_PRECOND_MG_AGG)
     return FS_BAD_ARG;
-  *bytes = make_layout(fs::make_dims(nx, ny, nz), nrhs, precision, precond).total;
+  MgParams m;
+  if (!mg_params_from(opt, &m)) return FS_BAD_ARG;
+  *bytes = make_layout(fs::make_dims(nx, ny, nz), nrhs, precision, precond,
+                       m.coarsest_nodes).total;
   return FS_OK;
+}
+
+int fs_pcg_workspace_bytes(int nx, int ny, int nz, int nrhs, int precision,
+                           int precond, size_t* bytes) {
+  return fs_pcg_workspace_bytes_opt(nx, ny, nz, nrhs, precision, precond, nullptr, bytes);
 }
 
 int fs_pcg_plan_create(int nx, int ny, int nz, int nrhs, int precision,
@@ -3716,16 +3750,29 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
                           const double* diag, int periodic, const uint8_t* label_in,
                           double* phi, const double* f, void* workspace,
                           size_t workspace_bytes, fs_pcg_plan** plan, void* stream) {
+  return fs_pcg_plan_create_opt(nx, ny, nz, nrhs, precision, precond, mx, my, mz, diag,
+                                periodic, nullptr, label_in, phi, f, workspace,
+                                workspace_bytes, plan, stream);
+}
+
+int fs_pcg_plan_create_opt(int nx, int ny, int nz, int nrhs, int precision, int precond,
+                           const double* mx, const double* my, const double* mz,
+                           const double* diag, int periodic, const fs_mg_params* opt,
+                           const uint8_t* label_in, double* phi, const double* f,
+                           void* workspace, size_t workspace_bytes, fs_pcg_plan** plan,
+                           void* stream) {
   if (!plan) return FS_BAD_ARG;
   *plan = nullptr;
   if (periodic < 0 || periodic > 7) return FS_BAD_ARG;
+  MgParams mgp;
+  if (!mg_params_from(opt, &mgp)) return FS_BAD_ARG;
   if (periodic && precond == FS_PRECOND_MG) {
     fs_set_error_msg("periodic axes: the rediscretised multigrid hierarchy does not wrap; "
                      "use FS_PRECOND_MG_AGG (aggregates wrap) or Jacobi PCG");
     return FS_BAD_ARG;
   }
   size_t need = 0;
-  int st = fs_pcg_workspace_bytes(nx, ny, nz, nrhs, precision, precond, &need);
+  int st = fs_pcg_workspace_bytes_opt(nx, ny, nz, nrhs, precision, precond, opt, &need);
   if (st != FS_OK) return st;
   if (!mx || !my || !mz || !label_in || !phi || !workspace ||
       workspace_bytes < need)
@@ -3741,7 +3788,7 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   P->precision = precision;
   P->precond = (precond == FS_PRECOND_MG || precond == FS_PRECOND_MG_AGG) ? 1 : 0;
   P->agg = precond == FS_PRECOND_MG_AGG ? 1 : 0;
-  P->mg = g_mg;
+  P->mg = mgp;
   P->launches_per_iter = 0;
   P->rz_request = 0;
   P->rz_fused = 0;
@@ -3751,7 +3798,7 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
   P->mz = mz;
   P->phi = phi;
   P->f = f;
-  Layout L = make_layout(P->d, nrhs, precision, precond);
+  Layout L = make_layout(P->d, nrhs, precision, precond, mgp.coarsest_nodes);
   char* w = (char*)workspace;
   P->nlev = L.nlev;
   for (int l = 0; l < L.nlev; ++l) {

@@ -288,8 +288,9 @@ class EliminatedSystem:
     def __init__(self, op: DeviceOperator, label, nrhs: int, *,
                  precision: str = "auto", with_source: bool = False,
                  preconditioner: str = "jacobi", learned=None, diag=None,
-                 coarsening: str = "auto"):
+                 coarsening: str = "auto", mg_params: dict | None = None):
         import torch
+        self.mg_params = L.mg_params(mg_params)  # validated names; None = defaults
         if coarsening not in ("auto", "geometric", "galerkin"):
             raise ValueError(f"coarsening must be 'auto', 'geometric' or 'galerkin', "
                              f"got {coarsening!r}")
@@ -359,18 +360,19 @@ class EliminatedSystem:
         prec = L.PRECISION_MIXED if precision == "mixed" else L.PRECISION_FP64
         nb = ctypes.c_size_t()
         nx, ny, nz = op.shape
+        opt = None if self.mg_params is None else ctypes.byref(self.mg_params)
         L.check("fs_pcg_workspace_bytes",
-                lib.fs_pcg_workspace_bytes(nx, ny, nz, self.k, prec, self._pc,
-                                           ctypes.byref(nb)))
+                lib.fs_pcg_workspace_bytes_opt(nx, ny, nz, self.k, prec, self._pc, opt,
+                                               ctypes.byref(nb)))
         ws = torch.empty(nb.value, dtype=torch.uint8, device=op.dev)
         if ws.data_ptr() % 256:
             raise RuntimeError("device allocation is not 256-byte aligned")
         plan = ctypes.c_void_p()
-        st = lib.fs_pcg_plan_create_ex(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
-                                       L.ptr(op.my), L.ptr(op.mz), L.ptr(self.diag),
-                                       int(op.periodic), L.ptr(self.label_in),
-                                       L.ptr(self.phi), L.ptr(self.f), L.ptr(ws), nb.value,
-                                       ctypes.byref(plan), L.stream_ptr())
+        st = lib.fs_pcg_plan_create_opt(nx, ny, nz, self.k, prec, self._pc, L.ptr(op.mx),
+                                        L.ptr(op.my), L.ptr(op.mz), L.ptr(self.diag),
+                                        int(op.periodic), opt, L.ptr(self.label_in),
+                                        L.ptr(self.phi), L.ptr(self.f), L.ptr(ws), nb.value,
+                                        ctypes.byref(plan), L.stream_ptr())
         L.check("fs_pcg_plan_create", st)
         return plan, ws
 

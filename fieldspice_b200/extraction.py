@@ -71,7 +71,7 @@ def resistance_matrix(grid, sigma_cell: np.ndarray, terminals: Sequence,
     Y, _, info = extract_capacitance(op, term_dev, empty, empty, tol=float(cfg.tol),
                                      precision=gcfg.precision, maxiter=gcfg.maxiter,
                                      preconditioner=resolve_preconditioner(cfg, gcfg),
-                                     coarsening=gcfg.coarsening)
+                                     coarsening=gcfg.coarsening, mg_params=gcfg.mg_params)
     if info["n_pinned"]:
         warnings.warn(
             f"{info['n_pinned']} unknown(s) are coupled to nothing (empty rows); "

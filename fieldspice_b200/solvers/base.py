@@ -83,12 +83,18 @@ class GPUConfig:
         robust when conductors sit in insulators, e.g. copper in oxide at a
         1e6 conductance ratio) or ``"auto"`` (default): galerkin when the
         operator's edge masses span more than three orders of magnitude.
+    mg_params
+        Multigrid and stencil options of the plans this solver creates, as a
+        dict of ``fs_mg_params`` fields (``smooth_deg``, ``smooth_lo``,
+        ``coarse_deg``, ``coarse_lo``, ``coarsest_nodes``, ``stencil_kind``);
+        None: the library defaults.  Each plan keeps its own copy.
     """
     precision: str = "auto"
     preconditioner: str | None = None
     maxiter: int | None = None
     learned: object | None = None
     coarsening: str = "auto"
+    mg_params: dict | None = None
 
 
 def resolve_preconditioner(cfg, gpu) -> str:

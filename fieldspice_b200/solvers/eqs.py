@@ -185,7 +185,8 @@ class EQSSolver:
         system = EliminatedSystem(op, label, 1, precision=self.gpu.precision,
                                   with_source=rhs_dev is not None,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                                  coarsening=self.gpu.coarsening)
+                                  coarsening=self.gpu.coarsening,
+                                  mg_params=self.gpu.mg_params)
         if fixed.size:
             system.phi[h2d(fixed.astype(np.int64), torch.int64, dev)] = \
                 h2d(vals, torch.float64, dev)
@@ -268,7 +269,8 @@ class EQSSolver:
         system = EliminatedSystem(K, label, 1, precision=self.gpu.precision,
                                   with_source=True,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                                  coarsening=self.gpu.coarsening)
+                                  coarsening=self.gpu.coarsening,
+                                  mg_params=self.gpu.mg_params)
         system.phi.copy_(h2d(phi0, torch.float64, dev))
         prev = system.phi.clone()
 

@@ -291,7 +291,8 @@ class PoissonSolver:
             precision=self.gpu.precision, maxiter=self.gpu.maxiter,
             preconditioner=resolve_preconditioner(self.cfg, self.gpu),
             learned=None if mask else self.gpu.learned, charges=charges,
-            coarsening=self.gpu.coarsening)
+            coarsening=self.gpu.coarsening,
+            mg_params=self.gpu.mg_params)
         info["solve_time"] = time.perf_counter() - t_start
         rep = capacitance_report(C, q_shield, info, symmetrise)
         mark("report")
@@ -384,7 +385,8 @@ class PoissonSolver:
         system = EliminatedSystem(self.op, label, 1, precision=self.gpu.precision,
                                   with_source=with_src,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                                  coarsening=self.gpu.coarsening)
+                                  coarsening=self.gpu.coarsening,
+                                  mg_params=self.gpu.mg_params)
         system.phi.zero_()
         system.phi[fixed_d] = torch.as_tensor(vals, dtype=torch.float64, device=dev)
         if with_src:
@@ -479,7 +481,8 @@ class PoissonSolver:
         system = EliminatedSystem(self.op, label, len(chunks[0]), precision=self.gpu.precision,
                                   with_source=with_src,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
-                                  coarsening=self.gpu.coarsening)
+                                  coarsening=self.gpu.coarsening,
+                                  mg_params=self.gpu.mg_params)
         tol = float(self.cfg.tol)
         Q = np.zeros((nf, ncol))
         sols, stats_all = [], []
@@ -572,7 +575,8 @@ class PoissonSolver:
 def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
                         tol: float, precision: str = "auto",
                         maxiter: int | None = None, preconditioner: str = "jacobi",
-                        learned=None, charges=None, coarsening: str = "auto"):
+                        learned=None, charges=None, coarsening: str = "auto",
+                        mg_params: dict | None = None):
     """Device core of the extraction: inputs already in HBM.
 
     ``term_dev``: sorted unique int64 node tensors, one per terminal;
@@ -617,7 +621,7 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
             mark("labels")
             system = EliminatedSystem(op, label, kb, precision=precision,
                                       preconditioner=preconditioner, learned=learned,
-                                      coarsening=coarsening)
+                                      coarsening=coarsening, mg_params=mg_params)
             setup_time += system.setup_time
             mark("plan")
         system.nrhs = kb

@@ -152,7 +152,8 @@ class ThermalSolver:
         system = EliminatedSystem(op, label, 1, precision=self.gpu.precision, with_source=True,
                                   preconditioner=resolve_preconditioner(self.cfg, self.gpu),
                                   diag=h2d(diag, torch.float64, dev),
-                                  coarsening=self.gpu.coarsening)
+                                  coarsening=self.gpu.coarsening,
+                                  mg_params=self.gpu.mg_params)
         return system, fixed_d
 
     def _q(self, q_node) -> np.ndarray:

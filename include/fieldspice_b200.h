@@ -181,6 +181,36 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
                           const double* diag, int periodic, const uint8_t* label_in,
                           double* phi, const double* f, void* workspace,
                           size_t workspace_bytes, fs_pcg_plan** plan, void* stream);
+/* Multigrid and stencil options of one plan.  The plan copies them when it is
+ * created; the library keeps no process-wide setting (the stencil autotuner's
+ * table is a cache of measured choices per shape class, nothing else).
+ * smooth_deg, smooth_lo: Chebyshev smoothing degree (pre and post, 1..16)
+ * and the lower end of its interval [smooth_lo, 2] on the unit-diagonal level
+ * operators; coarse_deg, coarse_lo: the same on the coarsest level (1..64);
+ * coarsest_nodes: coarsening stops at or below this node count (>= 8);
+ * stencil_kind: the CG stencil (0..5, see fs_pcg_plan_stencil_kind) or -1
+ * (the FS_STENCIL environment variable, else autotuned).
+ * fs_mg_params_default fills 2, 0.3, 32, 0.03, 4096, -1.                   */
+typedef struct fs_mg_params {
+  int smooth_deg;
+  double smooth_lo;
+  int coarse_deg;
+  double coarse_lo;
+  long long coarsest_nodes;
+  int stencil_kind;
+} fs_mg_params;
+void fs_mg_params_default(fs_mg_params* params);
+/* fs_pcg_workspace_bytes and fs_pcg_plan_create_ex with options (NULL: the
+ * defaults); FS_BAD_ARG if an option is out of range.  The workspace size
+ * depends on coarsest_nodes (the number of levels).                        */
+int fs_pcg_workspace_bytes_opt(int nx, int ny, int nz, int nrhs, int precision,
+                               int precond, const fs_mg_params* opt, size_t* bytes);
+int fs_pcg_plan_create_opt(int nx, int ny, int nz, int nrhs, int precision, int precond,
+                           const double* mx, const double* my, const double* mz,
+                           const double* diag, int periodic, const fs_mg_params* opt,
+                           const uint8_t* label_in, double* phi, const double* f,
+                           void* workspace, size_t workspace_bytes, fs_pcg_plan** plan,
+                           void* stream);
 /* Solve in place into phi.  warm_start != 0 keeps the free-node values of
  * phi as the initial guess (the tolerance stays relative to ||b||, as in
  * SciPy); otherwise the guess is 0.  maxiter <= 0 caps the iterations at the
@@ -199,13 +229,6 @@ int fs_pcg_plan_solve(fs_pcg_plan* plan, int warm_start, double tol,
 int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
                        void* const* streams, int warm_start, double tol,
                        int maxiter, fs_rhs_stats* const* stats, int* status);
-/* Multigrid parameters for plans created after the call (process-wide):
- * Chebyshev smoothing degree (pre and post) and the lower end of its
- * interval [smooth_lo, 2] on the unit-diagonal level operators, the
- * coarsest level's degree and interval, and the node count at or below
- * which coarsening stops.  Defaults: 2, 0.3, 32, 0.03, 4096.               */
-int fs_mg_set_params(int smooth_deg, double smooth_lo, int coarse_deg,
-                     double coarse_lo, long long coarsest_nodes);
 /* Label array after classification (free / fixed / solo / pinned), device. */
 const uint8_t* fs_pcg_plan_labels(const fs_pcg_plan* plan);
 /* Number of kernel launches issued by the last solve (host count).          */

@@ -74,13 +74,31 @@ def test_workspace_sizes_and_bad_arguments(dll):
 
 
 def test_multigrid_parameters_are_validated(dll):
-    # host-only setter: checks its arguments, touches no device
-    assert dll.fs_mg_set_params(0, 0.3, 32, 0.03, 4096) == L.FS_BAD_ARG
-    assert dll.fs_mg_set_params(2, 2.0, 32, 0.03, 4096) == L.FS_BAD_ARG
-    assert dll.fs_mg_set_params(2, 0.3, 65, 0.03, 4096) == L.FS_BAD_ARG
-    assert dll.fs_mg_set_params(2, 0.3, 32, 0.0, 4096) == L.FS_BAD_ARG
-    assert dll.fs_mg_set_params(2, 0.3, 32, 0.03, 4) == L.FS_BAD_ARG
-    assert dll.fs_mg_set_params(2, 0.3, 32, 0.03, 4096) == L.FS_OK
+    # per-plan options: the sizing call checks them and touches no device
+    p = L.FsMgParams()
+    dll.fs_mg_params_default(ctypes.byref(p))
+    assert (p.smooth_deg, p.smooth_lo, p.coarse_deg, p.coarse_lo, p.coarsest_nodes,
+            p.stencil_kind) == (2, 0.3, 32, 0.03, 4096, -1)
+    nb = ctypes.c_size_t()
+    args = (64, 64, 32, 8, L.PRECISION_MIXED, L.PRECOND_MG)
+    assert dll.fs_pcg_workspace_bytes_opt(*args, ctypes.byref(p), ctypes.byref(nb)) == L.FS_OK
+    default = nb.value
+    assert dll.fs_pcg_workspace_bytes_opt(*args, None, ctypes.byref(nb)) == L.FS_OK
+    assert nb.value == default
+    for field, bad in [("smooth_deg", 0), ("smooth_lo", 2.0), ("coarse_deg", 65),
+                       ("coarse_lo", 0.0), ("coarsest_nodes", 4), ("stencil_kind", 6),
+                       ("stencil_kind", -2)]:
+        q = L.FsMgParams()
+        dll.fs_mg_params_default(ctypes.byref(q))
+        setattr(q, field, bad)
+        assert dll.fs_pcg_workspace_bytes_opt(*args, ctypes.byref(q),
+                                              ctypes.byref(nb)) == L.FS_BAD_ARG, field
+    # a deeper hierarchy (smaller coarsest level) needs more workspace
+    q = L.mg_params({"coarsest_nodes": 64})
+    assert dll.fs_pcg_workspace_bytes_opt(*args, ctypes.byref(q), ctypes.byref(nb)) == L.FS_OK
+    assert nb.value > default
+    with pytest.raises(ValueError, match="unknown"):
+        L.mg_params({"smoothing": 3})
 
 
 def test_library_is_sm100a_only():

@@ -86,28 +86,55 @@ def test_multigrid_cuts_iterations(cuda, golden):
     assert its["mg"] * 5 < its["jacobi"], its
 
 
-@pytest.mark.parametrize("params", [(3, 0.3, 24, 0.03, 512), (1, 0.5, 8, 0.05, 64)])
+@pytest.mark.parametrize("params", [(3, 0.3, 24, 0.03, 512, -1), (1, 0.5, 8, 0.05, 64, 0),
+                                    (2, 0.3, 32, 0.03, 4096, 2)])
 def test_multigrid_parameters(cuda, golden, params):
     """Non-default smoothing degrees (the plain Chebyshev pre-smoothing path,
-    not the degree-2 residual form) and coarsest sizes give the same C."""
+    not the degree-2 residual form), coarsest sizes and stencil kinds, given
+    per solver, give the same C; a solver with the defaults created next to
+    it is not affected (no process-wide setting)."""
+    import ctypes
+
+    import torch
+
     from fieldspice_b200 import _lib as L
     from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.device import DeviceOperator, EliminatedSystem
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig
     from fieldspice_b200.solvers.poisson import PoissonSolver
     d = golden("layered_48x48x24_s1")
     g, terms = _layered(d)
-    L.check("fs_mg_set_params", L.lib().fs_mg_set_params(*params))
-    try:
-        ps = PoissonSolver(g, d["eps_cell"], SolverConfig(tol=1e-10),
-                           gpu=GPUConfig(preconditioner="mg"))
-        rep = {}
-        C = ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)), report=rep)
-    finally:
-        L.check("fs_mg_set_params", L.lib().fs_mg_set_params(2, 0.3, 32, 0.03, 4096))
+    names = ("smooth_deg", "smooth_lo", "coarse_deg", "coarse_lo", "coarsest_nodes",
+             "stencil_kind")
+    opts = dict(zip(names, params))
+    ps = PoissonSolver(g, d["eps_cell"], SolverConfig(tol=1e-10),
+                       gpu=GPUConfig(preconditioner="mg", mg_params=opts))
+    rep = {}
+    C = ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)), report=rep)
     scale = np.abs(np.diag(d["C"])).max()
     assert np.abs(C - d["C"]).max() / scale <= 1e-9
     assert max(rep["linear"]["relres_fp64"]) < 1e-10
     assert max(rep["linear"]["iterations"]) < 100
+    # two live plans, one with the options and one without: each keeps its own
+    op = DeviceOperator(g, d["eps_cell"])
+    label = torch.zeros(op.N, dtype=torch.uint8, device=op.dev)
+    label[:g.shape_nodes[1] * g.shape_nodes[2]] = L.LABEL_FIXED
+    a = EliminatedSystem(op, label, 8, precision="mixed", preconditioner="mg",
+                         coarsening="geometric", mg_params=opts)
+    b = EliminatedSystem(op, label, 8, precision="mixed", preconditioner="mg",
+                         coarsening="geometric")
+    coarsest = {}
+    for name, s in (("opt", a), ("default", b)):
+        n = ctypes.c_int()
+        dims = (ctypes.c_int * 48)()
+        L.check("levels", L.lib().fs_pcg_plan_levels(s.plan, ctypes.byref(n), dims))
+        coarsest[name] = int(np.prod(dims[3 * (n.value - 1):3 * n.value]))
+    assert coarsest["opt"] <= params[4]
+    assert coarsest["default"] == 864  # 48x48x24 -> 24x24x12 -> 12x12x6
+    if params[5] >= 0:
+        assert L.lib().fs_pcg_plan_stencil_kind(a.plan) in (params[5], 1)
+    a.close()
+    b.close()
 
 
 def test_many_terminals_and_padding(cuda):
