@@ -26,6 +26,7 @@ LABEL_FREE, LABEL_FIXED, LABEL_SOLO, LABEL_PINNED = range(4)
 DTYPE_F64, DTYPE_F32 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_MG, PRECOND_MG_AGG = 0, 1, 2
+PROP_STATS_WORKSPACE_BYTES = 16384  # FS_PROP_STATS_WORKSPACE_BYTES
 AVERAGE_PARALLEL, AVERAGE_HARMONIC = 0, 1
 
 
@@ -86,6 +87,8 @@ _SIGNATURES = {
     "fs_pcg_plan_create_ex": (c_int, [c_int] * 6 + [c_void_p] * 4 + [c_int] + [c_void_p] * 4
                               + [c_size_t, POINTER(c_void_p), c_void_p]),
     "fs_mg_params_default": (None, [POINTER(FsMgParams)]),
+    "fs_pcg_plan_solve_begin": (c_int, [c_void_p, c_int, c_double, c_int, c_void_p]),
+    "fs_pcg_plan_solve_poll": (c_int, [c_void_p, POINTER(FsRhsStats), POINTER(c_int)]),
     "fs_pcg_workspace_bytes_opt": (c_int, [c_int] * 6 + [POINTER(FsMgParams),
                                                          POINTER(c_size_t)]),
     "fs_pcg_plan_create_opt": (c_int, [c_int] * 6 + [c_void_p] * 4 + [c_int,
@@ -125,7 +128,8 @@ _SIGNATURES = {
                                      c_void_p]),
     "fs_pcg_plan_sync_unet": (c_int, [c_void_p, c_void_p]),
     "fs_selftest_wait_timeout": (c_int, [c_longlong, POINTER(c_int), c_void_p]),
-    "fs_prop_stats": (c_int, [c_void_p, c_longlong, POINTER(c_double), c_void_p]),
+    "fs_prop_stats": (c_int, [c_void_p, c_longlong, POINTER(c_double), c_void_p, c_size_t,
+                              c_void_p]),
     "fs_rhs_superpose": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double),
                                  c_void_p, c_void_p, c_longlong, c_void_p]),
     "fs_pcg_plan_precondition": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -182,6 +186,17 @@ def load_library(path=None) -> ctypes.CDLL:
     if path is None:
         _LIB = dll
     return dll
+
+
+def prop_stats(t) -> tuple[float, float, float]:
+    """``fs_prop_stats`` of an FP64 device tensor: (min, max, non-finite
+    count), with its workspace from the framework's caching allocator."""
+    import torch
+    ws = torch.empty(PROP_STATS_WORKSPACE_BYTES, dtype=torch.uint8, device=t.device)
+    stats = (ctypes.c_double * 3)()
+    check("fs_prop_stats", lib().fs_prop_stats(ptr(t), t.numel(), stats, ptr(ws),
+                                               PROP_STATS_WORKSPACE_BYTES, stream_ptr()))
+    return float(stats[0]), float(stats[1]), float(stats[2])
 
 
 def lib() -> ctypes.CDLL:

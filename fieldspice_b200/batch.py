@@ -4,10 +4,12 @@ The reference extracts one geometry per ``capacitance_matrix`` call
 (``fieldspice/extraction.py:41-56`` -> ``solvers/poisson.py:1100-1249``).
 :func:`capacitance_matrices` takes a batch of uneven geometries, builds one
 CG plan per geometry (all of its terminals as one block of right-hand sides)
-and hands every plan to ``fs_pcg_plans_solve``, which runs them together on a
-pool of CUDA streams: one graph chunk per unfinished geometry per round, so
-the iterations of small geometries overlap those of large ones.  Charges are
-integrated per geometry in FP64 exactly as in a single extraction.
+and runs them together on a pool of CUDA streams with the library's
+non-blocking solve (``fs_pcg_plan_solve_begin`` / ``fs_pcg_plan_solve_poll``):
+largest geometry first, each plan's next graph chunk enqueued as soon as its
+previous one has finished, and the host building the next plans while the GPU
+solves the ones already built.  Charges are integrated per geometry in FP64
+exactly as in a single extraction.
 
 With a process group of several ranks (one per GPU), the geometries are
 shared out by estimated cost (nodes x padded RHS, longest first onto the
@@ -31,6 +33,10 @@ from .solvers.poisson import (PoissonSolver, capacitance_report, check_terminals
                               raise_on_status, shield_nodes, upload_cell_property)
 
 __all__ = ["capacitance_matrices", "shard_by_cost", "problem_cost"]
+
+#: CG vectors at or above this size (bytes) make a new plan time the stencil
+#: kernels when it is created (the library's autotuner threshold).
+TUNE_MIN_BYTES = 32 << 20
 
 
 def problem_cost(problem) -> float:
@@ -148,39 +154,81 @@ def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
             reports[i] = rep
     if not batchable:
         return out
-    ex = {}
+    lib = L.lib()
+    tol = float(cfg.tol)
+    # Largest first (longest-processing-time order).  Plans whose CG vectors
+    # reach the stencil autotuner's 32 MB threshold (nodes x padded RHS x the
+    # element size) time kernels when they are created, so they are all built
+    # before any solve runs; after that each plan starts as soon as it is
+    # built and the host builds the next while the GPU solves.
+    order = sorted(batchable, key=lambda i: (-problem_cost(problems[i]), i))
+    es = 8 if gcfg.precision == "fp64" else 4
+    tuned = [i for i in order if problem_cost(problems[i]) * es >= TUNE_MIN_BYTES]
+    pool = [torch.cuda.Stream() for _ in range(max(1, min(streams, len(batchable))))]
+    ex: dict[int, _Extraction] = {}
+    running: dict[int, Any] = {}
+    started = 0
+
+    def build(i):
+        p = problems[i]
+        ex[i] = _Extraction(p[0], p[1], p[2], p[3] if len(p) > 3 else None, cfg, gcfg)
+
+    def start(i):
+        nonlocal started
+        s = pool[started % len(pool)]
+        started += 1
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream())  # set-up and excitation kernels
+        s.wait_event(ready)
+        stats = (L.FsRhsStats * ex[i].system.k)()
+        L.check("fs_pcg_plan_solve_begin", lib.fs_pcg_plan_solve_begin(
+            ex[i].system.plan, 0, tol, ex[i].maxiter, s.cuda_stream))
+        running[i] = stats
+
+    def finish(i, st, stats_arr):
+        e = ex[i]
+        stats = _stats_list(stats_arr, e.system.nrhs)
+        if st not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN, L.FS_STALLED):
+            L.check("fs_pcg_plan_solve_poll", st)
+        if e.system.preconditioner == "learned":
+            st, stats = e.system.finish_learned(st, stats, tol, e.maxiter)
+        _, stats = e.system.finish_auto(st, stats, tol, e.maxiter)
+        raise_on_status(stats, tol, "gpu-cg")
+        out[i], rep = e.collect(stats)
+        if reports is not None:
+            reports[i] = rep
+
+    def poll() -> bool:
+        progressed = False
+        done = ctypes.c_int()
+        for i in list(running):
+            stats_arr = running[i]
+            st = lib.fs_pcg_plan_solve_poll(ex[i].system.plan, stats_arr, ctypes.byref(done))
+            if done.value:
+                del running[i]
+                finish(i, st, stats_arr)
+                progressed = True
+            elif st != L.FS_OK:
+                del running[i]
+                L.check("fs_pcg_plan_solve_poll", st)
+        return progressed
+
     try:
-        for i in batchable:
-            p = problems[i]
-            ex[i] = _Extraction(p[0], p[1], p[2], p[3] if len(p) > 3 else None, cfg, gcfg)
-        torch.cuda.synchronize()  # plan set-up and excitations are on this stream
-        pool = [torch.cuda.Stream() for _ in range(max(1, min(streams, len(batchable))))]
-        n = len(batchable)
-        plans = (ctypes.c_void_p * n)(*[ex[i].system.plan.value for i in batchable])
-        strm = (ctypes.c_void_p * n)(*[pool[j % len(pool)].cuda_stream for j in range(n)])
-        stat_arrays = [(L.FsRhsStats * ex[i].system.k)() for i in batchable]
-        sp = (ctypes.POINTER(L.FsRhsStats) * n)(
-            *[ctypes.cast(a, ctypes.POINTER(L.FsRhsStats)) for a in stat_arrays])
-        status = (ctypes.c_int * n)()
-        tol = float(cfg.tol)
-        maxiter = max(ex[i].maxiter for i in batchable)
-        st = L.lib().fs_pcg_plans_solve(plans, n, strm, 0, tol, maxiter, sp, status)
-        if st == L.FS_CUDA_ERROR or st == L.FS_BAD_ARG:
-            L.check("fs_pcg_plans_solve", st)
-        for j, i in enumerate(batchable):
-            e = ex[i]
-            stats = _stats_list(stat_arrays[j], e.system.nrhs)
-            if status[j] not in (L.FS_OK, L.FS_NOT_CONVERGED, L.FS_NAN, L.FS_STALLED):
-                L.check("fs_pcg_plans_solve", status[j])
-            stj = status[j]
-            if e.system.preconditioner == "learned":
-                stj, stats = e.system.finish_learned(stj, stats, tol, e.maxiter)
-            _, stats = e.system.finish_auto(stj, stats, tol, e.maxiter)
-            raise_on_status(stats, tol, "gpu-cg")
-            out[i], rep = e.collect(stats)
-            if reports is not None:
-                reports[i] = rep
+        for i in tuned:
+            build(i)
+        for i in tuned:
+            start(i)
+        for i in order[len(tuned):]:
+            build(i)
+            start(i)
+            poll()
+        while running:
+            if not poll():
+                time.sleep(5e-5)
     finally:
+        # a failed batch may leave solves in flight: let them land before
+        # the plans and their buffers go
+        torch.cuda.synchronize()
         for e in ex.values():
             e.close()
     return out

@@ -189,9 +189,7 @@ class FieldRegion:
         if dt is not None:
             entry.K_hist = self.op_eps.combine(1.0 / dt, self.op_sig, 0.0)
         nE = len(self._elec)
-        stats = (ctypes.c_double * 3)()
-        L.check("fs_prop_stats", L.lib().fs_prop_stats(L.ptr(K.m), K.m.numel(), stats,
-                                                       L.stream_ptr()))
+        stats = L.prop_stats(K.m)
         if stats[0] == 0.0 and stats[1] == 0.0:
             # no coupling at all (e.g. sigma == 0 at dc): an open circuit
             entry.Y = np.zeros((nE, nE))

@@ -2681,6 +2681,13 @@ struct fs_pcg_plan {
   // Event samples around the kernels of the first iteration of every graph
   // launch: live per-kernel durations for the roofline figures.
   cudaEvent_t ev[8];
+  // fs_pcg_plan_solve_begin / _poll: the stream, the event after the last
+  // enqueued step, 0 idle / 1 a chunk in flight / 2 the finish in flight
+  cudaEvent_t ev_async = nullptr;
+  cudaStream_t async_s = nullptr;
+  int async_stage = 0;
+  int async_timed_out = 0;
+  long long async_chunks = 0, async_max_chunks = 0;
   double kernel_ms[6];
   int trace;               // record ev[6..7] around fine-level post-smoothing
   long long kernel_samples;
@@ -3971,9 +3978,8 @@ int solve_check(fs_pcg_plan* P) {
   return *P->h_flag ? 1 : 0;
 }
 
-// k_finalize, copy the per-RHS state back and fold it into a status.
-int solve_finish(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats,
-                 cudaStream_t s) {
+// k_finalize and the copy of the per-RHS state to the host, enqueued.
+int solve_finish_enqueue(fs_pcg_plan* P, cudaStream_t s) {
   cudaError_t e;
   dispatch(P, 4, s);
   FS_CHECK_LAUNCH("k_finalize");
@@ -3981,8 +3987,25 @@ int solve_finish(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats,
   if ((e = cudaMemcpyAsync(P->h_st, P->st, sizeof(RhsState) * P->nrhs,
                            cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return fs_cuda_status("cudaMemcpyAsync", e);
+  return FS_OK;
+}
+
+// The per-RHS state (on the host after solve_finish_enqueue's copy) folded
+// into stats and a status.
+int solve_finish_read(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats);
+
+// k_finalize, copy the per-RHS state back and fold it into a status.
+int solve_finish(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats,
+                 cudaStream_t s) {
+  cudaError_t e;
+  int st = solve_finish_enqueue(P, s);
+  if (st != FS_OK) return st;
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fs_cuda_status("cudaStreamSynchronize", e);
+  return solve_finish_read(P, timed_out, stats);
+}
+
+int solve_finish_read(fs_pcg_plan* P, int timed_out, fs_rhs_stats* stats) {
   int worst = FS_OK;
   for (int t = 0; t < P->nrhs; ++t) {
     const RhsState& h = P->h_st[t];
@@ -4081,6 +4104,65 @@ int fs_pcg_plans_solve(fs_pcg_plan* const* plans, int nplans,
   for (int i = 0; i < nplans; ++i)
     if (status[i] != FS_OK && (worst == FS_OK || status[i] == FS_CUDA_ERROR)) worst = status[i];
   return worst;
+}
+
+int fs_pcg_plan_solve_begin(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
+                            void* stream) {
+  if (!P || !(tol > 0.0) || P->async_stage != 0) return FS_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  if (!P->ev_async &&
+      (e = cudaEventCreateWithFlags(&P->ev_async, cudaEventDisableTiming)) != cudaSuccess)
+    return fs_cuda_status("cudaEventCreate", e);
+  int st = solve_begin(P, warm_start, tol, maxiter, s);
+  if (st != FS_OK) return st;
+  if ((st = solve_chunk(P, s)) != FS_OK) return st;
+  if ((e = cudaEventRecord(P->ev_async, s)) != cudaSuccess)
+    return fs_cuda_status("cudaEventRecord", e);
+  P->async_s = s;
+  P->async_chunks = 1;
+  P->async_max_chunks = host_maxiter(P, maxiter) / P->chunk + 4;
+  P->async_timed_out = 1;
+  P->async_stage = 1;
+  return FS_OK;
+}
+
+int fs_pcg_plan_solve_poll(fs_pcg_plan* P, fs_rhs_stats* stats, int* done) {
+  if (!P || !done || P->async_stage == 0) return FS_BAD_ARG;
+  *done = 0;
+  cudaError_t e = cudaEventQuery(P->ev_async);
+  if (e == cudaErrorNotReady) return FS_OK;
+  if (e != cudaSuccess) {
+    P->async_stage = 0;
+    return fs_cuda_status("cudaEventQuery", e);
+  }
+  int st;
+  if (P->async_stage == 1) {  // a chunk has finished: next chunk, or finish
+    if (solve_check(P)) {
+      P->async_timed_out = 0;
+    } else if (P->async_chunks < P->async_max_chunks) {
+      if ((st = solve_chunk(P, P->async_s)) != FS_OK) {
+        P->async_stage = 0;
+        return st;
+      }
+      ++P->async_chunks;
+      if ((e = cudaEventRecord(P->ev_async, P->async_s)) != cudaSuccess) {
+        P->async_stage = 0;
+        return fs_cuda_status("cudaEventRecord", e);
+      }
+      return FS_OK;
+    }
+    if ((st = solve_finish_enqueue(P, P->async_s)) != FS_OK ||
+        (e = cudaEventRecord(P->ev_async, P->async_s)) != cudaSuccess) {
+      P->async_stage = 0;
+      return st != FS_OK ? st : fs_cuda_status("cudaEventRecord", e);
+    }
+    P->async_stage = 2;
+    return FS_OK;
+  }
+  P->async_stage = 0;  // the finish has landed: the state is on the host
+  *done = 1;
+  return solve_finish_read(P, P->async_timed_out, stats);
 }
 
 }  // extern "C"
@@ -4286,6 +4368,7 @@ int fs_pcg_plan_destroy(fs_pcg_plan* P) {
   if (P->net) fs_unet_destroy(P->net);
   for (int t = 0; t < 8; ++t)
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
+  if (P->ev_async) cudaEventDestroy(P->ev_async);
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->cap) cudaStreamDestroy(P->cap);
   if (P->slot) host_slot_put(P->slot);

@@ -47,8 +47,6 @@ def upload_cell_property(a, grid, name: str):
     device: shape on the host, then one upload and one device reduction for
     non-finite entries, min and max.  Returns ``(host array, device tensor,
     min, max)``."""
-    import ctypes
-
     import torch
     arr = np.asarray(a, dtype=float)
     if arr.shape == ():
@@ -58,12 +56,10 @@ def upload_cell_property(a, grid, name: str):
                          f"got {arr.shape}")
     from ..device import device
     dev = h2d(arr, torch.float64, device())
-    stats = (ctypes.c_double * 3)()
-    L.check("fs_prop_stats", L.lib().fs_prop_stats(L.ptr(dev), dev.numel(), stats,
-                                                   L.stream_ptr()))
-    if stats[2] > 0:
+    lo, hi, bad = L.prop_stats(dev)
+    if bad > 0:
         raise ValueError(f"{name} contains non-finite values")
-    return arr, dev, float(stats[0]), float(stats[1])
+    return arr, dev, lo, hi
 
 
 def shield_nodes(wall_dev, term_dev, n_nodes: int):

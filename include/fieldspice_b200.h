@@ -181,6 +181,20 @@ int fs_pcg_plan_create_ex(int nx, int ny, int nz, int nrhs, int precision, int p
                           const double* diag, int periodic, const uint8_t* label_in,
                           double* phi, const double* f, void* workspace,
                           size_t workspace_bytes, fs_pcg_plan** plan, void* stream);
+/* The solve of fs_pcg_plan_solve without blocking the host: begin enqueues
+ * the initialisation and the first graph chunk on stream and returns; each
+ * poll returns at once.  While the plan runs, poll sets *done = 0 and, when
+ * the last enqueued step has completed, enqueues the next one (a chunk, or
+ * the finalisation once every RHS is done or the chunk cap is reached).
+ * When the finalisation has landed it sets *done = 1, fills stats (nrhs
+ * entries, or NULL) and returns what fs_pcg_plan_solve would.  Other
+ * returns with *done = 0 are errors (the plan is idle again).  A plan runs
+ * one solve at a time; it must not be destroyed or solved otherwise until
+ * poll has reported *done = 1.  Drives many plans from one host thread
+ * while it builds more of them (batched extraction).                       */
+int fs_pcg_plan_solve_begin(fs_pcg_plan* plan, int warm_start, double tol, int maxiter,
+                            void* stream);
+int fs_pcg_plan_solve_poll(fs_pcg_plan* plan, fs_rhs_stats* stats, int* done);
 /* Multigrid and stencil options of one plan.  The plan copies them when it is
  * created; the library keeps no process-wide setting (the stencil autotuner's
  * table is a cache of measured choices per shape class, nothing else).
@@ -407,8 +421,12 @@ int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* st
 
 
 /* min, max and the number of non-finite entries of an FP64 device array
- * (stats_host[3], host); the eager input checks of a cell property.        */
-int fs_prop_stats(const double* p, long long n, double* stats_host, void* stream);
+ * (stats_host[3], host); the eager input checks of a cell property.
+ * workspace: FS_PROP_STATS_WORKSPACE_BYTES of device memory, 16-byte
+ * aligned, free for the call (it returns after its stream is synchronised).  */
+#define FS_PROP_STATS_WORKSPACE_BYTES 16384
+int fs_prop_stats(const double* p, long long n, double* stats_host, void* workspace,
+                  size_t workspace_bytes, void* stream);
 
 /* ---- §8f: field region (fieldspice/circuit/coupling.py) ----------------------
  * out[i] = base[i] + sum_{c<ncols} coef_host[c] * phi[i*k + c0 + c] for

@@ -82,3 +82,60 @@ def test_batch64_matches_reference_at_scale(cuda):
         errs.append(float(np.abs(C - Cref).max() / np.abs(np.diag(Cref)).max()))
         assert max(rep["linear"]["relres_fp64"]) < 1e-10
     assert max(errs) <= 1e-9, (int(np.argmax(errs)), max(errs))
+
+
+def test_nonblocking_solve_equals_blocking_solve(cuda):
+    """fs_pcg_plan_solve_begin / _poll: the same iterates, stats and status
+    as fs_pcg_plan_solve on the same plan and inputs (bit-identical phi), with
+    poll returning at once while the plan runs; a second begin while one is
+    in flight and a poll of an idle plan are refused."""
+    import ctypes
+
+    import torch
+
+    from fieldspice_b200 import _lib as L
+    from fieldspice_b200.device import DeviceOperator, EliminatedSystem
+    ws, probs = _batch(1, seed=3)
+    grid, eps, terms, _ = probs[0]
+    op = DeviceOperator(grid, eps)
+    label = torch.zeros(op.N, dtype=torch.uint8, device=op.dev)
+    nid = np.arange(op.N).reshape(grid.shape_nodes)
+    label[torch.as_tensor(nid[:, :, 0].ravel(), device=op.dev)] = L.LABEL_FIXED
+    k = len(terms)
+    for t in terms:
+        label[torch.as_tensor(np.asarray(t.nodes), device=op.dev)] = L.LABEL_FIXED
+    system = EliminatedSystem(op, label, k, precision="mixed", preconditioner="mg")
+    phi0 = torch.zeros_like(system.phi)
+    view = phi0.view(op.N, system.k)
+    for c, t in enumerate(terms):
+        view[torch.as_tensor(np.asarray(t.nodes), device=op.dev), c] = 1.0
+    # (terminal columns past the last terminal stay 0: padded RHS)
+    lib = L.lib()
+    system.phi.copy_(phi0)
+    st_b = (L.FsRhsStats * system.k)()
+    s_blocking = lib.fs_pcg_plan_solve(system.plan, 0, 1e-10, 0, st_b, L.stream_ptr())
+    phi_b = system.phi.clone()
+    system.phi.copy_(phi0)
+    torch.cuda.synchronize()
+    done = ctypes.c_int()
+    assert lib.fs_pcg_plan_solve_poll(system.plan, None, ctypes.byref(done)) == L.FS_BAD_ARG
+    st_a = (L.FsRhsStats * system.k)()
+    L.check("begin", lib.fs_pcg_plan_solve_begin(system.plan, 0, 1e-10, 0, L.stream_ptr()))
+    assert lib.fs_pcg_plan_solve_begin(system.plan, 0, 1e-10, 0, L.stream_ptr()) == L.FS_BAD_ARG
+    polls = 0
+    while True:
+        s_async = lib.fs_pcg_plan_solve_poll(system.plan, st_a, ctypes.byref(done))
+        polls += 1
+        if done.value:
+            break
+        assert s_async == L.FS_OK
+        assert polls < 10_000_000
+    torch.cuda.synchronize()
+    assert s_async == s_blocking == L.FS_OK
+    assert polls > 2
+    for a, b in zip(st_a, st_b):
+        assert (a.iterations, a.status, a.reliable_updates) == (b.iterations, b.status,
+                                                               b.reliable_updates)
+        assert a.relres == b.relres
+    assert torch.equal(system.phi, phi_b)
+    system.close()
