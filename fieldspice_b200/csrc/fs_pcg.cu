@@ -1859,8 +1859,8 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
             o1[t] += c0 * fB[t] + cd * a[t];  // k_mg_post2: x + alpha r0 + beta A~r0
           }
           st16<T, W>(out1 + n * K + hf * W, o1);
-          if (rz_partials) {  // r~.z: b was read one plane ago (an L2 hit)
-            T bo2[W];
+          if (rz_partials) {  // r~.z: b was read one plane ago (an L2 hit; carrying
+            T bo2[W];          // it in registers spilled and was slower)
             ld16<T, W>(b + n * K + hf * W, bo2);
 #pragma unroll
             for (int t = 0; t < W; ++t) rzacc[t] += (double)bo2[t] * (double)o1[t];
@@ -1916,6 +1916,170 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
         rz_apply<K>(tot, st, ctl);
       }
     }
+  }
+}
+
+// ---- full-weighting restriction by x-march, fine planes staged by TMA ------------
+//   b_c(I) = s_c(I) * sum_f P(f, I) sd_f(f) r(f)
+// (k_mg_restrict's formula, trilinear weights per axis, the last fine node of
+// an even-length axis weighted 1 towards the last coarse node).  A CTA owns a
+// column of CZ x CY coarse nodes and marches its coarse planes I; the fine
+// planes 2I-1, 2I, 2I+1 stream through a ring as TMA boxes (the residual with
+// a one-node halo, 34 x 17 nodes, and sd from a 16-byte aligned start; out of
+// range reads zero, which is a zero contribution).  Each thread (one 16-byte
+// chunk of one coarse node) sums its 3 x 3 fine (y, z) neighbourhood per
+// plane and carries two coarse planes in registers: a fine plane 2I adds to I,
+// a plane 2I+1 adds to I and I+1, after which plane I is complete and stored.
+// The residual is read once from DRAM (k_mg_restrict's gather read each fine
+// node for up to 8 coarse threads from L1/L2); the sums run in another order,
+// so results agree with k_mg_restrict to FP rounding.
+template <typename T, int K>
+struct RestrictTile {
+  static constexpr int B = K * (int)sizeof(T);       // bytes per node
+  static constexpr int NCH = B / 16;                 // 16-byte chunks per node
+  static constexpr int W = 16 / (int)sizeof(T);      // values per chunk
+  static constexpr int CZ = 16, CY = 8;              // coarse nodes of a column tile
+  static constexpr int FZ = 2 * CZ + 2;              // residual box: z from 2*Z0 - 1
+  static constexpr int FY = 2 * CY + 1;              //               y from 2*Y0 - 1
+  static constexpr int ZP = 16 / (int)sizeof(T);     // sd box: z from 2*Z0 - ZP
+  static constexpr int SZ = 2 * CZ + 2 * ZP;
+  static constexpr int NS = 4;                       // fine planes in the ring
+  static constexpr int VBOX = FZ * FY * B;
+  static constexpr int SBOX = SZ * FY * (int)sizeof(T);
+  static constexpr int O_S = (VBOX + 127) / 128 * 128;
+  static constexpr int SLOT = O_S + (SBOX + 127) / 128 * 128;
+  static constexpr int O_BAR = NS * SLOT;
+  static constexpr size_t SMEM = (size_t)O_BAR + NS * 8 + 128;
+  static constexpr int THREADS = CZ * CY * (NCH > 0 ? NCH : 1);
+  static constexpr uint32_t TX = (uint32_t)(VBOX + SBOX);
+  static constexpr bool OK = (B == 16 || B == 32);
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(RestrictTile<T, K>::THREADS, 2)
+    k_mg_restrict_tma(Dims f, Dims c, const __grid_constant__ CUtensorMap tm_r,
+                      const __grid_constant__ CUtensorMap tm_sd, const T* __restrict__ sc,
+                      T* __restrict__ bc, const int* __restrict__ done,
+                      int* __restrict__ err) {
+  using R = RestrictTile<T, K>;
+  constexpr int W = R::W;
+  if (*done) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + R::O_BAR);
+  const int tid = threadIdx.x;
+  const int h = tid % R::NCH, v = tid / R::NCH;
+  const int cz = v % R::CZ, cy = v / R::CZ;
+  const int ncz = (c.nz + R::CZ - 1) / R::CZ, ncy = (c.ny + R::CY - 1) / R::CY;
+  int u = 0, u_end = 0;
+  fs::march_range<int>(c, ncz * ncy, u, u_end);
+  if (tid == 0) {
+    for (int s = 0; s < R::NS; ++s) fs::mbar_init(&bar[s], 1);
+    fs::fence_mbar_init();
+  }
+  __syncthreads();
+  int ticket = 0;
+  bool failed = false;
+  while (u < u_end && !failed) {
+    const int col = u / c.nx;
+    const int Ia = u - col * c.nx;
+    const int Ib = min(c.nx, Ia + (u_end - u));
+    const int by = col / ncz, bz = col - by * ncz;
+    const int Z0 = bz * R::CZ, Y0 = by * R::CY;
+    const int Kc = Z0 + cz, J = Y0 + cy;
+    const bool inb = Kc < c.nz && J < c.ny;
+    const int nin = 2 * (Ib - Ia) + 1;  // fine planes 2Ia-1 .. 2Ib-1
+    auto issue = [&](int j) {
+      const int s = (ticket + j) % R::NS;
+      unsigned char* slot = base + s * R::SLOT;
+      const int x = 2 * Ia - 1 + j;
+      fs::mbar_arrive_expect_tx(&bar[s], R::TX);
+      fs::tma_load_4d(slot, &tm_r, &bar[s], 0, 2 * Z0 - 1, 2 * Y0 - 1, x);
+      tma_load_3d(slot + R::O_S, &tm_sd, &bar[s], 2 * Z0 - R::ZP, 2 * Y0 - 1, x);
+    };
+    if (tid == 0)
+      for (int j = 0; j < R::NS && j < nin; ++j) issue(j);
+    // weight of the fine node 2I+1 towards I on each axis: 1/2, or 1 when I
+    // is the last coarse node (no I+1 to share it with)
+    const T wz1 = (Kc + 1 < c.nz) ? (T)0.5 : (T)1;
+    const T wy1 = (J + 1 < c.ny) ? (T)0.5 : (T)1;
+    T accI[W], accN[W];
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+      accI[t] = (T)0;
+      accN[t] = (T)0;
+    }
+    bool bad = false;
+    for (int j = 0; j < nin; ++j) {
+      const int tk = ticket + j;
+      const int s = tk % R::NS;
+      const int x = 2 * Ia - 1 + j;
+      bad |= !fs::mbar_wait_bounded(&bar[s], (uint32_t)((tk / R::NS) & 1), kWaitBudget);
+      T part[W];
+#pragma unroll
+      for (int t = 0; t < W; ++t) part[t] = (T)0;
+      if (inb && !bad) {
+        const T* vb = reinterpret_cast<const T*>(base + s * R::SLOT) + h * W;
+        const T* sdb = reinterpret_cast<const T*>(base + s * R::SLOT + R::O_S);
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+          const T wy = dy == 1 ? (T)1 : (dy == 0 ? (T)0.5 : wy1);
+          const int yi = 2 * cy + dy;
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) {
+            const T wz = dz == 1 ? (T)1 : (dz == 0 ? (T)0.5 : wz1);
+            const int zi = 2 * cz + dz;
+            const T w = (wy * wz) * sdb[yi * R::SZ + zi + R::ZP - 1];
+            if (w != (T)0) {
+              T val[W];
+              ld16<T, W>(vb + (yi * R::FZ + zi) * K, val);
+#pragma unroll
+              for (int t = 0; t < W; ++t) part[t] += w * val[t];
+            }
+          }
+        }
+      }
+      if ((x & 1) == 0) {  // x = 2I: weight 1 towards I
+#pragma unroll
+        for (int t = 0; t < W; ++t) accI[t] += part[t];
+      } else {  // x = 2I+1: towards I and I+1; plane I is then complete
+        const int I = (x - 1) >> 1;
+        const T wx1 = (I + 1 < c.nx) ? (T)0.5 : (T)1;
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+          accI[t] += wx1 * part[t];
+          accN[t] += (T)0.5 * part[t];
+        }
+        if (I >= Ia && inb && !bad) {
+          const long long n = ((long long)I * c.ny + J) * c.nz + Kc;
+          const T scale = sc[n];
+          T o[W];
+#pragma unroll
+          for (int t = 0; t < W; ++t) o[t] = scale != (T)0 ? accI[t] * scale : (T)0;
+          st16<T, W>(bc + n * K + h * W, o);
+        }
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+          accI[t] = accN[t];
+          accN[t] = (T)0;
+        }
+      }
+      // every thread is done with this plane's slot: it may refill
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0 && j + R::NS < nin) issue(j + R::NS);
+    }
+    ticket += nin;
+    u += (Ib - Ia);
+  }
+  if (failed) {
+    if (tid == 0) {
+      *err = 1;
+      for (int s = 0; s < R::NS; ++s) (void)fs::mbar_wait_bounded(&bar[s], 0, kWaitBudget / 8);
+    }
+    __syncthreads();
   }
 }
 
@@ -3146,6 +3310,8 @@ struct Impl {
     cudaFuncSetAttribute(fs::k_mg_coarse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fs::kCoarseSmemCap);
     pre_fused_setup();
+    for (int l = 0; l + 1 < P->nlev && !P->agg; ++l)  // kernel attributes before capture
+      (void)restrict_tma_ok(P->lev[l], P->lev[l + 1]);
     MgLevel& L0 = P->lev[0];
     L0.em[0] = P->ex;
     L0.em[1] = P->ey;
@@ -3385,6 +3551,79 @@ struct Impl {
       return true;
     }
   }
+  // k_mg_restrict_tma: resident CTAs per SM (0 = cannot run), per device.
+  static int& restrict_per_sm() {
+    static int v[fs::kMaxDevices] = {};
+    return v[fs::current_device_slot()];
+  }
+  // The TMA restriction from level L to C: 16- or 32-byte nodes, every axis
+  // halved, no wrap, sd rows whose stride is a multiple of 16 bytes;
+  // FS_MG_RESTRICT=plain keeps k_mg_restrict.
+  static bool restrict_tma_ok(const MgLevel& L, const MgLevel& C) {
+    using R = RestrictTile<T, K>;
+    if constexpr (!R::OK) {
+      return false;
+    } else {
+      const char* sel = getenv("FS_MG_RESTRICT");
+      if (sel && strcmp(sel, "plain") == 0) return false;
+      if (L.d.per || L.d.nx == C.d.nx || L.d.ny == C.d.ny || L.d.nz == C.d.nz) return false;
+      if (((long long)L.d.nz * (long long)sizeof(T)) % 16 != 0) return false;
+      if (restrict_per_sm() == 0) {
+        if (cudaFuncSetAttribute(k_mg_restrict_tma<T, K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)R::SMEM) != cudaSuccess)
+          return false;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_restrict_tma<T, K>,
+                                                          R::THREADS, R::SMEM) != cudaSuccess)
+          return false;
+        restrict_per_sm() = per_sm;
+      }
+      return restrict_per_sm() > 0;
+    }
+  }
+  // k_mg_restrict_tma from level L (residual `res`) into C.b; false if a
+  // tensor map cannot be made for these buffers (nothing launched).
+  static bool launch_restrict_tma(fs_pcg_plan* P, const MgLevel& L, MgLevel& C, const T* res,
+                                  cudaStream_t s) {
+    using R = RestrictTile<T, K>;
+    if constexpr (!R::OK) {
+      return false;
+    } else {
+      auto encode = encode_fn();
+      if (!encode) return false;
+      const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+      const cuuint64_t Bn = R::B, MB = sizeof(T);
+      CUtensorMap tr, tsd;
+      cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
+                            (cuuint64_t)L.d.nx};
+      cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
+      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)R::FZ, (cuuint32_t)R::FY, 1};
+      cuuint32_t es[4] = {1, 1, 1, 1};
+      if (encode(&tr, dt, 4, (void*)res, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+      cuuint64_t sdims[3] = {(cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
+      cuuint64_t sstr[2] = {MB * L.d.nz, MB * L.d.nz * L.d.ny};
+      cuuint32_t sbox[3] = {(cuuint32_t)R::SZ, (cuuint32_t)R::FY, 1};
+      if (encode(&tsd, dt, 3, (void*)L.sd, sdims, sstr, sbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long ncols = (long long)((C.d.nz + R::CZ - 1) / R::CZ) *
+                              ((C.d.ny + R::CY - 1) / R::CY);
+      Dims dc = C.d;
+      const int g = (int)fs::march_grid(&dc, ncols, (long long)sms * restrict_per_sm(), 0, 0);
+      k_mg_restrict_tma<T, K><<<g, R::THREADS, R::SMEM, s>>>(
+          L.d, dc, tr, tsd, (const T*)C.s, (T*)C.b, &P->ctl->all_done, &P->ctl->error);
+      return true;
+    }
+  }
   // Whether the finest post-smoothing runs as k_mg_smooth_split, which can
   // form r~.z in the same pass.
   static bool post_split(const MgLevel& L) {
@@ -3498,7 +3737,7 @@ struct Impl {
       if (P->agg)
         fs::k_agg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
             L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
-      else
+      else if (!(restrict_tma_ok(L, C) && launch_restrict_tma(P, L, C, rfine, s)))
         fs::k_mg_restrict<T, K><<<gc, fs::kBlock, 0, s>>>(
             L.d, C.d, rfine, (const T*)L.sd, (const T*)C.s, (T*)C.b, done);
     }
@@ -3927,10 +4166,12 @@ namespace {
 int solve_begin(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
                 cudaStream_t s) {
   // Mixed precision: refresh the residual after a 10x drop under Jacobi CG
-  // (hundreds of FP32 iterations per decade) and after a 1000x drop under
-  // multigrid (a decade every ~2 iterations, so little FP32 drift).
+  // (hundreds of FP32 iterations per decade) and after a 1e4 drop under
+  // multigrid (a decade every ~2 iterations, so little FP32 drift; measured
+  // at 256x256x128: 22 iterations with 1e-3 and 1e-4, one reliable update
+  // fewer and 0.96 ms less per extraction with 1e-4).
   const double delta = P->precision != FS_PRECISION_MIXED ? 0.0
-                       : (P->precond ? 1e-3 : 0.1);
+                       : (P->precond ? 1e-4 : 0.1);
   cudaError_t e;
   dispatch(P, 2, s, warm_start ? 1 : 0, tol, maxiter, delta);
   FS_CHECK_LAUNCH("k_init");

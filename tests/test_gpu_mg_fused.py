@@ -10,7 +10,10 @@ level's rows allow it (for 32-byte nodes with each node split over two threads,
 ``FS_MG_PRE=plain`` and ``FS_MG_POST=plain`` keep the two-kernel forms.  The arithmetic and its order are the same, so one V-cycle applied
 through ``fs_pcg_plan_precondition`` to the same vector agrees to round-off
 (the compilers of the two kernels may contract different products into
-FMAs).  The grid is ragged on purpose: y and z end inside a tile, x is odd,
+FMAs).  The restriction runs as a TMA-staged x-march (``k_mg_restrict_tma``)
+for 16- and 32-byte nodes; ``FS_MG_RESTRICT=plain`` keeps the gather kernel
+(``k_mg_restrict``), whose sums run in another order: the V-cycles agree to
+FP rounding.  The grid is ragged on purpose: y and z end inside a tile, x is odd,
 and two levels run fused while the coarser ones do not.
 """
 
@@ -54,7 +57,7 @@ def _vcycle(sys_, r):
 
 
 @pytest.mark.parametrize("split", ["1", "0"])
-@pytest.mark.parametrize("which", ["FS_MG_PRE", "FS_MG_POST"])
+@pytest.mark.parametrize("which", ["FS_MG_PRE", "FS_MG_POST", "FS_MG_RESTRICT"])
 @pytest.mark.parametrize("precision,nrhs", [("mixed", 8), ("mixed", 4), ("fp64", 4)])
 def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, which, split):
     """split "1": 32-byte nodes (8 FP32 / 4 FP64 RHS) run the two-threads-per-node
@@ -66,6 +69,7 @@ def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, 
     r = torch.randn(sys_.op.N * sys_.k, dtype=dt, device="cuda", generator=gen)
     monkeypatch.delenv("FS_MG_PRE", raising=False)
     monkeypatch.delenv("FS_MG_POST", raising=False)
+    monkeypatch.delenv("FS_MG_RESTRICT", raising=False)
     monkeypatch.setenv("FS_MG_SPLIT", split)
     z_fused = _vcycle(sys_, r)
     monkeypatch.setenv(which, "plain")
@@ -102,6 +106,7 @@ def test_fused_smoothing_extraction_iterations(cuda, golden, monkeypatch):
     C_f, it_f = run()
     monkeypatch.setenv("FS_MG_PRE", "plain")
     monkeypatch.setenv("FS_MG_POST", "plain")
+    monkeypatch.setenv("FS_MG_RESTRICT", "plain")
     C_p, it_p = run()
     scale = np.abs(np.diag(d["C"])).max()
     assert np.abs(C_f - d["C"]).max() / scale <= 1e-9
