@@ -3310,8 +3310,9 @@ struct Impl {
     cudaFuncSetAttribute(fs::k_mg_coarse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fs::kCoarseSmemCap);
     pre_fused_setup();
-    for (int l = 0; l + 1 < P->nlev && !P->agg; ++l)  // kernel attributes before capture
+    for (int l = 0; l + 1 < P->nlev && !P->agg; ++l) {  // kernel attributes before capture
       (void)restrict_tma_ok(P->lev[l], P->lev[l + 1]);
+    }
     MgLevel& L0 = P->lev[0];
     L0.em[0] = P->ex;
     L0.em[1] = P->ey;
