@@ -40,7 +40,8 @@ class FsMgParams(ctypes.Structure):
     """``fs_mg_params``: multigrid and stencil options of one plan."""
     _fields_ = [("smooth_deg", c_int32), ("smooth_lo", c_double),
                 ("coarse_deg", c_int32), ("coarse_lo", c_double),
-                ("coarsest_nodes", c_longlong), ("stencil_kind", c_int32)]
+                ("coarsest_nodes", c_longlong), ("stencil_kind", c_int32),
+                ("agg_alpha", c_double)]
 
 
 def mg_params(opts: dict | None):

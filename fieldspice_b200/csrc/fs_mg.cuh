@@ -718,12 +718,17 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// x_f(i) += sd_f(i) * s_c(I) * x_c(I), I the aggregate of fine node i (one
-// thread per fine node: coalesced fine accesses, coarse values from cache).
+// x_f(i) += alpha * sd_f(i) * s_c(I) * x_c(I), I the aggregate of fine node i
+// (one thread per fine node: coalesced fine accesses, coarse values from
+// cache).  alpha over-corrects: the piecewise-constant coarse space of
+// unsmoothed aggregation captures the error's coarse component with too little
+// energy, and a fixed factor in (1, 2) restores most of what smoothed
+// transfers would (the V-cycle stays symmetric, and positive definite for
+// alpha < 2).
 template <typename T, int K>
 __global__ void __launch_bounds__(kBlock)
     k_agg_prolong(Dims f, Dims c, const T* __restrict__ xc, const T* __restrict__ sc,
-                  const T* __restrict__ sdf, T* __restrict__ xf,
+                  const T* __restrict__ sdf, T* __restrict__ xf, T alpha,
                   const int* __restrict__ done) {
   if (*done) return;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < f.N;
@@ -734,7 +739,7 @@ __global__ void __launch_bounds__(kBlock)
     node_ijk(f, n, i, j, k);
     const int rx = ratio(f.nx, c.nx), ry = ratio(f.ny, c.ny), rz = ratio(f.nz, c.nz);
     const long long cn = ((long long)(i / rx) * c.ny + j / ry) * c.nz + k / rz;
-    const T w = sf * __ldg(sc + cn);
+    const T w = sf * __ldg(sc + cn) * alpha;
     T v[K], xv[K];
     ldv_ro<T, K>(xc, cn, v);
     ldv<T, K>(xf, n, xv);

@@ -2619,17 +2619,23 @@ size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 // ---- multigrid hierarchy ---------------------------------------------------------
 constexpr int kMaxLevels = 12;
 // Multigrid and stencil options of one plan (fs_mg_params, copied at
-// creation; nothing process-wide).  Defaults from a sweep on the
+// creation; nothing process-wide).  Defaults from sweeps on the
 // 256x256x128 8-terminal extraction: degree-2 smoothing on [0.3, 2] and a
-// degree-32 Chebyshev solve on a coarsest level of at most 4096 nodes gave
-// the shortest extraction (20-21 iterations).
+// degree-32 Chebyshev solve on [0.06, 2] on a coarsest level of at most 4096
+// nodes (21 iterations, 39.4 ms; [0.03, 2]: 22 iterations, 41.0 ms; degree 16
+// or 24, [0.1, 2], 512 or 32768 coarsest nodes, smoothing on [0.25, 2] or
+// [0.35, 2]: no faster).
 struct MgParams {
   int smooth_deg = 2;          // Chebyshev degree, pre and post
   double smooth_lo = 0.3;      // smoothing interval [lo, 2] of A~
   int coarse_deg = 32;         // coarsest-level Chebyshev degree
-  double coarse_lo = 0.03;
+  double coarse_lo = 0.06;
   long long coarsest_nodes = 4096;
   int stencil_kind = -1;       // CG stencil 0..5; -1: FS_STENCIL, else autotuned
+  // over-correction of the aggregation hierarchy's coarse corrections:
+  // measured on the copper/oxide EQS step at 192x192x96, 119 iterations at 1,
+  // 71 at 1.4, 67 at 1.7, 72 at 2.0 (early transient steps, FP64, 1e-10)
+  double agg_alpha = 1.7;
 };
 
 // Options from the caller's struct (NULL: defaults); false if out of range.
@@ -2639,7 +2645,8 @@ bool mg_params_from(const fs_mg_params* o, MgParams* out) {
     if (o->smooth_deg < 1 || o->smooth_deg > 16 || o->coarse_deg < 1 || o->coarse_deg > 64 ||
         !(o->smooth_lo > 0.0 && o->smooth_lo < 2.0) ||
         !(o->coarse_lo > 0.0 && o->coarse_lo < 2.0) || o->coarsest_nodes < 8 ||
-        o->stencil_kind < -1 || o->stencil_kind > 5)
+        o->stencil_kind < -1 || o->stencil_kind > 5 ||
+        !(o->agg_alpha > 0.0 && o->agg_alpha < 2.0))
       return false;
     m.smooth_deg = o->smooth_deg;
     m.smooth_lo = o->smooth_lo;
@@ -2647,6 +2654,7 @@ bool mg_params_from(const fs_mg_params* o, MgParams* out) {
     m.coarse_lo = o->coarse_lo;
     m.coarsest_nodes = o->coarsest_nodes;
     m.stencil_kind = o->stencil_kind;
+    m.agg_alpha = o->agg_alpha;
   }
   *out = m;
   return true;
@@ -3748,7 +3756,8 @@ struct Impl {
       if (P->agg) {
         const int gp = fs_grid_blocks((const void*)fs::k_agg_prolong<T, K>, L.d.N);
         fs::k_agg_prolong<T, K><<<gp, fs::kBlock, 0, s>>>(
-            L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd, (T*)L.x[cur], done);
+            L.d, C.d, (const T*)C.x[cc], (const T*)C.s, (const T*)L.sd, (T*)L.x[cur],
+            (T)P->mg.agg_alpha, done);
       } else {
         const int gp = fs_grid_blocks((const void*)fs::k_mg_prolong_cell<T, K>, C.d.N);
         fs::k_mg_prolong_cell<T, K><<<gp, fs::kBlock, 0, s>>>(
@@ -3952,6 +3961,7 @@ void fs_mg_params_default(fs_mg_params* p) {
   p->coarse_lo = m.coarse_lo;
   p->coarsest_nodes = m.coarsest_nodes;
   p->stencil_kind = m.stencil_kind;
+  p->agg_alpha = m.agg_alpha;
 }
 
 int fs_pcg_workspace_bytes_opt(int nx, int ny, int nz, int nrhs, int precision,

@@ -86,8 +86,9 @@ class GPUConfig:
     mg_params
         Multigrid and stencil options of the plans this solver creates, as a
         dict of ``fs_mg_params`` fields (``smooth_deg``, ``smooth_lo``,
-        ``coarse_deg``, ``coarse_lo``, ``coarsest_nodes``, ``stencil_kind``);
-        None: the library defaults.  Each plan keeps its own copy.
+        ``coarse_deg``, ``coarse_lo``, ``coarsest_nodes``, ``stencil_kind``,
+        ``agg_alpha``); None: the library defaults.  Each plan keeps its own
+        copy.
     """
     precision: str = "auto"
     preconditioner: str | None = None

@@ -203,8 +203,10 @@ int fs_pcg_plan_solve_poll(fs_pcg_plan* plan, fs_rhs_stats* stats, int* done);
  * operators; coarse_deg, coarse_lo: the same on the coarsest level (1..64);
  * coarsest_nodes: coarsening stops at or below this node count (>= 8);
  * stencil_kind: the CG stencil (0..5, see fs_pcg_plan_stencil_kind) or -1
- * (the FS_STENCIL environment variable, else autotuned).
- * fs_mg_params_default fills 2, 0.3, 32, 0.03, 4096, -1.                   */
+ * (the FS_STENCIL environment variable, else autotuned); agg_alpha: the
+ * factor (0 < agg_alpha < 2) on every coarse correction of the aggregation
+ * hierarchy (FS_PRECOND_MG_AGG; over-correction for its piecewise-constant
+ * prolongation).  fs_mg_params_default fills 2, 0.3, 32, 0.06, 4096, -1, 1.7. */
 typedef struct fs_mg_params {
   int smooth_deg;
   double smooth_lo;
@@ -212,6 +214,7 @@ typedef struct fs_mg_params {
   double coarse_lo;
   long long coarsest_nodes;
   int stencil_kind;
+  double agg_alpha;
 } fs_mg_params;
 void fs_mg_params_default(fs_mg_params* params);
 /* fs_pcg_workspace_bytes and fs_pcg_plan_create_ex with options (NULL: the

@@ -78,7 +78,7 @@ def test_multigrid_parameters_are_validated(dll):
     p = L.FsMgParams()
     dll.fs_mg_params_default(ctypes.byref(p))
     assert (p.smooth_deg, p.smooth_lo, p.coarse_deg, p.coarse_lo, p.coarsest_nodes,
-            p.stencil_kind) == (2, 0.3, 32, 0.03, 4096, -1)
+            p.stencil_kind, p.agg_alpha) == (2, 0.3, 32, 0.06, 4096, -1, 1.7)
     nb = ctypes.c_size_t()
     args = (64, 64, 32, 8, L.PRECISION_MIXED, L.PRECOND_MG)
     assert dll.fs_pcg_workspace_bytes_opt(*args, ctypes.byref(p), ctypes.byref(nb)) == L.FS_OK
@@ -87,7 +87,7 @@ def test_multigrid_parameters_are_validated(dll):
     assert nb.value == default
     for field, bad in [("smooth_deg", 0), ("smooth_lo", 2.0), ("coarse_deg", 65),
                        ("coarse_lo", 0.0), ("coarsest_nodes", 4), ("stencil_kind", 6),
-                       ("stencil_kind", -2)]:
+                       ("stencil_kind", -2), ("agg_alpha", 0.0), ("agg_alpha", 2.0)]:
         q = L.FsMgParams()
         dll.fs_mg_params_default(ctypes.byref(q))
         setattr(q, field, bad)
