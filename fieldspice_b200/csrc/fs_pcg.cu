@@ -1178,9 +1178,23 @@ struct SmoothTile {
   static constexpr int THREADS = TZ * TY;
   static constexpr int NHALO = 2 * RZ + 2 * (RY - 2);
   static constexpr size_t SMEM = (size_t)O_BAR + NS * 8 + 128;
-  // 16..32-byte nodes: TMA rows of at least 16 bytes, two CTAs per SM
-  static constexpr bool OK = B >= 16 && B <= 32 && NHALO <= THREADS;
+  // 8..32-byte nodes, two CTAs per SM.  16- and 32-byte nodes are staged by a
+  // 4-D map {K, z, y, x}; 8-byte nodes (one FP64 RHS, two FP32) by a 3-D map
+  // whose innermost dimension merges K and z (rows of IZ*K values from
+  // (z0 - 2)*K, 16-byte aligned because z0 is a multiple of 32).
+  static constexpr bool OK = B >= 8 && B <= 32 && B % 8 == 0 && NHALO <= THREADS;
+  static constexpr bool MERGED = B < 16;
 };
+
+// The vector tile of plane x for a fused smoothing pass (see SmoothTile).
+template <typename T, int K>
+__device__ __forceinline__ void smooth_tile_load(void* slot, const CUtensorMap* map,
+                                                 uint64_t* bar, int z0, int y0, int x) {
+  if constexpr (SmoothTile<T, K>::MERGED)
+    tma_load_3d(slot, map, bar, (z0 - 2) * K, y0 - 2, x);
+  else
+    fs::tma_load_4d(slot, map, bar, 0, z0 - 2, y0 - 2, x);
+}
 
 template <typename T, int K>
 __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
@@ -1233,7 +1247,7 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
       unsigned char* slot = base + s * C::SLOT;
       const int x = xa - 2 + j;
       fs::mbar_arrive_expect_tx(&bar[s], C::TX);
-      fs::tma_load_4d(slot, &tm_b, &bar[s], 0, z0 - 2, y0 - 2, x);
+      smooth_tile_load<T, K>(slot, &tm_b, &bar[s], z0, y0, x);
       tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
@@ -1435,7 +1449,7 @@ __global__ void __launch_bounds__(SmoothTile<T, K>::THREADS, 2)
       unsigned char* slot = base + s * C::SLOT;
       const int x = xa - 2 + j;
       fs::mbar_arrive_expect_tx(&bar[s], C::TX);
-      fs::tma_load_4d(slot, &tm_x, &bar[s], 0, z0 - 2, y0 - 2, x);
+      smooth_tile_load<T, K>(slot, &tm_x, &bar[s], z0, y0, x);
       tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
@@ -1705,7 +1719,7 @@ __global__ void __launch_bounds__(SplitTile<T, K>::THREADS, 2)
       unsigned char* slot = base + s * C::SLOT;
       const int x = xa - 2 + j;
       fs::mbar_arrive_expect_tx(&bar[s], C::TX);
-      fs::tma_load_4d(slot, &tm_s, &bar[s], 0, z0 - 2, y0 - 2, x);
+      smooth_tile_load<T, K>(slot, &tm_s, &bar[s], z0, y0, x);
       tma_load_3d(slot + C::O_M0, &tm_ex, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + C::MBOXP, &tm_ey, &bar[s], z0 - C::ZP, y0 - 2, x);
       tma_load_3d(slot + C::O_M0 + 2 * C::MBOXP, &tm_ez, &bar[s], z0 - C::ZP, y0 - 2, x);
@@ -3418,6 +3432,7 @@ struct Impl {
       if (sel && strcmp(sel, "plain") == 0) return false;
       if ((post ? post_per_sm() : pre_per_sm()) <= 0) return false;
       if (((long long)L.d.nz * (long long)sizeof(T)) % 16 != 0) return false;  // mass rows
+      if (((long long)L.d.nz * CP::B) % 16 != 0) return false;  // merged vector rows
       const long long cols = (long long)((L.d.nz + CP::TZ - 1) / CP::TZ) *
                              ((L.d.ny + CP::TY - 1) / CP::TY) * L.d.nx;
       return cols < (1LL << 30);
@@ -3498,15 +3513,26 @@ struct Impl {
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     const cuuint64_t Bn = CP::B, MB = sizeof(T);
-    cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
-                          (cuuint64_t)L.d.nx};
-    cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
-    cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)CP::IZ, (cuuint32_t)CP::IY, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
-    if (encode(tv, dt, 4, (void*)src, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return false;
+    if constexpr (CP::MERGED) {
+      // rows of nz*K values; boxes of IZ*K values from (z0 - 2)*K
+      cuuint64_t dims[3] = {(cuuint64_t)L.d.nz * K, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
+      cuuint64_t strides[2] = {Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
+      cuuint32_t box[3] = {(cuuint32_t)(CP::IZ * K), (cuuint32_t)CP::IY, 1};
+      if (encode(tv, dt, 3, (void*)src, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    } else {
+      cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny,
+                            (cuuint64_t)L.d.nx};
+      cuuint64_t strides[3] = {Bn, Bn * L.d.nz, Bn * L.d.nz * L.d.ny};
+      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)CP::IZ, (cuuint32_t)CP::IY, 1};
+      if (encode(tv, dt, 4, (void*)src, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    }
     cuuint64_t mdims[3] = {(cuuint64_t)L.d.nz, (cuuint64_t)L.d.ny, (cuuint64_t)L.d.nx};
     cuuint64_t mstr[2] = {MB * L.d.nz, MB * L.d.nz * L.d.ny};
     cuuint32_t mbox[3] = {(cuuint32_t)CP::WZ, (cuuint32_t)CP::WY, 1};

@@ -13,7 +13,8 @@ through ``fs_pcg_plan_precondition`` to the same vector agrees to round-off
 FMAs).  The restriction runs as a TMA-staged x-march (``k_mg_restrict_tma``)
 for 16- and 32-byte nodes; ``FS_MG_RESTRICT=plain`` keeps the gather kernel
 (``k_mg_restrict``), whose sums run in another order: the V-cycles agree to
-FP rounding.  The grid is ragged on purpose: y and z end inside a tile, x is odd,
+FP rounding.  8-byte nodes (one FP64 RHS, two FP32) are staged through a
+3-D tensor map whose rows merge the RHS and z.  The grid is ragged on purpose: y and z end inside a tile, x is odd,
 and two levels run fused while the coarser ones do not.
 """
 
@@ -58,7 +59,8 @@ def _vcycle(sys_, r):
 
 @pytest.mark.parametrize("split", ["1", "0"])
 @pytest.mark.parametrize("which", ["FS_MG_PRE", "FS_MG_POST", "FS_MG_RESTRICT"])
-@pytest.mark.parametrize("precision,nrhs", [("mixed", 8), ("mixed", 4), ("fp64", 4)])
+@pytest.mark.parametrize("precision,nrhs", [("mixed", 8), ("mixed", 4), ("fp64", 4),
+                                            ("fp64", 1), ("mixed", 2)])
 def test_fused_smoothing_equals_two_kernels(cuda, monkeypatch, precision, nrhs, which, split):
     """split "1": 32-byte nodes (8 FP32 / 4 FP64 RHS) run the two-threads-per-node
     pass (k_mg_smooth_split); "0" keeps one thread per node."""
