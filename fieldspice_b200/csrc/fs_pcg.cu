@@ -626,12 +626,14 @@ __global__ void __launch_bounds__(TmaTile<T, K>::THREADS)
 // Out-of-range boxes read zero, which is exactly the missing edge at a wall,
 // so the inner loop has no global loads and no boundary branches.  Smaller
 // tiles (TY = 8) keep three CTAs per SM with two planes in flight each.
-template <typename T, int K>
+// TYO > 0 overrides the tile height (the tile shapes the stencil autotuner
+// tries for the fused direction-update stencil).
+template <typename T, int K, int TYO = 0>
 struct TmaTileM {
   static constexpr int B = K * (int)sizeof(T);
   static constexpr int MB = (int)sizeof(T);
   static constexpr int TZ = 32;
-  static constexpr int TY = B <= 32 ? 8 : 4;
+  static constexpr int TY = TYO > 0 ? TYO : (B <= 32 ? 8 : 4);
   static constexpr int NS = 5;
   static constexpr int ZP = 16 / MB;
   static constexpr int HY = TY + 2, HZ = TZ + 2;
@@ -797,9 +799,9 @@ __global__ void __launch_bounds__(TmaTileM<T, K>::THREADS, (TmaTileM<T, K>::B <=
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 
-template <typename T, int K>
+template <typename T, int K, int TYO = 0>
 struct TmaTilePZ {
-  using M = TmaTileM<T, K>;
+  using M = TmaTileM<T, K, TYO>;
   static constexpr int B = M::B, MB = M::MB, TZ = M::TZ, TY = M::TY, HY = M::HY,
                        HZ = M::HZ, ZP = M::ZP;
   static constexpr int NS = 4;
@@ -816,8 +818,9 @@ struct TmaTilePZ {
   static constexpr bool OK = M::OK;
 };
 
-template <typename T, int K>
-__global__ void __launch_bounds__(TmaTilePZ<T, K>::THREADS, 2)
+template <typename T, int K, int TYO = 0>
+__global__ void __launch_bounds__(TmaTilePZ<T, K, TYO>::THREADS,
+                                  TmaTilePZ<T, K, TYO>::THREADS >= 512 ? 1 : 2)
     k_stencil_pz(Dims d, const __grid_constant__ CUtensorMap tm_z,
                  const __grid_constant__ CUtensorMap tm_pold,
                  const __grid_constant__ CUtensorMap tm_ex,
@@ -825,7 +828,7 @@ __global__ void __launch_bounds__(TmaTilePZ<T, K>::THREADS, 2)
                  const __grid_constant__ CUtensorMap tm_ez, T* __restrict__ pnew,
                  T* __restrict__ q, double* __restrict__ partials, RhsState* st,
                  Control* ctl) {
-  using C = TmaTilePZ<T, K>;
+  using C = TmaTilePZ<T, K, TYO>;
   if (ctl->all_done) return;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -956,7 +959,7 @@ __global__ void __launch_bounds__(TmaTilePZ<T, K>::THREADS, 2)
     __syncthreads();
   }
   unrotate<T, K>(acc, rot);
-  finish_pq<T, K, TmaTilePZ<T, K>::THREADS>(acc, partials, st, ctl);
+  finish_pq<T, K, TmaTilePZ<T, K, TYO>::THREADS>(acc, partials, st, ctl);
 }
 
 // ---- K1 variant: q written through shared memory by TMA stores -------------------
@@ -2659,7 +2662,7 @@ bool mg_params_from(const fs_mg_params* o, MgParams* out) {
     if (o->smooth_deg < 1 || o->smooth_deg > 16 || o->coarse_deg < 1 || o->coarse_deg > 64 ||
         !(o->smooth_lo > 0.0 && o->smooth_lo < 2.0) ||
         !(o->coarse_lo > 0.0 && o->coarse_lo < 2.0) || o->coarsest_nodes < 8 ||
-        o->stencil_kind < -1 || o->stencil_kind > 5 ||
+        o->stencil_kind < -1 || o->stencil_kind > 7 ||
         !(o->agg_alpha > 0.0 && o->agg_alpha < 2.0))
       return false;
     m.smooth_deg = o->smooth_deg;
@@ -2856,7 +2859,7 @@ struct fs_pcg_plan {
   int stencil_kind;        // 0: cached loads, 1: TMA p, 2: TMA p + masses,
                            // 3: as 2 with q written by TMA stores
   int autotune = 0;        // time kinds 2, 3, 0, 4, 5 at creation and keep the fastest
-  float tune_ms[6] = {-1.f, -1.f, -1.f, -1.f, -1.f, -1.f};  // ms per launch by kind (-1: untimed)
+  float tune_ms[8] = {-1.f, -1.f, -1.f, -1.f, -1.f, -1.f, -1.f, -1.f};  // ms by kind (-1: untimed)
   int chunk;
   cudaGraphExec_t exec;
   cudaStream_t cap;
@@ -2919,8 +2922,9 @@ int stencil_request(int opt) {
   if (opt >= 0) return opt;
   const char* sel = getenv("FS_STENCIL");
   if (!sel) return -1;
-  static const char* names[6] = {"plain", "tma1", "tma_m", "tmas", "tma_split", "pz"};
-  for (int k = 0; k < 6; ++k)
+  static const char* names[8] = {"plain", "tma1", "tma_m", "tmas", "tma_split", "pz",
+                                 "pz4", "pz16"};
+  for (int k = 0; k < 8; ++k)
     if (strcmp(sel, names[k]) == 0) return k;
   return -1;
 }
@@ -3008,6 +3012,16 @@ struct Impl {
     } else if (P->stencil_kind == 5) {
       using CZ = TmaTilePZ<T, K>;
       marching((const void*)k_stencil_pz<T, K>, CZ::THREADS, CZ::SMEM, CZ::TZ, CZ::TY);
+    } else if (P->stencil_kind == 6 || P->stencil_kind == 7) {
+      if constexpr (TmaTileM<T, K>::B <= 32) {
+        if (P->stencil_kind == 6) {
+          using CZ = TmaTilePZ<T, K, 4>;
+          marching((const void*)k_stencil_pz<T, K, 4>, CZ::THREADS, CZ::SMEM, CZ::TZ, CZ::TY);
+        } else {
+          using CZ = TmaTilePZ<T, K, 16>;
+          marching((const void*)k_stencil_pz<T, K, 16>, CZ::THREADS, CZ::SMEM, CZ::TZ, CZ::TY);
+        }
+      }
     } else if (P->stencil_kind == 4) {
       if constexpr (TmaTileSplit<T, K>::OK) {
         using CM = TmaTileM<T, K>;
@@ -3046,16 +3060,18 @@ struct Impl {
       // direction update fused in) once its z tensor map exists.  Every
       // candidate is timed with the direction update it needs: k_pnew and
       // the stencil, or the fused kernel alone.
-      const int cands[5] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1, P->zmap_ok ? 5 : -1};
+      // kinds 6 and 7: the fused stencil on 32x4 and 32x16 tiles (nodes of
+      // at most 32 bytes), with their own tensor-map boxes
+      const bool shapes = P->zmap_ok && TmaTileM<T, K>::B <= 32;
+      const int cands[7] = {2, 3, 0, TmaTileSplit<T, K>::OK ? 4 : -1, P->zmap_ok ? 5 : -1,
+                            shapes ? 6 : -1, shapes ? 7 : -1};
       float best = 3.4e38f;
       int bestk = 2;
-      for (int c = 0; c < 6; ++c) P->tune_ms[c] = -1.f;
+      for (int c = 0; c < 8; ++c) P->tune_ms[c] = -1.f;
       int* done = &P->ctl->all_done;
       for (int c : cands) {
         if (c < 0) continue;
-        P->stencil_kind = c;
-        P->use_tma = c != 0;
-        apply_grid(P);
+        if (set_kind(P, c) != FS_OK) continue;
         FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
         kernel(P, 0, 0, s);
         FS_CHECK(cudaMemsetAsync(done, 0, sizeof(int), s));
@@ -3079,9 +3095,7 @@ struct Impl {
           bestk = c;
         }
       }
-      P->stencil_kind = bestk;
-      P->use_tma = bestk != 0;
-      apply_grid(P);
+      if (set_kind(P, bestk) != FS_OK) (void)set_kind(P, 2);
       FS_CHECK(cudaMemcpyAsync(st0, saved.data(), sbytes, cudaMemcpyHostToDevice, s));
       FS_CHECK(cudaStreamSynchronize(s));
       stencil_choice_put(P->d, K, (int)sizeof(T), bestk);
@@ -3112,6 +3126,8 @@ struct Impl {
         P->stencil_kind = 2;
       } else if (want == 5) {
         P->stencil_kind = 5;  // falls back to 2 if the z tensor map cannot be made
+      } else if (want == 6 || want == 7) {
+        P->stencil_kind = TmaTileM<T, K>::B <= 32 ? want : 5;
       } else if (want == 4) {
         P->stencil_kind = TmaTileSplit<T, K>::OK ? 4 : 2;
       } else {
@@ -3131,6 +3147,30 @@ struct Impl {
   // The z (or r) tensor map of the fused direction-update stencil (kind 5),
   // once the multigrid output buffer is known; without it kind 5 is not
   // offered (a plan that asked for it runs kind 2).
+  // Tile height of the TMA stencil kinds 2..7 (their tensor-map boxes).
+  static int kind_ty(int kind) {
+    return kind == 6 ? 4 : (kind == 7 ? 16 : TmaTileM<T, K>::TY);
+  }
+  // Switch the plan to stencil kind c: the tensor maps of its tile shape,
+  // the z map of the fused kinds, its grid.  Not FS_OK if a map cannot be
+  // made (the plan keeps a consistent earlier kind in that case).
+  static int set_kind(fs_pcg_plan* P, int c) {
+    if ((c == 6 || c == 7) && TmaTileM<T, K>::B > 32) return FS_BAD_ARG;
+    const int prev = P->stencil_kind;
+    P->stencil_kind = c;
+    int st = maps(P);
+    if (st == FS_OK && c >= 5) {
+      zmap(P);
+      if (P->stencil_kind != c) st = FS_BAD_ARG;  // z map refused: fell back to 2
+    }
+    if (st != FS_OK) {
+      P->stencil_kind = prev;
+      (void)maps(P);
+      if (prev >= 5) zmap(P);
+    }
+    apply_grid(P);
+    return st;
+  }
   static int zmap(fs_pcg_plan* P) {
     P->zmap_ok = 0;
     if constexpr (!TmaTileM<T, K>::OK) {
@@ -3138,8 +3178,9 @@ struct Impl {
     } else {
       const void* zb = P->precond ? P->z : P->r;
       if (P->stencil_kind < 2 || !zb || P->d.per) {
-        if (P->stencil_kind == 5) {
+        if (P->stencil_kind >= 5) {
           P->stencil_kind = 2;
+          (void)maps(P);
           apply_grid(P);
         }
         return FS_OK;
@@ -3150,8 +3191,9 @@ struct Impl {
       cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)P->d.nz, (cuuint64_t)P->d.ny,
                             (cuuint64_t)P->d.nx};
       cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
-      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)TmaTileM<T, K>::HZ,
-                           (cuuint32_t)TmaTileM<T, K>::HY, 1};
+      // the z box has the p box's shape: the tile of the kind that runs
+      const int zhy = P->stencil_kind >= 5 ? kind_ty(P->stencil_kind) + 2 : TmaTileM<T, K>::HY;
+      cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)TmaTileM<T, K>::HZ, (cuuint32_t)zhy, 1};
       cuuint32_t es[4] = {1, 1, 1, 1};
       const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
@@ -3161,8 +3203,9 @@ struct Impl {
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (rc == CUDA_SUCCESS) {
         P->zmap_ok = 1;
-      } else if (P->stencil_kind == 5) {
+      } else if (P->stencil_kind >= 5) {
         P->stencil_kind = 2;
+        (void)maps(P);
       }
       apply_grid(P);
       return FS_OK;
@@ -3184,7 +3227,7 @@ struct Impl {
     cuuint64_t strides[3] = {B, B * P->d.nz, B * P->d.nz * P->d.ny};
     // the p box of the kernel that will run: its tile has its own halo height
     const int hz = P->stencil_kind >= 2 ? TmaTileM<T, K>::HZ : C::HZ;
-    const int hy = P->stencil_kind >= 2 ? TmaTileM<T, K>::HY : C::HY;
+    const int hy = P->stencil_kind >= 2 ? kind_ty(P->stencil_kind) + 2 : C::HY;
     cuuint32_t box[4] = {(cuuint32_t)K, (cuuint32_t)hz, (cuuint32_t)hy, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
@@ -3216,12 +3259,13 @@ struct Impl {
     if (P->stencil_kind >= 2) {
       using CM = TmaTileM<T, K>;
       const cuuint64_t MB = sizeof(T);
+      const int ty = kind_ty(P->stencil_kind);
       cuuint64_t mdims[3] = {(cuuint64_t)P->d.nz, (cuuint64_t)P->d.ny, (cuuint64_t)P->d.nx};
       cuuint64_t mstr[2] = {MB * P->d.nz, MB * P->d.nz * P->d.ny};
       cuuint32_t mes[3] = {1, 1, 1};
-      cuuint32_t boxes[3][3] = {{(cuuint32_t)CM::TZ, (cuuint32_t)CM::TY, 1},
-                                {(cuuint32_t)CM::TZ, (cuuint32_t)(CM::TY + 1), 1},
-                                {(cuuint32_t)(CM::TZ + CM::ZP), (cuuint32_t)CM::TY, 1}};
+      cuuint32_t boxes[3][3] = {{(cuuint32_t)CM::TZ, (cuuint32_t)ty, 1},
+                                {(cuuint32_t)CM::TZ, (cuuint32_t)(ty + 1), 1},
+                                {(cuuint32_t)(CM::TZ + CM::ZP), (cuuint32_t)ty, 1}};
       void* mb[3] = {P->ex, P->ey, P->ez};
       for (int m = 0; m < 3; ++m) {
         CUresult rc = encode(&P->tm_m[m], dt, 3, mb[m], mdims, mstr, boxes[m], mes,
@@ -3257,13 +3301,29 @@ struct Impl {
   static void kernel(fs_pcg_plan* P, int which, int par, cudaStream_t s) {
     switch (which) {
       case 0:
-        if (P->stencil_kind == 5) break;  // the fused stencil forms p itself
+        if (P->stencil_kind >= 5) break;  // the fused stencils form p themselves
         k_pnew<T, K><<<P->g_pnew, fs::kBlock, 0, s>>>(
             P->d, (const T*)(P->precond ? P->z : P->r), (const T*)P->p[par],
             (T*)P->p[1 - par], P->st, P->ctl);
         break;
       case 1:
         if constexpr (TmaTile<T, K>::OK) {
+          if (P->stencil_kind == 6 || P->stencil_kind == 7) {
+            if constexpr (TmaTileM<T, K>::B <= 32) {
+              if (P->stencil_kind == 6) {
+                using CZ = TmaTilePZ<T, K, 4>;
+                k_stencil_pz<T, K, 4><<<P->g_apply, CZ::THREADS, CZ::SMEM, s>>>(
+                    P->dm, P->tm_z, P->tm_p[par], P->tm_m[0], P->tm_m[1], P->tm_m[2],
+                    (T*)P->p[1 - par], (T*)P->q, P->partials, P->st, P->ctl);
+              } else {
+                using CZ = TmaTilePZ<T, K, 16>;
+                k_stencil_pz<T, K, 16><<<P->g_apply, CZ::THREADS, CZ::SMEM, s>>>(
+                    P->dm, P->tm_z, P->tm_p[par], P->tm_m[0], P->tm_m[1], P->tm_m[2],
+                    (T*)P->p[1 - par], (T*)P->q, P->partials, P->st, P->ctl);
+              }
+            }
+            break;
+          }
           if (P->stencil_kind == 5) {
             using CZ = TmaTilePZ<T, K>;
             k_stencil_pz<T, K><<<P->g_apply, CZ::THREADS, CZ::SMEM, s>>>(
@@ -4497,7 +4557,7 @@ int fs_pcg_plan_stencil_kind(const fs_pcg_plan* P) { return P ? P->stencil_kind 
 
 int fs_pcg_plan_stencil_times(const fs_pcg_plan* P, float* ms) {
   if (!P || !ms) return FS_BAD_ARG;
-  for (int c = 0; c < 6; ++c) ms[c] = P->tune_ms[c];
+  for (int c = 0; c < 8; ++c) ms[c] = P->tune_ms[c];
   return FS_OK;
 }
 

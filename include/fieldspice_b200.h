@@ -202,7 +202,7 @@ int fs_pcg_plan_solve_poll(fs_pcg_plan* plan, fs_rhs_stats* stats, int* done);
  * and the lower end of its interval [smooth_lo, 2] on the unit-diagonal level
  * operators; coarse_deg, coarse_lo: the same on the coarsest level (1..64);
  * coarsest_nodes: coarsening stops at or below this node count (>= 8);
- * stencil_kind: the CG stencil (0..5, see fs_pcg_plan_stencil_kind) or -1
+ * stencil_kind: the CG stencil (0..7, see fs_pcg_plan_stencil_kind) or -1
  * (the FS_STENCIL environment variable, else autotuned); agg_alpha: the
  * factor (0 < agg_alpha < 2) on every coarse correction of the aggregation
  * hierarchy (FS_PRECOND_MG_AGG; over-correction for its piecewise-constant
@@ -456,13 +456,15 @@ int fs_pcg_plan_label_counts(const fs_pcg_plan* plan, long long* counts, void* s
  * 2 TMA-staged p and masses, 3 as 2 with TMA stores of q, 4 as 2 with each
  * 32-byte node split over two threads, 5 as 2 with the direction update
  * p = z + beta p_old formed inside the stencil from staged z and p_old tiles
- * (no separate p-update kernel).  Unless the FS_STENCIL environment
- * variable names one, the first plan of each (grid, RHS block, precision)
- * times kinds 2, 3, 0, 5 (and 4 for 32-byte nodes), each with the direction
- * update it needs, on its own buffers at creation and later plans of that
- * shape reuse the fastest.                                                  */
+ * (no separate p-update kernel) on 32x8 tiles, 6 and 7 as 5 on 32x4 and
+ * 32x16 tiles (nodes of at most 32 bytes).  Unless the plan's options or the
+ * FS_STENCIL environment variable name one, the first plan of each shape
+ * class (RHS block, element size, log2 of the node count, nz a multiple of
+ * 32) with vectors of at least 32 MB times kinds 2, 3, 0, 5, 6, 7 (and 4 for
+ * 32-byte nodes), each with the direction update it needs, on its own
+ * buffers at creation, and later plans of that class reuse the fastest.     */
 int fs_pcg_plan_stencil_kind(const fs_pcg_plan* plan);
-/* ms[6] (host): the mean time per iteration of the direction update and the
+/* ms[8] (host): the mean time per iteration of the direction update and the
  * stencil for each kind (index = kind) measured by this plan's autotuner;
  * -1 for kinds it did not time (every entry is -1 when the plan reused an
  * earlier choice or FS_STENCIL chose).                                      */

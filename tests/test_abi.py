@@ -86,7 +86,7 @@ def test_multigrid_parameters_are_validated(dll):
     assert dll.fs_pcg_workspace_bytes_opt(*args, None, ctypes.byref(nb)) == L.FS_OK
     assert nb.value == default
     for field, bad in [("smooth_deg", 0), ("smooth_lo", 2.0), ("coarse_deg", 65),
-                       ("coarse_lo", 0.0), ("coarsest_nodes", 4), ("stencil_kind", 6),
+                       ("coarse_lo", 0.0), ("coarsest_nodes", 4), ("stencil_kind", 8),
                        ("stencil_kind", -2), ("agg_alpha", 0.0), ("agg_alpha", 2.0)]:
         q = L.FsMgParams()
         dll.fs_mg_params_default(ctypes.byref(q))

@@ -3,8 +3,10 @@
 ``FS_STENCIL`` selects the kernel of ``q = A~ p, p.q`` when a plan is built:
 ``plain`` (cached loads), ``tma1`` (p staged by TMA), the default (p and the
 three mass tiles staged by TMA), ``tmas`` (as the default, with q leaving
-through shared memory by TMA stores) and ``tma_split`` (as the default, each
-32-byte node split over two threads).  Each runs the 48x48x24 layered
+through shared memory by TMA stores), ``tma_split`` (as the default, each
+32-byte node split over two threads), ``pz`` (the direction update
+p = z + beta p_old formed inside the stencil) and ``pz4`` / ``pz16`` (the same
+on 32x4 / 32x16 tiles: the tile shapes the autotuner also tries).  Each runs the 48x48x24 layered
 extraction recorded from the reference (8 right-hand sides) and, against the
 cached-load kernel, the extraction of the first four terminals (4 RHS).
 """
@@ -35,7 +37,8 @@ def _extract(g, eps, terms, precision):
     return ps.capacitance_matrix(terms, BoundarySpec(zlo=Dirichlet(0.0)))
 
 
-@pytest.mark.parametrize("variant", ["plain", "tma1", "default", "tmas", "tma_split", "pz"])
+@pytest.mark.parametrize("variant", ["plain", "tma1", "default", "tmas", "tma_split", "pz",
+                                     "pz4", "pz16"])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_stencil_variant_matches_reference(cuda, golden, monkeypatch, variant, precision):
     d, g, terms = _problem(golden)
@@ -104,7 +107,7 @@ def test_stencil_autotuner_times_launches_that_work(cuda, monkeypatch):
     monkeypatch.delenv("FS_STENCIL", raising=False)
     shape = (200, 184, 100)
     sys_ = _uniform_system(shape, 8, "mixed")
-    ms = (ctypes.c_float * 6)()
+    ms = (ctypes.c_float * 8)()
     L.check("fs_pcg_plan_stencil_times", L.lib().fs_pcg_plan_stencil_times(sys_.plan, ms))
     kind = L.lib().fs_pcg_plan_stencil_kind(sys_.plan)
     sys_.close()
@@ -112,8 +115,8 @@ def test_stencil_autotuner_times_launches_that_work(cuda, monkeypatch):
     # at least the stencil's bytes (p, q, masses) over 10 TB/s for every
     # candidate (each is timed with its direction update, whose bytes add)
     floor_ms = N * (2 * 8 * 4 + 3 * 4) / 10e12 * 1e3
-    timed = {c: ms[c] for c in range(6) if ms[c] >= 0}
-    assert set(timed) == {0, 2, 3, 4, 5}, list(ms)
+    timed = {c: ms[c] for c in range(8) if ms[c] >= 0}
+    assert set(timed) == {0, 2, 3, 4, 5, 6, 7}, list(ms)
     for c, t in timed.items():
         assert t >= floor_ms, (c, t, floor_ms)
     assert timed[kind] == min(timed.values())
