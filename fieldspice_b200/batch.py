@@ -8,7 +8,9 @@ and runs them together on a pool of CUDA streams with the library's
 non-blocking solve (``fs_pcg_plan_solve_begin`` / ``fs_pcg_plan_solve_poll``):
 largest geometry first, each plan's next graph chunk enqueued as soon as its
 previous one has finished, and the host building the next plans while the GPU
-solves the ones already built.  Charges are integrated per geometry in FP64
+solves the ones already built.  A geometry with more terminals than one block
+of 32-byte nodes holds (8 FP32 / 4 FP64 RHS) solves its column blocks one
+after another on its plan.  Charges are integrated per geometry in FP64
 exactly as in a single extraction.
 
 With a process group of several ranks (one per GPU), the geometries are
@@ -27,10 +29,11 @@ import numpy as np
 
 from . import _lib as L
 from .boundaries import dirichlet_nodes
-from .device import DeviceOperator, EliminatedSystem, MAX_RHS, h2d, pad_rhs, upload_groups
+from .device import (DeviceOperator, EliminatedSystem, block_rhs, h2d, pad_rhs,
+                     rhs_blocks, upload_groups)
 from .solvers.base import GPUConfig, SolverConfig, resolve_preconditioner
-from .solvers.poisson import (PoissonSolver, capacitance_report, check_terminals, prepare_bc,
-                              raise_on_status, shield_nodes, upload_cell_property)
+from .solvers.poisson import (capacitance_report, check_terminals, prepare_bc, raise_on_status,
+                              shield_nodes, upload_cell_property)
 
 __all__ = ["capacitance_matrices", "shard_by_cost", "problem_cost"]
 
@@ -39,10 +42,12 @@ __all__ = ["capacitance_matrices", "shard_by_cost", "problem_cost"]
 TUNE_MIN_BYTES = 32 << 20
 
 
-def problem_cost(problem) -> float:
-    """Work estimate of one extraction: nodes x padded RHS width."""
+def problem_cost(problem, width: int = 8) -> float:
+    """Work estimate of one extraction: nodes x the padded RHS widths of its
+    column blocks."""
     grid, _, terms = problem[:3]
-    return float(np.prod(grid.shape_nodes)) * pad_rhs(min(len(terms), MAX_RHS))
+    blocks = rhs_blocks(len(terms), width)
+    return float(np.prod(grid.shape_nodes)) * pad_rhs(len(blocks[0])) * len(blocks)
 
 
 def shard_by_cost(costs: Sequence[float], world: int) -> list[list[int]]:
@@ -64,9 +69,12 @@ def shard_by_cost(costs: Sequence[float], world: int) -> list[list[int]]:
 
 
 class _Extraction:
-    """One geometry's eliminated system, excitations and charge groups."""
+    """One geometry's extraction: the eliminated system (one plan, as wide
+    as its largest column block), the charge groups of every terminal, and
+    its terminals' unit excitations in column blocks solved one after
+    another on that plan."""
 
-    def __init__(self, grid, eps_cell, terminals, bc, cfg, gcfg):
+    def __init__(self, grid, eps_cell, terminals, bc, cfg, gcfg, width):
         import torch
         self.grid = grid
         _, eps, eps_min, eps_max = upload_cell_property(eps_cell, grid, "eps_cell")
@@ -79,53 +87,74 @@ class _Extraction:
         nt = len(self.terms)
         if nt == 0:
             raise ValueError("capacitance extraction needs at least one terminal")
+        self.blocks = rhs_blocks(nt, width)
+        self.block = 0
         bc = prepare_bc(bc, grid)
         self.op = DeviceOperator(grid, eps, prop_range=(eps_min, eps_max))
         dev = self.op.dev
         wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
         term_nodes = [np.asarray(t.nodes, np.int64) for t in self.terms]
-        term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
+        self.term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
         wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
-        shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
+        shield_dev = shield_nodes(wall_dev, self.term_dev, self.op.N)
         label = torch.zeros(self.op.N, dtype=torch.uint8, device=dev)
         if wall_idx.size:
             label[wall_dev] = L.LABEL_FIXED
-        for n in term_dev:
+        for n in self.term_dev:
             label[n] = L.LABEL_FIXED
         self.has_shield = shield_dev.numel() > 0
-        groups = term_dev + ([shield_dev] if self.has_shield else [])
+        groups = self.term_dev + ([shield_dev] if self.has_shield else [])
         self.groups = groups
         self.gdev = upload_groups(groups, dev)
         self.tol = float(cfg.tol)
         self.system = EliminatedSystem(
-            self.op, label, nt, precision=gcfg.precision,
+            self.op, label, len(self.blocks[0]), precision=gcfg.precision,
             preconditioner=resolve_preconditioner(cfg, gcfg), learned=gcfg.learned,
             coarsening=gcfg.coarsening, mg_params=gcfg.mg_params)
         # 0: the reference's cap max(500, 10 sqrt(n_free)), per plan on the device
         self.maxiter = 0 if gcfg.maxiter is None else int(gcfg.maxiter)
-        group = torch.full((self.op.N,), -1, dtype=torch.int16, device=dev)
-        for c, n in enumerate(term_dev):
-            group[n] = c
+        self.group = torch.empty(self.op.N, dtype=torch.int16, device=dev)
+        self.C = np.zeros((nt, nt))
+        self.q_shield = np.zeros(nt)
+        self.stats: list[dict] = []
+        self.excite(0)
+
+    def excite(self, b: int) -> None:
+        """Unit excitations of column block b into the plan's phi (on the
+        current stream)."""
+        self.block = b
+        self.system.nrhs = len(self.blocks[b])
+        self.group.fill_(-1)
+        for c, j in enumerate(self.blocks[b]):
+            self.group[self.term_dev[j]] = c
         nx, ny, nz = self.op.shape
         L.check("fs_fill_unit_excitation", L.lib().fs_fill_unit_excitation(
-            L.ptr(group), L.ptr(self.system.label_in), L.ptr(self.system.phi),
+            L.ptr(self.group), L.ptr(self.system.label_in), L.ptr(self.system.phi),
             nx, ny, nz, self.system.k, L.stream_ptr()))
 
-    def collect(self, stats: list[dict]) -> tuple[np.ndarray, dict]:
+    def collect(self, stats: list[dict]) -> bool:
+        """The current block's columns of C and of the shield charge; True
+        when every block is in."""
         nt = len(self.terms)
-        k = self.system.k
-        Q = self.op.group_sums(self.system.phi, self.groups, nrhs=k, nodes_dev=self.gdev)
-        C = np.array(Q[:nt, :nt], dtype=float)
-        q_shield = np.array(Q[nt, :nt]) if self.has_shield else np.zeros(nt)
+        cols = self.blocks[self.block]
+        Q = self.op.group_sums(self.system.phi, self.groups, nrhs=self.system.k,
+                               nodes_dev=self.gdev)
+        self.C[:, cols] = np.asarray(Q[:nt, :len(cols)], dtype=float)
+        if self.has_shield:
+            self.q_shield[cols] = np.asarray(Q[nt, :len(cols)])
+        self.stats.extend(stats)
+        return self.block + 1 == len(self.blocks)
+
+    def result(self) -> tuple[np.ndarray, dict]:
         info = {"method": f"gpu-cg-{self.system.preconditioner}-{self.system.mode}",
-                "n": self.op.N, "iterations": [s["iterations"] for s in stats],
-                "relres_fp64": [s["relres"] for s in stats],
-                "residual": max(s["relres"] for s in stats),
+                "n": self.op.N, "iterations": [s["iterations"] for s in self.stats],
+                "relres_fp64": [s["relres"] for s in self.stats],
+                "residual": max(s["relres"] for s in self.stats),
                 "fp64_fallback": bool(self.system.fell_back),
-                "symmetric": True, "equilibrated": True}
-        rep = capacitance_report(C, q_shield, info)
+                "symmetric": True, "equilibrated": True, "blocks": len(self.blocks)}
+        rep = capacitance_report(self.C, self.q_shield, info)
         rep["terminals"] = tuple(t.name for t in self.terms)
-        return 0.5 * (C + C.T), rep
+        return 0.5 * (self.C + self.C.T), rep
 
     def close(self):
         self.system.close()
@@ -141,42 +170,39 @@ def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
     """Extract every problem on this GPU; returns the list of C matrices."""
     import torch
     out: list[Any] = [None] * len(problems)
-    batchable, singles = [], []
-    for i, p in enumerate(problems):
-        (batchable if len(p[2]) <= MAX_RHS else singles).append(i)
-    for i in singles:  # more terminals than one RHS block: the plain path
-        grid, eps, terms = problems[i][:3]
-        bc = problems[i][3] if len(problems[i]) > 3 else None
-        rep: dict = {}
-        out[i] = PoissonSolver(grid, eps, cfg, gpu=gcfg).capacitance_matrix(
-            terms, bc, report=rep)
-        if reports is not None:
-            reports[i] = rep
-    if not batchable:
+    if not problems:
         return out
     lib = L.lib()
     tol = float(cfg.tol)
+    # each geometry's terminals in column blocks of at most `width` (32-byte
+    # nodes: the widest the fused multigrid passes serve), one plan per
+    # geometry solving its blocks in turn
+    width = block_rhs(gcfg.precision)
     # Largest first (longest-processing-time order).  Plans whose CG vectors
     # reach the stencil autotuner's 32 MB threshold (nodes x padded RHS x the
     # element size) time kernels when they are created, so they are all built
     # before any solve runs; after that each plan starts as soon as it is
     # built and the host builds the next while the GPU solves.
-    order = sorted(batchable, key=lambda i: (-problem_cost(problems[i]), i))
+    order = sorted(range(len(problems)), key=lambda i: (-problem_cost(problems[i], width), i))
     es = 8 if gcfg.precision == "fp64" else 4
-    tuned = [i for i in order if problem_cost(problems[i]) * es >= TUNE_MIN_BYTES]
-    pool = [torch.cuda.Stream() for _ in range(max(1, min(streams, len(batchable))))]
+
+    def vector_bytes(i):
+        p = problems[i]
+        return float(np.prod(p[0].shape_nodes)) * pad_rhs(len(rhs_blocks(len(p[2]), width)[0])) * es
+    tuned = [i for i in order if vector_bytes(i) >= TUNE_MIN_BYTES]
+    rest = [i for i in order if vector_bytes(i) < TUNE_MIN_BYTES]
+    pool = [torch.cuda.Stream() for _ in range(max(1, min(streams, len(problems))))]
     ex: dict[int, _Extraction] = {}
     running: dict[int, Any] = {}
-    started = 0
+    stream_of: dict[int, Any] = {}
 
     def build(i):
         p = problems[i]
-        ex[i] = _Extraction(p[0], p[1], p[2], p[3] if len(p) > 3 else None, cfg, gcfg)
+        ex[i] = _Extraction(p[0], p[1], p[2], p[3] if len(p) > 3 else None, cfg, gcfg, width)
+        stream_of[i] = pool[len(stream_of) % len(pool)]
 
     def start(i):
-        nonlocal started
-        s = pool[started % len(pool)]
-        started += 1
+        s = stream_of[i]
         ready = torch.cuda.Event()
         ready.record(torch.cuda.current_stream())  # set-up and excitation kernels
         s.wait_event(ready)
@@ -194,9 +220,13 @@ def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
             st, stats = e.system.finish_learned(st, stats, tol, e.maxiter)
         _, stats = e.system.finish_auto(st, stats, tol, e.maxiter)
         raise_on_status(stats, tol, "gpu-cg")
-        out[i], rep = e.collect(stats)
-        if reports is not None:
-            reports[i] = rep
+        if e.collect(stats):
+            out[i], rep = e.result()
+            if reports is not None:
+                reports[i] = rep
+        else:  # the next column block on the same plan
+            e.excite(e.block + 1)
+            start(i)
 
     def poll() -> bool:
         progressed = False
@@ -218,7 +248,7 @@ def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
             build(i)
         for i in tuned:
             start(i)
-        for i in order[len(tuned):]:
+        for i in rest:
             build(i)
             start(i)
             poll()
@@ -231,6 +261,9 @@ def extract_local(problems, cfg, gcfg, streams: int, reports: list | None):
         torch.cuda.synchronize()
         for e in ex.values():
             e.close()
+    missing = [i for i, c in enumerate(out) if c is None]
+    if missing:
+        raise RuntimeError(f"batched extraction left geometries {missing} unsolved")
     return out
 
 
@@ -264,7 +297,8 @@ def capacitance_matrices(problems: Sequence, config: SolverConfig | None = None,
         rank = dist.get_rank(group)
     if world == 1:
         return run(problems, cfg, gcfg, streams, reports)
-    shards = shard_by_cost([problem_cost(p) for p in problems], world)
+    shards = shard_by_cost([problem_cost(p, block_rhs(gcfg.precision)) for p in problems],
+                           world)
     mine = shards[rank]
     my_reports = [None] * len(mine) if reports is not None else None
     res = run([problems[i] for i in mine], cfg, gcfg, streams, my_reports)

@@ -21,8 +21,8 @@ import numpy as np
 from .. import _lib as L
 from ..boundaries import (BoundarySpec, check_supported, dirichlet_nodes, neumann_load,
                           periodic_mask)
-from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, d2h, h2d, mark,
-                      pad_rhs, upload_groups)
+from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, block_rhs, d2h, h2d, mark,
+                      pad_rhs, rhs_blocks, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
 
 __all__ = ["PoissonSolver", "check_terminals", "as_cell_array", "raise_on_status",
@@ -607,15 +607,15 @@ def extract_capacitance(op: DeviceOperator, term_dev, wall_dev, shield_dev, *,
     launches = 0
     setup_time = 0.0
     nx, ny, nz = op.shape
-    for b0 in range(0, nt, MAX_RHS):
-        cols = list(range(b0, min(nt, b0 + MAX_RHS)))
+    # blocks of at most 32-byte nodes (8 FP32 / 4 FP64 RHS), near-equal in
+    # size so that one plan of one padded width solves them all
+    blocks = rhs_blocks(nt, block_rhs(precision))
+    k = pad_rhs(len(blocks[0]))
+    for cols in blocks:
         kb = len(cols)
-        k = pad_rhs(kb)
-        if system is None or system.k != k:
-            if system is not None:
-                system.close()
+        if system is None:
             mark("labels")
-            system = EliminatedSystem(op, label, kb, precision=precision,
+            system = EliminatedSystem(op, label, len(blocks[0]), precision=precision,
                                       preconditioner=preconditioner, learned=learned,
                                       coarsening=coarsening, mg_params=mg_params)
             setup_time += system.setup_time

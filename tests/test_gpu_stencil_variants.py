@@ -98,14 +98,15 @@ def test_stencil_autotuner_times_launches_that_work(cuda, monkeypatch):
     """Each candidate the autotuner times must do the stencil's work: its mean
     launch time is at least the algorithmic bytes over 10 TB/s (more than any
     B200 HBM can move), far above the few microseconds of a launch that
-    returns at once.  200x184x100 nodes (280 MB per apply), 8 FP32 RHS: a
-    shape class (node count, z extent not a multiple of 32) no other test
-    uses, so this plan runs the autotuner."""
+    returns at once.  220x200x100 nodes (2^22 <= N < 2^23, z extent not a
+    multiple of 32), 8 FP32 RHS: a shape class no other test uses (the batch
+    tests' 8-RHS blocks stop at 2.4 M nodes), so this plan runs the
+    autotuner."""
     import ctypes
 
     from fieldspice_b200 import _lib as L
     monkeypatch.delenv("FS_STENCIL", raising=False)
-    shape = (200, 184, 100)
+    shape = (220, 200, 100)
     sys_ = _uniform_system(shape, 8, "mixed")
     ms = (ctypes.c_float * 8)()
     L.check("fs_pcg_plan_stencil_times", L.lib().fs_pcg_plan_stencil_times(sys_.plan, ms))
