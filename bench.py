@@ -88,10 +88,13 @@ def committed_traffic():
 def kernel_names(s: int, k: int, stencil_kind: int) -> dict:
     """The kernel each timed role runs as (template names as ncu lists them)."""
     t = "float" if s == 4 else "double"
-    stencil = {5: "k_stencil_pz", 4: "k_stencil_split", 3: "k_stencil_tma_s",
-               2: "k_stencil_tma_m", 1: "k_stencil_tma"}.get(stencil_kind, "k_apply_pq")
+    stencil = {4: "k_stencil_split", 3: "k_stencil_tma_s", 2: "k_stencil_tma_m",
+               1: "k_stencil_tma"}.get(stencil_kind, "k_apply_pq")
+    # the fused direction-update stencil carries its tile height (0: 32x8)
+    pz = {5: 0, 6: 4, 7: 16}
     split = k * s == 32  # 32-byte nodes: the two-threads-per-node smoothing pass
-    return {"stencil": f"{stencil}<{t}, {k}>",
+    return {"stencil": (f"k_stencil_pz<{t}, {k}, {pz[stencil_kind]}>" if stencil_kind in pz
+                        else f"{stencil}<{t}, {k}>"),
             "pupdate": f"k_pnew<{t}, {k}>",
             "update": f"k_update<{t}, {k}>",
             "smoother": (f"k_mg_smooth_split<{t}, {k}, 1>" if split
@@ -199,8 +202,8 @@ def kernel_bytes(N: int, k: int, s: int, stencil_kind: int = 2) -> dict:
     """Algorithmic bytes per launch of the CG kernels (each array once)."""
     return {"pupdate": 3 * N * k * s,                 # read r|z, p_old; write p
             # read p, 3 masses; write q -- with the direction update inside
-            # (kind 5) read z and p_old, write p and q
-            "stencil": N * ((4 if stencil_kind == 5 else 2) * k * s + 3 * s),
+            # (kinds 5-7) read z and p_old, write p and q
+            "stencil": N * ((4 if stencil_kind >= 5 else 2) * k * s + 3 * s),
             "update": 6 * N * k * s,                  # read p, q, x, r; write x, r
             # fine-level post-smoothing, one fused pass (k_mg_smooth_split):
             # read x, b and the masses; write x2 = x + a r0 + b A~r0
