@@ -33,8 +33,8 @@ from typing import Any, Mapping, Sequence
 import numpy as np
 
 from .. import _lib as L
-from ..device import (MAX_RHS, DeviceOperator, EliminatedSystem, d2h, h2d, pad_rhs,
-                      upload_groups)
+from ..device import (DeviceOperator, EliminatedSystem, block_rhs, d2h, h2d, pad_rhs,
+                      rhs_blocks, upload_groups)
 from ..solvers.base import GPUConfig, SolverConfig, resolve_preconditioner
 from ..solvers.poisson import raise_on_status, upload_cell_property
 
@@ -198,8 +198,9 @@ class FieldRegion:
             return entry
         Y = np.zeros((nE, nE))
         tol = float(self.cfg.tol)
-        for b0 in range(0, nE, MAX_RHS):
-            cols = list(range(b0, min(nE, b0 + MAX_RHS)))
+        # electrodes in blocks of 32-byte nodes (8 FP32 / 4 FP64 RHS)
+        for cols in rhs_blocks(nE, block_rhs(self.gpu.precision)):
+            b0 = cols[0]
             k = pad_rhs(len(cols))
             if self.n_interior == 0:
                 phi = torch.zeros(self.N * k, dtype=torch.float64, device=self.op_eps.dev)

@@ -21,7 +21,7 @@ import numpy as np
 from .. import _lib as L
 from ..boundaries import (BoundarySpec, check_supported, dirichlet_nodes, neumann_load,
                           periodic_mask)
-from ..device import (DeviceOperator, EliminatedSystem, MAX_RHS, block_rhs, d2h, h2d, mark,
+from ..device import (DeviceOperator, EliminatedSystem, block_rhs, d2h, h2d, mark,
                       pad_rhs, rhs_blocks, upload_groups)
 from .base import ConvergenceError, GPUConfig, Result, SolverConfig, resolve_preconditioner
 
@@ -252,8 +252,8 @@ class PoissonSolver:
         Same algorithm and report as ``poisson.py:1100-1249``: terminal ``j``
         at 1 V, every other terminal and every Dirichlet wall at 0 V, and
         ``C[i, j] = sum_{n in T_i} (L phi_j)_n``.  All excitations share one
-        eliminated system and are solved together as a block of right-hand
-        sides (up to 16 per device solve).
+        eliminated system and are solved as blocks of right-hand sides (up to
+        8 per device solve in mixed precision, 4 in FP64: 32-byte nodes).
         """
         import torch
         t_start = time.perf_counter()
@@ -464,9 +464,9 @@ class PoissonSolver:
                 "a floating or charge-driven electrode touches a Dirichlet node")
         # columns: 0 = the driven potentials (every floating electrode at 0 V)
         # with the free charge, 1 + f = electrode f at 1 V and everything else
-        # at 0 V; solved in blocks of at most MAX_RHS columns on one system
+        # at 0 V; solved in blocks of 32-byte nodes on one system
         ncol = nf + 1
-        chunks = [list(range(c, min(ncol, c + MAX_RHS))) for c in range(0, ncol, MAX_RHS)]
+        chunks = rhs_blocks(ncol, block_rhs(self.gpu.precision))
         k = pad_rhs(len(chunks[0]))
         label = torch.zeros(N, dtype=torch.uint8, device=dev)
         fixed_d = torch.as_tensor(fixed, device=dev)

@@ -53,8 +53,9 @@ def test_floating_without_reference_raises(cuda):
 @pytest.mark.parametrize("preconditioner", ["mg", "jacobi"])
 def test_twenty_floating_electrodes_match_reference(cuda, golden, preconditioner):
     """20 floating and charge-driven conductors and a driven electrode
-    (``tests/golden/floating_many.npz``): more columns than one block of 16
-    right-hand sides, solved block after block on one system."""
+    (``tests/golden/floating_many.npz``): 21 columns, more than one block of
+    right-hand sides (8 per block in mixed precision), solved block after
+    block on one system."""
     from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
     from fieldspice_b200.grid import RectilinearGrid
     from fieldspice_b200.solvers.base import GPUConfig, SolverConfig, Terminal
@@ -71,7 +72,7 @@ def test_twenty_floating_electrodes_match_reference(cuda, golden, preconditioner
     ps = PoissonSolver(g, d["eps"], SolverConfig(tol=1e-12),
                        gpu=GPUConfig(preconditioner=preconditioner))
     r = ps.solve(terms, BoundarySpec(zlo=Dirichlet(0.0)))
-    assert r.meta["linear"]["blocks"] == 2
+    assert r.meta["linear"]["blocks"] == 3  # 21 columns in blocks of 7
     phi = r.fields["phi"][0].ravel()
     assert np.abs(phi - d["phi"]).max() <= 1e-9
     qscale = abs(float(d["q"][0]))
