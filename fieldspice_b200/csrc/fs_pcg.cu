@@ -4266,7 +4266,9 @@ int solve_begin(fs_pcg_plan* P, int warm_start, double tol, int maxiter,
   // (hundreds of FP32 iterations per decade) and after a 1e4 drop under
   // multigrid (a decade every ~2 iterations, so little FP32 drift; measured
   // at 256x256x128: 22 iterations with 1e-3 and 1e-4, one reliable update
-  // fewer and 0.96 ms less per extraction with 1e-4).
+  // fewer and 0.96 ms less per extraction with 1e-4; 1e-5 and 1e-6 let the
+  // FP32 recurrence drift until RHS stalled into FP64 continuations and
+  // 64-geometry batches failed to converge).
   const double delta = P->precision != FS_PRECISION_MIXED ? 0.0
                        : (P->precond ? 1e-4 : 0.1);
   cudaError_t e;
