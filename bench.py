@@ -51,8 +51,10 @@ FULLSIZE_JSON = ROOT / "tests" / "golden" / "layered_256x256x128_s0.json"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    # defaults: 20 timed steps after 5 warm-up ones for this implementation;
+    # 5 after 3 for the reference arm, whose every step is a ~14 s call
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
     ap.add_argument("--preconditioner", default="mg", choices=["mg", "jacobi"])
@@ -65,7 +67,13 @@ def parse():
                          "256x256x128 workload (64x64x32 nodes, 8 RHS), random weights")
     ap.add_argument("--single", action="store_true",
                     help="one device-resident extraction only (profiler runs)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    ref = args.impl == "reference"
+    if args.steps is None:
+        args.steps = 5 if ref else 20
+    if args.warmup is None:
+        args.warmup = 3 if ref else 5
+    return args
 
 
 def measured_peaks():
