@@ -118,6 +118,7 @@ _SIGNATURES = {
     "fs_unet_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                                    c_void_p, c_void_p]),
     "fs_unet_gradient": (c_int, [c_void_p] * 8),
+    "fs_unet_adam_step": (c_int, [c_void_p, c_void_p, c_float, c_void_p]),
     "fs_unet_error": (c_int, [c_void_p, POINTER(c_int), c_void_p]),
     "fs_unet_destroy": (c_int, [c_void_p]),
     "fs_eq_apply": (c_int, [c_void_p] * 6 + [c_int] * 4 + [c_void_p]),

@@ -394,6 +394,21 @@ int scale_inputs(fs_unet* U, const float* rhs, long long sn, long long sb, const
   return FS_OK;
 }
 
+// One Adam step of theta on gradient g (device, theta-sized; the net's own
+// gradient buffer, or a caller's, e.g. averaged over data-parallel ranks),
+// then the tensor-core weight images re-packed from the new theta.
+int adam_update(fs_unet* U, const float* g, float lr, cudaStream_t s) {
+  U->step += 1;
+  const double b1 = 0.9, b2 = 0.999;
+  const float c1 = (float)(1.0 / (1.0 - pow(b1, (double)U->step)));
+  const float c2 = (float)(1.0 / (1.0 - pow(b2, (double)U->step)));
+  const long long nt = theta_size();
+  fs::k_adam<<<blocks_for(nt), 256, 0, s>>>(nt, U->theta, g, U->adam_m, U->adam_v, lr,
+                                             (float)b1, (float)b2, 1e-8f, c1, c2);
+  FS_CHECK_LAUNCH("k_adam");
+  return pack_all(U, s);
+}
+
 }  // namespace
 
 int unet_forward(fs_unet* U, const float* rhs, long long rhs_sn, long long rhs_sb,
@@ -555,17 +570,14 @@ int fs_unet_train_step(fs_unet* net, const float* rhs, const float* em, const ui
   fs::k_sum_groups<<<1, 32, 0, s>>>(17, kRedBlocks, U->ph, U->grad + head_off());
   FS_CHECK_LAUNCH("unet loss");
   FS_TRY(body_backward(U, s));
-  U->step += 1;
-  const double b1 = 0.9, b2 = 0.999;
-  const float c1 = (float)(1.0 / (1.0 - pow(b1, (double)U->step)));
-  const float c2 = (float)(1.0 / (1.0 - pow(b2, (double)U->step)));
-  const long long nt = theta_size();
-  fs::k_adam<<<blocks_for(nt), 256, 0, s>>>(nt, U->theta, U->grad, U->adam_m, U->adam_v, lr,
-                                             (float)b1, (float)b2, 1e-8f, c1, c2);
-  FS_CHECK_LAUNCH("k_adam");
-  FS_TRY(pack_all(U, s));
+  FS_TRY(adam_update(U, U->grad, lr, s));
   if (loss) FS_CHECK(cudaMemcpyAsync(loss, U->loss, sizeof(float), cudaMemcpyDeviceToDevice, s));
   return FS_OK;
+}
+
+int fs_unet_adam_step(fs_unet* net, const float* grad, float lr, void* stream) {
+  if (!net || !net->train || !grad || !(lr >= 0.0f)) return FS_BAD_ARG;
+  return adam_update(net, grad, lr, (cudaStream_t)stream);
 }
 
 int fs_unet_gradient(fs_unet* net, const float* rhs, const float* em, const uint8_t* label,

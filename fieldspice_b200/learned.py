@@ -170,6 +170,39 @@ def training_pairs(workloads, *, level: int = 3, snapshots=(4, 8, 16, 32, 64, 12
     return data
 
 
+def dp_batches(S: int, batch: int, epochs: int, seed: int, rank: int = 0, world: int = 1):
+    """Training schedule, one ``(epoch, step, indices)`` per step: every epoch
+    one permutation of the S pairs (the same on every rank, from ``seed``)
+    cut into slices of ``world * batch``; rank r takes part r of each slice.
+    Every rank gets the same number of steps (the collectives line up); with
+    one rank this is the plain shuffled mini-batch schedule."""
+    rng = np.random.default_rng(seed)
+    steps = S // (batch * world)
+    for ep in range(epochs):
+        perm = rng.permutation(S)
+        for bi in range(steps):
+            base = (bi * world + rank) * batch
+            yield ep, bi, perm[base:base + batch]
+
+
+def dp_world(group=None) -> tuple[int, int]:
+    """(rank, world size) of ``group`` (the default group when one is
+    initialised), (0, 1) without torch.distributed."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(group), dist.get_world_size(group)
+    return 0, 1
+
+
+def allreduce_mean(t, group=None, world: int = 1):
+    """In place: the mean of ``t`` over the ranks of ``group``."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        t /= world
+    return t
+
+
 class LearnedPreconditioner:
     """A trained U-Net and the multigrid level it replaces.
 
@@ -207,16 +240,25 @@ class LearnedPreconditioner:
 
     # -- training ------------------------------------------------------------
     def fit(self, data, *, epochs: int = 3, batch: int = 8, lr: float = 1e-3, seed: int = 0,
-            log=None) -> list[float]:
+            log=None, group=None) -> list[float]:
         """Adam on the relative squared error of the network's coarse
         correction against the injected errors; returns the loss history
-        (one entry per 50 steps)."""
+        (one entry per 50 steps).
+
+        Data parallel over the ranks of ``group`` (the default process group
+        when one is initialised; one rank per GPU, each holding the pairs):
+        every rank computes the gradient of its own batch
+        (``fs_unet_gradient``), one all-reduce averages the gradients and
+        every rank applies the same Adam step (``fs_unet_adam_step``), so
+        theta stays identical on all ranks.  The network has ~0.7 M
+        parameters: one 2.7 MB all-reduce per step."""
         import torch
         lib = L.lib()
         dims = data["dims"]
         S = data["rhs"].shape[0]
-        if S < batch:
-            raise ValueError("fewer training pairs than one batch")
+        rank, world = dp_world(group)
+        if S < batch * world:
+            raise ValueError("fewer training pairs than one batch per rank")
         nb = ctypes.c_size_t()
         L.check("fs_unet_workspace_bytes", lib.fs_unet_workspace_bytes(*dims, batch, 1,
                                                                        ctypes.byref(nb)))
@@ -225,31 +267,37 @@ class LearnedPreconditioner:
         L.check("fs_unet_create", lib.fs_unet_create(*dims, batch, 1, L.ptr(self.theta), L.ptr(ws),
                                                      nb.value, ctypes.byref(net), L.stream_ptr()))
         loss = torch.zeros(1, dtype=torch.float32, device=self.theta.device)
-        rng = np.random.default_rng(seed)
-        steps_per_epoch = S // batch
-        total = epochs * steps_per_epoch
+        grad = (torch.empty_like(self.theta) if world > 1 else None)
+        total = epochs * (S // (batch * world))
         hist = []
         t0 = time.perf_counter()
         step = 0
         try:
-            for ep in range(epochs):
-                perm = torch.as_tensor(rng.permutation(S), device=self.theta.device)
-                for bi in range(steps_per_epoch):
-                    idx = perm[bi * batch:(bi + 1) * batch]
-                    rhs = data["rhs"].index_select(0, idx).contiguous()
-                    em = data["em"].index_select(0, idx).contiguous()
-                    lab = data["label"].index_select(0, idx).contiguous()
-                    tgt = data["target"].index_select(0, idx).contiguous()
-                    # cosine learning-rate decay
-                    lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+            for _, _, idx_h in dp_batches(S, batch, epochs, seed, rank, world):
+                idx = torch.as_tensor(idx_h, device=self.theta.device)
+                rhs = data["rhs"].index_select(0, idx).contiguous()
+                em = data["em"].index_select(0, idx).contiguous()
+                lab = data["label"].index_select(0, idx).contiguous()
+                tgt = data["target"].index_select(0, idx).contiguous()
+                # cosine learning-rate decay
+                lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+                if world == 1:
                     L.check("fs_unet_train_step", lib.fs_unet_train_step(
                         net, L.ptr(rhs), L.ptr(em), L.ptr(lab), L.ptr(tgt),
                         ctypes.c_float(lr_t), L.ptr(loss), L.stream_ptr()))
-                    step += 1
-                    if step % 50 == 0 or step == total:
-                        hist.append(float(loss.item()))
-                        if log is not None:
-                            log(f"step {step}/{total} loss {hist[-1]:.4f}")
+                else:
+                    L.check("fs_unet_gradient", lib.fs_unet_gradient(
+                        net, L.ptr(rhs), L.ptr(em), L.ptr(lab), L.ptr(tgt), L.ptr(grad),
+                        L.ptr(loss), L.stream_ptr()))
+                    allreduce_mean(grad, group, world)
+                    L.check("fs_unet_adam_step", lib.fs_unet_adam_step(
+                        net, L.ptr(grad), ctypes.c_float(lr_t), L.stream_ptr()))
+                step += 1
+                if step % 50 == 0 or step == total:
+                    allreduce_mean(loss, group, world)
+                    hist.append(float(loss.item()))
+                    if log is not None:
+                        log(f"step {step}/{total} loss {hist[-1]:.4f}")
             flag = ctypes.c_int()
             L.check("fs_unet_error", lib.fs_unet_error(net, ctypes.byref(flag), L.stream_ptr()))
             if flag.value:

@@ -384,6 +384,11 @@ int fs_unet_train_step(fs_unet* net, const float* rhs, const float* em, const ui
 /* The same loss and its gradient dL/dtheta (device, theta-sized), no update. */
 int fs_unet_gradient(fs_unet* net, const float* rhs, const float* em, const uint8_t* label,
                      const float* target, float* grad, float* loss, void* stream);
+/* One Adam step of theta on a caller's gradient (device, theta-sized), e.g.
+ * the gradients of fs_unet_gradient averaged over data-parallel ranks by an
+ * all-reduce; then the weight images are re-packed.  fs_unet_gradient
+ * followed by this step equals fs_unet_train_step on the same batch.       */
+int fs_unet_adam_step(fs_unet* net, const float* grad, float lr, void* stream);
 /* Host int: 1 if a staged load of a network convolution timed out.        */
 int fs_unet_error(const fs_unet* net, int* flag, void* stream);
 int fs_unet_destroy(fs_unet* net);

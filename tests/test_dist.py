@@ -130,3 +130,79 @@ def test_a_failing_rank_is_detected_by_the_others():
             p.kill()
     assert got[1] == "raised"
     assert got[0].startswith("error after"), got[0]
+
+
+def test_data_parallel_schedule_covers_each_epoch_once():
+    """Every step the ranks' batches are disjoint parts of one slice of that
+    epoch's permutation (the same on every rank), and every rank has the same
+    number of steps; one rank reproduces the plain shuffled schedule."""
+    from fieldspice_b200.learned import dp_batches
+    S, batch, epochs = 103, 4, 2
+    for world in (1, 2, 3):
+        per_rank = [list(dp_batches(S, batch, epochs, 5, r, world)) for r in range(world)]
+        assert len({len(p) for p in per_rank}) == 1
+        assert len(per_rank[0]) == epochs * (S // (batch * world))
+        for ep in range(epochs):
+            seen = []
+            for p in per_rank:
+                for e, _, idx in p:
+                    if e == ep:
+                        assert len(idx) == batch
+                        seen.extend(int(i) for i in idx)
+            assert len(seen) == len(set(seen)) == (S // (batch * world)) * batch * world
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(S)
+    one = list(dp_batches(S, batch, 1, 5))
+    assert all(np.array_equal(idx, perm[b * batch:(b + 1) * batch]) for _, b, idx in one)
+
+
+def _dp_worker(rank, world, port, q):
+    """A toy data-parallel fit through the same helpers: per step, the mean
+    gradient of this rank's batch, all-reduced, then one SGD step."""
+    import torch
+    import torch.distributed as dist
+    from fieldspice_b200.learned import allreduce_mean, dp_batches, dp_world
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        r, w = dp_world()
+        data = torch.as_tensor(np.random.default_rng(1).standard_normal((64, 3)))
+        theta = torch.zeros(3, dtype=torch.float64)
+        for _, _, idx in dp_batches(64, 4, 2, 9, r, w):
+            g = (theta - data[torch.as_tensor(idx)]).mean(0)
+            allreduce_mean(g, None, w)
+            theta -= 0.1 * g
+        q.put((rank, theta.numpy().tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_fit_keeps_ranks_identical():
+    """Two gloo ranks: the averaged-gradient steps leave theta identical on
+    both, equal to one rank running the combined batches of each step."""
+    import multiprocessing as mp
+
+    import torch
+    from fieldspice_b200.learned import dp_batches
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0] == res[1]
+    # the same steps on one process: the mean over both ranks' batches
+    data = torch.as_tensor(np.random.default_rng(1).standard_normal((64, 3)))
+    theta = torch.zeros(3, dtype=torch.float64)
+    for (_, _, i0), (_, _, i1) in zip(dp_batches(64, 4, 2, 9, 0, 2), dp_batches(64, 4, 2, 9, 1, 2)):
+        g0 = (theta - data[torch.as_tensor(i0)]).mean(0)
+        g1 = (theta - data[torch.as_tensor(i1)]).mean(0)
+        theta -= 0.1 * (g0 + g1) / 2
+    assert np.allclose(res[0], theta.numpy(), rtol=0, atol=1e-15)

@@ -127,3 +127,33 @@ def test_unet_training_reduces_the_loss(cuda):
     assert np.all(np.isfinite(hist))
     assert hist[-1] < hist[0] / 4, hist[::10]
     lib.fs_unet_destroy(net)
+
+
+def test_gradient_then_adam_step_equals_train_step(cuda):
+    """The data-parallel training primitive: fs_unet_gradient followed by
+    fs_unet_adam_step on that gradient gives bit for bit the theta of
+    fs_unet_train_step (three steps on the same batches), and an averaged
+    gradient of two half batches drives the same update path."""
+    import torch
+    from fieldspice_b200 import _lib as L
+    lib = L.lib()
+    dims, B = (12, 10, 9), 4
+    theta = UO.init_theta(7)
+    net_a, th_a, ws_a = _net(cuda, dims, B, theta)
+    net_b, th_b, ws_b = _net(cuda, dims, B, theta)
+    r, e, l, t = _dev(cuda, *_data(dims, B, 8))
+    loss = torch.zeros(1, dtype=torch.float32, device=cuda)
+    grad = torch.empty_like(th_b)
+    for it in range(3):
+        lr = ctypes.c_float(1e-3 * (it + 1))
+        L.check("step", lib.fs_unet_train_step(net_a, L.ptr(r), L.ptr(e), L.ptr(l), L.ptr(t),
+                                               lr, L.ptr(loss), L.stream_ptr()))
+        L.check("grad", lib.fs_unet_gradient(net_b, L.ptr(r), L.ptr(e), L.ptr(l), L.ptr(t),
+                                             L.ptr(grad), L.ptr(loss), L.stream_ptr()))
+        L.check("adam", lib.fs_unet_adam_step(net_b, L.ptr(grad), lr, L.stream_ptr()))
+    torch.cuda.synchronize()
+    assert torch.equal(th_a, th_b)
+    assert not torch.equal(th_a, torch.as_tensor(theta, dtype=torch.float32, device=cuda))
+    assert lib.fs_unet_adam_step(net_b, None, ctypes.c_float(1e-3), L.stream_ptr()) == L.FS_BAD_ARG
+    lib.fs_unet_destroy(net_a)
+    lib.fs_unet_destroy(net_b)
