@@ -117,6 +117,14 @@ __device__ __forceinline__ void edge6(const Dims& d, const M* __restrict__ mx,
 
 __device__ __forceinline__ void node_ijk(const Dims& d, long long n, int& i,
                                          int& j, int& k) {
+  if (n <= 0x7fffffffLL) {  // 32-bit divisions while the index fits
+    const unsigned u = (unsigned)n, nz = (unsigned)d.nz, ny = (unsigned)d.ny;
+    const unsigned t = u / nz;
+    k = (int)(u - t * nz);
+    i = (int)(t / ny);
+    j = (int)(t - (unsigned)i * ny);
+    return;
+  }
   long long t = n / d.nz;
   k = (int)(n - t * d.nz);
   i = (int)(t / d.ny);
@@ -314,6 +322,49 @@ __device__ __forceinline__ void stv(T* __restrict__ base, long long n,
   } else {
 #pragma unroll
     for (int c = 0; c < K; ++c) p[c] = v[c];
+  }
+}
+
+// ---- nodes split into FP64 chunks --------------------------------------------
+// The streaming per-node kernels that touch the FP64 solution (K doubles per
+// node, 64 bytes for 8 RHS) run one thread per 16-byte chunk of it:
+// Chunks<K>::NCH threads per node, W = 2 right-hand sides each (1 when
+// K == 1), so a warp request covers whole sectors instead of four 16-byte
+// pieces 64 bytes apart.  The grid-stride step is a multiple of NCH, so a
+// thread keeps its chunk h = threadIdx.x % NCH for the whole loop.
+template <int K>
+struct Chunks {
+  static constexpr int W = K >= 2 ? 2 : 1;  // right-hand sides per thread
+  static constexpr int NCH = K / W;         // threads per node
+  static_assert(NCH * W == K && (NCH & (NCH - 1)) == 0, "K must be a power of two");
+};
+
+// W consecutive values of T at p (8- or 16-byte aligned for W == 2)
+template <typename T, int W>
+__device__ __forceinline__ void ldw(const T* p, T (&v)[W]) {
+  if constexpr (W == 2 && std::is_same<T, float>::value) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else if constexpr (W == 2) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int t = 0; t < W; ++t) v[t] = p[t];
+  }
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void stw(T* p, const T (&v)[W]) {
+  if constexpr (W == 2 && std::is_same<T, float>::value) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else if constexpr (W == 2) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  } else {
+#pragma unroll
+    for (int t = 0; t < W; ++t) p[t] = v[t];
   }
 }
 

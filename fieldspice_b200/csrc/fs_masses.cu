@@ -138,19 +138,34 @@ __global__ void k_unit_excitation(long long N, int nrhs,
                                   const int16_t* __restrict__ group,
                                   const uint8_t* __restrict__ label,
                                   double* __restrict__ phi) {
-  // pairs of values as 16-byte stores where the width and the base allow it
+  // pairs of values as 16-byte stores where the width and the base allow it,
+  // one thread per pair (consecutive threads write consecutive 16 bytes)
   const bool pairs = (nrhs & 1) == 0 && (reinterpret_cast<uintptr_t>(phi) & 15) == 0;
+  if (pairs) {
+    const int np = nrhs / 2;
+    const long long total = N * np;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+      long long n;
+      int c;
+      if (total <= 0x7fffffffLL) {
+        n = (unsigned)t / (unsigned)np;
+        c = (int)((unsigned)t - (unsigned)n * (unsigned)np);
+      } else {
+        n = t / np;
+        c = (int)(t - n * np);
+      }
+      const int g = label[n] == FS_LABEL_FIXED ? group[n] : -1;
+      reinterpret_cast<double2*>(phi)[t] =
+          make_double2(g == 2 * c ? 1.0 : 0.0, g == 2 * c + 1 ? 1.0 : 0.0);
+    }
+    return;
+  }
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
        n += (long long)gridDim.x * blockDim.x) {
     const bool fixed = label[n] == FS_LABEL_FIXED;
     const int g = fixed ? group[n] : -1;
-    if (pairs) {
-      double2* p2 = reinterpret_cast<double2*>(phi + n * nrhs);
-      for (int r = 0; r < nrhs; r += 2)
-        p2[r / 2] = make_double2(g == r ? 1.0 : 0.0, g == r + 1 ? 1.0 : 0.0);
-    } else {
-      for (int r = 0; r < nrhs; ++r) phi[n * nrhs + r] = g == r ? 1.0 : 0.0;
-    }
+    for (int r = 0; r < nrhs; ++r) phi[n * nrhs + r] = g == r ? 1.0 : 0.0;
   }
 }
 
@@ -298,7 +313,7 @@ int fs_fill_unit_excitation(const int16_t* group, const uint8_t* label,
   if (!group || !label || !phi || nx < 1 || ny < 1 || nz < 1 || nrhs < 1)
     return FS_BAD_ARG;
   Dims d = fs::make_dims(nx, ny, nz);
-  int g = fs_grid_blocks((const void*)k_unit_excitation, d.N);
+  int g = fs_grid_blocks((const void*)k_unit_excitation, d.N * (nrhs > 1 ? nrhs / 2 : 1));
   k_unit_excitation<<<g, fs::kBlock, 0, (cudaStream_t)stream>>>(d.N, nrhs,
                                                                 group, label, phi);
   FS_CHECK_LAUNCH("k_unit_excitation");

@@ -2460,31 +2460,42 @@ __global__ void __launch_bounds__(fs::kBlock)
 // K3a folds the correction accumulated since the last update into the FP64
 // solution (phi += s x~, x~ = 0) for the flagged right-hand sides; K3b then
 // recomputes their TRUE residual r = f - L phi with the FP64 masses, replaces
-// the recurrence residual with it and decides convergence on it.
+// the recurrence residual with it and decides convergence on it.  K3a (and
+// k_finalize) stream the node's values one thread per FP64 chunk
+// (fs::Chunks): 0.32 -> 0.26 ms per fold at 256x256x128 with 8 RHS.  K3b
+// (and k_init) gather six neighbours and keep one thread per node: split
+// into chunks they were slower (k_reliable 0.63 -> 0.80 ms, k_init 0.64 ->
+// 0.96 ms; the masses, labels and index arithmetic repeat per chunk).
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_fold(Dims d, const double* __restrict__ s64, double* __restrict__ phi,
            T* __restrict__ x, RhsState* st, Control* ctl) {
   if (!ctl->any_ru) return;
+  using CH = fs::Chunks<K>;
+  constexpr int W = CH::W, NCH = CH::NCH;
+  const int h = threadIdx.x % NCH;
   __shared__ int ru[K];
   if (threadIdx.x < K) ru[threadIdx.x] = st[threadIdx.x].ru;
   __syncthreads();
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
-       n += (long long)gridDim.x * blockDim.x) {
+  const long long total = d.N * NCH;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long n = g / NCH;
     const double s = s64[n];
     if (s == 0.0) continue;  // x~ is 0 off the free nodes
-    T xv[K];
-    double ph[K];
-    fs::ldv<T, K>(x, n, xv);
-    fs::ldv<double, K>(phi, n, ph);  // whole node: vector accesses
+    const long long o = n * K + h * W;
+    T xv[W];
+    double ph[W];
+    fs::ldw<T, W>(x + o, xv);
+    fs::ldw<double, W>(phi + o, ph);
 #pragma unroll
-    for (int t = 0; t < K; ++t)
-      if (ru[t]) {
+    for (int t = 0; t < W; ++t)
+      if (ru[h * W + t]) {
         ph[t] += (double)xv[t] * s;
         xv[t] = (T)0;
       }
-    fs::stv<double, K>(phi, n, ph);
-    fs::stv<T, K>(x, n, xv);
+    fs::stw<double, W>(phi + o, ph);
+    fs::stw<T, W>(x + o, xv);
   }
 }
 
@@ -2606,25 +2617,31 @@ __global__ void k_finalize(Dims d, const uint8_t* __restrict__ label,
                            const double* __restrict__ s64,
                            double* __restrict__ phi, T* __restrict__ x,
                            RhsState* st, Control* ctl) {
+  using CH = fs::Chunks<K>;
+  constexpr int W = CH::W, NCH = CH::NCH;
+  const int h = threadIdx.x % NCH;
   __shared__ int zero[K];
   if (threadIdx.x < K) zero[threadIdx.x] = st[threadIdx.x].zero;
   __syncthreads();
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < d.N;
-       n += (long long)gridDim.x * blockDim.x) {
+  const long long total = d.N * NCH;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long n = g / NCH;
     if (label[n] != FS_LABEL_FREE) continue;
     const double s = s64[n];
-    T xv[K];
-    double ph[K];
-    fs::ldv<T, K>(x, n, xv);
-    fs::ldv<double, K>(phi, n, ph);  // whole node: vector accesses
+    const long long o = n * K + h * W;
+    T xv[W];
+    double ph[W];
+    fs::ldw<T, W>(x + o, xv);
+    fs::ldw<double, W>(phi + o, ph);
 #pragma unroll
-    for (int t = 0; t < K; ++t) {
+    for (int t = 0; t < W; ++t) {
       ph[t] += (double)xv[t] * s;  // correction since the last fold
       xv[t] = (T)0;
-      if (zero[t]) ph[t] = 0.0;
+      if (zero[h * W + t]) ph[t] = 0.0;
     }
-    fs::stv<double, K>(phi, n, ph);
-    fs::stv<T, K>(x, n, xv);
+    fs::stw<double, W>(phi + o, ph);
+    fs::stw<T, W>(x + o, xv);
   }
   if (fs::last_block(&ctl->tickets[kTicketFin])) {
     if (threadIdx.x < K) st[threadIdx.x].zero = 0;
@@ -3140,8 +3157,8 @@ struct Impl {
     apply_grid(P);
     P->g_update = fs_grid_blocks((const void*)k_update<T, K>, N);
     P->g_rel = fs_grid_blocks((const void*)k_reliable<T, K>, N);
-    P->g_fold = fs_grid_blocks((const void*)k_fold<T, K>, N);
-    P->g_fin = fs_grid_blocks((const void*)k_finalize<T, K>, N);
+    P->g_fold = fs_grid_blocks((const void*)k_fold<T, K>, N * fs::Chunks<K>::NCH);
+    P->g_fin = fs_grid_blocks((const void*)k_finalize<T, K>, N * fs::Chunks<K>::NCH);
     P->g_rz = fs_grid_blocks((const void*)k_rz<T, K>, N);
   }
   // The z (or r) tensor map of the fused direction-update stencil (kind 5),
