@@ -27,6 +27,7 @@ DTYPE_F64, DTYPE_F32 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_MG, PRECOND_MG_AGG = 0, 1, 2
 PROP_STATS_WORKSPACE_BYTES = 16384  # FS_PROP_STATS_WORKSPACE_BYTES
+PROP_STATS_RESULT_OFFSET = 14208    # FS_PROP_STATS_RESULT_OFFSET
 AVERAGE_PARALLEL, AVERAGE_HARMONIC = 0, 1
 
 
@@ -132,6 +133,7 @@ _SIGNATURES = {
     "fs_selftest_wait_timeout": (c_int, [c_longlong, POINTER(c_int), c_void_p]),
     "fs_prop_stats": (c_int, [c_void_p, c_longlong, POINTER(c_double), c_void_p, c_size_t,
                               c_void_p]),
+    "fs_prop_stats_enqueue": (c_int, [c_void_p, c_longlong, c_void_p, c_size_t, c_void_p]),
     "fs_rhs_superpose": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double),
                                  c_void_p, c_void_p, c_longlong, c_void_p]),
     "fs_pcg_plan_precondition": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -199,6 +201,37 @@ def prop_stats(t) -> tuple[float, float, float]:
     check("fs_prop_stats", lib().fs_prop_stats(ptr(t), t.numel(), stats, ptr(ws),
                                                PROP_STATS_WORKSPACE_BYTES, stream_ptr()))
     return float(stats[0]), float(stats[1]), float(stats[2])
+
+
+class PendingStats:
+    """An enqueued ``fs_prop_stats_enqueue``: the three results travel to a
+    page-locked host buffer behind it on the same stream; ``result()`` waits
+    for them."""
+
+    def __init__(self, workspace, host, event):
+        self._ws = workspace  # kept allocated until the copy has run
+        self._host = host
+        self._event = event
+
+    def result(self) -> tuple[float, float, float]:
+        self._event.synchronize()
+        h = self._host
+        return float(h[0]), float(h[1]), float(h[2])
+
+
+def prop_stats_begin(t) -> PendingStats:
+    """``prop_stats`` without waiting: the reduction and the copy of its three
+    results are enqueued on the current stream."""
+    import torch
+    ws = torch.empty(PROP_STATS_WORKSPACE_BYTES, dtype=torch.uint8, device=t.device)
+    check("fs_prop_stats_enqueue", lib().fs_prop_stats_enqueue(
+        ptr(t), t.numel(), ptr(ws), PROP_STATS_WORKSPACE_BYTES, stream_ptr()))
+    host = torch.empty(3, dtype=torch.float64, pin_memory=True)
+    host.copy_(ws[PROP_STATS_RESULT_OFFSET:PROP_STATS_RESULT_OFFSET + 24].view(torch.float64),
+               non_blocking=True)
+    ev = torch.cuda.Event()
+    ev.record()
+    return PendingStats(ws, host, ev)
 
 
 def lib() -> ctypes.CDLL:

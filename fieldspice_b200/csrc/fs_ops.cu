@@ -483,22 +483,33 @@ __global__ void k_prop_stats(const double* __restrict__ p, long long n, double* 
 // stream-ordered allocation here returned its memory to the driver at the
 // synchronisation below, which waited for the work of every stream (measured:
 // 0.4 s of a 64-geometry batch whose builds overlap other plans' solves).
-extern "C" int fs_prop_stats(const double* p, long long n, double* stats_host, void* workspace,
-                             size_t workspace_bytes, void* stream) {
+extern "C" int fs_prop_stats_enqueue(const double* p, long long n, void* workspace,
+                                     size_t workspace_bytes, void* stream) {
   constexpr int g = 592;
   static_assert(sizeof(double) * (3 * g + 3) + sizeof(unsigned int) <=
                     FS_PROP_STATS_WORKSPACE_BYTES, "workspace constant too small");
-  if (!p || n < 1 || !stats_host || !workspace ||
-      workspace_bytes < FS_PROP_STATS_WORKSPACE_BYTES || ((uintptr_t)workspace & 15))
+  static_assert(sizeof(double) * 3 * g == FS_PROP_STATS_RESULT_OFFSET,
+                "result offset constant out of date");
+  if (!p || n < 1 || !workspace || workspace_bytes < FS_PROP_STATS_WORKSPACE_BYTES ||
+      ((uintptr_t)workspace & 15))
     return FS_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   double* buf = (double*)workspace;
   unsigned int* ticket = (unsigned int*)(buf + 3 * g + 3);
   FS_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
   k_prop_stats<<<g, fs::kBlock, 0, s>>>(p, n, buf, ticket, buf + 3 * g);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(stats_host, buf + 3 * g, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  FS_CHECK_LAUNCH("k_prop_stats");
+  return FS_OK;
+}
+
+extern "C" int fs_prop_stats(const double* p, long long n, double* stats_host, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  if (!stats_host) return FS_BAD_ARG;
+  const int st = fs_prop_stats_enqueue(p, n, workspace, workspace_bytes, stream);
+  if (st != FS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(stats_host, (const char*)workspace + FS_PROP_STATS_RESULT_OFFSET,
+                                  3 * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fs_cuda_status("fs_prop_stats", e);
   return FS_OK;

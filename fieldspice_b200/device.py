@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes
 import math
 import time
+import weakref
 
 import numpy as np
 
@@ -36,13 +37,31 @@ def mark(phase: str) -> None:
         PHASES.append((phase, time.perf_counter(), time.process_time()))
 
 
+#: Host arrays up to this size go through a page-locked staging copy.
+STAGED_H2D_BYTES = 4 << 20
+
+
 def h2d(a, dtype, dev):
-    """Upload a host array (counted in ``TRANSFERS``)."""
+    """Upload a host array (counted in ``TRANSFERS``).
+
+    Small arrays are copied into page-locked staging memory and uploaded
+    asynchronously on the current stream, so the host does not wait for the
+    device work queued before (a copy from pageable memory would); the
+    staging block is reused only after the copy has run.  Larger arrays are
+    uploaded synchronously."""
     import torch
     arr = np.ascontiguousarray(a)
-    t = torch.as_tensor(arr).to(device=dev, dtype=dtype)
     TRANSFERS["h2d"] += arr.nbytes
-    return t
+    src = torch.as_tensor(arr)
+    if src.dtype != dtype:
+        src = src.to(dtype)
+    if src.numel() * src.element_size() > STAGED_H2D_BYTES:
+        return src.to(device=dev)
+    staged = torch.empty(src.shape, dtype=dtype, pin_memory=True)
+    staged.copy_(src)
+    out = torch.empty(src.shape, dtype=dtype, device=dev)
+    out.copy_(staged, non_blocking=True)
+    return out
 
 
 def d2h(t) -> np.ndarray:
@@ -88,6 +107,35 @@ def device():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+# Device copies of each grid's metric arrays (cell widths and dual widths),
+# reused while the grid's host values are unchanged.
+_METRIC_CACHE: "weakref.WeakKeyDictionary" = weakref.WeakKeyDictionary()
+
+
+def metric_dev(grid, dev):
+    """The six FP64 metric arrays of ``grid_metric(grid)`` on ``dev``.
+
+    Kept per grid object and reused as long as the grid's current metric
+    equals the cached host copy (so a grid changed in place is uploaded
+    again); grids that cannot be weakly referenced are uploaded each call."""
+    import torch
+    (hx, hy, hz), (hxd, hyd, hzd) = grid_metric(grid)
+    host = [np.asarray(a, dtype=np.float64) for a in (hx, hy, hz, hxd, hyd, hzd)]
+    try:
+        hit = _METRIC_CACHE.get(grid)
+    except TypeError:
+        hit = None
+    if hit is not None and hit[0] == dev and all(
+            a.shape == b.shape and np.array_equal(a, b) for a, b in zip(hit[1], host)):
+        return hit[2]
+    tensors = [h2d(a, torch.float64, dev) for a in host]
+    try:
+        _METRIC_CACHE[grid] = (dev, [a.copy() for a in host], tensors)
+    except TypeError:
+        pass
+    return tensors
+
+
 def _as_dev(a, dtype, dev):
     import torch
     if isinstance(a, torch.Tensor):
@@ -120,8 +168,7 @@ class DeviceOperator:
         if mode not in ("parallel", "arithmetic", "harmonic", "series"):
             raise ValueError(f"unknown averaging mode {mode!r}")
         avg = L.AVERAGE_HARMONIC if mode in ("harmonic", "series") else L.AVERAGE_PARALLEL
-        (hx, hy, hz), (hxd, hyd, hzd) = grid_metric(grid)
-        hs = [_as_dev(a, torch.float64, self.dev) for a in (hx, hy, hz, hxd, hyd, hzd)]
+        hs = metric_dev(grid, self.dev)
         prop = _as_dev(prop_cell, torch.float64, self.dev)
         if prop.numel() != int(np.prod(grid.shape_cells)):
             raise ValueError("prop_cell does not match the grid's cell shape")

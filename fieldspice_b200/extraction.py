@@ -31,7 +31,9 @@ def capacitance_matrix(grid, eps_cell: np.ndarray, terminals: Sequence,
     symmetrised; the pre-symmetrisation asymmetry is in ``report``.
     """
     from .solvers.poisson import PoissonSolver
-    solver = PoissonSolver(grid, eps_cell, config, gpu=gpu)
+    # the permittivity upload and check overlap the terminal checks; a bad
+    # eps_cell still raises before anything else is reported
+    solver = PoissonSolver(grid, eps_cell, config, gpu=gpu, check_later=True)
     return solver.capacitance_matrix(list(terminals), bc, report=report)
 
 

@@ -42,24 +42,41 @@ def as_cell_array(a, grid, name: str) -> np.ndarray:
     return arr
 
 
-def upload_cell_property(a, grid, name: str):
+def upload_cell_property(a, grid, name: str, *, wait: bool = True):
     """The checks of ``as_cell_array`` with the pass over the values on the
     device: shape on the host, then one upload and one device reduction for
     non-finite entries, min and max.  Returns ``(host array, device tensor,
-    min, max)``."""
+    min, max)``.
+
+    ``wait=False`` returns ``(host array, device tensor, pending)`` at once:
+    the upload (asynchronous from page-locked memory) and the reduction are
+    enqueued, and ``cell_property_range(pending, name)`` later waits for them
+    and raises as the eager form does, so the host can work meanwhile."""
     import torch
+    from ..device import TRANSFERS, device
     arr = np.asarray(a, dtype=float)
     if arr.shape == ():
         arr = np.full(grid.shape_cells, float(arr))
     if arr.shape != tuple(grid.shape_cells):
         raise ValueError(f"{name} must have shape {tuple(grid.shape_cells)}, "
                          f"got {arr.shape}")
-    from ..device import device
-    dev = h2d(arr, torch.float64, device())
-    lo, hi, bad = L.prop_stats(dev)
+    src = torch.as_tensor(arr)
+    dev = torch.empty(arr.shape, dtype=torch.float64, device=device())
+    dev.copy_(src, non_blocking=True)
+    TRANSFERS["h2d"] += arr.nbytes
+    pending = L.prop_stats_begin(dev)
+    if not wait:
+        return arr, dev, pending
+    lo, hi = cell_property_range(pending, name)
+    return arr, dev, lo, hi
+
+
+def cell_property_range(pending, name: str) -> tuple[float, float]:
+    """(min, max) of an uploaded cell property; raises on non-finite values."""
+    lo, hi, bad = pending.result()
     if bad > 0:
         raise ValueError(f"{name} contains non-finite values")
-    return arr, dev, lo, hi
+    return lo, hi
 
 
 def shield_nodes(wall_dev, term_dev, n_nodes: int):
@@ -186,11 +203,32 @@ class PoissonSolver:
 
     def __init__(self, grid, eps_cell, config: SolverConfig | None = None,
                  operators=None, *, eps_mode: str = "parallel",
-                 gpu: GPUConfig | None = None) -> None:
+                 gpu: GPUConfig | None = None, check_later: bool = False) -> None:
         self.grid = grid
         self.cfg = config or SolverConfig()
         self.gpu = gpu or GPUConfig()
-        eps_cell, eps_dev, eps_min, eps_max = upload_cell_property(eps_cell, grid, "eps_cell")
+        # check_later (the one-call extraction): the upload and the device
+        # check of eps run while the host checks the terminals; the value
+        # errors below are raised by the first method that needs eps
+        eps_cell, eps_dev, self._eps_pending = upload_cell_property(
+            eps_cell, grid, "eps_cell", wait=False)
+        self.eps_cell = eps_cell
+        self.eps_mode = eps_mode
+        if not check_later:
+            self._check_eps()
+        mark("eps_upload_and_check")
+        self.op = DeviceOperator(grid, eps_dev, mode=eps_mode)
+        mark("masses")
+        if self._eps_range is not None:
+            self._set_contrast()
+
+    _eps_range = None
+
+    def _check_eps(self) -> None:
+        """Wait for the eps check (once) and raise on a bad permittivity."""
+        if self._eps_range is not None:
+            return
+        eps_min, eps_max = cell_property_range(self._eps_pending, "eps_cell")
         if eps_min <= 0.0:
             raise ValueError("eps_cell must be strictly positive [F/m]")
         if eps_min >= 1e-6:
@@ -198,11 +236,14 @@ class PoissonSolver:
                 f"eps_cell looks like a RELATIVE permittivity (min "
                 f"{eps_min:.4g}); fieldspice is strict SI and wants the "
                 "absolute value in F/m. Multiply by eps0.")
-        self.eps_cell = eps_cell
-        self.eps_mode = eps_mode
-        mark("eps_upload_and_check")
-        self.op = DeviceOperator(grid, eps_dev, mode=eps_mode, prop_range=(eps_min, eps_max))
-        mark("masses")
+        self._eps_range = (eps_min, eps_max)
+        self._eps_pending = None
+        if getattr(self, "op", None) is not None:
+            self._set_contrast()
+
+    def _set_contrast(self) -> None:
+        lo, hi = self._eps_range
+        self.op.material_contrast = hi / lo if lo > 0.0 else None
         self._L = None
         self.last_capacitance_report: dict[str, Any] = {}
         self.last_device_time = 0.0
@@ -215,6 +256,7 @@ class PoissonSolver:
         Assembled from the device masses for callers that want the matrix;
         the solve itself never forms it.
         """
+        self._check_eps()
         if self._L is None:
             self._L = assemble_csr(self.grid, self.op.edge_vector())
         return self._L
@@ -224,6 +266,7 @@ class PoissonSolver:
         """Permittivity averaged onto edges [F/m] in [x|y|z] edge order
         (``poisson.py:894-897``), recovered from the device masses as
         ``m_e * L_e / A_e``."""
+        self._check_eps()
         return self.op.edge_vector() / edge_area_over_length(self.grid)
 
     @property
@@ -232,6 +275,7 @@ class PoissonSolver:
 
     def _phi_dev(self, phi):
         import torch
+        self._check_eps()
         p = as_node_vector(phi, self.grid, "phi")
         return torch.as_tensor(p, dtype=torch.float64, device=self.op.dev)
 
@@ -258,18 +302,25 @@ class PoissonSolver:
         import torch
         t_start = time.perf_counter()
         grid = self.grid
-        terms = check_terminals(terminals, grid)
-        if not terms:
-            raise ValueError("capacitance extraction needs at least one terminal")
-        bc = prepare_bc(bc, grid, allow_periodic=True)
-        mask = periodic_mask(bc)
-        dev = self.op.dev
-        wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
-        mark("terminal_checks")
-        term_nodes = [np.asarray(t.nodes, np.int64) for t in terms]
-        term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
-        wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
-        shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
+        try:
+            # host-side checks while the eps upload and check may still run;
+            # a bad eps is reported first, as the constructor would
+            terms = check_terminals(terminals, grid)
+            if not terms:
+                raise ValueError("capacitance extraction needs at least one terminal")
+            bc = prepare_bc(bc, grid, allow_periodic=True)
+            mask = periodic_mask(bc)
+            dev = self.op.dev
+            wall_idx, _ = dirichlet_nodes(bc, grid, 0.0)
+            mark("terminal_checks")
+            term_nodes = [np.asarray(t.nodes, np.int64) for t in terms]
+            term_dev = [h2d(n, torch.int64, dev) for n in term_nodes]
+            wall_dev = h2d(wall_idx.astype(np.int64), torch.int64, dev)
+            shield_dev = shield_nodes(wall_dev, term_dev, self.op.N)
+        except Exception:
+            self._check_eps()
+            raise
+        self._check_eps()
         mark("node_upload")
         op, charges = self.op, None
         if mask:
@@ -331,6 +382,7 @@ class PoissonSolver:
         Periodic walls (also a node merge) are not implemented.
         """
         import torch
+        self._check_eps()
         t0 = time.perf_counter()
         grid = self.grid
         terms = check_terminals(terminals, grid)

@@ -436,6 +436,15 @@ int fs_selftest_wait_timeout(long long budget_cycles, int* status_host, void* st
 int fs_prop_stats(const double* p, long long n, double* stats_host, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* The same reduction, only enqueued on `stream` (no copy, no synchronisation):
+ * min, max and the non-finite count land as three doubles at byte offset
+ * FS_PROP_STATS_RESULT_OFFSET of the workspace, which must stay allocated
+ * until the caller has read them (stream-ordered).  Lets a host overlap the
+ * upload and check of a cell property with other work.                      */
+#define FS_PROP_STATS_RESULT_OFFSET 14208
+int fs_prop_stats_enqueue(const double* p, long long n, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
 /* ---- §8f: field region (fieldspice/circuit/coupling.py) ----------------------
  * out[i] = base[i] + sum_{c<ncols} coef_host[c] * phi[i*k + c0 + c] for
  * i < n (FP64; base may be NULL for 0; ncols <= 16, c0 + ncols <= k): the

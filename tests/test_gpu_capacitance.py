@@ -240,6 +240,37 @@ def test_input_rejection(cuda):
         ps.capacitance_matrix([Terminal("a", [0, 1]), Terminal("b", [1, 2])])
 
 
+def test_one_call_extraction_rejects_like_the_solver(cuda):
+    """extraction.capacitance_matrix checks eps while the host checks the
+    terminals: the same errors, a bad eps reported before bad terminals, and
+    page-locked inputs give the same C as pageable ones."""
+    import torch
+    from fieldspice_b200 import extraction as EX
+    from fieldspice_b200 import workloads as W
+    from fieldspice_b200.boundaries import BoundarySpec, Dirichlet
+    from fieldspice_b200.grid import RectilinearGrid
+    from fieldspice_b200.solvers.base import Terminal
+    g = RectilinearGrid.uniform([(0, 1e-6)] * 3, [4, 4, 4])
+    good = [Terminal("a", [0, 1])]
+    bad_terms = [Terminal("a", [0, 1]), Terminal("b", [1, 2])]
+    nan = np.full(g.shape_cells, 1e-11)
+    nan[1, 2, 0] = np.nan
+    for eps, match in ((np.full(g.shape_cells, 3.9), "RELATIVE"),
+                       (np.full(g.shape_cells, -1e-11), "positive"), (nan, "non-finite")):
+        with pytest.raises(ValueError, match=match):
+            EX.capacitance_matrix(g, eps, good)
+        with pytest.raises(ValueError, match=match):
+            EX.capacitance_matrix(g, eps, bad_terms)
+    with pytest.raises(ValueError, match="share node"):
+        EX.capacitance_matrix(g, np.full(g.shape_cells, 1e-11), bad_terms)
+    w = W.layered_boxes((32, 32, 16), seed=2)
+    bc = BoundarySpec(zlo=Dirichlet(0.0))
+    C = EX.capacitance_matrix(w.grid(), w.eps_cell, w.terminal_objects(), bc)
+    pinned = torch.from_numpy(np.ascontiguousarray(w.eps_cell)).pin_memory().numpy()
+    C_p = EX.capacitance_matrix(w.grid(), pinned, w.terminal_objects(), bc)
+    assert np.array_equal(C, C_p)
+
+
 @pytest.mark.slow
 def test_full_size_extraction_properties(cuda):
     """256x256x128 nodes, 8 terminals: size-independent properties of the

@@ -109,3 +109,22 @@ def test_quadform_and_group_sums(cuda, golden):
     y = Lm @ x
     for gi, gr in enumerate(groups):
         assert np.allclose(s[gi], y[gr].sum(axis=0), rtol=1e-12, atol=1e-12 * np.abs(y).max())
+
+
+def test_grid_metric_cache_reuses_and_refreshes(cuda, golden):
+    """The device copy of a grid's metric is reused while the grid's values
+    are unchanged and uploaded again (with the masses following) once they
+    change in place."""
+    from fieldspice_b200.device import DeviceOperator, metric_dev
+    d = golden("masses")
+    g = _grid(d, "graded")
+    dev = DeviceOperator(g, np.full(g.shape_cells, 1e-11)).dev
+    a = metric_dev(g, dev)
+    assert all(x is y for x, y in zip(a, metric_dev(g, dev)))
+    m0 = DeviceOperator(g, np.full(g.shape_cells, 1e-11)).m.cpu().numpy()
+    g.hx[0] *= 2.0  # changed in place: a new upload, and masses that follow it
+    b = metric_dev(g, dev)
+    assert b[0] is not a[0]
+    assert float(b[0][0]) == float(g.hx[0])
+    m1 = DeviceOperator(g, np.full(g.shape_cells, 1e-11)).m.cpu().numpy()
+    assert not np.array_equal(m0, m1)
