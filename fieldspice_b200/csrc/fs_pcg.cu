@@ -223,13 +223,13 @@ __global__ void __launch_bounds__(fs::kBlock)
     // no free neighbours that read them)
     double res[K], bres[K], c[K];
     if (f) {
-      fs::ldv<double, K>(f, n, res);
+      fs::ldv<double, K, true>(f, n, res);
     } else {
 #pragma unroll
       for (int t = 0; t < K; ++t) res[t] = 0.0;
     }
     if (lab == FS_LABEL_FREE && warm) {
-      fs::ldv<double, K>(phi, n, c);
+      fs::ldv<double, K, true>(phi, n, c);
     } else {
 #pragma unroll
       for (int t = 0; t < K; ++t) c[t] = 0.0;
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(fs::kBlock)
 #pragma unroll
         for (int t = 0; t < K; ++t) v[t] = 0.0;
       } else {
-        fs::ldv<double, K>(phi, nb, v);
+        fs::ldv<double, K, true>(phi, nb, v);
       }
 #pragma unroll
       for (int t = 0; t < K; ++t) {
@@ -273,14 +273,14 @@ __global__ void __launch_bounds__(fs::kBlock)
         acc[K + t] += bs * bs;
         c[t] = 0.0;
       }
-      if (!warm) fs::stv<double, K>(phi, n, c);
+      if (!warm) fs::stv<double, K, true>(phi, n, c);
       fs::stv<T, K, true>(r, n, rv);
     } else {
       // Solo: every coupled neighbour is fixed, so x = b / diag exactly
       // (poisson.py:559-564).  Pinned: coupled to nothing, x = 0 (:522).
 #pragma unroll
       for (int t = 0; t < K; ++t) c[t] = (lab == FS_LABEL_SOLO) ? bres[t] / dg : 0.0;
-      fs::stv<double, K>(phi, n, c);
+      fs::stv<double, K, true>(phi, n, c);
       fs::stv<T, K, true>(r, n, zero);
     }
   }
@@ -2465,7 +2465,9 @@ __global__ void __launch_bounds__(fs::kBlock)
 // (fs::Chunks): 0.32 -> 0.26 ms per fold at 256x256x128 with 8 RHS.  K3b
 // (and k_init) gather six neighbours and keep one thread per node: split
 // into chunks they were slower (k_reliable 0.63 -> 0.80 ms, k_init 0.64 ->
-// 0.96 ms; the masses, labels and index arithmetic repeat per chunk).
+// 0.96 ms; the masses, labels and index arithmetic repeat per chunk).  They
+// move the FP64 solution with 256-bit accesses instead (two per 64-byte
+// node): 0.4 ms less per extraction.
 template <typename T, int K>
 __global__ void __launch_bounds__(fs::kBlock)
     k_fold(Dims d, const double* __restrict__ s64, double* __restrict__ phi,
@@ -2521,7 +2523,7 @@ __global__ void __launch_bounds__(fs::kBlock)
     int i, j, k;
     fs::node_ijk(d, n, i, j, k);
     double c[K], res[K];
-    fs::ldv_ro<double, K>(phi, n, c);
+    fs::ldv_ro<double, K, true>(phi, n, c);
     if (f) {
       fs::ldv_ro<double, K>(f, n, res);
     } else {
@@ -2531,7 +2533,7 @@ __global__ void __launch_bounds__(fs::kBlock)
     auto edge = [&](bool ok, double m, long long nb) {
       if (!ok || m == 0.0) return;
       double v[K];
-      fs::ldv_ro<double, K>(phi, nb, v);
+      fs::ldv_ro<double, K, true>(phi, nb, v);
 #pragma unroll
       for (int t = 0; t < K; ++t) res[t] -= m * (c[t] - v[t]);
     };
