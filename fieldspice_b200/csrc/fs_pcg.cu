@@ -2880,7 +2880,13 @@ struct fs_pcg_plan {
   int autotune = 0;        // time kinds 2, 3, 0, 4, 5 at creation and keep the fastest
   float tune_ms[8] = {-1.f, -1.f, -1.f, -1.f, -1.f, -1.f, -1.f, -1.f};  // ms by kind (-1: untimed)
   int chunk;
+  // A chunk of `chunk` CG iterations runs as the graph `exec` (the first
+  // `head` iterations, the event samples in the first) followed by `reps`
+  // launches of the graph `body` (`body_iters` iterations each), so only
+  // head + body_iters iterations are captured and instantiated per plan.
   cudaGraphExec_t exec;
+  cudaGraphExec_t body = nullptr;
+  int head = 0, body_iters = 0, reps = 0;
   cudaStream_t cap;
   HostSlot* slot = nullptr;  // page-locked flag and stats (h_flag, h_st point in)
   int* h_flag = nullptr;
@@ -4022,34 +4028,43 @@ void dispatch_first(fs_pcg_plan* P, cudaStream_t s) {
 
 void locate_z_all(fs_pcg_plan* P) { dispatch(P, 11, nullptr); }
 
-// (Re)capture the graph of `chunk` CG iterations on the plan's capture
-// stream; chunk is even, so every launch starts on parity 0 (p[0] = p_old).
+// (Re)capture the graphs of a chunk on the plan's capture stream: the head
+// (its first iteration with the event samples) and, when the chunk repeats
+// one, the body.  head and body_iters are even, so every launch starts on
+// parity 0 (p[0] = p_old).
 int capture_graph(fs_pcg_plan* P) {
   cudaError_t e;
   if (P->exec) {
     cudaGraphExecDestroy(P->exec);
     P->exec = nullptr;
   }
+  if (P->body) {
+    cudaGraphExecDestroy(P->body);
+    P->body = nullptr;
+  }
   if (P->precond) locate_z_all(P);
-  cudaGraph_t graph = nullptr;
-  if ((e = cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
-    return fs_cuda_status("cudaStreamBeginCapture", e);
-  for (int it = 0; it < P->chunk; ++it) {
-    if (it == 0) {
-      dispatch_first(P, P->cap);
-    } else {
-      dispatch(P, 3, P->cap, 0, 0, 0, 0, it & 1);
+  for (int part = 0; part < (P->body_iters > 0 ? 2 : 1); ++part) {
+    cudaGraph_t graph = nullptr;
+    if ((e = cudaStreamBeginCapture(P->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return fs_cuda_status("cudaStreamBeginCapture", e);
+    const int n = part == 0 ? P->head : P->body_iters;
+    for (int it = 0; it < n; ++it) {
+      if (part == 0 && it == 0) {
+        dispatch_first(P, P->cap);
+      } else {
+        dispatch(P, 3, P->cap, 0, 0, 0, 0, it & 1);
+      }
     }
-  }
-  e = cudaStreamEndCapture(P->cap, &graph);
-  if (e != cudaSuccess) return fs_cuda_status("cudaStreamEndCapture", e);
-  if (P->net_status != FS_OK) {
+    e = cudaStreamEndCapture(P->cap, &graph);
+    if (e != cudaSuccess) return fs_cuda_status("cudaStreamEndCapture", e);
+    if (P->net_status != FS_OK) {
+      cudaGraphDestroy(graph);
+      return P->net_status;
+    }
+    e = cudaGraphInstantiate(part == 0 ? &P->exec : &P->body, graph, 0);
     cudaGraphDestroy(graph);
-    return P->net_status;
+    if (e != cudaSuccess) return fs_cuda_status("cudaGraphInstantiate", e);
   }
-  e = cudaGraphInstantiate(&P->exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) return fs_cuda_status("cudaGraphInstantiate", e);
   return FS_OK;
 }
 
@@ -4250,6 +4265,12 @@ int fs_pcg_plan_create_opt(int nx, int ny, int nz, int nrhs, int precision, int 
   // return at once after convergence (16 wasted up to 10); Jacobi takes
   // thousands, where longer graphs save host round trips.
   P->chunk = P->precond ? 12 : 32;
+  // multigrid: a 2-iteration head and a 2-iteration body launched 5 times
+  // (capture and instantiation of 4 iterations instead of 12: 0.3 ms less
+  // per plan); Jacobi's 5 launches per iteration are captured whole
+  P->head = P->precond ? 2 : P->chunk;
+  P->body_iters = P->precond ? 2 : 0;
+  P->reps = P->body_iters > 0 ? (P->chunk - P->head) / P->body_iters : 0;
   if ((e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking)) !=
       cudaSuccess)
     return fail("cudaStreamCreate", e);
@@ -4309,6 +4330,9 @@ int solve_chunk(fs_pcg_plan* P, cudaStream_t s) {
   cudaError_t e;
   if ((e = cudaGraphLaunch(P->exec, s)) != cudaSuccess)
     return fs_cuda_status("cudaGraphLaunch", e);
+  for (int r = 0; r < P->reps; ++r)
+    if ((e = cudaGraphLaunch(P->body, s)) != cudaSuccess)
+      return fs_cuda_status("cudaGraphLaunch", e);
   P->launches += (5LL + (P->precond ? P->launches_per_iter : 0)) * P->chunk;
   if ((e = cudaMemcpyAsync(P->h_flag, &P->ctl->all_done, sizeof(int),
                            cudaMemcpyDeviceToHost, s)) != cudaSuccess)
@@ -4729,6 +4753,7 @@ int fs_pcg_plan_destroy(fs_pcg_plan* P) {
     if (P->ev[t]) cudaEventDestroy(P->ev[t]);
   if (P->ev_async) cudaEventDestroy(P->ev_async);
   if (P->exec) cudaGraphExecDestroy(P->exec);
+  if (P->body) cudaGraphExecDestroy(P->body);
   if (P->cap) cudaStreamDestroy(P->cap);
   if (P->slot) host_slot_put(P->slot);
   delete P;
