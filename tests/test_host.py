@@ -148,3 +148,31 @@ def test_preconditioner_follows_linear_solver():
                                   GPUConfig(preconditioner="mg")) == "mg"
     with pytest.raises(ValueError):
         resolve_preconditioner(SolverConfig(linear_solver="lu"), None)
+
+
+def test_metric_cache_hits_and_refreshes(monkeypatch):
+    """metric_dev: one upload per grid while its values are unchanged, a new
+    upload after an in-place change or for another device (uploads counted
+    through a stand-in for the device copy)."""
+    import torch
+    from fieldspice_b200 import device as D
+    calls = []
+
+    def fake_h2d(a, dtype, dev):
+        calls.append(dev)
+        return torch.as_tensor(np.array(a, copy=True), dtype=dtype)
+
+    monkeypatch.setattr(D, "h2d", fake_h2d)
+    g = RectilinearGrid(np.linspace(0, 1, 6), np.linspace(0, 2, 5), np.linspace(0, 3, 4))
+    a = D.metric_dev(g, "dev0")
+    assert len(calls) == 6 and float(a[0][0]) == float(g.hx[0])
+    b = D.metric_dev(g, "dev0")
+    assert len(calls) == 6 and all(x is y for x, y in zip(a, b))
+    g.hx[1] *= 3.0
+    c = D.metric_dev(g, "dev0")
+    assert len(calls) == 12 and float(c[0][1]) == float(g.hx[1])
+    D.metric_dev(g, "dev1")
+    assert len(calls) == 18
+    g2 = RectilinearGrid(np.linspace(0, 1, 6), np.linspace(0, 2, 5), np.linspace(0, 3, 4))
+    D.metric_dev(g2, "dev1")
+    assert len(calls) == 24  # another grid object: its own entry
