@@ -9,8 +9,8 @@ of a 256x256x128 grid, 8 RHS); on the fine grid the same network would cost
 more than the whole multigrid iteration it replaces.  A "hybrid" mode adds a
 V-cycle on the residual of the network's guess.  The network is nonlinear
 (ReLU), so the outer iteration is flexible CG; if FCG stalls the plan falls
-back to plain multigrid PCG, which is also the judge of its answer (same
-FP64 stopping rule, same charge integration).
+back to plain multigrid PCG, which also checks its answer (same FP64
+stopping rule, same charge integration).
 
 Training data.  Residual-to-error pairs generated by the path's own PCG on
 seeded geometries of the layered-box family at 128^3: Jacobi-PCG iterates
