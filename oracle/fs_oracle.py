@@ -1,9 +1,9 @@
 """CPU oracle of fieldspice's elliptic solve path -- TEST INFRASTRUCTURE ONLY.
 
 This module restates, in NumPy/SciPy, the reference algorithm of the path the
-GPU library replaces.  It is the checker: only ``tests/``,
-``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may
-import it, and never as the thing measured or shipped.  The product path
+GPU library replaces.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import it, to check results against,
+never as the thing measured or shipped.  The product path
 (``fieldspice_b200``) does not import it and has no CPU fallback.
 
 Parity pin: ``tests/golden/make_golden.py`` imported the reference package

@@ -1,8 +1,8 @@
 """CPU FP64 restatement of the learned preconditioner's U-Net (test infrastructure).
 
-Only the tests use this module: it is the checker of the library's network
-kernels (``fs_unet_forward`` / ``fs_unet_gradient``), never part of the
-product path.  The network has no counterpart in the reference project (the
+Only the tests use this module, to check the library's network kernels
+(``fs_unet_forward`` / ``fs_unet_gradient``) against it; it is never part of
+the product path.  The network has no counterpart in the reference project (the
 reference has no learned preconditioner), so this file restates the
 library's own architecture in PyTorch CPU float64 with autograd:
 
