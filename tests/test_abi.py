@@ -71,6 +71,19 @@ def test_workspace_sizes_and_bad_arguments(dll):
     assert dll.fs_pcg_plan_destroy(null) == L.FS_OK
     assert dll.fs_group_apply_workspace_bytes(0, 8, ctypes.byref(nb)) == L.FS_BAD_ARG
     assert dll.fs_quadform_workspace_bytes(17, ctypes.byref(nb)) == L.FS_BAD_ARG
+    # the property statistics validate before touching the device
+    one = ctypes.c_void_p(256)
+    stats = (ctypes.c_double * 3)()
+    ws = L.PROP_STATS_WORKSPACE_BYTES
+    assert dll.fs_prop_stats_enqueue(null, 10, one, ws, null) == L.FS_BAD_ARG
+    assert dll.fs_prop_stats_enqueue(one, 0, one, ws, null) == L.FS_BAD_ARG
+    assert dll.fs_prop_stats_enqueue(one, 10, one, ws - 16, null) == L.FS_BAD_ARG
+    assert dll.fs_prop_stats_enqueue(one, 10, ctypes.c_void_p(264), ws, null) == L.FS_BAD_ARG
+    assert dll.fs_prop_stats(one, 10, None, one, ws, null) == L.FS_BAD_ARG
+    assert dll.fs_prop_stats(null, 10, stats, one, ws, null) == L.FS_BAD_ARG
+    # the result offset the host reads is inside the workspace, 16-byte aligned
+    assert L.PROP_STATS_RESULT_OFFSET % 16 == 0
+    assert L.PROP_STATS_RESULT_OFFSET + 24 <= ws
 
 
 def test_multigrid_parameters_are_validated(dll):
@@ -114,3 +127,11 @@ def test_product_path_fails_loudly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError, match="CUDA device"):
         L.lib()
+
+
+def test_header_constants_match_the_binding():
+    """The #define values the Python binding repeats."""
+    text = (ROOT / "include" / "fieldspice_b200.h").read_text()
+    defs = dict(re.findall(r"#define\s+(FS_[A-Z0-9_]+)\s+(\d+)", text))
+    assert int(defs["FS_PROP_STATS_WORKSPACE_BYTES"]) == L.PROP_STATS_WORKSPACE_BYTES
+    assert int(defs["FS_PROP_STATS_RESULT_OFFSET"]) == L.PROP_STATS_RESULT_OFFSET
