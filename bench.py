@@ -451,8 +451,8 @@ def run_ours(args, rank, world, local_rank):
     if line["learned_value"] and line["plain_pcg_value"]:
         line["learned_vs_plain_pcg"] = line["learned_value"] / line["plain_pcg_value"]
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(shape, info["iterations"],
-                                            max(2, args.cpu_sample_iters // NBOX))
+        jac = variants.get("plain_pcg_jacobi", {}).get("iterations")
+        line["cpu_baseline"] = cpu_baseline(shape, jac, max(2, args.cpu_sample_iters // NBOX))
     # the variants and the e2e phase record in full on their own line first;
     # the headline line last
     print(json.dumps({"variants": variants, "e2e_calls": e2e_detail,
@@ -831,10 +831,11 @@ class _BoundedReferenceCG:
             raise MemoryError("incomplete LU disabled: Jacobi branch forced")
 
         def cg(A, b, **kw):
-            kw["maxiter"] = sample
-            for key in ("rtol", "tol"):
-                if key in kw:
-                    kw[key] = 1e-300
+            if sample is not None:  # None: the reference's own stopping rule
+                kw["maxiter"] = sample
+                for key in ("rtol", "tol"):
+                    if key in kw:
+                        kw[key] = 1e-300
             t0 = time.perf_counter()
             out = orig_cg(A, b, **kw)
             log.append(time.perf_counter() - t0)
@@ -847,21 +848,31 @@ class _BoundedReferenceCG:
         return False
 
 
-def _reference_iterations(gpu_iters=None):
-    if FULLSIZE_JSON.exists():
+def _reference_iterations(shape, jacobi_iters=None):
+    """Jacobi-CG iterations to 1e-10 of the 8 right-hand sides of ``shape``,
+    and where they come from; (None, reason) when none are known."""
+    if tuple(shape) == SHAPE and FULLSIZE_JSON.exists():
         d = json.loads(FULLSIZE_JSON.read_text())
         return [int(v) for v in d["iterations_1e-10"]], "oracle full-size run (tests/golden)"
-    if gpu_iters:
-        return [int(v) for v in gpu_iters], "GPU solve of the same system"
-    return [1765] * NBOX, "Jacobi-CG iterations to 1e-10 measured on this workload earlier"
+    if jacobi_iters:
+        return ([int(v) for v in jacobi_iters],
+                "the GPU's Jacobi PCG of the same system (mixed precision; its FP64 "
+                "iteration counts equal the reference's)")
+    return None, f"no Jacobi-CG iteration counts recorded for {tuple(shape)}"
+
+
+#: Below this many nodes a reference extraction runs to convergence in a few
+#: seconds and is measured whole instead of projected.
+WHOLE_REFERENCE_NODES = 1 << 17
 
 
 def reference_sample(shape, sample_iters, seed=0):
     """One call of the reference's public ``extraction.capacitance_matrix``
     (``fieldspice/extraction.py:41-56``) on the seeded workload with the
     Jacobi branch forced and each right-hand side bounded to
-    ``sample_iters`` CG iterations.  Returns (call seconds, seconds in CG,
-    CG iterations run)."""
+    ``sample_iters`` CG iterations (None: the reference's own stopping rule,
+    a whole extraction).  Returns (call seconds, seconds in CG, CG
+    iterations run, 0 when unbounded)."""
     fs = _reference_package()
     from fieldspice.boundaries import BoundarySpec, Dirichlet
     from fieldspice.grid import RectilinearGrid
@@ -880,7 +891,8 @@ def reference_sample(shape, sample_iters, seed=0):
                                              SolverConfig(linear_solver="cg", tol=TOL))
         except ConvergenceError:
             pass
-    return time.perf_counter() - t0, sum(ctx.cg_seconds), sample_iters * len(ctx.cg_seconds)
+    n_cg = sample_iters * len(ctx.cg_seconds) if sample_iters else 0
+    return time.perf_counter() - t0, sum(ctx.cg_seconds), n_cg
 
 
 def _project(t_call, t_cg, n_cg, iters):
@@ -894,12 +906,23 @@ def _project(t_call, t_cg, n_cg, iters):
     return t_setup + t_iter * sum(iters), t_setup, t_iter
 
 
-def cpu_baseline(shape, gpu_iters, sample_iters):
+def cpu_baseline(shape, jacobi_iters, sample_iters):
     if _reference_package() is None:
         return {"value": None, "unit": "solves/s", "kind": "reference",
                 "sample": "reference not installed in baseline/_ref"}
+    iters, src = _reference_iterations(shape, jacobi_iters)
+    if iters is None:
+        if int(np.prod(shape)) > WHOLE_REFERENCE_NODES:
+            return {"value": None, "unit": "solves/s", "kind": "reference",
+                    "sample": f"not projected: {src}"}
+        t_call, _, _ = reference_sample(shape, None)
+        return {"value": NBOX / t_call, "unit": "solves/s", "cores": 1, "kind": "reference",
+                "projected": False,
+                "sample": (f"one whole reference extraction.capacitance_matrix (baseline/_ref, "
+                           f"SciPy Jacobi-CG forced, relres 1e-10) of the {shape} workload: "
+                           f"{t_call:.2f} s"),
+                "seconds_per_extraction": t_call, "measured_call_seconds": t_call}
     t_call, t_cg, n_cg = reference_sample(shape, sample_iters)
-    iters, src = _reference_iterations(gpu_iters)
     t_ext, t_setup, t_iter = _project(t_call, t_cg, n_cg, iters)
     return {"value": NBOX / t_ext, "unit": "solves/s", "cores": 1, "kind": "reference",
             "projected": True,
@@ -924,8 +947,15 @@ def run_reference(args, rank, world):
                           "unavailable": "reference package not installed in baseline/_ref"}),
               flush=True)
         return
-    sample = max(2, args.cpu_sample_iters // 16)
-    iters, src = _reference_iterations()
+    iters, src = _reference_iterations(shape)
+    whole = iters is None and int(np.prod(shape)) <= WHOLE_REFERENCE_NODES
+    if iters is None and not whole:
+        print(json.dumps({"impl": "reference", "metric": "C solves/s @relres 1e-10",
+                          "value": None, "unit": "solves/s",
+                          "reason": f"not projected: {src}; measured whole only up to "
+                                    f"{WHOLE_REFERENCE_NODES} nodes"}), flush=True)
+        return
+    sample = None if whole else max(2, args.cpu_sample_iters // 16)
     calls = []
     for s_ in range(args.warmup + args.steps):
         r = reference_sample(shape, sample)
@@ -934,25 +964,33 @@ def run_reference(args, rank, world):
     t_call = statistics.median(c[0] for c in calls)
     t_cg = statistics.median(c[1] for c in calls)
     n_cg = calls[0][2]
-    t_ext, t_setup, t_iter = _project(t_call, t_cg, n_cg, iters)
-    value = NBOX / t_ext
     ncores = os.cpu_count() or 1
-    sample_txt = (f"reference extraction.capacitance_matrix from baseline/_ref (SciPy "
-                  f"Jacobi-CG forced), one call per step with each of the 8 RHS bounded to "
-                  f"{n_cg // NBOX} CG iterations: median call {t_call:.2f} s (set-up outside CG {t_setup:.2f} s, "
-                  f"{t_iter*1e3:.1f} ms/iteration); projected extraction = set-up + "
-                  f"ms/iteration x iterations to 1e-10 of the 8 RHS ({src}: {iters}); "
-                  f"BLAS threads unrestricted on {ncores} cores, SpMV single-threaded")
+    if whole:
+        t_ext, t_setup, t_iter = t_call, t_call - t_cg, 0.0
+        sample_txt = (f"one whole reference extraction.capacitance_matrix from baseline/_ref "
+                      f"(SciPy Jacobi-CG forced, relres 1e-10) per step: median {t_call:.2f} s; "
+                      f"BLAS threads unrestricted on {ncores} cores, SpMV single-threaded")
+    else:
+        t_ext, t_setup, t_iter = _project(t_call, t_cg, n_cg, iters)
+        sample_txt = (f"reference extraction.capacitance_matrix from baseline/_ref (SciPy "
+                      f"Jacobi-CG forced), one call per step with each of the 8 RHS bounded to "
+                      f"{n_cg // NBOX} CG iterations: median call {t_call:.2f} s (set-up outside "
+                      f"CG {t_setup:.2f} s, {t_iter*1e3:.1f} ms/iteration); projected extraction "
+                      f"= set-up + ms/iteration x iterations to 1e-10 of the 8 RHS ({src}: "
+                      f"{iters}); BLAS threads unrestricted on {ncores} cores, SpMV "
+                      f"single-threaded")
+    value = NBOX / t_ext
     line = {
         "impl": "reference",
         "metric": "C solves/s @relres 1e-10",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_call * 1e3,
-        "projected": True,
+        "projected": not whole,
         "projected_ms_per_extraction": t_ext * 1e3,
         "measured": {"call_s": t_call, "setup_outside_cg_s": t_setup,
                      "ms_per_cg_iteration": t_iter * 1e3, "cg_iterations_per_call": n_cg},
-        "extrapolated": {"iterations_per_rhs": iters, "cg_s": t_iter * sum(iters)},
+        "extrapolated": (None if whole else
+                         {"iterations_per_rhs": iters, "cg_s": t_iter * sum(iters)}),
         "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded layered dielectric + 8 conductor boxes)",
